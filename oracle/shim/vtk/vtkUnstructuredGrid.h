@@ -1,0 +1,4 @@
+// Declaration-only stand-in (see vtkSmartPointer.h).  ORACLE TEST INFRASTRUCTURE ONLY.
+#pragma once
+#include "vtkSmartPointer.h"
+class vtkUnstructuredGrid {};

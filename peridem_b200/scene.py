@@ -1,0 +1,533 @@
+"""Synthetic PeriDEM scenes: reference-particle meshes, particle packings,
+walls, and the input decks PeriDEM reads.
+
+Two outputs from one scene description:
+
+* ``write_deck(spec, directory)`` writes the YAML deck, CSV meshes and the
+  particle-location CSV in the formats the reference reads
+  (src/inp/input.cpp:189-1395, src/rw/reader.cpp:16-57 and 101-123), so the
+  reference's own ``DEMModel::init`` can set the scene up.
+* ``build_scene(spec)`` performs the same set-up directly in numpy and returns
+  a :class:`peridem_b200.model.Scene` ready for the device, for workloads too
+  large to set up through the reference.  It restates the reference's
+  ``DEMModel::init`` steps (src/model/dem/demModel.cpp:109-266): particle
+  creation by transform (src/particle/baseParticle.cpp:122-143,
+  particleTransform.h:96-100), mesh size and horizon
+  (baseParticle.cpp:146-154), material constants (material.h:541-620 RNP,
+  919-997 PMB, 1257-1305 PD elastic, 1579-1700 PD state), internal contact
+  (baseParticle.cpp:175-179), contact set-up (demModel.cpp:1531-1600) and
+  fixity (particleULoading.cpp:90-113).
+
+Synthetic inputs stand in for the reference's gmsh-built example scenes:
+meshes are uniform square / cubic grids clipped to the shape, nodal volume
+h^d, as the reference's finite-difference CSV meshes allow.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+# ---------------------------------------------------------------------------
+# reference-particle meshes (local coordinates, centred on the origin)
+# ---------------------------------------------------------------------------
+
+
+def _grid(n: int, dim: int) -> np.ndarray:
+    r = np.arange(-n, n + 1, dtype=np.int64)
+    if dim == 2:
+        a, b = np.meshgrid(r, r, indexing="ij")
+        return np.stack([a.ravel(), b.ravel()], axis=1)
+    a, b, c = np.meshgrid(r, r, r, indexing="ij")
+    return np.stack([a.ravel(), b.ravel(), c.ravel()], axis=1)
+
+
+def disc_mesh(radius: float, h: float) -> Tuple[np.ndarray, np.ndarray]:
+    """Square-grid nodes (spacing h) inside a disc; returns (nodes[n,3], vol[n])."""
+    n = int(math.floor(radius / h + 1e-9))
+    ij = _grid(n, 2)
+    keep = (ij[:, 0] ** 2 + ij[:, 1] ** 2) <= (radius / h) ** 2 * (1 + 1e-12)
+    ij = ij[keep]
+    x = np.zeros((len(ij), 3))
+    x[:, :2] = ij * h
+    return x, np.full(len(ij), h * h)
+
+
+def hexagon_mesh(radius: float, h: float) -> Tuple[np.ndarray, np.ndarray]:
+    """Square-grid nodes inside a regular hexagon of circumradius ``radius``
+    with a vertex on the +x axis (the reference's hexagon with axis (1,0,0))."""
+    n = int(math.floor(radius / h + 1e-9))
+    ij = _grid(n, 2)
+    x = ij[:, 0] * h
+    y = ij[:, 1] * h
+    s3 = math.sqrt(3.0)
+    tol = 1e-12 * radius
+    keep = (np.abs(y) <= 0.5 * s3 * radius + tol) & (
+        s3 * np.abs(x) + np.abs(y) <= s3 * radius + tol)
+    pts = np.zeros((int(keep.sum()), 3))
+    pts[:, 0] = x[keep]
+    pts[:, 1] = y[keep]
+    return pts, np.full(len(pts), h * h)
+
+
+def sphere_mesh(radius: float, h: float) -> Tuple[np.ndarray, np.ndarray]:
+    """Cubic-grid nodes (spacing h) inside a ball."""
+    n = int(math.floor(radius / h + 1e-9))
+    ijk = _grid(n, 3)
+    keep = (ijk ** 2).sum(axis=1) <= (radius / h) ** 2 * (1 + 1e-12)
+    return ijk[keep] * h + 0.0, np.full(int(keep.sum()), h ** 3)
+
+
+def box_mesh(lo: Sequence[float], hi: Sequence[float], h: float, dim: int,
+             hole_lo: Optional[Sequence[float]] = None,
+             hole_hi: Optional[Sequence[float]] = None) -> Tuple[np.ndarray, np.ndarray]:
+    """Grid nodes filling the box [lo, hi] (minus an optional open hole)."""
+    axes = []
+    for d in range(dim):
+        m = int(math.floor((hi[d] - lo[d]) / h + 1e-9))
+        axes.append(lo[d] + h * np.arange(m + 1))
+    mesh = np.meshgrid(*axes, indexing="ij")
+    pts = np.stack([m.ravel() for m in mesh], axis=1)
+    if hole_lo is not None:
+        inside = np.ones(len(pts), dtype=bool)
+        for d in range(dim):
+            inside &= (pts[:, d] > hole_lo[d]) & (pts[:, d] < hole_hi[d])
+        pts = pts[~inside]
+    x = np.zeros((len(pts), 3))
+    x[:, :dim] = pts
+    return x, np.full(len(pts), h ** dim)
+
+
+# ---------------------------------------------------------------------------
+# scene description
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class MaterialSpec:
+    """One zone's material deck (keys of src/inp/input.cpp:1048-1180)."""
+    kind: str = "RNPBond"            # RNPBond | PMBBond | PDElasticBond | PDState
+    density: float = 1200.0
+    E: float = -1.0
+    K: float = -1.0
+    G: float = -1.0
+    nu: float = -1.0
+    Gc: float = -1.0
+    horizon_mesh_ratio: float = 3.0
+    influence_type: int = 1
+    check_sc_factor: float = 1.0
+    irreversible: bool = True
+
+
+@dataclass
+class ContactSpec:
+    """One zone pair's contact deck (src/inp/input.cpp:665-833)."""
+    radius_factor: float = 0.95
+    kn: float = 0.0                  # Kn before Kn_Factor
+    kn_factor: float = 1.0
+    epsilon: float = 0.95
+    friction_on: bool = False
+    friction_coeff: float = 0.5
+    damping_on: bool = True
+    betan_factor: float = 100.0
+
+
+@dataclass
+class ZoneSpec:
+    name: str                        # circle | hexagon | sphere | rectangle | cuboid | ...
+    is_wall: bool
+    geom_type: str
+    geom_params: List[float]
+    mesh_nodes: np.ndarray           # local reference mesh [n,3]
+    mesh_vol: np.ndarray
+    material: MaterialSpec
+    all_dofs_constrained: bool = False
+    # particles of this zone: (centre[3], radius, orientation); walls use none
+    sites: List[Tuple[Tuple[float, float, float], float, float]] = field(default_factory=list)
+
+
+@dataclass
+class BCSpec:
+    particles: List[int]
+    directions: List[int]            # 1-based, as in the deck
+    time_fn: str = "constant"
+    time_params: List[float] = field(default_factory=lambda: [0.0])
+    spatial_fn: str = "constant"
+    spatial_params: List[float] = field(default_factory=list)
+    zero: bool = False
+
+
+@dataclass
+class SceneSpec:
+    name: str
+    dim: int
+    dt: float
+    nt: int
+    zones: List[ZoneSpec]
+    contact: Dict[Tuple[int, int], ContactSpec]
+    container: Tuple[List[float], List[float]]
+    gravity: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    search_factor: float = 5.0
+    search_interval: int = 40
+    test_name: str = ""
+    compressive_wall: int = 0
+    compressive_dir: int = 2
+    test_output_interval: int = 10
+    ubc: List[BCSpec] = field(default_factory=list)
+    fbc: List[BCSpec] = field(default_factory=list)
+    ic_velocity: Optional[Tuple[float, float, float]] = None
+    ic_particles: List[int] = field(default_factory=list)
+    time_scheme: str = "central_difference"
+    seed: int = 0
+
+    @property
+    def num_particles(self) -> int:
+        return sum(len(z.sites) if not z.is_wall else 1 for z in self.zones)
+
+
+def elastic_material(kind: str, E: float, Gc: float = 500.0, density: float = 1200.0,
+                     nu: float = 0.25) -> MaterialSpec:
+    """Material deck with Young's and bulk modulus both given: the reference's
+    contact set-up needs K in the deck (demModel.cpp:1559-1565); the bond
+    laws derive their constants from E (material.h:584-586), and PD state
+    takes (E, K) as its elastic pair (material.h:1592-1616)."""
+    K = E / (3.0 * (1.0 - 2.0 * nu))
+    return MaterialSpec(kind=kind, density=density, E=E, K=K, Gc=Gc)
+
+
+# ---------------------------------------------------------------------------
+# deck writer (formats read by the reference)
+# ---------------------------------------------------------------------------
+
+
+def _f(v: float) -> str:
+    return repr(float(v))
+
+
+def _flist(v: Sequence[float]) -> str:
+    return "[" + ", ".join(_f(x) for x in v) + "]"
+
+
+def write_deck(spec: SceneSpec, directory: str, threads_note: str = "") -> str:
+    """Write deck.yaml + meshes + particle CSV under ``directory``; return the
+    YAML path.  Output is switched off (``Perform_Out: false``)."""
+    os.makedirs(directory, exist_ok=True)
+    L = []
+    w = L.append
+    w("Model:")
+    w(f"  Dimension: {spec.dim}")
+    w("  Discretization_Type:")
+    w("    Spatial: finite_difference")
+    w(f"    Time: {spec.time_scheme}")
+    w(f"  Final_Time: {_f(spec.dt * spec.nt)}")
+    w(f"  Time_Steps: {spec.nt}")
+    w(f"  Seed: {spec.seed}")
+    w("Container:")
+    w("  Geometry:")
+    w("    Type: " + ("rectangle" if spec.dim == 2 else "cuboid"))
+    lo, hi = spec.container
+    w("    Parameters: " + _flist(list(lo) + list(hi)))
+    nz = len(spec.zones)
+    w("Zone:")
+    w(f"  Zones: {nz}")
+    for z, zs in enumerate(spec.zones):
+        w(f"  Zone_{z + 1}:")
+        w(f"    Is_Wall: {'true' if zs.is_wall else 'false'}")
+    w("Particle:")
+    if spec.test_name:
+        w(f"  Test_Name: {spec.test_name}")
+    if spec.test_name == "compressive_test":
+        w("  Compressive_Test:")
+        w(f"    Particle_Id: {spec.compressive_wall}")
+        w(f"    Particle_Force_Direction: {spec.compressive_dir}")
+    for z, zs in enumerate(spec.zones):
+        w(f"  Zone_{z + 1}:")
+        if zs.is_wall:
+            w("    Is_Wall: true")
+        w(f"    Type: {zs.geom_type}")
+        w("    Parameters: " + _flist(zs.geom_params))
+        if zs.is_wall:
+            w(f"    All_Dofs_Constrained: {'true' if zs.all_dofs_constrained else 'false'}")
+            w("    Create_Particle_Using_ParticleZone_GeomObject: true")
+        elif zs.all_dofs_constrained:
+            w("    All_Dofs_Constrained: true")
+    w("Particle_Generation:")
+    w("  From_File: particle_locations.csv")
+    w("  File_Data_Type: loc_rad_orient")
+    w("Mesh:")
+    for z, zs in enumerate(spec.zones):
+        w(f"  Zone_{z + 1}:")
+        w(f"    File: mesh_zone_{z + 1}.csv")
+    w("Contact:")
+    for i in range(nz):
+        for j in range(i, nz):
+            c = spec.contact[(i, j)]
+            w(f"  Zone_{i + 1}{j + 1}:")
+            w(f"    Contact_Radius_Factor: {_f(c.radius_factor)}")
+            if not c.damping_on:
+                w("    Damping_On: false")
+            if not c.friction_on:
+                w("    Friction_On: false")
+            w(f"    Kn: {_f(c.kn)}")
+            w(f"    Epsilon: {_f(c.epsilon)}")
+            w(f"    Friction_Coeff: {_f(c.friction_coeff)}")
+            w(f"    Kn_Factor: {_f(c.kn_factor)}")
+            w(f"    Beta_n_Factor: {_f(c.betan_factor)}")
+    w("Neighbor:")
+    w("  Update_Criteria: simple_all")
+    w(f"  Search_Factor: {_f(spec.search_factor)}")
+    w(f"  Search_Interval: {spec.search_interval}")
+    w("Material:")
+    for z, zs in enumerate(spec.zones):
+        m = zs.material
+        w(f"  Zone_{z + 1}:")
+        w(f"    Type: {m.kind}")
+        w(f"    Horizon_Mesh_Ratio: {_f(m.horizon_mesh_ratio)}")
+        w(f"    Density: {_f(m.density)}")
+        w("    Compute_From_Classical: true")
+        for key, val in (("E", m.E), ("K", m.K), ("G", m.G), ("Poisson_Ratio", m.nu), ("Gc", m.Gc)):
+            if val > 0:
+                w(f"    {key}: {_f(val)}")
+        w("    Influence_Function:")
+        w(f"      Type: {m.influence_type}")
+        if m.kind == "RNPBond":
+            w("    Bond_Potential:")
+            w(f"      Check_Sc_Factor: {_f(m.check_sc_factor)}")
+            w(f"      Irreversible_Bond_Fracture: {'true' if m.irreversible else 'false'}")
+    if any(g != 0.0 for g in spec.gravity) or spec.fbc:
+        w("Force_BC:")
+        if any(g != 0.0 for g in spec.gravity):
+            w("  Gravity: " + _flist(spec.gravity))
+        if spec.fbc:
+            _write_bc_sets(w, spec.fbc)
+    if spec.ubc:
+        w("Displacement_BC:")
+        _write_bc_sets(w, spec.ubc)
+    if spec.ic_velocity is not None:
+        w("IC:")
+        w("  Constant_Velocity:")
+        w("    Velocity_Vector: " + _flist(spec.ic_velocity))
+        w("    Particle_List: [" + ", ".join(str(p) for p in spec.ic_particles) + "]")
+    w("Output:")
+    w("  Path: ./")
+    w("  Tags:")
+    w("    - Displacement")
+    w(f"  Output_Interval: {max(1, spec.nt)}")
+    w("  Perform_FE_Out: false")
+    w("  Perform_Out: false")
+    w(f"  Test_Output_Interval: {spec.test_output_interval}")
+    w("  Debug: 0")
+    w("  Tag_PP: 0")
+    path = os.path.join(directory, "deck.yaml")
+    with open(path, "w") as fh:
+        fh.write("\n".join(L) + "\n")
+
+    # meshes
+    for z, zs in enumerate(spec.zones):
+        with open(os.path.join(directory, f"mesh_zone_{z + 1}.csv"), "w") as fh:
+            if spec.dim == 2:
+                fh.write("id,x,y,volume\n")
+                for i, (p, v) in enumerate(zip(zs.mesh_nodes, zs.mesh_vol)):
+                    fh.write(f"{i},{_f(p[0])},{_f(p[1])},{_f(v)}\n")
+            else:
+                fh.write("id,x,y,z,volume\n")
+                for i, (p, v) in enumerate(zip(zs.mesh_nodes, zs.mesh_vol)):
+                    fh.write(f"{i},{_f(p[0])},{_f(p[1])},{_f(p[2])},{_f(v)}\n")
+    with open(os.path.join(directory, "particle_locations.csv"), "w") as fh:
+        fh.write("i, x, y, z, r, o\n")
+        for z, zs in enumerate(spec.zones):
+            if zs.is_wall:
+                continue
+            for (c, r, o) in zs.sites:
+                fh.write(f"{z}, {_f(c[0])}, {_f(c[1])}, {_f(c[2])}, {_f(r)}, {_f(o)}\n")
+    return path
+
+
+def _write_bc_sets(w, sets: List[BCSpec]) -> None:
+    w(f"  Sets: {len(sets)}")
+    for s, bc in enumerate(sets):
+        w(f"  Set_{s + 1}:")
+        w("    Particle_List: [" + ", ".join(str(p) for p in bc.particles) + "]")
+        w("    Direction: [" + ",".join(str(d) for d in bc.directions) + "]")
+        if bc.zero:
+            w("    Zero_Displacement: true")
+        else:
+            w("    Time_Function:")
+            w(f"      Type: {bc.time_fn}")
+            w("      Parameters:")
+            for p in bc.time_params:
+                w(f"        - {_f(p)}")
+            w("    Spatial_Function:")
+            w(f"      Type: {bc.spatial_fn}")
+            if bc.spatial_params:
+                w("      Parameters:")
+                for p in bc.spatial_params:
+                    w(f"        - {_f(p)}")
+
+
+# ---------------------------------------------------------------------------
+# named workloads
+# ---------------------------------------------------------------------------
+
+
+def _all_pairs(nz: int, c: ContactSpec) -> Dict[Tuple[int, int], ContactSpec]:
+    return {(i, j): c for i in range(nz) for j in range(i, nz)}
+
+
+def two_particle(h_div: int = 10, radius: float = 1e-3, material: str = "RNPBond",
+                 nt: int = 20000, dt: float = 1e-7, v0: float = -0.1,
+                 gap: Optional[float] = None) -> SceneSpec:
+    """Two discs of radius R, square-grid nodes h = R/h_div, horizon 3h; the
+    top disc starts at v0 under gravity; the bottom disc's force is off
+    (test name two_particle, demModel.cpp:218-220)."""
+    h = radius / h_div
+    nodes, vol = disc_mesh(radius, h)
+    mat = elastic_material(material, 2.0e9)
+    K = 2.0e9 / (3.0 * (1.0 - 2.0 * 0.25))
+    horizon = 3.0 * h
+    kn = 18.0 * K / (math.pi * horizon ** 5)
+    gap = 0.5 * h if gap is None else gap
+    sites = [((radius, radius, 0.0), radius, 0.0),
+             ((radius, 3.0 * radius + 0.95 * h + gap, 0.0), radius, 0.0)]
+    z = ZoneSpec("disc", False, "circle", [radius, 0.0, 0.0, 0.0], nodes, vol, mat, sites=sites)
+    c = ContactSpec(radius_factor=0.95, kn=kn, kn_factor=10.0, epsilon=0.7,
+                    friction_on=True, friction_coeff=0.5, damping_on=True, betan_factor=1.0)
+    return SceneSpec(name=f"two_particle_h{h_div}", dim=2, dt=dt, nt=nt, zones=[z],
+                     contact=_all_pairs(1, c),
+                     container=([0.0, 0.0, 0.0], [2 * radius, 4 * radius + 2 * h, 0.0]),
+                     gravity=(0.0, -10.0, 0.0), search_factor=5.0, search_interval=40,
+                     test_name="two_particle", test_output_interval=10,
+                     ic_velocity=(0.0, v0, 0.0), ic_particles=[1])
+
+
+def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3, 1.5e-3),
+                   h_div: int = 15, width: float = 40e-3, seed: int = 0,
+                   material: str = "RNPBond", wall_speed: float = -0.1,
+                   dt: float = 5e-8, nt: int = 50000, gravity: float = -10.0,
+                   search_factor: float = 5.0, search_interval: int = 40,
+                   friction: bool = True) -> SceneSpec:
+    """2-D compression: discs and hexagons (50/50) on a jittered triangular
+    lattice inside a fixed frame, pressed by a top wall moving at
+    ``wall_speed``.  One reference mesh per shape at h = R_ref/h_div, scaled
+    per particle, so every particle has the same node count."""
+    rng = np.random.default_rng(seed)
+    r_ref = r_range[0]
+    h_ref = r_ref / h_div
+    disc_n, disc_v = disc_mesh(r_ref, h_ref)
+    hex_n, hex_v = hexagon_mesh(r_ref, h_ref)
+    radii = rng.uniform(r_range[0], r_range[1], size=n_particles)
+    orients = rng.uniform(0.0, 2.0 * math.pi, size=n_particles)
+    shapes = np.arange(n_particles) % 2          # 0 disc, 1 hexagon
+    rng.shuffle(shapes)
+    h_min = r_range[0] / h_div
+    spacing = 2.0 * r_range[1] + 2.0 * h_min
+    per_row = max(1, int(math.floor((width - 2.0 * h_min) / spacing)))
+    rows = int(math.ceil(n_particles / per_row))
+    dy = spacing * math.sqrt(3.0) / 2.0
+    t_wall = 3.0 * h_min                          # wall thickness
+    x0 = 0.0
+    y0 = 0.0
+    height = rows * dy + spacing
+    sites_by_shape = {0: [], 1: []}
+    for p in range(n_particles):
+        row, col = divmod(p, per_row)
+        cx = x0 + h_min + 0.5 * spacing + col * spacing + (0.5 * spacing if row % 2 else 0.0)
+        cx = min(cx, width - h_min - 0.5 * spacing)
+        cy = y0 + h_min + 0.5 * spacing + row * dy
+        jx, jy = rng.uniform(-0.5, 0.5, size=2) * (spacing - 2.0 * radii[p] - 1.5 * h_min) * 0.5
+        sites_by_shape[int(shapes[p])].append(((cx + jx, cy + jy, 0.0), float(radii[p]), float(orients[p])))
+    mat = elastic_material(material, 2.0e9)
+    zones = [
+        ZoneSpec("disc", False, "circle", [r_ref, 0.0, 0.0, 0.0], disc_n, disc_v, mat,
+                 sites=sites_by_shape[0]),
+        ZoneSpec("hexagon", False, "hexagon", [r_ref, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0], hex_n, hex_v,
+                 mat, sites=sites_by_shape[1]),
+    ]
+    # fixed frame (left, right, bottom) and moving top bar, walls meshed at h_min
+    lo = [x0 - t_wall - h_min, y0 - t_wall - h_min]
+    hi = [width + t_wall + h_min, y0 + height + 2.0 * t_wall]
+    frame_n, frame_v = box_mesh([lo[0], lo[1]], [hi[0], hi[1]], h_min, 2,
+                                hole_lo=[x0 - 0.5 * h_min, y0 - 0.5 * h_min],
+                                hole_hi=[width + 0.5 * h_min, hi[1] + 1.0])
+    bar_lo = [x0 + 0.5 * h_min, y0 + height]
+    bar_hi = [width - 0.5 * h_min, y0 + height + t_wall]
+    bar_n, bar_v = box_mesh(bar_lo, bar_hi, h_min, 2)
+    wall_mat = elastic_material(material, 2.0e9)
+    zones.append(ZoneSpec("frame", True, "rectangle", [lo[0], lo[1], 0.0, hi[0], hi[1], 0.0],
+                          frame_n, frame_v, wall_mat, all_dofs_constrained=True))
+    zones.append(ZoneSpec("top_wall", True, "rectangle",
+                          [bar_lo[0], bar_lo[1], 0.0, bar_hi[0], bar_hi[1], 0.0],
+                          bar_n, bar_v, wall_mat, all_dofs_constrained=True))
+    K = 2.0e9 / (3.0 * (1.0 - 2.0 * 0.25))
+    kn = 18.0 * K / (math.pi * (3.0 * h_min) ** 5)
+    c = ContactSpec(radius_factor=0.95, kn=kn, kn_factor=10.0, epsilon=0.7,
+                    friction_on=friction, friction_coeff=0.5, damping_on=True, betan_factor=1.0)
+    n_part = n_particles
+    wall_fixed, wall_moving = n_part, n_part + 1
+    ubc = [BCSpec(particles=[wall_fixed], directions=[1, 2], zero=True),
+           BCSpec(particles=[wall_moving], directions=[2], time_fn="linear",
+                  time_params=[wall_speed])]
+    return SceneSpec(name=f"compressive_{n_particles}", dim=2, dt=dt, nt=nt, zones=zones,
+                     contact=_all_pairs(4, c),
+                     container=([lo[0], lo[1], 0.0], [hi[0], hi[1], 0.0]),
+                     gravity=(0.0, gravity, 0.0), search_factor=search_factor,
+                     search_interval=search_interval, test_name="compressive_test",
+                     compressive_wall=wall_moving, compressive_dir=2, test_output_interval=10,
+                     ubc=ubc, seed=seed)
+
+
+def column_3d(n_spheres: int = 4096, median_r: float = 1e-3, sigma: float = 0.2,
+              h_div: int = 10, box: Tuple[float, float, float] = (20e-3, 20e-3, 60e-3),
+              seed: int = 0, material: str = "PDState", piston_speed: float = -0.05,
+              dt: float = 2e-8, nt: int = 5000) -> SceneSpec:
+    """3-D granular column: spheres with lognormal radii on a jittered cubic
+    lattice inside a fixed box, a piston on top moving at ``piston_speed``."""
+    rng = np.random.default_rng(seed)
+    r_ref = median_r
+    h_ref = r_ref / h_div
+    s_n, s_v = sphere_mesh(r_ref, h_ref)
+    radii = np.clip(median_r * np.exp(sigma * rng.standard_normal(n_spheres)), 0.6 * median_r,
+                    1.6 * median_r)
+    h_min = float(radii.min()) / h_div
+    spacing = 2.0 * float(radii.max()) + 2.0 * h_min
+    nx = max(1, int(math.floor(box[0] / spacing)))
+    ny = max(1, int(math.floor(box[1] / spacing)))
+    sites = []
+    for p in range(n_spheres):
+        layer, rem = divmod(p, nx * ny)
+        iy, ix = divmod(rem, nx)
+        c = (0.5 * spacing + ix * spacing, 0.5 * spacing + iy * spacing,
+             0.5 * spacing + layer * spacing)
+        j = rng.uniform(-0.5, 0.5, size=3) * (spacing - 2 * radii[p] - 1.5 * h_min) * 0.5
+        sites.append(((c[0] + j[0], c[1] + j[1], c[2] + j[2]), float(radii[p]), 0.0))
+    height = (int(math.ceil(n_spheres / (nx * ny)))) * spacing
+    mat = elastic_material(material, 5.0e9)
+    t = 3.0 * h_min
+    W = (nx * spacing, ny * spacing)
+    lo = [-t - h_min, -t - h_min, -t - h_min]
+    hi = [W[0] + t + h_min, W[1] + t + h_min, height + 2 * t]
+    box_n, box_v = box_mesh(lo, hi, h_min, 3, hole_lo=[-0.5 * h_min, -0.5 * h_min, -0.5 * h_min],
+                            hole_hi=[W[0] + 0.5 * h_min, W[1] + 0.5 * h_min, hi[2] + 1.0])
+    pis_n, pis_v = box_mesh([0.5 * h_min, 0.5 * h_min, height], [W[0] - 0.5 * h_min,
+                                                                 W[1] - 0.5 * h_min, height + t],
+                            h_min, 3)
+    zones = [ZoneSpec("sphere", False, "sphere", [r_ref, 0.0, 0.0, 0.0], s_n, s_v, mat, sites=sites),
+             ZoneSpec("box", True, "cuboid", lo + hi, box_n, box_v, mat, all_dofs_constrained=True),
+             ZoneSpec("piston", True, "cuboid",
+                      [0.5 * h_min, 0.5 * h_min, height, W[0] - 0.5 * h_min, W[1] - 0.5 * h_min,
+                       height + t], pis_n, pis_v, mat, all_dofs_constrained=True)]
+    K = 5.0e9 / (3.0 * (1.0 - 2.0 * 0.25))
+    kn = 18.0 * K / (math.pi * (3.0 * h_min) ** 5)
+    c = ContactSpec(radius_factor=0.95, kn=kn, kn_factor=10.0, epsilon=0.7, friction_on=True,
+                    friction_coeff=0.5, damping_on=True, betan_factor=1.0)
+    ubc = [BCSpec(particles=[n_spheres], directions=[1, 2, 3], zero=True),
+           BCSpec(particles=[n_spheres + 1], directions=[3], time_fn="linear",
+                  time_params=[piston_speed])]
+    return SceneSpec(name=f"column_{n_spheres}", dim=3, dt=dt, nt=nt, zones=zones,
+                     contact=_all_pairs(3, c), container=(lo, hi), gravity=(0.0, 0.0, -10.0),
+                     search_factor=5.0, search_interval=40, test_name="compressive_test",
+                     compressive_wall=n_spheres + 1, compressive_dir=3, test_output_interval=10,
+                     ubc=ubc, seed=seed)
