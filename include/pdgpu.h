@@ -1,0 +1,306 @@
+/*
+ * pdgpu — B200 (sm_100a) explicit time step for PeriDEM, behind a plain C ABI.
+ *
+ * The entry points below replace, one for one, the virtual steps of the
+ * reference's model::DEMModel (src/model/dem/demModel.h:74-233): a host-side
+ * DEMModel subclass keeps the reference's own set-up (DEMModel::init), copies
+ * ModelData into a context with the pdgpu_upload_* calls, and from then on
+ * calls pdgpu_integrate_begin / pdgpu_step instead of
+ * DEMModel::integrate / integrateStep.  All arrays are the reference's own
+ * layouts: node vectors are util::Point (3 contiguous doubles, also in 2-D),
+ * indices are size_t (uint64), fixity is the uint8 bit mask of
+ * ModelData::d_fix.
+ *
+ * Every call returns PDGPU_OK (0) or a negative PDGPU_ERR_* code; the message
+ * of the last failure is available from pdgpu_last_error().  The library owns
+ * all device memory; it copies caller buffers on upload and writes caller
+ * buffers on download, and keeps no caller pointer.  One context is used by
+ * one host thread at a time; work runs on the context's own CUDA stream.
+ */
+#ifndef PDGPU_H
+#define PDGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PDGPU_API __attribute__((visibility("default")))
+#else
+#define PDGPU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define PDGPU_OK 0
+#define PDGPU_ERR_ARG (-1)      /* bad argument or call order */
+#define PDGPU_ERR_CUDA (-2)     /* a CUDA runtime call failed */
+#define PDGPU_ERR_NOMEM (-3)    /* device allocation failed */
+#define PDGPU_ERR_OVERFLOW (-4) /* a device list outgrew its capacity */
+#define PDGPU_ERR_NAN (-5)      /* non-finite force or position detected */
+#define PDGPU_ERR_STATE (-6)    /* context not ready for this call */
+#define PDGPU_ERR_NODEVICE (-7) /* no CUDA device / wrong architecture */
+
+/* material laws (src/material/mparticle/material.h) */
+#define PDGPU_MAT_RNP 0       /* RnpMaterial, "RNPBond" (material.h:251-659)     */
+#define PDGPU_MAT_PMB 1       /* PmbMaterial, "PMBBond" (material.h:665-1019)    */
+#define PDGPU_MAT_PDELASTIC 2 /* PdElastic, "PDElasticBond" (material.h:1025-1324) */
+#define PDGPU_MAT_PDSTATE 3   /* PdState, "PDState" (material.h:1330-1724)       */
+
+/* influence functions (src/material/mparticle/influenceFn.cpp:13-122) */
+#define PDGPU_INF_CONST 0
+#define PDGPU_INF_LINEAR 1
+#define PDGPU_INF_GAUSSIAN 2
+
+/* time functions of a boundary-condition set (particleULoading.cpp:115-230,
+ * particleFLoading.cpp:85-173) */
+#define PDGPU_TIME_CONSTANT 0
+#define PDGPU_TIME_LINEAR 1
+#define PDGPU_TIME_QUADRATIC 2
+#define PDGPU_TIME_SIN 3
+#define PDGPU_TIME_ROTATION 4
+#define PDGPU_TIME_LINEAR_STEP 5
+#define PDGPU_TIME_LINEAR_SLOW_FAST 6
+
+/* spatial functions of a boundary-condition set */
+#define PDGPU_SPACE_CONSTANT 0
+#define PDGPU_SPACE_HAT_X 1
+#define PDGPU_SPACE_HAT_Y 2
+#define PDGPU_SPACE_SIN_X 3
+#define PDGPU_SPACE_SIN_Y 4
+#define PDGPU_SPACE_LINEAR_X 5
+#define PDGPU_SPACE_LINEAR_Y 6
+
+/* post-processing test (DEMModel::integrate, demModel.cpp:304-313) */
+#define PDGPU_TEST_NONE 0
+#define PDGPU_TEST_TWO_PARTICLE 1
+#define PDGPU_TEST_COMPRESSIVE 2
+
+/* arithmetic of the bond loop */
+#define PDGPU_PREC_FP64 0  /* plain FP64 everywhere: the drop-in form */
+#define PDGPU_PREC_MIXED 1 /* FP32 bond loop on particle-local coordinates,
+                              FP64 integration and reductions */
+
+/* fields for pdgpu_download / pdgpu_upload_field */
+#define PDGPU_FIELD_X 0       /* double[N*3] current position  (d_x)      */
+#define PDGPU_FIELD_U 1       /* double[N*3] displacement      (d_u)      */
+#define PDGPU_FIELD_V 2       /* double[N*3] velocity          (d_v)      */
+#define PDGPU_FIELD_F 3       /* double[N*3] force density     (d_f)      */
+#define PDGPU_FIELD_Z 4       /* float[N]    damage            (d_Z)      */
+#define PDGPU_FIELD_VMAG 5    /* double[N]   |v|               (d_vMag)   */
+#define PDGPU_FIELD_THETA 6   /* double[N]   dilatation        (d_thetaX) */
+#define PDGPU_FIELD_MX 7      /* double[N]   weighted volume   (d_mX)     */
+#define PDGPU_FIELD_BONDS 8   /* uint8[B]    1 = broken, in neighbour-list order */
+#define PDGPU_FIELD_FIX 9     /* uint8[N]    fixity mask       (d_fix)    */
+
+/* Context description: the scalar parts of the reference's ModelDeck,
+ * ParticleDeck (gravity, neighbour search, test) and OutputDeck. */
+typedef struct pdgpu_desc {
+  int32_t dim;             /* ModelDeck::d_dim: 2 or 3 */
+  int32_t time_scheme;     /* 0 central_difference, 1 velocity_verlet */
+  int32_t precision;       /* PDGPU_PREC_* */
+  int32_t device;          /* CUDA device ordinal */
+  double dt;               /* ModelDeck::d_dt */
+  double gravity[3];       /* ParticleDeck::d_gravity */
+  int32_t multi_particle;  /* Input::isMultiParticle(): contact on/off */
+  int32_t test;            /* PDGPU_TEST_* */
+  int64_t test_wall;       /* ParticleDeck::d_particleIdCompressiveTest */
+  int32_t test_dir;        /* ParticleDeck::d_particleForceDirectionCompressiveTest - 1 */
+  int32_t pad0;
+  int64_t test_interval;   /* OutputDeck::d_dtTestOut */
+  double search_factor;    /* PNeighborDeck::d_sFactor */
+  int64_t search_interval; /* PNeighborDeck::d_neighUpdateInterval */
+  double max_contact_r;    /* ModelData::d_maxContactR (after setupContact) */
+  /* Capacity hints (0 = library default); lists that outgrow them are
+   * regrown by the library between steps. */
+  int64_t contact_capacity;   /* total contact candidate entries */
+  int64_t wall_pair_capacity; /* particle-wall node pairs per particle */
+} pdgpu_desc;
+
+/* One particle or wall (particle::BaseParticle, baseParticle.cpp:60-189). */
+typedef struct pdgpu_particle {
+  int64_t glob_start;    /* d_globStart */
+  int64_t glob_end;      /* d_globEnd */
+  int64_t center_node;   /* d_globStart + RefParticle::getCenterNodeId() */
+  int32_t type;          /* d_typeIndex: 0 particle, 1 wall */
+  int32_t zone;          /* d_zoneId */
+  int32_t compute_force; /* d_computeForce (after the two_particle override) */
+  int32_t all_dofs_constrained; /* d_allDofsConstrained */
+  int32_t material;      /* PDGPU_MAT_* */
+  int32_t pad0;
+  double horizon;        /* d_horizon */
+  double h;              /* d_h (mesh size) */
+  double density;        /* d_density */
+  double rc;             /* d_Rc, internal contact radius of broken bonds */
+  double kn;             /* d_Kn, internal contact stiffness */
+  double bound_r;        /* d_geom_p->boundingRadius() */
+  /* Bond-law constants of d_material_p:
+   *   RNP:        {C, beta, rbar, invFactor, factorSc, irreversible(0/1)}
+   *   PMB:        {c, s0}
+   *   PDElastic:  {c}
+   *   PDState:    {K, G, s0}                                            */
+  double mat[6];
+} pdgpu_particle;
+
+/* One boundary-condition set (inp::PBCData, src/inp/pdecks/pBCData.h). */
+typedef struct pdgpu_bc_set {
+  int32_t time_fn;       /* PDGPU_TIME_* */
+  int32_t spatial_fn;    /* PDGPU_SPACE_* */
+  int32_t dir_mask;      /* bit d set = direction d+1 is in d_direction */
+  int32_t zero;          /* d_isDisplacementZero */
+  double time_params[4]; /* d_timeFnParams (unused entries 0) */
+  double spatial_params[2];
+} pdgpu_bc_set;
+
+/* Scalars after the last step. */
+typedef struct pdgpu_scalars {
+  int64_t n;                     /* ModelData::d_n */
+  double time;                   /* ModelData::d_time */
+  double reaction;               /* last ppCompressiveTest reaction (reference definition) */
+  double contact_reaction;       /* -sum over particle nodes of (contact force from the test wall)*vol */
+  double wall_penetration;       /* last ppCompressiveTest penetration */
+  double max_velocity;           /* ModelData::d_maxVelocity */
+  double contact_search_radius;  /* d_contNeighSearchRadius */
+  int64_t contact_update_interval; /* d_contNeighUpdateInterval */
+  int64_t contact_counter;       /* d_contNeighTimestepCounter */
+  int64_t contact_updates;       /* contact list rebuilds so far */
+  int64_t contact_entries;       /* current contact candidate entries */
+  int64_t broken_bonds;          /* bonds with the broken bit set */
+  double pen_dist;               /* ppTwoParticleTest key data */
+  double max_y;
+  double contact_area_radius;
+} pdgpu_scalars;
+
+typedef struct pdgpu_ctx pdgpu_ctx;
+
+/* Library / device check.  Returns PDGPU_OK when a device of compute
+ * capability 10.0 is visible. */
+PDGPU_API int pdgpu_device_check(int device, char *msg, size_t msg_len);
+
+/* Context lifetime: the DEMModel constructor / destructor. */
+PDGPU_API int pdgpu_create(const pdgpu_desc *desc, pdgpu_ctx **out);
+PDGPU_API void pdgpu_destroy(pdgpu_ctx *ctx);
+PDGPU_API int pdgpu_last_error(const pdgpu_ctx *ctx, char *buf, size_t len);
+
+/* Node data after DEMModel::init (ModelData::d_xRef, d_x, d_u, d_v, d_vol,
+ * d_fix, d_ptId; modelData.h:531-760).  Any of x/u/v may be NULL (x defaults
+ * to xref, u and v to 0). */
+PDGPU_API int pdgpu_upload_nodes(pdgpu_ctx *ctx, int64_t n_nodes, const double *xref, const double *x,
+                       const double *u, const double *v, const double *vol, const uint8_t *fix,
+                       const uint64_t *pt_id);
+
+/* Particles and walls (ModelData::d_particlesListTypeAll). */
+PDGPU_API int pdgpu_upload_particles(pdgpu_ctx *ctx, int64_t n_particles, const pdgpu_particle *particles);
+
+/* The process-wide influence function (material.h:23-54). */
+PDGPU_API int pdgpu_set_influence(pdgpu_ctx *ctx, int32_t type, const double params[2]);
+
+/* Contact parameters per zone pair after DEMModel::setupContact
+ * (demModel.cpp:1531-1600): row-major n_zones x n_zones arrays of
+ * ContactPairDeck::d_contactR, d_Kn, d_mu, d_betan, d_kappa. */
+PDGPU_API int pdgpu_upload_contact(pdgpu_ctx *ctx, int32_t n_zones, const double *rc, const double *kn,
+                         const double *mu, const double *betan, const double *kappa);
+
+/* Peridynamic neighbour lists (ModelData::d_neighPd) in CSR form, in the
+ * caller's order; bond_state (optional) gives the geometry::Fracture bits
+ * one byte per bond.  Replaces DEMModel::updatePeridynamicNeighborlist. */
+PDGPU_API int pdgpu_upload_pd_neighbors(pdgpu_ctx *ctx, const uint64_t *rowptr, const uint64_t *col,
+                              const uint8_t *bond_state);
+
+/* Builds the peridynamic neighbour lists on the device instead
+ * (DEMModel::updatePeridynamicNeighborlist, demModel.cpp:1659-1694, with the
+ * kd-tree include-tag search of nsearch.h:340-364 replaced by a cell list;
+ * same strict squared-distance test, so the same sets).  Lists are sorted
+ * by node index. */
+PDGPU_API int pdgpu_build_pd_neighbors(pdgpu_ctx *ctx);
+
+/* Weighted volume m_x: upload (ModelData::d_mX) or compute on the device
+ * (material::computeStateMx, materialUtil.cpp:211-245). */
+PDGPU_API int pdgpu_upload_mx(pdgpu_ctx *ctx, const double *mx);
+PDGPU_API int pdgpu_compute_mx(pdgpu_ctx *ctx);
+
+/* Boundary conditions (ParticleULoading / ParticleFLoading).  particle_sel
+ * [n_particles] is needToProcessParticle() per particle; node_sel [n_nodes]
+ * is needToComputeDof() per node; particle_box [n_particles*6] is the box
+ * (lo xyz, hi xyz) the spatial function uses for each particle. */
+PDGPU_API int pdgpu_add_displacement_bc(pdgpu_ctx *ctx, const pdgpu_bc_set *set, const uint8_t *particle_sel,
+                              const uint8_t *node_sel, const double *particle_box);
+PDGPU_API int pdgpu_add_force_bc(pdgpu_ctx *ctx, const pdgpu_bc_set *set, const uint8_t *particle_sel,
+                       const uint8_t *node_sel, const double *particle_box);
+
+/* Initial condition (PICDeck; DEMModel::applyInitialCondition). */
+PDGPU_API int pdgpu_set_initial_condition(pdgpu_ctx *ctx, const double velocity[3],
+                                const uint64_t *particle_list, int64_t n_list);
+
+/* Contact neighbour list of DEMModel::init (demModel.cpp:181-189): builds the
+ * first contact candidate lists.  Call after all uploads. */
+PDGPU_API int pdgpu_init_contact(pdgpu_ctx *ctx);
+
+/* The prelude of DEMModel::integrate (demModel.cpp:277-283):
+ * applyInitialCondition (if n == 0), computeExternalDisplacementBC,
+ * computeForces. */
+PDGPU_API int pdgpu_integrate_begin(pdgpu_ctx *ctx);
+
+/* nsteps x (DEMModel::integrateStep + ppTwoParticleTest / ppCompressiveTest),
+ * demModel.cpp:285-324.  Runs asynchronously on the context stream; errors
+ * found on the device are reported by the next synchronising call. */
+PDGPU_API int pdgpu_step(pdgpu_ctx *ctx, int64_t nsteps);
+
+/* Same as pdgpu_step, issued as replays of a CUDA graph of `graph_steps`
+ * steps captured on first use (kernels only; no host work per step). */
+PDGPU_API int pdgpu_step_graph(pdgpu_ctx *ctx, int64_t nsteps, int32_t graph_steps);
+
+/* Waits for the context stream and reports device-side errors. */
+PDGPU_API int pdgpu_sync(pdgpu_ctx *ctx);
+
+/* Copies a field into a caller buffer (blocking). */
+PDGPU_API int pdgpu_download(pdgpu_ctx *ctx, int32_t field, void *dst);
+
+/* Overwrites u, v or x from a caller buffer (blocking); used by the
+ * host-buffer step below and by restarts. */
+PDGPU_API int pdgpu_upload_field(pdgpu_ctx *ctx, int32_t field, const void *src);
+
+/* One reference-facing step on host buffers, as a DEMModel::integrateStep
+ * override that keeps ModelData on the host: uploads u, v, x from the caller
+ * (N*3 doubles each), runs nsteps steps, downloads u, v, x and f back into
+ * the same buffers, and fills *out (may be NULL). */
+PDGPU_API int pdgpu_step_host(pdgpu_ctx *ctx, double *u, double *v, double *x, double *f, int64_t nsteps,
+                    pdgpu_scalars *out);
+
+PDGPU_API int pdgpu_get_scalars(pdgpu_ctx *ctx, pdgpu_scalars *out);
+
+/* The ppCompressiveTest history (time, wall penetration, reaction) recorded
+ * every test_interval steps; writes up to cap rows, sets *count to the
+ * number recorded so far. */
+PDGPU_API int pdgpu_get_history(pdgpu_ctx *ctx, double *t, double *delta, double *force,
+                      double *contact_force, int64_t cap, int64_t *count);
+
+/* Contact candidate lists (ModelData::d_neighC) in CSR form: rowptr has
+ * N+1 entries; col must hold scalars.contact_entries entries. */
+PDGPU_API int pdgpu_download_contact(pdgpu_ctx *ctx, uint64_t *rowptr, uint64_t *col);
+
+/* Peridynamic neighbour lists as held on the device. */
+PDGPU_API int pdgpu_num_bonds(pdgpu_ctx *ctx, int64_t *n_bonds);
+PDGPU_API int pdgpu_download_pd_neighbors(pdgpu_ctx *ctx, uint64_t *rowptr, uint64_t *col);
+
+/* Launch shape of the bond loop and the contact kernel: lanes per node
+ * (4, 8, 16 or 32 for the bond loop; 4, 8 or 32 for contact); 0 keeps the
+ * current choice.  Set before the first step. */
+PDGPU_API int pdgpu_set_tuning(pdgpu_ctx *ctx, int32_t pd_lanes, int32_t contact_lanes);
+
+/* The context's CUDA stream (a cudaStream_t) for callers that time work. */
+PDGPU_API int pdgpu_get_stream(pdgpu_ctx *ctx, void **stream);
+
+/* Per-kernel device time accumulated since the last reset (CUDA events
+ * around each launch when enabled); names are static strings. */
+PDGPU_API int pdgpu_enable_timing(pdgpu_ctx *ctx, int32_t on);
+PDGPU_API int pdgpu_kernel_times(pdgpu_ctx *ctx, int32_t max_kernels, const char **names, double *ms,
+                       int64_t *launches, int32_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PDGPU_H */

@@ -1,0 +1,207 @@
+// Device-side data of one pdgpu context and the kernel launchers shared by
+// the FP64 kernels (pdgpu_kernels.cu), the mixed-precision bond loop
+// (pdgpu_mixed.cu) and the host runtime (pdgpu_runtime.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "../../include/pdgpu.h"
+
+namespace pdgpu {
+
+// node flag bits
+enum : uint8_t {
+  NODE_ACTIVE = 1,   // in d_fPdCompNodes: integrated, peridynamic force computed
+  NODE_SEARCH = 2,   // searches for contact candidates (non-wall, computeForce, not all fixed)
+  NODE_WALL = 4,     // node of a wall
+  NODE_PARTICLE = 8, // node of a non-wall particle (receives particle damping)
+  NODE_SEARCH0 = 16, // searched at DEMModel::init (before the two_particle override)
+};
+
+// device error codes (CtrlState::error)
+enum : int {
+  DEV_OK = 0,
+  DEV_ERR_CONTACT_OVERFLOW = 1,
+  DEV_ERR_WALLPAIR_OVERFLOW = 2,
+  DEV_ERR_CELL_OVERFLOW = 3,
+  DEV_ERR_NONFINITE = 4,
+};
+
+struct DevParticle {
+  int64_t start, end, center;
+  int32_t type, zone, compute_force, all_fixed, material, pad;
+  double horizon, h, density, rc, kn, bound_r;
+  double check_low, check_up;  // horizon -/+ 0.5 h (volume correction bounds)
+  double mat[6];
+};
+
+struct ContactPair {
+  double rc, kn, mu, betan, kappa;
+};
+
+struct Influence {
+  int32_t type;
+  int32_t pad;
+  double p0, p1;  // const: a0 | linear: a0, a1 | gaussian: alpha, beta
+};
+
+// Step control, resident on the device so that a whole step can be replayed
+// from a CUDA graph without host work.
+struct CtrlState {
+  int64_t n;
+  double time;
+  // contact neighbour search (DEMModel::updateContactNeighborSearchParameters)
+  int64_t interval, counter, init_calls;
+  double radius;
+  double max_velocity;
+  unsigned long long vmax_bits;  // running max of |v| (non-negative doubles compare as integers)
+  double static_vmax;            // |v| max over nodes that are never integrated
+  int32_t update;                // this step rebuilds the contact candidate lists
+  int32_t first_bc;              // zero-displacement sets still to be applied
+  int64_t updates;
+  int64_t entries;
+  // device-side error word; once set, every kernel returns immediately
+  int32_t error;
+  int32_t pad;
+  int64_t error_info;
+  // post-processing results of the latest test step
+  double reaction, contact_reaction, penetration;
+  double pen_dist, max_y, contact_area_radius;
+  int64_t history_count;
+};
+
+// Cell grid fixed at set-up; nodes outside are clamped to the border cells,
+// which keeps every pair within one cell of each other in each direction.
+struct Grid {
+  double lo[3];
+  double inv_cell;
+  int32_t dims[3];
+  int32_t ncells;
+};
+
+struct BcSetDev {
+  int32_t time_fn, spatial_fn, dir_mask, zero;
+  double tp[4];
+  double sp[2];
+};
+
+// Per-particle constants of the FP32 bond loop (mixed precision form).
+struct MixParticle {
+  int64_t start;
+  int32_t material, irreversible;
+  float inv_horizon, check_low, check_up, inv_h;
+  float rc, kn;
+  float k_force;   // RNP: 4 C beta / invFactor | PMB, PD elastic: c | PD state: unused
+  float beta, rbar, factor_sc, s0;
+  float K, G;
+};
+
+struct DevData {
+  int32_t dim;
+  int32_t precision;
+  int64_t n_nodes;
+  int32_t n_particles;
+  int32_t n_zones;
+  double dt;
+  double gravity[3];
+  int32_t gravity_on;
+  int32_t time_scheme;
+
+  // nodes (stride 2 doubles in 2-D, 4 in 3-D)
+  double *xref, *x, *u, *v, *f;
+  double *vol, *mx, *theta, *vmag;
+  float *Z;
+  int32_t *ptid;
+  uint8_t *fix, *flags;
+
+  // particles, contact, influence
+  DevParticle *particles;
+  ContactPair *contact;  // n_zones * n_zones
+  Influence inf;
+
+  // peridynamic bonds (CSR, one bit per bond: 1 = broken)
+  int64_t n_bonds;
+  int64_t *pd_row;
+  int32_t *pd_col;
+  uint32_t *bond_bits;
+
+  // contact candidates (CSR)
+  double max_contact_r, search_factor;
+  int64_t search_interval;
+  int64_t contact_cap;
+  int64_t *c_row;
+  int32_t *c_col;
+  int64_t *c_cnt;  // per-node candidate counts of the last rebuild
+  Grid grid;
+  int32_t *cell_of, *cell_cnt, *cell_start, *cell_fill, *cell_tmp, *cell_nodes;
+  int64_t cell_cap;  // max nodes in one cell handled by the in-cell sort
+
+  // particle-wall damping pairs
+  int32_t wp_cap;
+  int32_t *wp, *wp_cnt;
+  double *fdamp;  // n_particles * 4
+
+  // boundary conditions: per BC node, a run of entries applied in set order
+  int32_t n_ubc_sets, n_fbc_sets;
+  BcSetDev *ubc_sets, *fbc_sets;
+  int32_t n_ubc_nodes, n_fbc_nodes;
+  int32_t *ubc_node, *ubc_row, *ubc_set;
+  double *ubc_val;
+  uint8_t *ubc_once;
+  int32_t *fbc_node, *fbc_row, *fbc_set;
+  double *fbc_val;
+
+  // initial condition
+  int32_t ic_active;
+  double ic_v[3];
+  uint8_t *ic_particle;  // per particle: in the IC list
+
+  // post-processing
+  int32_t test;
+  int64_t test_wall;
+  int32_t test_dir;
+  int64_t test_interval;
+  int64_t history_cap;
+  double *history;        // [cap][4]: t, delta, reaction, contact reaction
+  double *cr_partial;     // contact-reaction partial sums per contact block
+  int32_t cr_blocks;
+
+  CtrlState *ctrl;
+
+  // mixed-precision bond loop: particle-local FP32 reference coordinates,
+  // FP32 volumes, particle-local 16-bit neighbour offsets when they fit
+  float *xl;
+  float *volf;
+  uint16_t *pd_col16;
+  MixParticle *mixp;
+  int32_t use16;
+  float inf_p0, inf_p1;
+};
+
+// ---- launchers (all asynchronous on `s`) ----
+void launch_pack_vec(const DevData &d, const double *aos3, double *dst, cudaStream_t s);
+void launch_unpack_vec(const DevData &d, const double *src, double *aos3, cudaStream_t s);
+void launch_apply_ic(const DevData &d, cudaStream_t s);
+void launch_integrate(const DevData &d, int half_kick_only, cudaStream_t s);  // CD or Verlet first half
+void launch_verlet_second(const DevData &d, cudaStream_t s);
+void launch_ctrl(const DevData &d, int mode, cudaStream_t s);  // mode 0 step, 1 prelude, 2 init list
+void launch_bc(const DevData &d, cudaStream_t s);
+void launch_pd_prepass(const DevData &d, cudaStream_t s);
+void launch_pd_force(const DevData &d, int lanes, cudaStream_t s);
+void launch_pd_force_mixed(const DevData &d, int lanes, cudaStream_t s);
+void launch_pd_prepass_mixed(const DevData &d, int lanes, cudaStream_t s);
+void launch_mixed_setup(const DevData &d, cudaStream_t s);
+void launch_contact_update(const DevData &d, void *scan_tmp, size_t scan_tmp_bytes, int lanes,
+                           int init, cudaStream_t s);
+void launch_contact_force(const DevData &d, int lanes, cudaStream_t s);
+void launch_damping(const DevData &d, cudaStream_t s);
+void launch_external(const DevData &d, cudaStream_t s);
+void launch_postprocess(const DevData &d, cudaStream_t s);
+void launch_build_pd(const DevData &d, double cell, int64_t *row_tmp, int32_t *cnt, void *scan_tmp,
+                     size_t scan_bytes, int pass, cudaStream_t s);
+void launch_compute_mx(const DevData &d, cudaStream_t s);
+size_t scan_temp_bytes(int64_t n);
+void launch_vec_reduce_check(const DevData &d, cudaStream_t s);
+
+}  // namespace pdgpu

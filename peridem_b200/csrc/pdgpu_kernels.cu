@@ -1,0 +1,1321 @@
+// FP64 kernels of the explicit step.  This file is compiled with
+// --fmad=false: every product and sum rounds separately, as in the
+// reference's x86-64 build (no -march, so no FMA contraction), which keeps
+// the bond-break, contact and neighbour-search decisions bit-identical to
+// the reference for the same inputs.
+//
+// Layout in HBM: node vectors are stored with a stride of 2 doubles in 2-D
+// (double2) and 4 doubles in 3-D (double4, last lane unused), so one node is
+// one aligned 16- or 32-byte access; peridynamic bonds are CSR (int64 row
+// offsets, int32 columns) with one broken-bit per bond in a uint32 bitmap.
+#include <cub/cub.cuh>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "pdgpu_internal.h"
+
+namespace pdgpu {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;  // M_PI
+constexpr int kBlock = 256;
+
+// util::isGreater / util::isLess with COMPARE_EPS = 1e-5
+// (src/util/function.cpp:15-23, function.h:18)
+__device__ __forceinline__ bool is_greater(double a, double b) {
+  const double fa = fabs(a), fb = fabs(b);
+  return (a - b) > ((fa < fb ? fb : fa) * 1.0e-5);
+}
+__device__ __forceinline__ bool is_less(double a, double b) {
+  const double fa = fabs(a), fb = fabs(b);
+  return (b - a) > ((fa < fb ? fb : fa) * 1.0e-5);
+}
+
+template <int DIM>
+__device__ __forceinline__ void ldv(const double *__restrict__ a, int64_t i, double (&o)[3]) {
+  if constexpr (DIM == 2) {
+    const double2 t = reinterpret_cast<const double2 *>(a)[i];
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = 0.0;
+  } else {
+    const double2 *p = reinterpret_cast<const double2 *>(a) + 2 * i;
+    const double2 t0 = p[0], t1 = p[1];
+    o[0] = t0.x;
+    o[1] = t0.y;
+    o[2] = t1.x;
+  }
+}
+
+template <int DIM>
+__device__ __forceinline__ void ldg_v(const double *__restrict__ a, int64_t i, double (&o)[3]) {
+  if constexpr (DIM == 2) {
+    const double2 t = __ldg(reinterpret_cast<const double2 *>(a) + i);
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = 0.0;
+  } else {
+    const double2 *p = reinterpret_cast<const double2 *>(a) + 2 * i;
+    const double2 t0 = __ldg(p), t1 = __ldg(p + 1);
+    o[0] = t0.x;
+    o[1] = t0.y;
+    o[2] = t1.x;
+  }
+}
+
+template <int DIM>
+__device__ __forceinline__ void stv(double *__restrict__ a, int64_t i, const double (&o)[3]) {
+  if constexpr (DIM == 2) {
+    reinterpret_cast<double2 *>(a)[i] = make_double2(o[0], o[1]);
+  } else {
+    double2 *p = reinterpret_cast<double2 *>(a) + 2 * i;
+    p[0] = make_double2(o[0], o[1]);
+    p[1] = make_double2(o[2], 0.0);
+  }
+}
+
+// util::Point::length / dot: ((x*x + y*y) + z*z); the z term is an exact
+// no-op in 2-D (z = 0), so it is skipped there.
+template <int DIM>
+__device__ __forceinline__ double dot3(const double (&a)[3], const double (&b)[3]) {
+  double s = a[0] * b[0] + a[1] * b[1];
+  if constexpr (DIM == 3) s = s + a[2] * b[2];
+  return s;
+}
+template <int DIM>
+__device__ __forceinline__ double len3(const double (&a)[3]) {
+  return sqrt(dot3<DIM>(a, a));
+}
+
+// J(r / horizon) of the process-wide influence function
+// (influenceFn.cpp:21-23, 55-57, 86-88; material.h:431-433)
+__device__ __forceinline__ double influence(const Influence &f, double r, double horizon) {
+  const double q = r / horizon;
+  if (f.type == PDGPU_INF_LINEAR) return f.p0 + f.p1 * q;
+  if (f.type == PDGPU_INF_CONST) return f.p0;
+  return f.p0 * exp(-q * q / f.p1);
+}
+
+template <int LPN>
+__device__ __forceinline__ unsigned group_mask() {
+  if constexpr (LPN == 32) {
+    return 0xffffffffu;
+  } else {
+    const unsigned lane = threadIdx.x & 31u;
+    return ((1u << LPN) - 1u) << (lane / LPN * LPN);
+  }
+}
+
+template <int LPN>
+__device__ __forceinline__ double group_sum(double v, unsigned m) {
+#pragma unroll
+  for (int o = LPN / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o);
+  return v;
+}
+template <int LPN>
+__device__ __forceinline__ double group_max(double v, unsigned m) {
+#pragma unroll
+  for (int o = LPN / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(m, v, o));
+  return v;
+}
+template <int LPN>
+__device__ __forceinline__ int64_t group_sum_i(int64_t v, unsigned m) {
+#pragma unroll
+  for (int o = LPN / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void set_error(CtrlState *c, int code, int64_t info) {
+  if (atomicCAS(&c->error, 0, code) == 0) c->error_info = info;
+}
+
+// non-negative doubles order like their bit patterns
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long *a, double v) {
+  atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+template <int DIM>
+__device__ __forceinline__ int cell_coord(double x, const Grid &g, int d) {
+  double c = floor((x - g.lo[d]) * g.inv_cell);
+  if (c < 0.0) c = 0.0;
+  const double hi = (double)(g.dims[d] - 1);
+  if (c > hi) c = hi;
+  return (int)c;
+}
+
+template <int DIM>
+__device__ __forceinline__ int cell_index(const double (&p)[3], const Grid &g) {
+  int c = cell_coord<DIM>(p[0], g, 0) + g.dims[0] * cell_coord<DIM>(p[1], g, 1);
+  if constexpr (DIM == 3) c += g.dims[0] * g.dims[1] * cell_coord<DIM>(p[2], g, 2);
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+__global__ void k_pack(const double *__restrict__ aos3, double *__restrict__ dst, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double o[3] = {aos3[3 * i], aos3[3 * i + 1], aos3[3 * i + 2]};
+  stv<DIM>(dst, i, o);
+}
+
+template <int DIM>
+__global__ void k_unpack(const double *__restrict__ src, double *__restrict__ aos3, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double o[3];
+  ldv<DIM>(src, i, o);
+  aos3[3 * i] = o[0];
+  aos3[3 * i + 1] = o[1];
+  aos3[3 * i + 2] = (DIM == 3) ? o[2] : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// DEMModel::applyInitialCondition (demModel.cpp:1068-1095): every node of a
+// listed particle gets the IC velocity (all three components).
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void k_apply_ic(DevData d) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_nodes) return;
+  if (!d.ic_particle[d.ptid[i]]) return;
+  double o[3] = {d.ic_v[0], d.ic_v[1], d.ic_v[2]};
+  stv<DIM>(d.v, i, o);
+}
+
+// ---------------------------------------------------------------------------
+// DEMModel::integrateCD (demModel.cpp:349-390) and the first half of
+// DEMModel::integrateVerlet (:392-424), over d_fPdCompNodes, free dofs only.
+// Also folds |v| into the running maximum that the contact-search control
+// reads (updateContactNeighborSearchParameters, :1862-1883).
+// ---------------------------------------------------------------------------
+template <int DIM, bool VERLET>
+__global__ void __launch_bounds__(kBlock) k_integrate(DevData d) {
+  __shared__ double smax[kBlock / 32];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double vm = 0.0;
+  if (i < d.n_nodes && (d.flags[i] & NODE_ACTIVE) && !d.ctrl->error) {
+    const double rho = d.particles[d.ptid[i]].density;
+    const uint8_t fix = d.fix[i];
+    double v[3], u[3], x[3], f[3];
+    ldv<DIM>(d.v, i, v);
+    ldv<DIM>(d.u, i, u);
+    ldv<DIM>(d.x, i, x);
+    ldv<DIM>(d.f, i, f);
+    const double dt = d.dt;
+    const double k = VERLET ? 0.5 * (dt / rho) : dt / rho;
+#pragma unroll
+    for (int dof = 0; dof < DIM; dof++) {
+      if (!((fix >> dof) & 1u)) {
+        v[dof] += k * f[dof];
+        u[dof] += dt * v[dof];
+        x[dof] += dt * v[dof];
+      }
+    }
+    stv<DIM>(d.v, i, v);
+    stv<DIM>(d.u, i, u);
+    stv<DIM>(d.x, i, x);
+    vm = len3<DIM>(v);
+    d.vmag[i] = vm;
+  }
+  // block max of |v| -> one atomic per block
+  for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+  if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = vm;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double m = threadIdx.x < kBlock / 32 ? smax[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0 && m > 0.0) atomic_max_nonneg(&d.ctrl->vmax_bits, m);
+  }
+}
+
+// second half kick of DEMModel::integrateVerlet (:436-459)
+template <int DIM>
+__global__ void k_verlet_second(DevData d) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_nodes || !(d.flags[i] & NODE_ACTIVE) || d.ctrl->error) return;
+  const double rho = d.particles[d.ptid[i]].density;
+  const uint8_t fix = d.fix[i];
+  double v[3], f[3];
+  ldv<DIM>(d.v, i, v);
+  ldv<DIM>(d.f, i, f);
+  const double k = 0.5 * (d.dt / rho);
+#pragma unroll
+  for (int dof = 0; dof < DIM; dof++)
+    if (!((fix >> dof) & 1u)) v[dof] += k * f[dof];
+  stv<DIM>(d.v, i, v);
+  d.vmag[i] = len3<DIM>(v);
+}
+
+// ---------------------------------------------------------------------------
+// Step control (one thread): time advance (integrateCD :381-383) and the
+// contact-list update decision of
+// DEMModel::updateContactNeighborSearchParameters (demModel.cpp:1808-1955).
+// mode 0: a time step; 1: the computeForces call of the integrate() prelude;
+// 2: the contact list build of DEMModel::init.
+// ---------------------------------------------------------------------------
+__global__ void k_ctrl(DevData d, int mode) {
+  CtrlState *c = d.ctrl;
+  if (c->error) return;
+  if (mode == 0) {
+    c->n += 1;
+    c->time += d.dt;
+    c->first_bc = 0;
+  }
+  const double vmax_now =
+      fmax(__longlong_as_double((long long)c->vmax_bits), c->static_vmax);
+  c->vmax_bits = 0ull;
+  if (!d.n_zones) {  // single particle: no contact
+    c->update = 0;
+    return;
+  }
+  int upd = 0;
+  const int64_t n = c->n;
+  if (n == 0) {
+    c->init_calls += 1;
+    if (c->init_calls == 1) {
+      c->update = 1;
+      return;
+    }
+    if (c->init_calls == 2) {
+      c->counter += 1;
+      c->update = ((c->counter - 1) % c->interval) == 0;
+      return;
+    }
+  }
+  if (c->interval == 1) {
+    c->radius = d.max_contact_r;
+    c->counter += 1;
+    c->update = ((c->counter - 1) % c->interval) == 0;
+    return;
+  }
+  const int64_t upi = c->interval > 5 ? (int64_t)(0.2 * (double)c->interval) : 1;
+  if (c->counter > 0 && c->counter % upi != 0) {
+    c->counter += 1;
+    c->update = ((c->counter - 1) % c->interval) == 0;
+    return;
+  }
+  c->max_velocity = vmax_now;
+  const double safety = d.search_factor > 5 ? d.search_factor : 10.0;
+  const double r_contact = d.search_factor * d.max_contact_r;
+  const double r_vel = c->max_velocity * d.dt * (double)d.search_interval * safety;
+  if (is_greater(r_vel, r_contact)) {
+    c->interval = (int64_t)(d.max_contact_r / (c->max_velocity * d.dt));
+    c->radius = r_contact;
+    c->counter = 0;
+    if (c->interval < 1) {
+      c->interval = 1;
+      c->radius = d.max_contact_r;
+    }
+  } else {
+    c->radius = c->interval < 2 ? d.max_contact_r : r_contact;
+  }
+  c->counter += 1;
+  upd = ((c->counter - 1) % c->interval) == 0;
+  c->update = upd;
+}
+
+// ---------------------------------------------------------------------------
+// DEMModel::computeExternalDisplacementBC -> ParticleULoading::apply
+// (particleULoading.cpp:115-230).  One thread per BC node applies that node's
+// sets in deck order; the spatial factor of each (node, set) is precomputed
+// on the host from the reference configuration.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void k_bc(DevData d) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.n_ubc_nodes || d.ctrl->error) return;
+  const int64_t i = d.ubc_node[t];
+  const double time = d.ctrl->time;
+  const int first = d.ctrl->first_bc;
+  double u[3], v[3], x[3], xr[3];
+  ldv<DIM>(d.u, i, u);
+  ldv<DIM>(d.v, i, v);
+  ldv<DIM>(d.x, i, x);
+  ldg_v<DIM>(d.xref, i, xr);
+  for (int e = d.ubc_row[t]; e < d.ubc_row[t + 1]; e++) {
+    if (d.ubc_once[e] && !first) continue;
+    const BcSetDev bc = d.ubc_sets[d.ubc_set[e]];
+    const double umax = d.ubc_val[e];
+    double du = 0.0, dv = 0.0;
+    switch (bc.time_fn) {
+      case PDGPU_TIME_CONSTANT: du = umax; break;
+      case PDGPU_TIME_LINEAR: du = umax * time; dv = umax; break;
+      case PDGPU_TIME_QUADRATIC:
+        du = umax * time + bc.tp[1] * time * time;
+        dv = umax + bc.tp[1] * time;
+        break;
+      case PDGPU_TIME_SIN: {
+        const double a = kPi * bc.tp[1];
+        du = umax * sin(a * time);
+        dv = umax * a * cos(a * time);
+        break;
+      }
+      default: break;
+    }
+    double ui[3] = {0.0, 0.0, 0.0}, vi[3] = {0.0, 0.0, 0.0};
+    for (int q = 0; q < 3; q++)
+      if ((bc.dir_mask >> q) & 1) {
+        ui[q] = du;
+        vi[q] = dv;
+      }
+    if (bc.time_fn == PDGPU_TIME_ROTATION) {
+      const double dx0 = xr[0] - bc.tp[1], dx1 = xr[1] - bc.tp[2];
+      const double th = bc.tp[0] * time;
+      const double ct = cos(th), st = sin(th);
+      // util::rotate2D / derRotate2D (transformation.cpp:53-65)
+      const double r0 = dx0 * ct - dx1 * st, r1 = dx0 * st + dx1 * ct;
+      const double d0 = -dx0 * st - dx1 * ct, d1 = dx0 * ct - dx1 * st;
+      ui[0] += r0 - dx0;
+      ui[1] += r1 - dx1;
+      ui[2] += 0.0 - (xr[2] - bc.tp[3]);
+      vi[0] += bc.tp[0] * d0;
+      vi[1] += bc.tp[0] * d1;
+      vi[2] += bc.tp[0] * 0.0;
+    }
+    for (int q = 0; q < DIM; q++)
+      if ((bc.dir_mask >> q) & 1) {
+        u[q] = ui[q];
+        v[q] = vi[q];
+        x[q] = ui[q] + xr[q];
+      }
+  }
+  stv<DIM>(d.u, i, u);
+  stv<DIM>(d.v, i, v);
+  stv<DIM>(d.x, i, x);
+}
+
+// ---------------------------------------------------------------------------
+// State-based pre-pass of DEMModel::computePeridynamicForces
+// (demModel.cpp:610-679): bond breaking and dilatation theta_i.
+// LPN lanes per node, lane-strided over the node's bonds.
+// ---------------------------------------------------------------------------
+template <int DIM, int LPN>
+__global__ void __launch_bounds__(kBlock) k_pd_prepass(DevData d) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
+  const int lane = threadIdx.x % LPN;
+  if (i >= d.n_nodes) return;
+  if (!(d.flags[i] & NODE_ACTIVE) || d.ctrl->error) return;
+  const DevParticle &P = d.particles[d.ptid[i]];
+  if (P.material != PDGPU_MAT_PDSTATE) return;
+  const unsigned gm = group_mask<LPN>();
+  double xi[3], ui[3];
+  ldg_v<DIM>(d.xref, i, xi);
+  ldg_v<DIM>(d.u, i, ui);
+  const double sc = P.mat[2];
+  double theta = 0.0;
+  const int64_t k0 = d.pd_row[i], k1 = d.pd_row[i + 1];
+  for (int64_t k = k0 + lane; k < k1; k += LPN) {
+    const int32_t j = __ldg(d.pd_col + k);
+    double xj[3], uj[3];
+    ldg_v<DIM>(d.xref, j, xj);
+    ldg_v<DIM>(d.u, j, uj);
+    double dx[3], y[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      dx[q] = xj[q] - xi[q];
+      y[q] = dx[q] + uj[q] - ui[q];  // (xj - xi + uj - ui), left to right
+    }
+    const double rji = len3<DIM>(dx);
+    const double cl = len3<DIM>(y) - rji;
+    const double s = cl / rji;
+    const uint32_t bit = 1u << (k & 31);
+    bool fs = (d.bond_bits[k >> 5] & bit) != 0;
+    if (!fs && is_greater(fabs(s), sc + 1.0e-10)) {
+      fs = true;
+      atomicOr(d.bond_bits + (k >> 5), bit);
+    }
+    if (!fs) {
+      double volj = __ldg(d.vol + j);
+      if (is_greater(rji, P.check_low)) volj *= (P.check_up - rji) / P.h;
+      theta += rji * cl * influence(d.inf, rji, P.horizon) * volj;
+    }
+  }
+  theta = group_sum<LPN>(theta, gm);
+  if (lane == 0) d.theta[i] = 3.0 * theta / d.mx[i];
+}
+
+// ---------------------------------------------------------------------------
+// Main bond loop of DEMModel::computePeridynamicForces (demModel.cpp:681-789)
+// with the bond laws of RnpMaterial (material.h:342-417), PmbMaterial
+// (:732-801), PdElastic (:1090-1144) and PdState (:1415-1459).  Overwrites
+// f_i (the reference zeroes f then sets d_f[i] = force_i) and Z_i.
+// ---------------------------------------------------------------------------
+template <int DIM, int LPN>
+__global__ void __launch_bounds__(kBlock) k_pd_force(DevData d) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
+  const int lane = threadIdx.x % LPN;
+  if (i >= d.n_nodes) return;
+  if (d.ctrl->error) return;
+  if (!(d.flags[i] & NODE_ACTIVE)) {
+    if (lane == 0) {
+      const double z[3] = {0.0, 0.0, 0.0};
+      stv<DIM>(d.f, i, z);
+    }
+    return;
+  }
+  const unsigned gm = group_mask<LPN>();
+  const DevParticle &P = d.particles[d.ptid[i]];
+  const int mat = P.material;
+  double xi[3], ui[3];
+  ldg_v<DIM>(d.xref, i, xi);
+  ldg_v<DIM>(d.u, i, ui);
+  const double mi = d.mx[i];
+  const double thi = d.theta[i];
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  double zmax = 0.0;
+  const int64_t k0 = d.pd_row[i], k1 = d.pd_row[i + 1];
+  for (int64_t k = k0 + lane; k < k1; k += LPN) {
+    const int32_t j = __ldg(d.pd_col + k);
+    const uint32_t bit = 1u << (k & 31);
+    bool fs = (d.bond_bits[k >> 5] & bit) != 0;
+    double xj[3], uj[3];
+    ldg_v<DIM>(d.xref, j, xj);
+    ldg_v<DIM>(d.u, j, uj);
+    double volj = __ldg(d.vol + j);
+    double dx[3], du[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      dx[q] = xj[q] - xi[q];
+      du[q] = uj[q] - ui[q];
+    }
+    const double rji = len3<DIM>(dx);
+    double S, dpl[3], ldpl = 0.0;
+    if (mat == PDGPU_MAT_RNP) {
+      S = dot3<DIM>(dx, du) / dot3<DIM>(dx, dx);  // material.h:405-407
+    } else {
+#pragma unroll
+      for (int q = 0; q < 3; q++) dpl[q] = dx[q] + du[q];
+      ldpl = len3<DIM>(dpl);
+      S = (ldpl - rji) / rji;  // material.h:791-793
+    }
+    double sc;
+    if (mat == PDGPU_MAT_RNP) sc = P.mat[2] / sqrt(rji);
+    else if (mat == PDGPU_MAT_PDELASTIC) sc = DBL_MAX;
+    else if (mat == PDGPU_MAT_PMB) sc = P.mat[1];
+    else sc = P.mat[2];
+    if (!fs) {
+      if (is_greater(rji, P.check_low)) volj *= (P.check_up - rji) / P.h;
+      double ef = 0.0;
+      const double J = influence(d.inf, rji, P.horizon);
+      if (mat == PDGPU_MAT_PDSTATE) {
+        const double mj = __ldg(d.mx + j), thj = __ldg(d.theta + j);
+        const double K = P.mat[0], G = P.mat[1];
+        const double cl = S * rji;
+        const double ai = 15. * G / mi, aj = 15. * G / mj;
+        const double fi = (3. * K / mi) - ai / 3., fj = (3. * K / mj) - aj / 3.;
+        const double efi = J * (rji * thi * fi + cl * ai);
+        const double efj = J * (rji * thj * fj + cl * aj);
+        const double sf = (efi + efj) * volj;
+        const double inv = ldpl;
+        fx += sf * (dpl[0] / inv);
+        fy += sf * (dpl[1] / inv);
+        if constexpr (DIM == 3) fz += sf * (dpl[2] / inv);
+      } else {
+        if (mat == PDGPU_MAT_RNP) {
+          if (P.mat[5] != 0.0 && !fs && is_greater(fabs(S), P.mat[4] * sc)) {
+            fs = true;
+            atomicOr(d.bond_bits + (k >> 5), bit);
+          }
+          if (!fs)
+            ef = J * 4. * S * P.mat[0] * P.mat[1] * exp(-P.mat[1] * rji * S * S) / P.mat[3];
+          const double sf = ef * volj;
+          fx += sf * (dx[0] / rji);
+          fy += sf * (dx[1] / rji);
+          if constexpr (DIM == 3) fz += sf * (dx[2] / rji);
+        } else {
+          if (mat == PDGPU_MAT_PMB && !fs && is_greater(fabs(S), P.mat[1] + 1.0e-10)) {
+            fs = true;
+            atomicOr(d.bond_bits + (k >> 5), bit);
+          }
+          if (!fs) ef = J * P.mat[0] * S;
+          const double sf = ef * volj;
+          fx += sf * (dpl[0] / ldpl);
+          fy += sf * (dpl[1] / ldpl);
+          if constexpr (DIM == 3) fz += sf * (dpl[2] / ldpl);
+        }
+      }
+    } else {
+      // broken bond: internal normal contact (demModel.cpp:760-768)
+      double y[3];
+#pragma unroll
+      for (int q = 0; q < 3; q++) y[q] = (xj[q] + uj[q]) - (xi[q] + ui[q]);
+      const double R = len3<DIM>(y);
+      double sf = P.kn * volj * (R - P.rc) / R;
+      if (sf > 0.) sf = 0.;
+      fx += sf * y[0];
+      fy += sf * y[1];
+      if constexpr (DIM == 3) fz += sf * y[2];
+    }
+    // damage Z = max |S / Sc| (demModel.cpp:770-773)
+    zmax = fmax(zmax, fabs(S / sc));
+  }
+  fx = group_sum<LPN>(fx, gm);
+  fy = group_sum<LPN>(fy, gm);
+  if constexpr (DIM == 3) fz = group_sum<LPN>(fz, gm);
+  zmax = group_max<LPN>(zmax, gm);
+  if (lane == 0) {
+    const double o[3] = {fx, fy, fz};
+    stv<DIM>(d.f, i, o);
+    d.Z[i] = (float)zmax;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Contact candidate lists: DEMModel::updateContactNeighborlist
+// (demModel.cpp:1696-1756) with the kd-tree exclude-tag radius search
+// (nsearch.h:278-301; strict  sum_d (q_d - p_d)^2 < r*r  of
+// nanoflann.hpp:611-621 / nflannSetup.h:272) replaced by a cell list.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void k_cell_count(DevData d, const double *__restrict__ pos, Grid g) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_nodes) return;
+  if (d.ctrl->error || !d.ctrl->update) return;
+  double p[3];
+  ldv<DIM>(pos, i, p);
+  const int c = cell_index<DIM>(p, g);
+  d.cell_of[i] = c;
+  atomicAdd(d.cell_cnt + c, 1);
+}
+
+__global__ void k_cell_scatter(DevData d) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_nodes) return;
+  if (d.ctrl->error || !d.ctrl->update) return;
+  const int c = d.cell_of[i];
+  const int pos = d.cell_start[c] + atomicAdd(d.cell_fill + c, 1);
+  d.cell_tmp[pos] = (int32_t)i;
+}
+
+// one warp per cell: order the cell's nodes by index (rank counting), so
+// candidate lists do not depend on atomic arrival order
+__global__ void k_cell_sort(DevData d) {
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (c >= d.grid.ncells) return;
+  if (d.ctrl->error || !d.ctrl->update) return;
+  const int s = d.cell_start[c], e = d.cell_start[c + 1];
+  for (int a = s + lane; a < e; a += 32) {
+    const int32_t va = d.cell_tmp[a];
+    int rank = 0;
+    for (int b = s; b < e; b++) rank += d.cell_tmp[b] < va;
+    d.cell_nodes[s + rank] = va;
+  }
+  if (lane == 0) d.cell_fill[c] = 0;
+}
+
+__global__ void k_zero_cells(DevData d) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > d.grid.ncells) return;
+  if (!d.ctrl->update) return;
+  d.cell_cnt[c] = 0;
+}
+
+// candidate search: COUNT pass writes per-node counts into c_cnt; the scan
+// c_cnt -> c_row[1..N] is out of place, so replaying it on a step without a
+// rebuild reproduces the same offsets.  FILL pass writes the columns in
+// (cell, node index) order.
+template <int DIM, int LPN, bool FILL>
+__global__ void __launch_bounds__(kBlock) k_cand(DevData d, uint8_t search_bit) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
+  const int lane = threadIdx.x % LPN;
+  if (i >= d.n_nodes) return;
+  if (d.ctrl->error || !d.ctrl->update) return;
+  const unsigned gm = group_mask<LPN>();
+  const unsigned lane_base = (threadIdx.x & 31u) / LPN * LPN;
+  if (!(d.flags[i] & search_bit)) {
+    if (!FILL && lane == 0) d.c_cnt[i] = 0;
+    return;
+  }
+  const Grid g = d.grid;
+  double q[3];
+  ldv<DIM>(d.x, i, q);
+  const int32_t pi = d.ptid[i];
+  const double r = d.ctrl->radius;
+  const double r2 = r * r;
+  int c[3] = {cell_coord<DIM>(q[0], g, 0), cell_coord<DIM>(q[1], g, 1),
+              DIM == 3 ? cell_coord<DIM>(q[2], g, 2) : 0};
+  int64_t out = FILL ? d.c_row[i] : 0;
+  const int64_t out_end = FILL ? d.c_row[i + 1] : 0;
+  int64_t count = 0;
+  const int zlo = DIM == 3 ? max(c[2] - 1, 0) : 0;
+  const int zhi = DIM == 3 ? min(c[2] + 1, g.dims[2] - 1) : 0;
+  for (int cz = zlo; cz <= zhi; cz++)
+    for (int cy = max(c[1] - 1, 0); cy <= min(c[1] + 1, g.dims[1] - 1); cy++)
+      for (int cx = max(c[0] - 1, 0); cx <= min(c[0] + 1, g.dims[0] - 1); cx++) {
+        const int cell = cx + g.dims[0] * (cy + g.dims[1] * cz);
+        const int s = d.cell_start[cell], e = d.cell_start[cell + 1];
+        for (int base = s; base < e; base += LPN) {
+          const int a = base + lane;
+          bool hit = false;
+          int32_t j = -1;
+          if (a < e) {
+            j = d.cell_nodes[a];
+            if (d.ptid[j] != pi) {
+              double p[3];
+              ldv<DIM>(d.x, j, p);
+              double dd = 0.0;
+#pragma unroll
+              for (int t = 0; t < DIM; t++) {
+                const double df = q[t] - p[t];
+                dd += df * df;
+              }
+              hit = dd < r2;
+            }
+          }
+          const unsigned bal = (__ballot_sync(gm, hit) & gm) >> lane_base;
+          if (FILL) {
+            if (hit) {
+              const int64_t at = out + __popc(bal & ((1u << lane) - 1u));
+              if (at < out_end) d.c_col[at] = j;
+            }
+            out += __popc(bal);
+          } else {
+            count += __popc(bal);
+          }
+        }
+      }
+  if (!FILL && lane == 0) d.c_cnt[i] = count;
+}
+
+__global__ void k_cand_check(DevData d) {
+  if (d.ctrl->error || !d.ctrl->update) return;
+  const int64_t total = d.c_row[d.n_nodes];
+  d.ctrl->entries = total;
+  d.ctrl->updates += 1;
+  if (total > d.contact_cap) set_error(d.ctrl, DEV_ERR_CONTACT_OVERFLOW, total);
+}
+
+// ---------------------------------------------------------------------------
+// Node pass of DEMModel::computeContactForces (demModel.cpp:832-934):
+// penalty normal force + Coulomb-type friction for candidates inside the
+// zone-pair contact radius; f_i += sum.  Particle-wall pairs inside the
+// contact radius are recorded for the particle-wall damping (:994-1017),
+// and the test wall's contact reaction is summed per block.
+// ---------------------------------------------------------------------------
+template <int DIM, int LPN>
+__global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
+  __shared__ double scr[kBlock / LPN];
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
+  const int lane = threadIdx.x % LPN;
+  double crd = 0.0;
+  const bool live = i < d.n_nodes && (d.flags[i] & NODE_SEARCH) && !d.ctrl->error;
+  if (live) {
+    const unsigned gm = group_mask<LPN>();
+    const int32_t pi = d.ptid[i];
+    const int zi = d.particles[pi].zone;
+    double yi[3], vi[3];
+    ldv<DIM>(d.x, i, yi);
+    ldv<DIM>(d.v, i, vi);
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    const int64_t k0 = d.c_row[i], k1 = d.c_row[i + 1];
+    for (int64_t k = k0 + lane; k < k1; k += LPN) {
+      const int32_t j = d.c_col[k];
+      double yj[3];
+      ldv<DIM>(d.x, j, yj);
+      double yji[3];
+#pragma unroll
+      for (int q = 0; q < 3; q++) yji[q] = yj[q] - yi[q];
+      const double R = len3<DIM>(yji);
+      const int32_t pj = d.ptid[j];
+      const DevParticle &Pj = d.particles[pj];
+      const ContactPair cp = d.contact[zi * d.n_zones + Pj.zone];
+      if (is_less(R, cp.rc)) {
+        double vj[3], vji[3], en[3], et[3];
+        ldv<DIM>(d.v, j, vj);
+        const double volj = d.vol[j];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          vji[q] = vj[q] - vi[q];
+          en[q] = yji[q] / R;
+        }
+        const double vn = dot3<DIM>(vji, en);
+#pragma unroll
+        for (int q = 0; q < 3; q++) et[q] = vji[q] - vn * en[q];
+        const double etl = len3<DIM>(et);
+        if (is_greater(etl, 0.)) {
+#pragma unroll
+          for (int q = 0; q < 3; q++) et[q] = et[q] / etl;
+        } else {
+          et[0] = et[1] = et[2] = 0.0;
+        }
+        double sf = cp.kn * (R - cp.rc) * volj;
+        if (sf > 0.) sf = 0.;
+        const double mf = cp.mu * sf;
+        const double cx = sf * en[0], cy = sf * en[1], cz = sf * en[2];
+        fx += cx;
+        fy += cy;
+        if constexpr (DIM == 3) fz += cz;
+        fx += mf * et[0];
+        fy += mf * et[1];
+        if constexpr (DIM == 3) fz += mf * et[2];
+        if (Pj.type == 1) {
+          const int slot = atomicAdd(d.wp_cnt + pi, 1);
+          if (slot < d.wp_cap) d.wp[(int64_t)pi * d.wp_cap + slot] = j;
+          else set_error(d.ctrl, DEV_ERR_WALLPAIR_OVERFLOW, pi);
+        }
+        if (pj == d.test_wall) {
+          const double c3[3] = {cx + mf * et[0], cy + mf * et[1], cz + mf * et[2]};
+          crd += c3[d.test_dir];
+        }
+      }
+    }
+    fx = group_sum<LPN>(fx, gm);
+    fy = group_sum<LPN>(fy, gm);
+    if constexpr (DIM == 3) fz = group_sum<LPN>(fz, gm);
+    crd = group_sum<LPN>(crd, gm);
+    if (lane == 0) {
+      double f[3];
+      ldv<DIM>(d.f, i, f);
+      f[0] += fx;
+      f[1] += fy;
+      f[2] += fz;
+      stv<DIM>(d.f, i, f);
+      crd *= d.vol[i];
+    }
+  }
+  // deterministic per-block partial of the test wall's contact reaction
+  if (lane == 0) scr[threadIdx.x / LPN] = live ? crd : 0.0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int g = 0; g < kBlock / LPN; g++) s += scr[g];
+    d.cr_partial[blockIdx.x] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Particle damping of DEMModel::computeContactForces (demModel.cpp:937-1050):
+// particle-particle through particle centres and particle-wall through the
+// condensed wall nodes.  One block per particle; the force density is applied
+// to all nodes of the particle by k_external.
+// ---------------------------------------------------------------------------
+constexpr int kDampBlock = 256;
+constexpr int kWallSort = 4096;
+
+__global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
+  __shared__ int32_t wn[kWallSort];
+  __shared__ double red[3][kDampBlock / 32];
+  const int p = blockIdx.x;
+  const DevParticle P = d.particles[p];
+  if (P.type != 0) return;
+  if (d.ctrl->error) return;
+  const double Ri = P.bound_r;
+  const double vol_pi = kPi * Ri * Ri;
+  const double rhoi = P.density;
+  double xc[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
+  const int st = dim == 2 ? 2 : 4;
+  for (int q = 0; q < dim; q++) {
+    xc[q] = d.x[st * P.center + q];
+    vc[q] = d.v[st * P.center + q];
+  }
+  double acc[3] = {0.0, 0.0, 0.0};
+  // particle-particle
+  for (int q = threadIdx.x; q < d.n_particles; q += blockDim.x) {
+    if (q == p) continue;
+    const DevParticle &Q = d.particles[q];
+    if (Q.type != 0) continue;
+    const double Rj = Q.bound_r;
+    double xcj[3] = {0, 0, 0}, vcj[3] = {0, 0, 0};
+    for (int t = 0; t < dim; t++) {
+      xcj[t] = d.x[st * Q.center + t] - xc[t];
+      vcj[t] = d.v[st * Q.center + t] - vc[t];
+    }
+    const double dist = sqrt(xcj[0] * xcj[0] + xcj[1] * xcj[1] + xcj[2] * xcj[2]);
+    const ContactPair cp = d.contact[P.zone * d.n_zones + Q.zone];
+    if (is_less(dist, Rj + Ri + 1.01 * cp.rc)) {
+      const double vol_pj = kPi * Rj * Rj;
+      const double m1 = rhoi * vol_pi, m2 = Q.density * vol_pj;
+      const double meq = 2. * m1 * m2 / (m1 + m2);  // util::equivalentMass
+      const double bn = cp.betan * sqrt(cp.kappa * cp.rc * meq);
+      double hat[3] = {0.0, 0.0, 0.0};
+      if (is_greater(dist, 0.))
+        for (int t = 0; t < 3; t++) hat[t] = xcj[t] / dist;
+      double vm = vcj[0] * hat[0] + vcj[1] * hat[1] + vcj[2] * hat[2];
+      if (vm > 0.) vm = 0.;
+      for (int t = 0; t < 3; t++) acc[t] += bn * vm * hat[t] / vol_pi;
+    }
+  }
+  // particle-wall: unique wall nodes within the contact radius of any node
+  int nw = d.wp_cnt[p];
+  if (nw > d.wp_cap) nw = d.wp_cap;
+  if (nw > kWallSort) nw = kWallSort;  // capacity is validated on the host
+  int sz = 1;
+  while (sz < nw) sz <<= 1;
+  for (int a = threadIdx.x; a < sz; a += blockDim.x)
+    wn[a] = a < nw ? d.wp[(int64_t)p * d.wp_cap + a] : INT32_MAX;
+  __syncthreads();
+  for (int k = 2; k <= sz; k <<= 1)
+    for (int jj = k >> 1; jj > 0; jj >>= 1) {
+      for (int a = threadIdx.x; a < sz; a += blockDim.x) {
+        const int b = a ^ jj;
+        if (b > a) {
+          const bool up = (a & k) == 0;
+          const int32_t va = wn[a], vb = wn[b];
+          if ((va > vb) == up) {
+            wn[a] = vb;
+            wn[b] = va;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  for (int a = threadIdx.x; a < nw; a += blockDim.x) {
+    const int32_t k = wn[a];
+    if (a > 0 && wn[a - 1] == k) continue;
+    const DevParticle &W = d.particles[d.ptid[k]];
+    const ContactPair cp = d.contact[P.zone * d.n_zones + W.zone];
+    const double meq = rhoi * vol_pi;
+    const double bn = cp.betan * sqrt(cp.kappa * cp.rc * meq);
+    double xk[3] = {0, 0, 0}, vk[3] = {0, 0, 0};
+    for (int t = 0; t < dim; t++) {
+      xk[t] = d.x[st * (int64_t)k + t] - xc[t];
+      vk[t] = d.v[st * (int64_t)k + t] - vc[t];
+    }
+    const double l = sqrt(xk[0] * xk[0] + xk[1] * xk[1] + xk[2] * xk[2]);
+    double hat[3] = {0.0, 0.0, 0.0};
+    if (is_greater(l, 0.))
+      for (int t = 0; t < 3; t++) hat[t] = xk[t] / l;
+    double vm = vk[0] * hat[0] + vk[1] * hat[1] + vk[2] * hat[2];
+    if (vm > 0.) vm = 0.;
+    for (int t = 0; t < 3; t++) acc[t] += bn * vm * hat[t] / vol_pi;
+  }
+  // block reduction (fixed order)
+  for (int t = 0; t < 3; t++) {
+    double v = acc[t];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[t][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int t = 0; t < 3; t++) {
+      double s = 0.0;
+      for (int w = 0; w < kDampBlock / 32; w++) s += red[t][w];
+      d.fdamp[4 * p + t] = s;
+    }
+    d.wp_cnt[p] = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Damping force to all nodes of each particle (demModel.cpp:1053-1064), then
+// DEMModel::computeExternalForces (:791-812): gravity, then force BCs
+// (ParticleFLoading::apply, particleFLoading.cpp:85-173).
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void k_external(DevData d) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_nodes || d.ctrl->error) return;
+  double f[3];
+  ldv<DIM>(d.f, i, f);
+  const int32_t p = d.ptid[i];
+  if (d.flags[i] & NODE_PARTICLE) {
+#pragma unroll
+    for (int q = 0; q < DIM; q++) f[q] += d.fdamp[4 * p + q];
+  }
+  if (d.gravity_on) {
+    const double rho = d.particles[p].density;
+#pragma unroll
+    for (int q = 0; q < DIM; q++) f[q] += rho * d.gravity[q];
+  }
+  stv<DIM>(d.f, i, f);
+}
+
+template <int DIM>
+__global__ void k_force_bc(DevData d) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.n_fbc_nodes || d.ctrl->error) return;
+  const int64_t i = d.fbc_node[t];
+  const double time = d.ctrl->time;
+  double f[3];
+  ldv<DIM>(d.f, i, f);
+  for (int e = d.fbc_row[t]; e < d.fbc_row[t + 1]; e++) {
+    const BcSetDev bc = d.fbc_sets[d.fbc_set[e]];
+    double fmax = d.fbc_val[e];
+    switch (bc.time_fn) {
+      case PDGPU_TIME_LINEAR: fmax *= time; break;
+      case PDGPU_TIME_LINEAR_STEP: {
+        // util::linearStepFunc (function.cpp:62-85)
+        const double x1 = bc.tp[1], x2 = bc.tp[2];
+        const double period = floor(time / (x1 + x2));
+        const double val =
+            is_less(time, period * (x1 + x2) + x1) ? time - period * x2 : (period + 1.) * x1;
+        fmax *= val;
+        break;
+      }
+      case PDGPU_TIME_LINEAR_SLOW_FAST:
+        if (is_greater(time, bc.tp[1])) fmax *= bc.tp[3] * time;
+        else fmax *= bc.tp[2] * time;
+        break;
+      case PDGPU_TIME_SIN: fmax *= sin(kPi * bc.tp[1] * time); break;
+      default: break;
+    }
+    fmax *= bc.tp[0];
+    for (int q = 0; q < DIM; q++)
+      if ((bc.dir_mask >> q) & 1) f[q] += fmax;
+  }
+  stv<DIM>(d.f, i, f);
+}
+
+// ---------------------------------------------------------------------------
+// Post-processing every test_interval steps: DEMModel::ppCompressiveTest
+// (demModel.cpp:2202-2250) or ppTwoParticleTest (:2096-2149).
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(1024) k_postprocess(DevData d) {
+  __shared__ double red[2][32];
+  CtrlState *c = d.ctrl;
+  if (c->error) return;
+  const int64_t n = c->n;
+  if (!(n % d.test_interval == 0 && n >= d.test_interval)) return;
+  const int st = DIM == 2 ? 2 : 4;
+  if (d.test == PDGPU_TEST_COMPRESSIVE) {
+    const DevParticle W = d.particles[d.test_wall];
+    const int dir = d.test_dir;
+    double s = 0.0;
+    for (int64_t i = W.start + threadIdx.x; i < W.end; i += blockDim.x)
+      s += d.f[st * i + dir] * d.vol[i];
+    double cr = 0.0;
+    for (int b = threadIdx.x; b < d.cr_blocks; b += blockDim.x) cr += d.cr_partial[b];
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      cr += __shfl_xor_sync(0xffffffffu, cr, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      red[0][threadIdx.x >> 5] = s;
+      red[1][threadIdx.x >> 5] = cr;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double rs = 0.0, rc = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+        rs += red[0][w];
+        rc += red[1][w];
+      }
+      const double delta = d.x[st * W.start + dir] - d.xref[st * W.start + dir];
+      c->reaction = rs;
+      c->contact_reaction = -rc;
+      c->penetration = delta;
+      const int64_t h = c->history_count;
+      if (h < d.history_cap) {
+        d.history[4 * h] = c->time;
+        d.history[4 * h + 1] = delta;
+        d.history[4 * h + 2] = rs;
+        d.history[4 * h + 3] = -rc;
+      }
+      c->history_count = h + 1;
+    }
+  } else if (d.test == PDGPU_TEST_TWO_PARTICLE && d.n_particles >= 2) {
+    const DevParticle P0 = d.particles[0], P1 = d.particles[1];
+    double m = -DBL_MAX;
+    for (int64_t i = P1.start + threadIdx.x; i < P1.end; i += blockDim.x) m = fmax(m, d.x[st * i + 1]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[0][threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double my = -DBL_MAX;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) my = fmax(my, red[0][w]);
+      double dx[3] = {0, 0, 0};
+      for (int q = 0; q < DIM; q++) dx[q] = d.x[st * P1.center + q] - d.x[st * P0.center + q];
+      const double r = P0.bound_r;
+      const ContactPair cp = d.contact[P0.zone * d.n_zones + P1.zone];
+      const double re = r + cp.rc;
+      double pen = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]) - re - r;
+      double car = 0.0;
+      if (is_less(pen, 0.)) car = sqrt(re * re - (re + pen) * (re + pen));
+      else if (is_greater(pen, 0.)) {
+        pen = 0.;
+        car = 0.;
+      }
+      c->pen_dist = pen;
+      c->contact_area_radius = car;
+      c->max_y = is_less(0.0, my) ? my : 0.0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Set-up kernels
+// ---------------------------------------------------------------------------
+
+// DEMModel::updatePeridynamicNeighborlist (demModel.cpp:1659-1694): same
+// particle, j != i, strict squared distance against horizon^2, computed in
+// nanoflann's order (query minus point, dims 0..2).
+template <int DIM, int LPN, bool FILL>
+__global__ void __launch_bounds__(kBlock) k_pd_cand(DevData d, Grid g, int64_t *row) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
+  const int lane = threadIdx.x % LPN;
+  if (i >= d.n_nodes) return;
+  const unsigned gm = group_mask<LPN>();
+  const unsigned lane_base = (threadIdx.x & 31u) / LPN * LPN;
+  double q[3];
+  ldv<DIM>(d.x, i, q);
+  const int32_t pi = d.ptid[i];
+  const double r = d.particles[pi].horizon;
+  const double r2 = r * r;
+  int c[3] = {cell_coord<DIM>(q[0], g, 0), cell_coord<DIM>(q[1], g, 1),
+              DIM == 3 ? cell_coord<DIM>(q[2], g, 2) : 0};
+  int64_t out = FILL ? row[i] : 0;
+  int64_t count = 0;
+  const int zlo = DIM == 3 ? max(c[2] - 1, 0) : 0;
+  const int zhi = DIM == 3 ? min(c[2] + 1, g.dims[2] - 1) : 0;
+  for (int cz = zlo; cz <= zhi; cz++)
+    for (int cy = max(c[1] - 1, 0); cy <= min(c[1] + 1, g.dims[1] - 1); cy++)
+      for (int cx = max(c[0] - 1, 0); cx <= min(c[0] + 1, g.dims[0] - 1); cx++) {
+        const int cell = cx + g.dims[0] * (cy + g.dims[1] * cz);
+        const int s = d.cell_start[cell], e = d.cell_start[cell + 1];
+        for (int base = s; base < e; base += LPN) {
+          const int a = base + lane;
+          bool hit = false;
+          int32_t j = -1;
+          if (a < e) {
+            j = d.cell_nodes[a];
+            if (j != i && d.ptid[j] == pi) {
+              double p[3];
+              ldv<DIM>(d.x, j, p);
+              double dd = 0.0;
+#pragma unroll
+              for (int t = 0; t < DIM; t++) {
+                const double df = q[t] - p[t];
+                dd += df * df;
+              }
+              hit = dd < r2;
+            }
+          }
+          const unsigned bal = (__ballot_sync(gm, hit) & gm) >> lane_base;
+          if (FILL) {
+            if (hit) d.pd_col[out + __popc(bal & ((1u << lane) - 1u))] = j;
+            out += __popc(bal);
+          } else {
+            count += __popc(bal);
+          }
+        }
+      }
+  if (!FILL && lane == 0) row[i + 1] = count;
+}
+
+// order each node's neighbour list by node index (one warp per node)
+__global__ void k_pd_sort_rows(DevData d, int32_t *tmp) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= d.n_nodes) return;
+  const int64_t s = d.pd_row[i], e = d.pd_row[i + 1];
+  for (int64_t a = s + lane; a < e; a += 32) tmp[a] = d.pd_col[a];
+  __syncwarp();
+  for (int64_t a = s + lane; a < e; a += 32) {
+    const int32_t va = tmp[a];
+    int64_t rank = 0;
+    for (int64_t b = s; b < e; b++) rank += tmp[b] < va;
+    d.pd_col[s + rank] = va;
+  }
+}
+
+// material::computeStateMxI (materialUtil.cpp:21-73)
+template <int DIM, int LPN>
+__global__ void k_mx(DevData d) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
+  const int lane = threadIdx.x % LPN;
+  if (i >= d.n_nodes) return;
+  const unsigned gm = group_mask<LPN>();
+  const DevParticle &P = d.particles[d.ptid[i]];
+  double xi[3];
+  ldv<DIM>(d.xref, i, xi);
+  double m = 0.0;
+  for (int64_t k = d.pd_row[i] + lane; k < d.pd_row[i + 1]; k += LPN) {
+    const int32_t j = d.pd_col[k];
+    double xj[3], dx[3];
+    ldv<DIM>(d.xref, j, xj);
+    for (int q = 0; q < 3; q++) dx[q] = xj[q] - xi[q];
+    const double rji = len3<DIM>(dx);
+    if (is_greater(rji, P.horizon)) continue;
+    double volj = d.vol[j];
+    if (is_greater(rji, P.check_low)) volj *= (P.check_up - rji) / P.h;
+    m += rji * rji * influence(d.inf, rji, P.horizon) * volj;
+  }
+  m = group_sum<LPN>(m, gm);
+  if (lane == 0) {
+    d.mx[i] = m;
+    if (is_less(m, 1.0e-18)) set_error(d.ctrl, DEV_ERR_NONFINITE, i);
+  }
+}
+
+inline unsigned blocks_for(int64_t n, int per_block) {
+  return (unsigned)((n + per_block - 1) / per_block);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+#define PDGPU_DIM_DISPATCH(d, KERNEL, ...)            \
+  do {                                               \
+    if ((d).dim == 2) KERNEL<2> __VA_ARGS__;         \
+    else KERNEL<3> __VA_ARGS__;                      \
+  } while (0)
+
+void launch_pack_vec(const DevData &d, const double *aos3, double *dst, cudaStream_t s) {
+  PDGPU_DIM_DISPATCH(d, k_pack, <<<blocks_for(d.n_nodes, kBlock), kBlock, 0, s>>>(aos3, dst, d.n_nodes));
+}
+void launch_unpack_vec(const DevData &d, const double *src, double *aos3, cudaStream_t s) {
+  PDGPU_DIM_DISPATCH(d, k_unpack, <<<blocks_for(d.n_nodes, kBlock), kBlock, 0, s>>>(src, aos3, d.n_nodes));
+}
+void launch_apply_ic(const DevData &d, cudaStream_t s) {
+  PDGPU_DIM_DISPATCH(d, k_apply_ic, <<<blocks_for(d.n_nodes, kBlock), kBlock, 0, s>>>(d));
+}
+void launch_integrate(const DevData &d, int verlet, cudaStream_t s) {
+  const unsigned g = blocks_for(d.n_nodes, kBlock);
+  if (d.dim == 2) {
+    if (verlet) k_integrate<2, true><<<g, kBlock, 0, s>>>(d);
+    else k_integrate<2, false><<<g, kBlock, 0, s>>>(d);
+  } else {
+    if (verlet) k_integrate<3, true><<<g, kBlock, 0, s>>>(d);
+    else k_integrate<3, false><<<g, kBlock, 0, s>>>(d);
+  }
+}
+void launch_verlet_second(const DevData &d, cudaStream_t s) {
+  PDGPU_DIM_DISPATCH(d, k_verlet_second, <<<blocks_for(d.n_nodes, kBlock), kBlock, 0, s>>>(d));
+}
+void launch_ctrl(const DevData &d, int mode, cudaStream_t s) { k_ctrl<<<1, 1, 0, s>>>(d, mode); }
+void launch_bc(const DevData &d, cudaStream_t s) {
+  if (!d.n_ubc_nodes) return;
+  PDGPU_DIM_DISPATCH(d, k_bc, <<<blocks_for(d.n_ubc_nodes, 128), 128, 0, s>>>(d));
+}
+
+template <int DIM>
+static void pd_prepass_dim(const DevData &d, int lanes, cudaStream_t s) {
+  const int64_t threads = d.n_nodes * lanes;
+  const unsigned g = blocks_for(threads, kBlock);
+  switch (lanes) {
+    case 4: k_pd_prepass<DIM, 4><<<g, kBlock, 0, s>>>(d); break;
+    case 8: k_pd_prepass<DIM, 8><<<g, kBlock, 0, s>>>(d); break;
+    case 16: k_pd_prepass<DIM, 16><<<g, kBlock, 0, s>>>(d); break;
+    default: k_pd_prepass<DIM, 32><<<g, kBlock, 0, s>>>(d); break;
+  }
+}
+void launch_pd_prepass(const DevData &d, cudaStream_t s) {
+  const int lanes = d.dim == 2 ? 8 : 32;
+  if (d.dim == 2) pd_prepass_dim<2>(d, lanes, s);
+  else pd_prepass_dim<3>(d, lanes, s);
+}
+
+template <int DIM>
+static void pd_force_dim(const DevData &d, int lanes, cudaStream_t s) {
+  const int64_t threads = d.n_nodes * lanes;
+  const unsigned g = blocks_for(threads, kBlock);
+  switch (lanes) {
+    case 4: k_pd_force<DIM, 4><<<g, kBlock, 0, s>>>(d); break;
+    case 8: k_pd_force<DIM, 8><<<g, kBlock, 0, s>>>(d); break;
+    case 16: k_pd_force<DIM, 16><<<g, kBlock, 0, s>>>(d); break;
+    default: k_pd_force<DIM, 32><<<g, kBlock, 0, s>>>(d); break;
+  }
+}
+void launch_pd_force(const DevData &d, int lanes, cudaStream_t s) {
+  if (d.dim == 2) pd_force_dim<2>(d, lanes, s);
+  else pd_force_dim<3>(d, lanes, s);
+}
+
+size_t scan_temp_bytes(int64_t n) {
+  size_t a = 0, b = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, a, (int32_t *)nullptr, (int32_t *)nullptr, (int)n);
+  cub::DeviceScan::InclusiveSum(nullptr, b, (int64_t *)nullptr, (int64_t *)nullptr, n);
+  return a > b ? a : b;
+}
+
+template <int DIM, int LPN>
+static void cand_dim(const DevData &d, uint8_t bit, cudaStream_t s, void *tmp, size_t bytes) {
+  const unsigned g = blocks_for(d.n_nodes * LPN, kBlock);
+  k_cand<DIM, LPN, false><<<g, kBlock, 0, s>>>(d, bit);
+  cub::DeviceScan::InclusiveSum(tmp, bytes, d.c_cnt, d.c_row + 1, d.n_nodes, s);
+  k_cand<DIM, LPN, true><<<g, kBlock, 0, s>>>(d, bit);
+}
+
+void launch_contact_update(const DevData &d, void *tmp, size_t bytes, int lanes, int init,
+                           cudaStream_t s) {
+  // the build of DEMModel::init searches with the flags it had before the
+  // two_particle override switched particle 0's force off
+  const uint8_t bit = init ? NODE_SEARCH0 : NODE_SEARCH;
+  const unsigned gn = blocks_for(d.n_nodes, kBlock);
+  k_zero_cells<<<blocks_for(d.grid.ncells + 1, kBlock), kBlock, 0, s>>>(d);
+  PDGPU_DIM_DISPATCH(d, k_cell_count, <<<gn, kBlock, 0, s>>>(d, d.x, d.grid));
+  cub::DeviceScan::ExclusiveSum(tmp, bytes, d.cell_cnt, d.cell_start, d.grid.ncells + 1, s);
+  k_cell_scatter<<<gn, kBlock, 0, s>>>(d);
+  k_cell_sort<<<blocks_for((int64_t)d.grid.ncells * 32, kBlock), kBlock, 0, s>>>(d);
+  if (d.dim == 2) {
+    if (lanes <= 8) cand_dim<2, 8>(d, bit, s, tmp, bytes);
+    else cand_dim<2, 32>(d, bit, s, tmp, bytes);
+  } else {
+    if (lanes <= 8) cand_dim<3, 8>(d, bit, s, tmp, bytes);
+    else cand_dim<3, 32>(d, bit, s, tmp, bytes);
+  }
+  k_cand_check<<<1, 1, 0, s>>>(d);
+}
+
+void launch_contact_force(const DevData &d, int lanes, cudaStream_t s) {
+  const unsigned g = blocks_for(d.n_nodes * lanes, kBlock);
+  if (d.dim == 2) {
+    if (lanes == 4) k_contact<2, 4><<<g, kBlock, 0, s>>>(d);
+    else if (lanes == 8) k_contact<2, 8><<<g, kBlock, 0, s>>>(d);
+    else k_contact<2, 32><<<g, kBlock, 0, s>>>(d);
+  } else {
+    if (lanes == 4) k_contact<3, 4><<<g, kBlock, 0, s>>>(d);
+    else if (lanes == 8) k_contact<3, 8><<<g, kBlock, 0, s>>>(d);
+    else k_contact<3, 32><<<g, kBlock, 0, s>>>(d);
+  }
+}
+
+void launch_damping(const DevData &d, cudaStream_t s) {
+  if (d.n_particles <= 0) return;
+  k_damping<<<d.n_particles, kDampBlock, 0, s>>>(d, d.dim);
+}
+
+void launch_external(const DevData &d, cudaStream_t s) {
+  PDGPU_DIM_DISPATCH(d, k_external, <<<blocks_for(d.n_nodes, kBlock), kBlock, 0, s>>>(d));
+  if (d.n_fbc_nodes)
+    PDGPU_DIM_DISPATCH(d, k_force_bc, <<<blocks_for(d.n_fbc_nodes, 128), 128, 0, s>>>(d));
+}
+
+void launch_postprocess(const DevData &d, cudaStream_t s) {
+  if (d.test == PDGPU_TEST_NONE) return;
+  PDGPU_DIM_DISPATCH(d, k_postprocess, <<<1, 1024, 0, s>>>(d));
+}
+
+void launch_build_pd(const DevData &d, double cell, int64_t *row, int32_t *tmp, void *scan_tmp,
+                     size_t scan_bytes, int pass, cudaStream_t s) {
+  // pass 0: grid + counts; pass 1: fill + sort rows.  d.grid holds the
+  // horizon-sized grid built by the caller; d.ctrl->update must be 1.
+  const int lanes = d.dim == 2 ? 8 : 32;
+  const unsigned g = blocks_for(d.n_nodes * lanes, kBlock);
+  (void)cell;
+  if (pass == 0) {
+    const unsigned gn = blocks_for(d.n_nodes, kBlock);
+    k_zero_cells<<<blocks_for(d.grid.ncells + 1, kBlock), kBlock, 0, s>>>(d);
+    PDGPU_DIM_DISPATCH(d, k_cell_count, <<<gn, kBlock, 0, s>>>(d, d.x, d.grid));
+    cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, d.cell_cnt, d.cell_start, d.grid.ncells + 1, s);
+    k_cell_scatter<<<gn, kBlock, 0, s>>>(d);
+    k_cell_sort<<<blocks_for((int64_t)d.grid.ncells * 32, kBlock), kBlock, 0, s>>>(d);
+    if (d.dim == 2) k_pd_cand<2, 8, false><<<g, kBlock, 0, s>>>(d, d.grid, row);
+    else k_pd_cand<3, 32, false><<<g, kBlock, 0, s>>>(d, d.grid, row);
+    cub::DeviceScan::InclusiveSum(scan_tmp, scan_bytes, row + 1, row + 1, d.n_nodes, s);
+  } else {
+    if (d.dim == 2) k_pd_cand<2, 8, true><<<g, kBlock, 0, s>>>(d, d.grid, row);
+    else k_pd_cand<3, 32, true><<<g, kBlock, 0, s>>>(d, d.grid, row);
+    k_pd_sort_rows<<<blocks_for(d.n_nodes * 32, kBlock), kBlock, 0, s>>>(d, tmp);
+  }
+}
+
+void launch_compute_mx(const DevData &d, cudaStream_t s) {
+  const int lanes = d.dim == 2 ? 8 : 32;
+  const unsigned g = blocks_for(d.n_nodes * lanes, kBlock);
+  if (d.dim == 2) k_mx<2, 8><<<g, kBlock, 0, s>>>(d);
+  else k_mx<3, 32><<<g, kBlock, 0, s>>>(d);
+}
+
+}  // namespace pdgpu

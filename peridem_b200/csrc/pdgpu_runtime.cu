@@ -1,0 +1,1218 @@
+// Host runtime of the pdgpu C ABI: context, uploads, the step sequence of
+// DEMModel::integrate / integrateStep / computeForces, CUDA-graph replay,
+// downloads and per-kernel timing.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "pdgpu_internal.h"
+
+using namespace pdgpu;
+
+namespace {
+
+constexpr int kMaxTimed = 64;
+constexpr int64_t kHistoryCap = 1 << 16;
+
+struct TimedLaunch {
+  int slot;
+  cudaEvent_t a, b;
+};
+
+}  // namespace
+
+struct pdgpu_ctx {
+  pdgpu_desc desc{};
+  cudaStream_t stream = nullptr;
+  DevData d{};
+  std::string err;
+
+  bool nodes = false, particles = false, bonds = false, mx = false, contact = false;
+  bool prepared = false, contact_init = false, begun = false;
+
+  // host copies used for set-up
+  std::vector<double> xref;      // N*3
+  std::vector<int32_t> ptid;     // N
+  std::vector<uint8_t> fix;      // N
+  std::vector<DevParticle> hp;   // particles
+  std::vector<double> vmag0;     // initial |v|
+  std::vector<uint8_t> ic_sel;   // per particle
+  std::vector<BcSetDev> ubc_sets, fbc_sets;
+  struct Entry {
+    int32_t node, set;
+    double val;
+    uint8_t once;
+  };
+  std::vector<Entry> ubc_e, fbc_e;
+
+  // scratch
+  double *stage = nullptr;  // N*3 AoS staging
+  void *scan_tmp = nullptr;
+  size_t scan_bytes = 0;
+  int pd_lanes = 0, contact_lanes = 8;
+  bool state_prepass = false;
+
+  // graph replay
+  cudaGraphExec_t gexec = nullptr;
+  int graph_steps = 0;
+
+  // timing
+  bool timing = false;
+  std::vector<TimedLaunch> pending;
+  std::vector<cudaEvent_t> pool;
+  const char *names[kMaxTimed] = {};
+  double ms[kMaxTimed] = {};
+  int64_t launches[kMaxTimed] = {};
+  int n_names = 0;
+
+  // allocations to free
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+int fail(pdgpu_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e__ = (call);                                                          \
+    if (e__ != cudaSuccess)                                                            \
+      return fail(ctx, PDGPU_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e__), \
+                  __FILE__, __LINE__);                                                 \
+  } while (0)
+
+template <class T>
+int dalloc(pdgpu_ctx *ctx, T **p, size_t count) {
+  void *q = nullptr;
+  size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess)
+    return fail(ctx, PDGPU_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+  ctx->allocs.push_back(q);
+  *p = (T *)q;
+  return PDGPU_OK;
+}
+
+template <class T>
+void dfree(pdgpu_ctx *ctx, T *&p) {
+  if (!p) return;
+  auto it = std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)p);
+  if (it != ctx->allocs.end()) ctx->allocs.erase(it);
+  cudaFree(p);
+  p = nullptr;
+}
+
+#define TRY(x)                \
+  do {                        \
+    int r__ = (x);            \
+    if (r__ != PDGPU_OK) return r__; \
+  } while (0)
+
+int stride(const pdgpu_ctx *ctx) { return ctx->desc.dim == 2 ? 2 : 4; }
+
+// ---- timing ----
+int timed_slot(pdgpu_ctx *c, const char *name) {
+  for (int i = 0; i < c->n_names; i++)
+    if (c->names[i] == name || std::strcmp(c->names[i], name) == 0) return i;
+  if (c->n_names >= kMaxTimed) return -1;
+  c->names[c->n_names] = name;
+  return c->n_names++;
+}
+
+cudaEvent_t take_event(pdgpu_ctx *c) {
+  if (!c->pool.empty()) {
+    cudaEvent_t e = c->pool.back();
+    c->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+template <class F>
+void run(pdgpu_ctx *c, const char *name, F &&f) {
+  if (!c->timing) {
+    f();
+    return;
+  }
+  const int slot = timed_slot(c, name);
+  cudaEvent_t a = take_event(c), b = take_event(c);
+  cudaEventRecord(a, c->stream);
+  f();
+  cudaEventRecord(b, c->stream);
+  c->pending.push_back({slot, a, b});
+}
+
+void resolve_timing(pdgpu_ctx *c) {
+  if (c->pending.empty()) return;
+  cudaStreamSynchronize(c->stream);
+  for (auto &t : c->pending) {
+    float m = 0.f;
+    cudaEventElapsedTime(&m, t.a, t.b);
+    if (t.slot >= 0) {
+      c->ms[t.slot] += m;
+      c->launches[t.slot] += 1;
+    }
+    c->pool.push_back(t.a);
+    c->pool.push_back(t.b);
+  }
+  c->pending.clear();
+}
+
+// ---- spatial factors of BC sets (particleULoading.cpp:146-172,
+//      particleFLoading.cpp:112-134), evaluated once on the host ----
+bool h_greater(double a, double b) {
+  return (a - b) > ((std::abs(a) < std::abs(b) ? std::abs(b) : std::abs(a)) * 1.0e-5);
+}
+bool h_less(double a, double b) {
+  return (b - a) > ((std::abs(a) < std::abs(b) ? std::abs(b) : std::abs(a)) * 1.0e-5);
+}
+// util::hatFunction (function.cpp:24-42)
+double hat(double x, double lo, double hi) {
+  if (h_greater(x, lo - 1.0E-12) && h_less(x, hi + 1.0E-12)) {
+    const double mid = 0.5 * (lo + hi);
+    const double l = mid - lo;
+    if (l < 1.0E-12) return 1.0;
+    if (h_less(x, mid)) return (x - lo) / l;
+    return (hi - x) / l;
+  }
+  return 0.0;
+}
+
+double spatial_u(const BcSetDev &bc, const double *x, const double *box) {
+  double umax = bc.tp[0];
+  const double kPi = 3.14159265358979323846;
+  switch (bc.spatial_fn) {
+    case PDGPU_SPACE_HAT_X: umax = bc.sp[0] * hat(x[0], box[0], box[3]); break;
+    case PDGPU_SPACE_HAT_Y: umax = bc.sp[0] * hat(x[1], box[1], box[4]); break;
+    case PDGPU_SPACE_SIN_X: umax = umax * std::sin(kPi * bc.sp[0] * x[0]); break;
+    case PDGPU_SPACE_SIN_Y: umax = umax * std::sin(kPi * bc.sp[0] * x[1]); break;
+    case PDGPU_SPACE_LINEAR_X: umax = umax * bc.sp[0] * x[0]; break;
+    case PDGPU_SPACE_LINEAR_Y: umax = umax * bc.sp[0] * x[1]; break;
+    default: break;
+  }
+  return umax;
+}
+
+double spatial_f(const BcSetDev &bc, const double *x, const double *box) {
+  double fmax = 1.0;
+  const double kPi = 3.14159265358979323846;
+  switch (bc.spatial_fn) {
+    case PDGPU_SPACE_HAT_X: fmax = bc.sp[0] * hat(x[0], box[0], box[3]); break;
+    case PDGPU_SPACE_HAT_Y: fmax = bc.sp[0] * hat(x[1], box[1], box[4]); break;
+    case PDGPU_SPACE_SIN_X: fmax = bc.sp[0] * std::sin(kPi * bc.sp[0] * x[0]); break;
+    case PDGPU_SPACE_SIN_Y: fmax = bc.sp[0] * std::sin(kPi * bc.sp[0] * x[1]); break;
+    case PDGPU_SPACE_LINEAR_X: fmax = bc.sp[0] * bc.sp[0] * x[0]; break;
+    case PDGPU_SPACE_LINEAR_Y: fmax = bc.sp[0] * bc.sp[0] * x[1]; break;
+    default: break;
+  }
+  return fmax;
+}
+
+int add_bc(pdgpu_ctx *ctx, bool disp, const pdgpu_bc_set *set, const uint8_t *psel,
+           const uint8_t *nsel, const double *pbox) {
+  if (!ctx || !set || !psel || !nsel || !pbox) return fail(ctx, PDGPU_ERR_ARG, "add_bc: null argument");
+  if (!ctx->nodes || !ctx->particles)
+    return fail(ctx, PDGPU_ERR_STATE, "add_bc: upload nodes and particles first");
+  if (ctx->prepared) return fail(ctx, PDGPU_ERR_STATE, "add_bc: boundary conditions are fixed once stepping starts");
+  BcSetDev b{};
+  b.time_fn = set->time_fn;
+  b.spatial_fn = set->spatial_fn;
+  b.dir_mask = set->dir_mask;
+  b.zero = set->zero;
+  for (int q = 0; q < 4; q++) b.tp[q] = set->time_params[q];
+  for (int q = 0; q < 2; q++) b.sp[q] = set->spatial_params[q];
+  auto &sets = disp ? ctx->ubc_sets : ctx->fbc_sets;
+  auto &ent = disp ? ctx->ubc_e : ctx->fbc_e;
+  const int sidx = (int)sets.size();
+  sets.push_back(b);
+  const int64_t np = (int64_t)ctx->hp.size();
+  for (int64_t p = 0; p < np; p++) {
+    if (!psel[p]) continue;
+    // zero-displacement sets act once, at the first apply() call, which the
+    // reference makes for particle 0 only (particleULoading.cpp:120-131)
+    if (disp && b.zero && p != 0) continue;
+    for (int64_t i = ctx->hp[p].start; i < ctx->hp[p].end; i++) {
+      if (!nsel[i]) continue;
+      const double *x = &ctx->xref[3 * i];
+      const double v = disp ? spatial_u(b, x, pbox + 6 * p) : spatial_f(b, x, pbox + 6 * p);
+      ent.push_back({(int32_t)i, sidx, v, (uint8_t)(disp && b.zero ? 1 : 0)});
+    }
+  }
+  return PDGPU_OK;
+}
+
+int upload_bc_tables(pdgpu_ctx *ctx, bool disp) {
+  auto &ent = disp ? ctx->ubc_e : ctx->fbc_e;
+  auto &sets = disp ? ctx->ubc_sets : ctx->fbc_sets;
+  std::stable_sort(ent.begin(), ent.end(), [](const pdgpu_ctx::Entry &a, const pdgpu_ctx::Entry &b) {
+    return a.node < b.node;
+  });
+  std::vector<int32_t> nodes, row{0}, set;
+  std::vector<double> val;
+  std::vector<uint8_t> once;
+  for (size_t k = 0; k < ent.size(); k++) {
+    if (k == 0 || ent[k].node != ent[k - 1].node) {
+      if (k) row.push_back((int32_t)k);
+      nodes.push_back(ent[k].node);
+    }
+    set.push_back(ent[k].set);
+    val.push_back(ent[k].val);
+    once.push_back(ent[k].once);
+  }
+  if (!ent.empty()) row.push_back((int32_t)ent.size());
+  DevData &d = ctx->d;
+  BcSetDev *dsets;
+  int32_t *dn, *dr, *ds;
+  double *dv;
+  TRY(dalloc(ctx, &dsets, sets.size()));
+  TRY(dalloc(ctx, &dn, nodes.size()));
+  TRY(dalloc(ctx, &dr, row.size()));
+  TRY(dalloc(ctx, &ds, set.size()));
+  TRY(dalloc(ctx, &dv, val.size()));
+  if (!sets.empty()) CK(cudaMemcpy(dsets, sets.data(), sets.size() * sizeof(BcSetDev), cudaMemcpyHostToDevice));
+  if (!nodes.empty()) {
+    CK(cudaMemcpy(dn, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dr, row.data(), row.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ds, set.data(), set.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dv, val.data(), val.size() * 8, cudaMemcpyHostToDevice));
+  }
+  if (disp) {
+    uint8_t *donce;
+    TRY(dalloc(ctx, &donce, once.size()));
+    if (!once.empty()) CK(cudaMemcpy(donce, once.data(), once.size(), cudaMemcpyHostToDevice));
+    d.n_ubc_sets = (int32_t)sets.size();
+    d.ubc_sets = dsets;
+    d.n_ubc_nodes = (int32_t)nodes.size();
+    d.ubc_node = dn;
+    d.ubc_row = dr;
+    d.ubc_set = ds;
+    d.ubc_val = dv;
+    d.ubc_once = donce;
+  } else {
+    d.n_fbc_sets = (int32_t)sets.size();
+    d.fbc_sets = dsets;
+    d.n_fbc_nodes = (int32_t)nodes.size();
+    d.fbc_node = dn;
+    d.fbc_row = dr;
+    d.fbc_set = ds;
+    d.fbc_val = dv;
+  }
+  return PDGPU_OK;
+}
+
+// Grid of cells at least `cell` wide over the current positions (with a
+// margin); positions outside are clamped to the border cells.
+int make_grid(pdgpu_ctx *ctx, double cell, Grid *g) {
+  const int dim = ctx->desc.dim;
+  std::vector<double> x(3 * ctx->d.n_nodes);
+  std::vector<double> tmp((size_t)stride(ctx) * ctx->d.n_nodes);
+  CK(cudaMemcpy(tmp.data(), ctx->d.x, tmp.size() * 8, cudaMemcpyDeviceToHost));
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int64_t i = 0; i < ctx->d.n_nodes; i++)
+    for (int q = 0; q < dim; q++) {
+      lo[q] = std::min(lo[q], tmp[stride(ctx) * i + q]);
+      hi[q] = std::max(hi[q], tmp[stride(ctx) * i + q]);
+    }
+  const int64_t limit = dim == 2 ? (int64_t)1 << 24 : (int64_t)1 << 26;
+  for (;;) {
+    int64_t total = 1;
+    for (int q = 0; q < 3; q++) {
+      if (q < dim) {
+        const double margin = 4.0 * cell + 0.05 * (hi[q] - lo[q]);
+        g->lo[q] = lo[q] - margin;
+        g->dims[q] = (int32_t)std::max<double>(1.0, std::floor((hi[q] - lo[q] + 2 * margin) / cell));
+      } else {
+        g->lo[q] = 0.0;
+        g->dims[q] = 1;
+      }
+      total *= g->dims[q];
+    }
+    if (total <= limit) {
+      g->ncells = (int32_t)total;
+      break;
+    }
+    cell *= 1.5;
+  }
+  // a cell is at least `cell` wide: floor() above can only widen it
+  g->inv_cell = 1.0 / cell;
+  for (int q = 0; q < dim; q++) {
+    const double ext = (double)g->dims[q] * cell;
+    (void)ext;
+  }
+  return PDGPU_OK;
+}
+
+int ensure_cells(pdgpu_ctx *ctx, const Grid &g) {
+  DevData &d = ctx->d;
+  if (d.cell_cnt && d.grid.ncells >= g.ncells) {
+    d.grid = g;
+    return PDGPU_OK;
+  }
+  dfree(ctx, d.cell_cnt);
+  dfree(ctx, d.cell_start);
+  dfree(ctx, d.cell_fill);
+  TRY(dalloc(ctx, &d.cell_cnt, (size_t)g.ncells + 1));
+  TRY(dalloc(ctx, &d.cell_start, (size_t)g.ncells + 1));
+  TRY(dalloc(ctx, &d.cell_fill, (size_t)g.ncells + 1));
+  CK(cudaMemset(d.cell_cnt, 0, ((size_t)g.ncells + 1) * 4));
+  CK(cudaMemset(d.cell_fill, 0, ((size_t)g.ncells + 1) * 4));
+  d.grid = g;
+  const size_t need = scan_temp_bytes(std::max<int64_t>(d.n_nodes, (int64_t)g.ncells + 1) + 1);
+  if (need > ctx->scan_bytes) {
+    if (ctx->scan_tmp) {
+      auto it = std::find(ctx->allocs.begin(), ctx->allocs.end(), ctx->scan_tmp);
+      if (it != ctx->allocs.end()) ctx->allocs.erase(it);
+      cudaFree(ctx->scan_tmp);
+      ctx->scan_tmp = nullptr;
+    }
+    char *t;
+    TRY(dalloc(ctx, &t, need));
+    ctx->scan_tmp = t;
+    ctx->scan_bytes = need;
+  }
+  return PDGPU_OK;
+}
+
+int read_ctrl(pdgpu_ctx *ctx, CtrlState *c) {
+  CK(cudaMemcpyAsync(c, ctx->d.ctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PDGPU_OK;
+}
+
+int device_error(pdgpu_ctx *ctx) {
+  CtrlState c;
+  TRY(read_ctrl(ctx, &c));
+  switch (c.error) {
+    case DEV_OK: return PDGPU_OK;
+    case DEV_ERR_CONTACT_OVERFLOW:
+      return fail(ctx, PDGPU_ERR_OVERFLOW,
+                  "contact candidate list needs %lld entries, capacity is %lld (step %lld); "
+                  "raise pdgpu_desc.contact_capacity",
+                  (long long)c.error_info, (long long)ctx->d.contact_cap, (long long)c.n);
+    case DEV_ERR_WALLPAIR_OVERFLOW:
+      return fail(ctx, PDGPU_ERR_OVERFLOW,
+                  "particle %lld has more particle-wall pairs than wall_pair_capacity=%d (step %lld)",
+                  (long long)c.error_info, ctx->d.wp_cap, (long long)c.n);
+    case DEV_ERR_NONFINITE:
+      return fail(ctx, PDGPU_ERR_NAN, "weighted volume of node %lld is too close to zero",
+                  (long long)c.error_info);
+    default:
+      return fail(ctx, PDGPU_ERR_STATE, "device error %d (info %lld)", c.error, (long long)c.error_info);
+  }
+}
+
+// FP32 constants per particle for the mixed-precision bond loop
+int prepare_mixed(pdgpu_ctx *ctx) {
+  DevData &d = ctx->d;
+  const int64_t N = d.n_nodes;
+  std::vector<MixParticle> mp(ctx->hp.size());
+  bool fits16 = true;
+  for (size_t k = 0; k < ctx->hp.size(); k++) {
+    const DevParticle &P = ctx->hp[k];
+    MixParticle &M = mp[k];
+    M = MixParticle{};
+    M.start = P.start;
+    M.material = P.material;
+    M.inv_horizon = (float)(1.0 / P.horizon);
+    M.check_low = (float)P.check_low;
+    M.check_up = (float)P.check_up;
+    M.inv_h = (float)(1.0 / P.h);
+    M.rc = (float)P.rc;
+    M.kn = (float)P.kn;
+    switch (P.material) {
+      case PDGPU_MAT_RNP:
+        M.k_force = (float)(4.0 * P.mat[0] * P.mat[1] / P.mat[3]);
+        M.beta = (float)P.mat[1];
+        M.rbar = (float)P.mat[2];
+        M.factor_sc = (float)P.mat[4];
+        M.irreversible = P.mat[5] != 0.0;
+        break;
+      case PDGPU_MAT_PMB:
+        M.k_force = (float)P.mat[0];
+        M.s0 = (float)P.mat[1];
+        break;
+      case PDGPU_MAT_PDELASTIC: M.k_force = (float)P.mat[0]; break;
+      default:
+        M.K = (float)P.mat[0];
+        M.G = (float)P.mat[1];
+        M.s0 = (float)P.mat[2];
+        break;
+    }
+    if (P.compute_force && P.end - P.start > 65536) fits16 = false;
+  }
+  TRY(dalloc(ctx, &d.mixp, mp.size()));
+  CK(cudaMemcpy(d.mixp, mp.data(), mp.size() * sizeof(MixParticle), cudaMemcpyHostToDevice));
+  TRY(dalloc(ctx, &d.xl, (size_t)(d.dim == 2 ? 2 : 4) * N));
+  TRY(dalloc(ctx, &d.volf, N));
+  d.use16 = fits16 ? 1 : 0;
+  if (fits16) TRY(dalloc(ctx, &d.pd_col16, d.n_bonds));
+  d.inf_p0 = (float)d.inf.p0;
+  d.inf_p1 = (float)d.inf.p1;
+  launch_mixed_setup(d, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PDGPU_OK;
+}
+
+// flags, BC tables, grid and contact buffers: done once before stepping
+int prepare(pdgpu_ctx *ctx) {
+  if (ctx->prepared) return PDGPU_OK;
+  if (!ctx->nodes || !ctx->particles)
+    return fail(ctx, PDGPU_ERR_STATE, "upload nodes and particles before stepping");
+  if (!ctx->bonds) return fail(ctx, PDGPU_ERR_STATE, "peridynamic neighbour lists missing");
+  if (!ctx->mx) return fail(ctx, PDGPU_ERR_STATE, "weighted volume m_x missing");
+  if (ctx->desc.multi_particle && !ctx->contact)
+    return fail(ctx, PDGPU_ERR_STATE, "contact parameters missing for a multi-particle run");
+  DevData &d = ctx->d;
+  const int64_t N = d.n_nodes;
+  // node flags
+  std::vector<uint8_t> flags(N, 0);
+  double svmax = 0.0;
+  int64_t nsearch = 0;
+  for (size_t p = 0; p < ctx->hp.size(); p++) {
+    const DevParticle &P = ctx->hp[p];
+    for (int64_t i = P.start; i < P.end; i++) {
+      uint8_t f = 0;
+      if (P.compute_force) f |= NODE_ACTIVE;
+      if (P.type == 1) f |= NODE_WALL;
+      else f |= NODE_PARTICLE;
+      if (P.type == 0 && P.compute_force && !P.all_fixed) f |= NODE_SEARCH;
+      // DEMModel::init searches before the two_particle override
+      if (P.type == 0 && !P.all_fixed) f |= NODE_SEARCH0;
+      if (f & NODE_SEARCH) nsearch++;
+      flags[i] = f;
+      if (!(f & NODE_ACTIVE)) svmax = std::max(svmax, ctx->vmag0[i]);
+    }
+  }
+  TRY(dalloc(ctx, &d.flags, N));
+  CK(cudaMemcpy(d.flags, flags.data(), N, cudaMemcpyHostToDevice));
+  // IC particle flags
+  TRY(dalloc(ctx, &d.ic_particle, ctx->hp.size()));
+  if (ctx->ic_sel.size() != ctx->hp.size()) ctx->ic_sel.assign(ctx->hp.size(), 0);
+  CK(cudaMemcpy(d.ic_particle, ctx->ic_sel.data(), ctx->hp.size(), cudaMemcpyHostToDevice));
+  TRY(upload_bc_tables(ctx, true));
+  TRY(upload_bc_tables(ctx, false));
+  // lanes per node: average bonds per node decides (autotuned later)
+  const double bpn = N ? (double)d.n_bonds / (double)N : 0.0;
+  if (ctx->pd_lanes <= 0) ctx->pd_lanes = bpn > 48 ? 32 : (bpn > 20 ? 8 : 4);
+  // contact buffers
+  const int64_t lanes_c = ctx->contact_lanes;
+  d.cr_blocks = (int32_t)((N * lanes_c + 255) / 256);
+  TRY(dalloc(ctx, &d.cr_partial, (size_t)d.cr_blocks + 1));
+  CK(cudaMemset(d.cr_partial, 0, ((size_t)d.cr_blocks + 1) * 8));
+  TRY(dalloc(ctx, &d.history, (size_t)kHistoryCap * 4));
+  d.history_cap = kHistoryCap;
+  TRY(dalloc(ctx, &d.fdamp, ctx->hp.size() * 4));
+  CK(cudaMemset(d.fdamp, 0, ctx->hp.size() * 4 * 8));
+  TRY(dalloc(ctx, &d.c_row, (size_t)N + 1));
+  CK(cudaMemset(d.c_row, 0, ((size_t)N + 1) * 8));
+  TRY(dalloc(ctx, &d.c_cnt, (size_t)N));
+  CK(cudaMemset(d.c_cnt, 0, (size_t)N * 8));
+  if (ctx->desc.multi_particle) {
+    d.contact_cap = ctx->desc.contact_capacity > 0 ? ctx->desc.contact_capacity
+                                                   : std::max<int64_t>(64 * nsearch, 1 << 20);
+    TRY(dalloc(ctx, &d.c_col, (size_t)d.contact_cap));
+    d.wp_cap = ctx->desc.wall_pair_capacity > 0 ? (int32_t)ctx->desc.wall_pair_capacity : 2048;
+    if (d.wp_cap > 4096) return fail(ctx, PDGPU_ERR_ARG, "wall_pair_capacity is limited to 4096");
+    TRY(dalloc(ctx, &d.wp, ctx->hp.size() * (size_t)d.wp_cap));
+    TRY(dalloc(ctx, &d.wp_cnt, ctx->hp.size()));
+    CK(cudaMemset(d.wp_cnt, 0, ctx->hp.size() * 4));
+    TRY(dalloc(ctx, &d.cell_of, N));
+    TRY(dalloc(ctx, &d.cell_tmp, N));
+    TRY(dalloc(ctx, &d.cell_nodes, N));
+    Grid g{};
+    const double cell = std::max(1.0, ctx->desc.search_factor) * ctx->desc.max_contact_r;
+    if (!(cell > 0)) return fail(ctx, PDGPU_ERR_ARG, "max_contact_r must be positive");
+    TRY(make_grid(ctx, cell, &g));
+    TRY(ensure_cells(ctx, g));
+  }
+  // step control
+  CtrlState c{};
+  c.interval = ctx->desc.search_interval;
+  c.radius = ctx->desc.search_factor * ctx->desc.max_contact_r;
+  c.static_vmax = svmax;
+  c.first_bc = 1;
+  CK(cudaMemcpy(d.ctrl, &c, sizeof c, cudaMemcpyHostToDevice));
+  // the state pre-pass runs when particle 0 is state-based (demModel.cpp:607-610)
+  ctx->state_prepass = !ctx->hp.empty() && ctx->hp[0].material == PDGPU_MAT_PDSTATE;
+  if (d.precision == PDGPU_PREC_MIXED) TRY(prepare_mixed(ctx));
+  ctx->prepared = true;
+  return PDGPU_OK;
+}
+
+// DEMModel::computeForces (demModel.cpp:462-600)
+void compute_forces(pdgpu_ctx *ctx) {
+  DevData &d = ctx->d;
+  cudaStream_t s = ctx->stream;
+  if (ctx->state_prepass) {
+    if (d.precision == PDGPU_PREC_MIXED)
+      run(ctx, "pd_prepass_mixed", [&] { launch_pd_prepass_mixed(d, ctx->pd_lanes, s); });
+    else
+      run(ctx, "pd_prepass", [&] { launch_pd_prepass(d, s); });
+  }
+  if (d.precision == PDGPU_PREC_MIXED)
+    run(ctx, "pd_force_mixed", [&] { launch_pd_force_mixed(d, ctx->pd_lanes, s); });
+  else
+    run(ctx, "pd_force", [&] { launch_pd_force(d, ctx->pd_lanes, s); });
+  if (ctx->desc.multi_particle) {
+    run(ctx, "contact_update", [&] {
+      launch_contact_update(d, ctx->scan_tmp, ctx->scan_bytes, ctx->contact_lanes, 0, s);
+    });
+    run(ctx, "contact_force", [&] { launch_contact_force(d, ctx->contact_lanes, s); });
+    run(ctx, "damping", [&] { launch_damping(d, s); });
+  }
+  run(ctx, "external", [&] { launch_external(d, s); });
+}
+
+// DEMModel::integrateStep (demModel.cpp:342-460) + post-processing
+void one_step(pdgpu_ctx *ctx) {
+  DevData &d = ctx->d;
+  cudaStream_t s = ctx->stream;
+  const bool verlet = ctx->desc.time_scheme == 1;
+  run(ctx, "integrate", [&] { launch_integrate(d, verlet ? 1 : 0, s); });
+  run(ctx, "ctrl", [&] { launch_ctrl(d, 0, s); });
+  run(ctx, "displacement_bc", [&] { launch_bc(d, s); });
+  compute_forces(ctx);
+  if (verlet) run(ctx, "integrate_second", [&] { launch_verlet_second(d, s); });
+  run(ctx, "postprocess", [&] { launch_postprocess(d, s); });
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int pdgpu_device_check(int device, char *msg, size_t len) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  auto say = [&](const char *t) {
+    if (msg && len) snprintf(msg, len, "%s", t);
+  };
+  if (e != cudaSuccess || n <= device) {
+    say("no CUDA device visible");
+    return PDGPU_ERR_NODEVICE;
+  }
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) {
+    say("cudaGetDeviceProperties failed");
+    return PDGPU_ERR_NODEVICE;
+  }
+  if (p.major != 10 || p.minor != 0) {
+    char b[128];
+    snprintf(b, sizeof b, "device %d is sm_%d%d; this library is built for sm_100a", device, p.major,
+             p.minor);
+    say(b);
+    return PDGPU_ERR_NODEVICE;
+  }
+  say(p.name);
+  return PDGPU_OK;
+}
+
+int pdgpu_create(const pdgpu_desc *desc, pdgpu_ctx **out) {
+  if (!desc || !out) return PDGPU_ERR_ARG;
+  *out = nullptr;
+  if (desc->dim != 2 && desc->dim != 3) return PDGPU_ERR_ARG;
+  if (!(desc->dt > 0)) return PDGPU_ERR_ARG;
+  if (desc->precision != PDGPU_PREC_FP64 && desc->precision != PDGPU_PREC_MIXED) return PDGPU_ERR_ARG;
+  int rc = pdgpu_device_check(desc->device, nullptr, 0);
+  if (rc != PDGPU_OK) return rc;
+  auto *ctx = new pdgpu_ctx();
+  ctx->desc = *desc;
+  if (cudaSetDevice(desc->device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return PDGPU_ERR_CUDA;
+  }
+  DevData &d = ctx->d;
+  d.dim = desc->dim;
+  d.precision = desc->precision;
+  d.dt = desc->dt;
+  for (int q = 0; q < 3; q++) d.gravity[q] = desc->gravity[q];
+  const double gl = std::sqrt(desc->gravity[0] * desc->gravity[0] + desc->gravity[1] * desc->gravity[1] +
+                              desc->gravity[2] * desc->gravity[2]);
+  d.gravity_on = gl > 1.0E-8;  // demModel.cpp:797
+  d.time_scheme = desc->time_scheme;
+  d.max_contact_r = desc->max_contact_r;
+  d.search_factor = desc->search_factor;
+  d.search_interval = desc->search_interval;
+  d.test = desc->test;
+  d.test_wall = desc->test_wall;
+  d.test_dir = desc->test_dir;
+  d.test_interval = desc->test_interval > 0 ? desc->test_interval : 1;
+  if (dalloc(ctx, &d.ctrl, 1) != PDGPU_OK) {
+    pdgpu_destroy(ctx);
+    return PDGPU_ERR_NOMEM;
+  }
+  cudaMemset(d.ctrl, 0, sizeof(CtrlState));
+  *out = ctx;
+  return PDGPU_OK;
+}
+
+void pdgpu_destroy(pdgpu_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->desc.device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  for (auto &t : ctx->pending) {
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  for (auto e : ctx->pool) cudaEventDestroy(e);
+  for (void *p : ctx->allocs) cudaFree(p);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int pdgpu_last_error(const pdgpu_ctx *ctx, char *buf, size_t len) {
+  if (!ctx || !buf || !len) return PDGPU_ERR_ARG;
+  snprintf(buf, len, "%s", ctx->err.c_str());
+  return PDGPU_OK;
+}
+
+int pdgpu_upload_nodes(pdgpu_ctx *ctx, int64_t n, const double *xref, const double *x,
+                       const double *u, const double *v, const double *vol, const uint8_t *fix,
+                       const uint64_t *pt_id) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  if (n <= 0 || n >= INT32_MAX || !xref || !vol || !fix || !pt_id)
+    return fail(ctx, PDGPU_ERR_ARG, "upload_nodes: bad arguments (n=%lld)", (long long)n);
+  if (ctx->nodes) return fail(ctx, PDGPU_ERR_STATE, "upload_nodes: nodes already uploaded");
+  CK(cudaSetDevice(ctx->desc.device));
+  DevData &d = ctx->d;
+  d.n_nodes = n;
+  const size_t sv = (size_t)stride(ctx) * n;
+  TRY(dalloc(ctx, &d.xref, sv));
+  TRY(dalloc(ctx, &d.x, sv));
+  TRY(dalloc(ctx, &d.u, sv));
+  TRY(dalloc(ctx, &d.v, sv));
+  TRY(dalloc(ctx, &d.f, sv));
+  TRY(dalloc(ctx, &d.vol, n));
+  TRY(dalloc(ctx, &d.mx, n));
+  TRY(dalloc(ctx, &d.theta, n));
+  TRY(dalloc(ctx, &d.vmag, n));
+  TRY(dalloc(ctx, &d.Z, n));
+  TRY(dalloc(ctx, &d.ptid, n));
+  TRY(dalloc(ctx, &d.fix, n));
+  TRY(dalloc(ctx, &ctx->stage, (size_t)3 * n));
+  CK(cudaMemset(d.f, 0, sv * 8));
+  CK(cudaMemset(d.mx, 0, n * 8));
+  CK(cudaMemset(d.theta, 0, n * 8));
+  CK(cudaMemset(d.Z, 0, n * 4));
+  CK(cudaMemset(d.xref, 0, sv * 8));
+  cudaStream_t s = ctx->stream;
+  auto put = [&](const double *src, double *dst) -> int {
+    CK(cudaMemcpyAsync(ctx->stage, src, (size_t)3 * n * 8, cudaMemcpyHostToDevice, s));
+    launch_pack_vec(d, ctx->stage, dst, s);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    return PDGPU_OK;
+  };
+  TRY(put(xref, d.xref));
+  TRY(put(x ? x : xref, d.x));
+  if (u) TRY(put(u, d.u));
+  else CK(cudaMemset(d.u, 0, sv * 8));
+  if (v) TRY(put(v, d.v));
+  else CK(cudaMemset(d.v, 0, sv * 8));
+  CK(cudaMemcpy(d.vol, vol, n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d.fix, fix, n, cudaMemcpyHostToDevice));
+  ctx->ptid.resize(n);
+  for (int64_t i = 0; i < n; i++) {
+    if (pt_id[i] > (uint64_t)INT32_MAX) return fail(ctx, PDGPU_ERR_ARG, "particle id out of range");
+    ctx->ptid[i] = (int32_t)pt_id[i];
+  }
+  CK(cudaMemcpy(d.ptid, ctx->ptid.data(), n * 4, cudaMemcpyHostToDevice));
+  ctx->xref.assign(xref, xref + 3 * n);
+  ctx->fix.assign(fix, fix + n);
+  ctx->vmag0.assign(n, 0.0);
+  if (v)
+    for (int64_t i = 0; i < n; i++)
+      ctx->vmag0[i] = std::sqrt(v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+  // |v| as held by ModelData::d_vMag at upload (zero after init)
+  CK(cudaMemcpy(d.vmag, ctx->vmag0.data(), n * 8, cudaMemcpyHostToDevice));
+  ctx->nodes = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_upload_particles(pdgpu_ctx *ctx, int64_t np, const pdgpu_particle *p) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  if (!ctx->nodes) return fail(ctx, PDGPU_ERR_STATE, "upload_particles: upload nodes first");
+  if (np <= 0 || !p) return fail(ctx, PDGPU_ERR_ARG, "upload_particles: bad arguments");
+  if (ctx->particles) return fail(ctx, PDGPU_ERR_STATE, "upload_particles: already uploaded");
+  ctx->hp.resize(np);
+  for (int64_t k = 0; k < np; k++) {
+    DevParticle &P = ctx->hp[k];
+    P = DevParticle{};
+    P.start = p[k].glob_start;
+    P.end = p[k].glob_end;
+    P.center = p[k].center_node;
+    if (P.start < 0 || P.end > ctx->d.n_nodes || P.start >= P.end || P.center < P.start || P.center >= P.end)
+      return fail(ctx, PDGPU_ERR_ARG, "particle %lld: bad node range", (long long)k);
+    P.type = p[k].type;
+    P.zone = p[k].zone;
+    P.compute_force = p[k].compute_force;
+    P.all_fixed = p[k].all_dofs_constrained;
+    P.material = p[k].material;
+    if (P.material < 0 || P.material > 3) return fail(ctx, PDGPU_ERR_ARG, "particle %lld: bad material", (long long)k);
+    P.horizon = p[k].horizon;
+    P.h = p[k].h;
+    P.density = p[k].density;
+    P.rc = p[k].rc;
+    P.kn = p[k].kn;
+    P.bound_r = p[k].bound_r;
+    // bounds of the volume correction (demModel.cpp:636-637, 708-709)
+    P.check_up = P.horizon + 0.5 * P.h;
+    P.check_low = P.horizon - 0.5 * P.h;
+    for (int q = 0; q < 6; q++) P.mat[q] = p[k].mat[q];
+    for (int64_t i = P.start; i < P.end; i++)
+      if (ctx->ptid[i] != (int32_t)k)
+        return fail(ctx, PDGPU_ERR_ARG, "node %lld: particle id %d does not match particle range %lld",
+                    (long long)i, ctx->ptid[i], (long long)k);
+  }
+  DevData &d = ctx->d;
+  d.n_particles = (int32_t)np;
+  TRY(dalloc(ctx, &d.particles, np));
+  CK(cudaMemcpy(d.particles, ctx->hp.data(), np * sizeof(DevParticle), cudaMemcpyHostToDevice));
+  ctx->particles = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_set_influence(pdgpu_ctx *ctx, int32_t type, const double params[2]) {
+  if (!ctx || !params || type < 0 || type > 2) return fail(ctx, PDGPU_ERR_ARG, "set_influence: bad arguments");
+  ctx->d.inf.type = type;
+  ctx->d.inf.p0 = params[0];
+  ctx->d.inf.p1 = params[1];
+  return PDGPU_OK;
+}
+
+int pdgpu_upload_contact(pdgpu_ctx *ctx, int32_t nz, const double *rc, const double *kn,
+                         const double *mu, const double *betan, const double *kappa) {
+  if (!ctx || nz <= 0 || !rc || !kn || !mu || !betan || !kappa)
+    return fail(ctx, PDGPU_ERR_ARG, "upload_contact: bad arguments");
+  std::vector<ContactPair> cp((size_t)nz * nz);
+  for (size_t k = 0; k < cp.size(); k++) cp[k] = {rc[k], kn[k], mu[k], betan[k], kappa[k]};
+  DevData &d = ctx->d;
+  if (!d.contact) TRY(dalloc(ctx, &d.contact, cp.size()));
+  CK(cudaMemcpy(d.contact, cp.data(), cp.size() * sizeof(ContactPair), cudaMemcpyHostToDevice));
+  d.n_zones = nz;
+  for (auto &P : ctx->hp)
+    if (P.zone < 0 || P.zone >= nz) return fail(ctx, PDGPU_ERR_ARG, "particle zone out of range");
+  ctx->contact = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_upload_pd_neighbors(pdgpu_ctx *ctx, const uint64_t *rowptr, const uint64_t *col,
+                              const uint8_t *bond_state) {
+  if (!ctx || !rowptr || !col) return fail(ctx, PDGPU_ERR_ARG, "upload_pd_neighbors: null argument");
+  if (!ctx->nodes) return fail(ctx, PDGPU_ERR_STATE, "upload nodes first");
+  if (ctx->bonds) return fail(ctx, PDGPU_ERR_STATE, "neighbour lists already set");
+  DevData &d = ctx->d;
+  const int64_t N = d.n_nodes;
+  const int64_t B = (int64_t)rowptr[N];
+  std::vector<int64_t> row(N + 1);
+  std::vector<int32_t> c32(B);
+  for (int64_t i = 0; i <= N; i++) {
+    row[i] = (int64_t)rowptr[i];
+    if (i && row[i] < row[i - 1]) return fail(ctx, PDGPU_ERR_ARG, "rowptr not monotone at %lld", (long long)i);
+  }
+  for (int64_t k = 0; k < B; k++) {
+    if (col[k] >= (uint64_t)N) return fail(ctx, PDGPU_ERR_ARG, "neighbour index out of range");
+    c32[k] = (int32_t)col[k];
+  }
+  std::vector<uint32_t> bits((B + 31) / 32 + 1, 0u);
+  if (bond_state)
+    for (int64_t k = 0; k < B; k++)
+      if (bond_state[k]) bits[k >> 5] |= 1u << (k & 31);
+  d.n_bonds = B;
+  TRY(dalloc(ctx, &d.pd_row, N + 1));
+  TRY(dalloc(ctx, &d.pd_col, B));
+  TRY(dalloc(ctx, &d.bond_bits, bits.size()));
+  CK(cudaMemcpy(d.pd_row, row.data(), (N + 1) * 8, cudaMemcpyHostToDevice));
+  if (B) CK(cudaMemcpy(d.pd_col, c32.data(), B * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d.bond_bits, bits.data(), bits.size() * 4, cudaMemcpyHostToDevice));
+  ctx->bonds = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_build_pd_neighbors(pdgpu_ctx *ctx) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  if (!ctx->nodes || !ctx->particles) return fail(ctx, PDGPU_ERR_STATE, "upload nodes and particles first");
+  if (ctx->bonds) return fail(ctx, PDGPU_ERR_STATE, "neighbour lists already set");
+  DevData &d = ctx->d;
+  const int64_t N = d.n_nodes;
+  double hmax = 0.0;
+  for (auto &P : ctx->hp) hmax = std::max(hmax, P.horizon);
+  if (!(hmax > 0)) return fail(ctx, PDGPU_ERR_ARG, "horizon must be positive");
+  Grid g{};
+  TRY(make_grid(ctx, hmax, &g));
+  if (!d.cell_of) TRY(dalloc(ctx, &d.cell_of, N));
+  if (!d.cell_tmp) TRY(dalloc(ctx, &d.cell_tmp, N));
+  if (!d.cell_nodes) TRY(dalloc(ctx, &d.cell_nodes, N));
+  TRY(ensure_cells(ctx, g));
+  TRY(dalloc(ctx, &d.pd_row, N + 1));
+  CK(cudaMemset(d.pd_row, 0, (N + 1) * 8));
+  // the cell kernels run only when ctrl.update is set
+  CtrlState c{};
+  c.update = 1;
+  CK(cudaMemcpy(d.ctrl, &c, sizeof c, cudaMemcpyHostToDevice));
+  launch_build_pd(d, hmax, d.pd_row, nullptr, ctx->scan_tmp, ctx->scan_bytes, 0, ctx->stream);
+  CK(cudaGetLastError());
+  int64_t B = 0;
+  CK(cudaMemcpyAsync(&B, d.pd_row + N, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  d.n_bonds = B;
+  TRY(dalloc(ctx, &d.pd_col, B));
+  int32_t *tmp;
+  TRY(dalloc(ctx, &tmp, B));
+  launch_build_pd(d, hmax, d.pd_row, tmp, ctx->scan_tmp, ctx->scan_bytes, 1, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, tmp);
+  TRY(dalloc(ctx, &d.bond_bits, (B + 31) / 32 + 1));
+  CK(cudaMemset(d.bond_bits, 0, ((B + 31) / 32 + 1) * 4));
+  CtrlState z{};
+  CK(cudaMemcpy(d.ctrl, &z, sizeof z, cudaMemcpyHostToDevice));
+  ctx->bonds = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_upload_mx(pdgpu_ctx *ctx, const double *mx) {
+  if (!ctx || !mx) return fail(ctx, PDGPU_ERR_ARG, "upload_mx: null argument");
+  if (!ctx->nodes) return fail(ctx, PDGPU_ERR_STATE, "upload nodes first");
+  CK(cudaMemcpy(ctx->d.mx, mx, ctx->d.n_nodes * 8, cudaMemcpyHostToDevice));
+  ctx->mx = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_compute_mx(pdgpu_ctx *ctx) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  if (!ctx->bonds || !ctx->particles) return fail(ctx, PDGPU_ERR_STATE, "neighbour lists and particles first");
+  CtrlState z{};
+  CK(cudaMemcpy(ctx->d.ctrl, &z, sizeof z, cudaMemcpyHostToDevice));
+  launch_compute_mx(ctx->d, ctx->stream);
+  CK(cudaGetLastError());
+  TRY(device_error(ctx));
+  ctx->mx = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_add_displacement_bc(pdgpu_ctx *ctx, const pdgpu_bc_set *set, const uint8_t *psel,
+                              const uint8_t *nsel, const double *pbox) {
+  return add_bc(ctx, true, set, psel, nsel, pbox);
+}
+
+int pdgpu_add_force_bc(pdgpu_ctx *ctx, const pdgpu_bc_set *set, const uint8_t *psel,
+                       const uint8_t *nsel, const double *pbox) {
+  return add_bc(ctx, false, set, psel, nsel, pbox);
+}
+
+int pdgpu_set_initial_condition(pdgpu_ctx *ctx, const double vel[3], const uint64_t *plist,
+                                int64_t n) {
+  if (!ctx || !vel || (n > 0 && !plist)) return fail(ctx, PDGPU_ERR_ARG, "set_initial_condition: bad arguments");
+  if (!ctx->particles) return fail(ctx, PDGPU_ERR_STATE, "upload particles first");
+  ctx->ic_sel.assign(ctx->hp.size(), 0);
+  for (int64_t k = 0; k < n; k++) {
+    if (plist[k] >= ctx->hp.size()) return fail(ctx, PDGPU_ERR_ARG, "IC particle out of range");
+    ctx->ic_sel[plist[k]] = 1;
+  }
+  ctx->d.ic_active = 1;
+  for (int q = 0; q < 3; q++) ctx->d.ic_v[q] = vel[q];
+  return PDGPU_OK;
+}
+
+int pdgpu_init_contact(pdgpu_ctx *ctx) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  TRY(prepare(ctx));
+  if (!ctx->desc.multi_particle) return PDGPU_OK;
+  if (ctx->contact_init) return fail(ctx, PDGPU_ERR_STATE, "contact lists already initialised");
+  launch_ctrl(ctx->d, 2, ctx->stream);
+  launch_contact_update(ctx->d, ctx->scan_tmp, ctx->scan_bytes, ctx->contact_lanes, 1, ctx->stream);
+  CK(cudaGetLastError());
+  TRY(device_error(ctx));
+  ctx->contact_init = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_integrate_begin(pdgpu_ctx *ctx) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  TRY(prepare(ctx));
+  if (ctx->desc.multi_particle && !ctx->contact_init) TRY(pdgpu_init_contact(ctx));
+  if (ctx->begun) return fail(ctx, PDGPU_ERR_STATE, "integrate_begin called twice");
+  DevData &d = ctx->d;
+  cudaStream_t s = ctx->stream;
+  if (d.ic_active) run(ctx, "initial_condition", [&] { launch_apply_ic(d, s); });
+  run(ctx, "displacement_bc", [&] { launch_bc(d, s); });
+  run(ctx, "ctrl", [&] { launch_ctrl(d, 1, s); });
+  compute_forces(ctx);
+  CK(cudaGetLastError());
+  TRY(device_error(ctx));
+  ctx->begun = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_step(pdgpu_ctx *ctx, int64_t nsteps) {
+  if (!ctx || nsteps < 0) return PDGPU_ERR_ARG;
+  if (!ctx->begun) return fail(ctx, PDGPU_ERR_STATE, "call pdgpu_integrate_begin first");
+  for (int64_t k = 0; k < nsteps; k++) one_step(ctx);
+  CK(cudaGetLastError());
+  return PDGPU_OK;
+}
+
+int pdgpu_step_graph(pdgpu_ctx *ctx, int64_t nsteps, int32_t graph_steps) {
+  if (!ctx || nsteps < 0 || graph_steps <= 0) return PDGPU_ERR_ARG;
+  if (!ctx->begun) return fail(ctx, PDGPU_ERR_STATE, "call pdgpu_integrate_begin first");
+  if (ctx->gexec && ctx->graph_steps != graph_steps) {
+    cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+  }
+  if (!ctx->gexec) {
+    const bool was_timing = ctx->timing;
+    ctx->timing = false;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < graph_steps; k++) one_step(ctx);
+    CK(cudaStreamEndCapture(ctx->stream, &g));
+    ctx->timing = was_timing;
+    CK(cudaGraphInstantiate(&ctx->gexec, g, 0));
+    cudaGraphDestroy(g);
+    ctx->graph_steps = graph_steps;
+  }
+  int64_t left = nsteps;
+  while (left >= graph_steps) {
+    CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
+    left -= graph_steps;
+  }
+  for (int64_t k = 0; k < left; k++) one_step(ctx);
+  CK(cudaGetLastError());
+  return PDGPU_OK;
+}
+
+int pdgpu_sync(pdgpu_ctx *ctx) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  resolve_timing(ctx);
+  return device_error(ctx);
+}
+
+int pdgpu_download(pdgpu_ctx *ctx, int32_t field, void *dst) {
+  if (!ctx || !dst) return PDGPU_ERR_ARG;
+  if (!ctx->nodes) return fail(ctx, PDGPU_ERR_STATE, "no nodes");
+  DevData &d = ctx->d;
+  const int64_t N = d.n_nodes;
+  cudaStream_t s = ctx->stream;
+  double *vec = nullptr;
+  switch (field) {
+    case PDGPU_FIELD_X: vec = d.x; break;
+    case PDGPU_FIELD_U: vec = d.u; break;
+    case PDGPU_FIELD_V: vec = d.v; break;
+    case PDGPU_FIELD_F: vec = d.f; break;
+    case PDGPU_FIELD_Z: CK(cudaMemcpyAsync(dst, d.Z, N * 4, cudaMemcpyDeviceToHost, s)); break;
+    case PDGPU_FIELD_VMAG: CK(cudaMemcpyAsync(dst, d.vmag, N * 8, cudaMemcpyDeviceToHost, s)); break;
+    case PDGPU_FIELD_THETA: CK(cudaMemcpyAsync(dst, d.theta, N * 8, cudaMemcpyDeviceToHost, s)); break;
+    case PDGPU_FIELD_MX: CK(cudaMemcpyAsync(dst, d.mx, N * 8, cudaMemcpyDeviceToHost, s)); break;
+    case PDGPU_FIELD_FIX: CK(cudaMemcpyAsync(dst, d.fix, N, cudaMemcpyDeviceToHost, s)); break;
+    case PDGPU_FIELD_BONDS: {
+      if (!ctx->bonds) return fail(ctx, PDGPU_ERR_STATE, "no bonds");
+      std::vector<uint32_t> bits((d.n_bonds + 31) / 32 + 1);
+      CK(cudaMemcpyAsync(bits.data(), d.bond_bits, bits.size() * 4, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      uint8_t *o = (uint8_t *)dst;
+      for (int64_t k = 0; k < d.n_bonds; k++) o[k] = (bits[k >> 5] >> (k & 31)) & 1u;
+      return PDGPU_OK;
+    }
+    default: return fail(ctx, PDGPU_ERR_ARG, "download: unknown field %d", field);
+  }
+  if (vec) {
+    launch_unpack_vec(d, vec, ctx->stage, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst, ctx->stage, (size_t)3 * N * 8, cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  return PDGPU_OK;
+}
+
+int pdgpu_upload_field(pdgpu_ctx *ctx, int32_t field, const void *src) {
+  if (!ctx || !src) return PDGPU_ERR_ARG;
+  DevData &d = ctx->d;
+  double *vec = field == PDGPU_FIELD_X ? d.x : field == PDGPU_FIELD_U ? d.u : field == PDGPU_FIELD_V ? d.v : nullptr;
+  if (!vec) return fail(ctx, PDGPU_ERR_ARG, "upload_field: only x, u, v can be written");
+  CK(cudaMemcpyAsync(ctx->stage, src, (size_t)3 * d.n_nodes * 8, cudaMemcpyHostToDevice, ctx->stream));
+  launch_pack_vec(d, ctx->stage, vec, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PDGPU_OK;
+}
+
+int pdgpu_get_scalars(pdgpu_ctx *ctx, pdgpu_scalars *out) {
+  if (!ctx || !out) return PDGPU_ERR_ARG;
+  CtrlState c;
+  TRY(read_ctrl(ctx, &c));
+  std::memset(out, 0, sizeof *out);
+  out->n = c.n;
+  out->time = c.time;
+  out->reaction = c.reaction;
+  out->contact_reaction = c.contact_reaction;
+  out->wall_penetration = c.penetration;
+  out->max_velocity = c.max_velocity;
+  out->contact_search_radius = c.radius;
+  out->contact_update_interval = c.interval;
+  out->contact_counter = c.counter;
+  out->contact_updates = c.updates;
+  out->contact_entries = c.entries;
+  out->pen_dist = c.pen_dist;
+  out->max_y = c.max_y;
+  out->contact_area_radius = c.contact_area_radius;
+  if (ctx->bonds && ctx->d.n_bonds) {
+    std::vector<uint32_t> bits((ctx->d.n_bonds + 31) / 32 + 1);
+    CK(cudaMemcpy(bits.data(), ctx->d.bond_bits, bits.size() * 4, cudaMemcpyDeviceToHost));
+    int64_t nb = 0;
+    for (auto w : bits) nb += __builtin_popcount(w);
+    out->broken_bonds = nb;
+  }
+  return c.error ? device_error(ctx) : PDGPU_OK;
+}
+
+int pdgpu_step_host(pdgpu_ctx *ctx, double *u, double *v, double *x, double *f, int64_t nsteps,
+                    pdgpu_scalars *out) {
+  if (!ctx || !u || !v || !x || !f) return PDGPU_ERR_ARG;
+  if (!ctx->begun) return fail(ctx, PDGPU_ERR_STATE, "call pdgpu_integrate_begin first");
+  DevData &d = ctx->d;
+  cudaStream_t s = ctx->stream;
+  const size_t bytes = (size_t)3 * d.n_nodes * 8;
+  double *vecs[3] = {d.u, d.v, d.x};
+  double *hosts[3] = {u, v, x};
+  for (int k = 0; k < 3; k++) {
+    CK(cudaMemcpyAsync(ctx->stage, hosts[k], bytes, cudaMemcpyHostToDevice, s));
+    launch_pack_vec(d, ctx->stage, vecs[k], s);
+  }
+  for (int64_t k = 0; k < nsteps; k++) one_step(ctx);
+  double *outs[4] = {d.u, d.v, d.x, d.f};
+  double *hout[4] = {u, v, x, f};
+  for (int k = 0; k < 4; k++) {
+    launch_unpack_vec(d, outs[k], ctx->stage, s);
+    CK(cudaMemcpyAsync(hout[k], ctx->stage, bytes, cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  if (out) return pdgpu_get_scalars(ctx, out);
+  return device_error(ctx);
+}
+
+int pdgpu_get_history(pdgpu_ctx *ctx, double *t, double *delta, double *force, double *cforce,
+                      int64_t cap, int64_t *count) {
+  if (!ctx || !count) return PDGPU_ERR_ARG;
+  CtrlState c;
+  TRY(read_ctrl(ctx, &c));
+  *count = c.history_count;
+  const int64_t n = std::min<int64_t>({cap, c.history_count, ctx->d.history_cap});
+  if (n <= 0 || !ctx->d.history) return PDGPU_OK;
+  std::vector<double> h(4 * n);
+  CK(cudaMemcpy(h.data(), ctx->d.history, h.size() * 8, cudaMemcpyDeviceToHost));
+  for (int64_t k = 0; k < n; k++) {
+    if (t) t[k] = h[4 * k];
+    if (delta) delta[k] = h[4 * k + 1];
+    if (force) force[k] = h[4 * k + 2];
+    if (cforce) cforce[k] = h[4 * k + 3];
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_download_contact(pdgpu_ctx *ctx, uint64_t *rowptr, uint64_t *col) {
+  if (!ctx || !rowptr) return PDGPU_ERR_ARG;
+  DevData &d = ctx->d;
+  if (!d.c_row) return fail(ctx, PDGPU_ERR_STATE, "no contact lists");
+  std::vector<int64_t> row(d.n_nodes + 1);
+  CK(cudaMemcpy(row.data(), d.c_row, row.size() * 8, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < row.size(); i++) rowptr[i] = (uint64_t)row[i];
+  const int64_t E = row.back();
+  if (col && E > 0) {
+    std::vector<int32_t> c(E);
+    CK(cudaMemcpy(c.data(), d.c_col, E * 4, cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < E; k++) col[k] = (uint64_t)c[k];
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_num_bonds(pdgpu_ctx *ctx, int64_t *n) {
+  if (!ctx || !n) return PDGPU_ERR_ARG;
+  *n = ctx->d.n_bonds;
+  return PDGPU_OK;
+}
+
+int pdgpu_download_pd_neighbors(pdgpu_ctx *ctx, uint64_t *rowptr, uint64_t *col) {
+  if (!ctx || !rowptr || !col) return PDGPU_ERR_ARG;
+  DevData &d = ctx->d;
+  if (!ctx->bonds) return fail(ctx, PDGPU_ERR_STATE, "no bonds");
+  std::vector<int64_t> row(d.n_nodes + 1);
+  std::vector<int32_t> c(d.n_bonds);
+  CK(cudaMemcpy(row.data(), d.pd_row, row.size() * 8, cudaMemcpyDeviceToHost));
+  if (d.n_bonds) CK(cudaMemcpy(c.data(), d.pd_col, c.size() * 4, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < row.size(); i++) rowptr[i] = (uint64_t)row[i];
+  for (size_t k = 0; k < c.size(); k++) col[k] = (uint64_t)c[k];
+  return PDGPU_OK;
+}
+
+int pdgpu_set_tuning(pdgpu_ctx *ctx, int32_t pd_lanes, int32_t contact_lanes) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  if (ctx->prepared && contact_lanes) return fail(ctx, PDGPU_ERR_STATE, "set_tuning: contact lanes are fixed once stepping starts");
+  if (pd_lanes && pd_lanes != 4 && pd_lanes != 8 && pd_lanes != 16 && pd_lanes != 32)
+    return fail(ctx, PDGPU_ERR_ARG, "set_tuning: pd_lanes must be 4, 8, 16 or 32");
+  if (contact_lanes && contact_lanes != 4 && contact_lanes != 8 && contact_lanes != 32)
+    return fail(ctx, PDGPU_ERR_ARG, "set_tuning: contact_lanes must be 4, 8 or 32");
+  if (pd_lanes) ctx->pd_lanes = pd_lanes;
+  if (contact_lanes) ctx->contact_lanes = contact_lanes;
+  if (ctx->gexec) {
+    cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_get_stream(pdgpu_ctx *ctx, void **stream) {
+  if (!ctx || !stream) return PDGPU_ERR_ARG;
+  *stream = (void *)ctx->stream;
+  return PDGPU_OK;
+}
+
+int pdgpu_enable_timing(pdgpu_ctx *ctx, int32_t on) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  resolve_timing(ctx);
+  ctx->timing = on != 0;
+  for (int i = 0; i < kMaxTimed; i++) {
+    ctx->ms[i] = 0.0;
+    ctx->launches[i] = 0;
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_kernel_times(pdgpu_ctx *ctx, int32_t maxk, const char **names, double *ms,
+                       int64_t *launches, int32_t *count) {
+  if (!ctx || !count) return PDGPU_ERR_ARG;
+  resolve_timing(ctx);
+  const int n = std::min(maxk, ctx->n_names);
+  for (int i = 0; i < n; i++) {
+    if (names) names[i] = ctx->names[i];
+    if (ms) ms[i] = ctx->ms[i];
+    if (launches) launches[i] = ctx->launches[i];
+  }
+  *count = n;
+  return PDGPU_OK;
+}
+
+}  // extern "C"

@@ -373,12 +373,30 @@ def _write_bc_sets(w, sets: List[BCSpec]) -> None:
 # ---------------------------------------------------------------------------
 
 
+def stable_dt(E: float, density: float, h: float, courant: float = 0.2) -> float:
+    """Explicit step for a bond-based PD body of Young's modulus E, mesh size
+    h, horizon 3h: dt = courant * h / sqrt(E / rho).  The linearised bond
+    stiffness of RNP/PMB on a square grid gives omega_max*dt ~ 2.5 * h/c-units,
+    so courant = 0.2 keeps omega_max*dt near 0.5 (the limit is 2)."""
+    return courant * h / math.sqrt(E / density)
+
+
+def stable_kn(density: float, node_volume: float, dt: float, omega_dt: float = 0.3) -> float:
+    """Contact stiffness Kn whose node-pair penalty spring has omega*dt =
+    omega_dt.  A pair inside the contact radius feels the force density
+    Kn*(R - Rc)*vol_j (demModel.cpp:895-899), so omega^2 = Kn*vol_j/rho; the
+    bulk-modulus choice 18K/(pi eps^5) of the reference's examples is
+    thousands of times stiffer than an explicit step of 5e-8..1e-7 s allows
+    for E = 2 GPa at these mesh sizes."""
+    return density * (omega_dt / dt) ** 2 / node_volume
+
+
 def _all_pairs(nz: int, c: ContactSpec) -> Dict[Tuple[int, int], ContactSpec]:
     return {(i, j): c for i in range(nz) for j in range(i, nz)}
 
 
 def two_particle(h_div: int = 10, radius: float = 1e-3, material: str = "RNPBond",
-                 nt: int = 20000, dt: float = 1e-7, v0: float = -0.1,
+                 nt: int = 20000, dt: Optional[float] = None, v0: float = -0.1,
                  gap: Optional[float] = None) -> SceneSpec:
     """Two discs of radius R, square-grid nodes h = R/h_div, horizon 3h; the
     top disc starts at v0 under gravity; the bottom disc's force is off
@@ -386,14 +404,13 @@ def two_particle(h_div: int = 10, radius: float = 1e-3, material: str = "RNPBond
     h = radius / h_div
     nodes, vol = disc_mesh(radius, h)
     mat = elastic_material(material, 2.0e9)
-    K = 2.0e9 / (3.0 * (1.0 - 2.0 * 0.25))
-    horizon = 3.0 * h
-    kn = 18.0 * K / (math.pi * horizon ** 5)
+    dt = stable_dt(2.0e9, 1200.0, h) if dt is None else dt
+    kn = stable_kn(1200.0, h * h, dt)
     gap = 0.5 * h if gap is None else gap
     sites = [((radius, radius, 0.0), radius, 0.0),
              ((radius, 3.0 * radius + 0.95 * h + gap, 0.0), radius, 0.0)]
     z = ZoneSpec("disc", False, "circle", [radius, 0.0, 0.0, 0.0], nodes, vol, mat, sites=sites)
-    c = ContactSpec(radius_factor=0.95, kn=kn, kn_factor=10.0, epsilon=0.7,
+    c = ContactSpec(radius_factor=0.95, kn=kn, kn_factor=1.0, epsilon=0.7,
                     friction_on=True, friction_coeff=0.5, damping_on=True, betan_factor=1.0)
     return SceneSpec(name=f"two_particle_h{h_div}", dim=2, dt=dt, nt=nt, zones=[z],
                      contact=_all_pairs(1, c),
@@ -406,13 +423,18 @@ def two_particle(h_div: int = 10, radius: float = 1e-3, material: str = "RNPBond
 def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3, 1.5e-3),
                    h_div: int = 15, width: float = 40e-3, seed: int = 0,
                    material: str = "RNPBond", wall_speed: float = -0.1,
-                   dt: float = 5e-8, nt: int = 50000, gravity: float = -10.0,
+                   dt: Optional[float] = None, nt: int = 50000, gravity: float = -10.0,
                    search_factor: float = 5.0, search_interval: int = 40,
-                   friction: bool = True) -> SceneSpec:
+                   friction: bool = True, gap: Optional[float] = None,
+                   jitter: float = 0.5) -> SceneSpec:
     """2-D compression: discs and hexagons (50/50) on a jittered triangular
     lattice inside a fixed frame, pressed by a top wall moving at
     ``wall_speed``.  One reference mesh per shape at h = R_ref/h_div, scaled
-    per particle, so every particle has the same node count."""
+    per particle, so every particle has the same node count.  ``gap`` is the
+    clearance between lattice neighbours of maximal radius and between the
+    packing and the walls (default 1.05 h_min, just beyond the contact
+    radius 0.95 h_min, so nothing starts in contact); the top wall starts
+    ``gap`` above the highest particle."""
     rng = np.random.default_rng(seed)
     r_ref = r_range[0]
     h_ref = r_ref / h_div
@@ -423,22 +445,36 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
     shapes = np.arange(n_particles) % 2          # 0 disc, 1 hexagon
     rng.shuffle(shapes)
     h_min = r_range[0] / h_div
-    spacing = 2.0 * r_range[1] + 2.0 * h_min
-    per_row = max(1, int(math.floor((width - 2.0 * h_min) / spacing)))
-    rows = int(math.ceil(n_particles / per_row))
+    gap = 1.05 * h_min if gap is None else gap
+    dt = stable_dt(2.0e9, 1200.0, h_min) if dt is None else dt
+    spacing = 2.0 * r_range[1] + gap
+    # triangular-lattice slots; odd rows shift by half a spacing and drop the
+    # slots that would leave the box, so no two lattice neighbours are closer
+    # than `spacing`
     dy = spacing * math.sqrt(3.0) / 2.0
     t_wall = 3.0 * h_min                          # wall thickness
-    x0 = 0.0
-    y0 = 0.0
-    height = rows * dy + spacing
+    slots = []
+    row = 0
+    while len(slots) < n_particles:
+        x = gap + 0.5 * spacing + (0.5 * spacing if row % 2 else 0.0)
+        cy = gap + r_range[1] + row * dy
+        while x + 0.5 * spacing <= width + 1e-12 and len(slots) < n_particles:
+            slots.append((x, cy))
+            x += spacing
+        row += 1
+        if row > 100000:
+            raise ValueError("box too narrow for one particle")
     sites_by_shape = {0: [], 1: []}
+    top = 0.0
     for p in range(n_particles):
-        row, col = divmod(p, per_row)
-        cx = x0 + h_min + 0.5 * spacing + col * spacing + (0.5 * spacing if row % 2 else 0.0)
-        cx = min(cx, width - h_min - 0.5 * spacing)
-        cy = y0 + h_min + 0.5 * spacing + row * dy
-        jx, jy = rng.uniform(-0.5, 0.5, size=2) * (spacing - 2.0 * radii[p] - 1.5 * h_min) * 0.5
-        sites_by_shape[int(shapes[p])].append(((cx + jx, cy + jy, 0.0), float(radii[p]), float(orients[p])))
+        cx, cy = slots[p]
+        room = max(0.0, spacing - 2.0 * radii[p] - gap)
+        jx, jy = rng.uniform(-0.5, 0.5, size=2) * room * jitter
+        jy = max(jy, -(cy - radii[p] - gap))
+        sites_by_shape[int(shapes[p])].append(((cx + jx, cy + jy, 0.0), float(radii[p]),
+                                               float(orients[p])))
+        top = max(top, cy + jy + radii[p])
+    height = top + gap
     mat = elastic_material(material, 2.0e9)
     zones = [
         ZoneSpec("disc", False, "circle", [r_ref, 0.0, 0.0, 0.0], disc_n, disc_v, mat,
@@ -447,13 +483,13 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
                  mat, sites=sites_by_shape[1]),
     ]
     # fixed frame (left, right, bottom) and moving top bar, walls meshed at h_min
-    lo = [x0 - t_wall - h_min, y0 - t_wall - h_min]
-    hi = [width + t_wall + h_min, y0 + height + 2.0 * t_wall]
+    lo = [-t_wall, -t_wall]
+    hi = [width + t_wall, height + 2.0 * t_wall]
     frame_n, frame_v = box_mesh([lo[0], lo[1]], [hi[0], hi[1]], h_min, 2,
-                                hole_lo=[x0 - 0.5 * h_min, y0 - 0.5 * h_min],
-                                hole_hi=[width + 0.5 * h_min, hi[1] + 1.0])
-    bar_lo = [x0 + 0.5 * h_min, y0 + height]
-    bar_hi = [width - 0.5 * h_min, y0 + height + t_wall]
+                                hole_lo=[0.5 * h_min, 0.5 * h_min],
+                                hole_hi=[width - 0.5 * h_min, hi[1] + 1.0])
+    bar_lo = [h_min, height]
+    bar_hi = [width - h_min, height + t_wall]
     bar_n, bar_v = box_mesh(bar_lo, bar_hi, h_min, 2)
     wall_mat = elastic_material(material, 2.0e9)
     zones.append(ZoneSpec("frame", True, "rectangle", [lo[0], lo[1], 0.0, hi[0], hi[1], 0.0],
@@ -461,12 +497,10 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
     zones.append(ZoneSpec("top_wall", True, "rectangle",
                           [bar_lo[0], bar_lo[1], 0.0, bar_hi[0], bar_hi[1], 0.0],
                           bar_n, bar_v, wall_mat, all_dofs_constrained=True))
-    K = 2.0e9 / (3.0 * (1.0 - 2.0 * 0.25))
-    kn = 18.0 * K / (math.pi * (3.0 * h_min) ** 5)
-    c = ContactSpec(radius_factor=0.95, kn=kn, kn_factor=10.0, epsilon=0.7,
+    kn = stable_kn(1200.0, h_min * h_min, dt)
+    c = ContactSpec(radius_factor=0.95, kn=kn, kn_factor=1.0, epsilon=0.7,
                     friction_on=friction, friction_coeff=0.5, damping_on=True, betan_factor=1.0)
-    n_part = n_particles
-    wall_fixed, wall_moving = n_part, n_part + 1
+    wall_fixed, wall_moving = n_particles, n_particles + 1
     ubc = [BCSpec(particles=[wall_fixed], directions=[1, 2], zero=True),
            BCSpec(particles=[wall_moving], directions=[2], time_fn="linear",
                   time_params=[wall_speed])]
@@ -482,7 +516,7 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
 def column_3d(n_spheres: int = 4096, median_r: float = 1e-3, sigma: float = 0.2,
               h_div: int = 10, box: Tuple[float, float, float] = (20e-3, 20e-3, 60e-3),
               seed: int = 0, material: str = "PDState", piston_speed: float = -0.05,
-              dt: float = 2e-8, nt: int = 5000) -> SceneSpec:
+              dt: Optional[float] = None, nt: int = 5000) -> SceneSpec:
     """3-D granular column: spheres with lognormal radii on a jittered cubic
     lattice inside a fixed box, a piston on top moving at ``piston_speed``."""
     rng = np.random.default_rng(seed)
@@ -492,6 +526,7 @@ def column_3d(n_spheres: int = 4096, median_r: float = 1e-3, sigma: float = 0.2,
     radii = np.clip(median_r * np.exp(sigma * rng.standard_normal(n_spheres)), 0.6 * median_r,
                     1.6 * median_r)
     h_min = float(radii.min()) / h_div
+    dt = stable_dt(5.0e9, 1200.0, h_min) if dt is None else dt
     spacing = 2.0 * float(radii.max()) + 2.0 * h_min
     nx = max(1, int(math.floor(box[0] / spacing)))
     ny = max(1, int(math.floor(box[1] / spacing)))
@@ -519,9 +554,8 @@ def column_3d(n_spheres: int = 4096, median_r: float = 1e-3, sigma: float = 0.2,
              ZoneSpec("piston", True, "cuboid",
                       [0.5 * h_min, 0.5 * h_min, height, W[0] - 0.5 * h_min, W[1] - 0.5 * h_min,
                        height + t], pis_n, pis_v, mat, all_dofs_constrained=True)]
-    K = 5.0e9 / (3.0 * (1.0 - 2.0 * 0.25))
-    kn = 18.0 * K / (math.pi * (3.0 * h_min) ** 5)
-    c = ContactSpec(radius_factor=0.95, kn=kn, kn_factor=10.0, epsilon=0.7, friction_on=True,
+    kn = stable_kn(1200.0, h_min ** 3, dt)
+    c = ContactSpec(radius_factor=0.95, kn=kn, kn_factor=1.0, epsilon=0.7, friction_on=True,
                     friction_coeff=0.5, damping_on=True, betan_factor=1.0)
     ubc = [BCSpec(particles=[n_spheres], directions=[1, 2, 3], zero=True),
            BCSpec(particles=[n_spheres + 1], directions=[3], time_fn="linear",
