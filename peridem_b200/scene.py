@@ -565,3 +565,382 @@ def column_3d(n_spheres: int = 4096, median_r: float = 1e-3, sigma: float = 0.2,
                      search_factor=5.0, search_interval=40, test_name="compressive_test",
                      compressive_wall=n_spheres + 1, compressive_dir=3, test_output_interval=10,
                      ubc=ubc, seed=seed)
+
+
+# ---------------------------------------------------------------------------
+# direct set-up (DEMModel::init restated)
+# ---------------------------------------------------------------------------
+
+
+def csv_float(text: str) -> float:
+    """The reference's CSV number parser (external/csv/csv.h:964-1024,
+    fast-cpp-csv-parser): digit accumulation and repeated multiplication, not
+    correctly rounded.  Meshes and particle locations pass through it, so the
+    direct set-up parses the same strings the same way."""
+    col = text.strip()
+    neg = False
+    p = 0
+    if col[p:p + 1] == "-":
+        neg = True
+        p += 1
+    elif col[p:p + 1] == "+":
+        p += 1
+    x = 0.0
+    while p < len(col) and col[p].isdigit():
+        x = x * 10
+        x = x + float(ord(col[p]) - 48)
+        p += 1
+    if p < len(col) and col[p] in ".,":
+        p += 1
+        pos = 1.0
+        while p < len(col) and col[p].isdigit():
+            pos = pos / 10
+            y = ord(col[p]) - 48
+            p += 1
+            x = x + y * pos
+    if p < len(col) and col[p] in "eE":
+        p += 1
+        e = int(col[p:])
+        if e != 0:
+            if e < 0:
+                base = 0.1
+                e = -e
+            else:
+                base = 10.0
+            while e != 1:
+                if (e & 1) == 0:
+                    base = base * base
+                    e >>= 1
+                else:
+                    x = x * base
+                    e -= 1
+            x = x * base
+    return -x if neg else x
+
+
+def _csvv(v: float) -> float:
+    return csv_float(_f(v))
+
+
+def _is_less(a: float, b: float) -> bool:
+    return (b - a) > (max(abs(a), abs(b)) * 1.0e-5)
+
+
+def _is_greater(a: float, b: float) -> bool:
+    return (a - b) > (max(abs(a), abs(b)) * 1.0e-5)
+
+
+def mesh_size(x: np.ndarray) -> float:
+    """util::computeMeshSize (src/util/geom.cpp:578-603): scan i, j in
+    order, keep the first distance that is isLess than the running guess."""
+    n = len(x)
+    if n < 2:
+        return 0.0
+    guess = float(np.sqrt(((x[0] - x[1]) ** 2).sum(axis=-1)))
+    for i in range(n):
+        d = x[i] - x
+        dist = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+        dist[i] = np.inf
+        start = 0
+        while True:
+            thr = dist[start:]
+            cand = (guess - thr) > (np.maximum(np.abs(thr), abs(guess)) * 1.0e-5)
+            if not cand.any():
+                break
+            k = int(np.argmax(cand)) + start
+            guess = float(dist[k])
+            start = k + 1
+    return guess
+
+
+def _moment(inf_type: int, params: np.ndarray, i: int) -> float:
+    """BaseInfluenceFn::getMoment (influenceFn.cpp:25-27, 59-61, 90-121)."""
+    if inf_type == 0:
+        return params[0] / float(i + 1)
+    if inf_type == 1:
+        return (params[0] / float(i + 1)) + (params[1] / float(i + 2))
+    a, b = params
+    sq1, sq2 = math.sqrt(b), math.sqrt(math.pi)
+    if i == 0:
+        return 0.5 * a * sq1 * sq2 * math.erf(1. / sq1)
+    if i == 1:
+        return 0.5 * a * b * (1. - math.exp(-1. / b))
+    if i == 2:
+        return 0.5 * a * b * sq1 * (0.5 * sq2 * math.erf(1. / sq1) - (1. / sq1) * math.exp(-1. / b))
+    return 0.5 * a * b * b * (1. - (1. + 1. / b) * math.exp(-1. / b))
+
+
+def influence_params(m: MaterialSpec, dim: int) -> Tuple[int, np.ndarray]:
+    """Default influence-function constants (influenceFn.cpp:14-84)."""
+    t = m.influence_type
+    if t == 0:
+        return 0, np.array([float(dim + 1), 0.0])
+    if t == 1:
+        a0 = {1: 6., 2: 12., 3: 20.}[dim]
+        return 1, np.array([a0, -a0])
+    b = 0.2
+    if dim == 1:
+        a = 2. / (b * (1. - math.exp(-1. / b)))
+    elif dim == 2:
+        a = (4.0 / b) * 1.0 / (math.sqrt(math.pi * b) * math.erf(1.0 / math.sqrt(b))
+                               - 2.0 * math.exp(-1.0 / b))
+    else:
+        a = (2.0 / b) * 1.0 / (b - (b + 1.) * math.exp(-1.0 / b))
+    return 2, np.array([a, b])
+
+
+def material_constants(m: MaterialSpec, dim: int, horizon: float, inf_type: int,
+                       inf: np.ndarray) -> Tuple[int, np.ndarray, float]:
+    """Bond-law constants and the bulk modulus that BaseParticle uses for the
+    internal contact stiffness (baseParticle.cpp:156-179): RnpMaterial
+    (material.h:541-620, 461-489), PmbMaterial (:919-997, 846-871),
+    PdElastic (:1257-1305, 1189-1210), PdState (:1579-1700, 1504-1530)."""
+    E, K, G, nu, Gc = m.E, m.K, m.G, m.nu, m.Gc
+    mat = np.zeros(6)
+    toK = lambda E_, nu_: E_ / (3. * (1. - 2. * nu_))
+    toLambdaE = lambda E_, nu_: E_ * nu_ / ((1. + nu_) * (1. - 2. * nu_))
+    toGE = lambda E_, nu_: E_ / (2. * (1. + nu_))
+    toELambda = lambda l_, nu_: l_ * (1. + nu_) * (1. - 2. * nu_) / nu_
+    code = MATERIAL_CODE[m.kind]
+    if code in (0, 1, 2):
+        nu = 0.25
+        if E > 0.:
+            K = toK(E, nu)
+        if K > 0. and E < 0.:
+            E = K * (3. * (1. - 2. * nu))
+        lam = toLambdaE(E, nu)
+        M = _moment(inf_type, inf, dim)
+        if code == 0:
+            if dim == 2:
+                C = math.pi * Gc / (4. * M)
+                beta = 4. * lam / (C * M)
+                inv = math.pow(horizon, 3) * math.pi
+            else:
+                C = 2. * Gc / (3. * M)
+                beta = 5. * lam / (C * M)
+                inv = math.pow(horizon, 4) * 4. * math.pi / 3.
+            mat[:] = [C, beta, math.sqrt(0.5 / beta), inv, m.check_sc_factor,
+                      1.0 if m.irreversible else 0.0]
+            lam2 = C * M * beta / 4. if dim == 2 else C * M * beta / 5.
+            Kp = toK(toELambda(lam2, 0.25), 0.25)
+        elif code == 1:
+            if dim == 2:
+                c = 24.0 * E / (math.pi * math.pow(horizon, 3.0) * (1. - nu))
+            else:
+                c = 24.0 * lam / (math.pi * math.pow(horizon, 3.0))
+            s0 = math.sqrt(5.0 * math.pi * Gc / (9.0 * E * horizon))
+            mat[:2] = [c, s0]
+            lam2 = c * (math.pi * math.pow(horizon, 3.0)) / 24.0
+            Kp = toK(toELambda(lam2, 0.25), 0.25)
+        else:
+            c = 24.0 * lam / (math.pi * math.pow(horizon, 3.0))
+            mat[0] = c
+            lam2 = c * (math.pi * math.pow(horizon, 3.0)) / 24.0
+            Kp = toK(toELambda(lam2, 0.25), 0.25)
+        return code, mat, Kp
+    # PD state: exactly two of E, K, G, nu
+    fE, fK, fG, fnu = E > 0, K > 0, G > 0, nu > 0
+    if not fnu:
+        if fE and fG:
+            nu = (0.5 * E / G) - 1.
+        if fE and fK:
+            nu = (3. * K - E) / (6. * K)
+        if fG and fK:
+            nu = (3. * K - 2. * G) / (2. * (3. * K + G))
+    if not fE:
+        if fK:
+            E = K * (3. * (1. - 2. * nu))
+        if fG:
+            E = 2. * G * (1. + nu)
+    if not fK:
+        K = toK(E, nu)
+    if not fG:
+        G = toGE(E, nu)
+    d = (3. * G + math.pow(3. / 4., 4) * (K - 5. * G / 3.)) * horizon
+    s0 = math.sqrt(Gc / d)
+    mat[:3] = [K, G, s0]
+    return 3, mat, K
+
+
+MATERIAL_CODE = {"RNPBond": 0, "PMBBond": 1, "PDElasticBond": 2, "PDState": 3}
+TIME_CODE = {"constant": 0, "linear": 1, "quadratic": 2, "sin": 3, "rotation": 4,
+             "linear_step": 5, "linear_slow_fast": 6}
+SPATIAL_CODE = {"constant": 0, "hat_x": 1, "hat_y": 2, "sin_x": 3, "sin_y": 4, "linear_x": 5,
+                "linear_y": 6}
+
+
+def _rotate_z(v: np.ndarray, theta: float) -> np.ndarray:
+    """util::rotate about (0,0,1) (transformation.cpp:67-79), in its
+    evaluation order: (1-ct)(p.n) n + ct p + st (n x p)."""
+    ct, st = math.cos(theta), math.sin(theta)
+    pdn = v[:, 0] * 0.0 + v[:, 1] * 0.0 + v[:, 2] * 1.0
+    a = (1. - ct) * pdn
+    nx = 0.0 * v[:, 2] - 1.0 * v[:, 1]
+    ny = 1.0 * v[:, 0] - 0.0 * v[:, 2]
+    nz = 0.0 * v[:, 1] - 0.0 * v[:, 0]
+    out = np.empty_like(v)
+    out[:, 0] = (a * 0.0 + ct * v[:, 0]) + st * nx
+    out[:, 1] = (a * 0.0 + ct * v[:, 1]) + st * ny
+    out[:, 2] = (a * 1.0 + ct * v[:, 2]) + st * nz
+    return out
+
+
+def _bounding_radius(geom_type: str, params: List[float]) -> float:
+    """GeomObject::boundingRadius: circle/sphere/hexagon radius, half the
+    rectangle diagonal, the full cuboid diagonal (geomObjects.h:855, 1693)."""
+    if geom_type in ("circle", "sphere", "hexagon"):
+        return params[0]
+    L = [params[3 + q] - params[q] for q in range(3)]
+    if geom_type == "cuboid":
+        return math.sqrt(math.pow(L[0], 2) + math.pow(L[1], 2) + math.pow(L[2], 2))
+    return 0.5 * math.sqrt(math.pow(L[0], 2) + math.pow(L[1], 2))
+
+
+def build_scene(spec: SceneSpec):
+    """The ModelData the reference's DEMModel::init would produce for
+    ``spec`` (same transforms, mesh sizes, constants and selections).  The
+    peridynamic neighbour lists and m_x are left to the device
+    (GpuDEMModel(build_neighbors=True, compute_mx=True)) or the oracle."""
+    from .model import Scene, BCSet
+    dim = spec.dim
+    xs, vols, pts = [], [], []
+    parts = []
+    zone_K = []
+    inf_type, inf = influence_params(spec.zones[0].material, dim)
+    # the first particle's material fixes the influence function
+    # (material.h:273-288); particles are created zone by zone
+    for z, zs in enumerate(spec.zones):
+        zone_K.append(zs.material.K)
+        node_txt = np.vectorize(lambda v: csv_float(_f(v)))
+        local = node_txt(zs.mesh_nodes) if len(zs.mesh_nodes) else zs.mesh_nodes
+        local[:, 2] = local[:, 2] if dim == 3 else 0.0
+        lvol = np.array([csv_float(_f(v)) for v in zs.mesh_vol])
+        # RefParticle centre node: closest to the geometry centre
+        # (refParticle.cpp:27-36)
+        gc = np.zeros(3) if not zs.is_wall else (
+            0.5 * (np.array(zs.geom_params[:3]) + np.array(zs.geom_params[3:6])))
+        best = _bounding_radius(zs.geom_type, zs.geom_params)
+        center = 0
+        dd = np.sqrt(((gc - local) ** 2).sum(axis=1))
+        for i in range(len(local)):
+            if _is_less(float(dd[i]), best):
+                best = float(dd[i])
+                center = i
+        if zs.is_wall:
+            sites = [(None, None, None)]
+        else:
+            sites = zs.sites
+        rep_r = zs.geom_params[0]
+        for (c, r, o) in sites:
+            if zs.is_wall:
+                xg = local.copy()
+                vg = lvol.copy()
+                bound = _bounding_radius(zs.geom_type, zs.geom_params)
+            else:
+                cc = np.array([csv_float(_f(c[0])), csv_float(_f(c[1])), csv_float(_f(c[2]))])
+                rr, oo = csv_float(_f(r)), csv_float(_f(o))
+                scale = rr / rep_r
+                rot = _rotate_z(local, oo)
+                xg = cc + scale * rot
+                vg = lvol * math.pow(scale, dim)
+                bound = rr
+            pid = len(parts)
+            start = sum(len(a) for a in xs)
+            xs.append(xg)
+            vols.append(vg)
+            pts.append(np.full(len(xg), pid, dtype=np.uint64))
+            h = mesh_size(xg)
+            horizon = zs.material.horizon_mesh_ratio * h
+            code, mat, Kp = material_constants(zs.material, dim, horizon, inf_type, inf)
+            parts.append(dict(start=start, end=start + len(xg), center=start + center,
+                              type=1 if zs.is_wall else 0, zone=z,
+                              all_fixed=1 if zs.all_dofs_constrained else 0,
+                              compute_force=0 if zs.all_dofs_constrained else 1,
+                              material=code, horizon=horizon, h=h,
+                              density=zs.material.density, rc=0.95 * h,
+                              kn=(18. / (math.pi * math.pow(horizon, 5))) * Kp,
+                              bound_r=bound, mat=mat))
+    if spec.test_name == "two_particle":
+        parts[0]["compute_force"] = 0  # demModel.cpp:218-220
+    xref = np.concatenate(xs)
+    vol = np.concatenate(vols)
+    ptid = np.concatenate(pts)
+    N, Np = len(xref), len(parts)
+    P = {k: np.array([p[k] for p in parts]) for k in parts[0] if k != "mat"}
+    pmat = np.stack([p["mat"] for p in parts])
+    # contact (DEMModel::setupContact, demModel.cpp:1531-1600)
+    nz = len(spec.zones)
+    hmin = hmax = None
+    for p in parts:
+        if hmin is None:
+            hmin = hmax = p["h"]
+        if _is_greater(hmin, p["h"]):
+            hmin = p["h"]
+        if _is_greater(p["h"], hmax):
+            hmax = p["h"]
+    crc = np.zeros((nz, nz)); ckn = np.zeros((nz, nz)); cmu = np.zeros((nz, nz))
+    cbn = np.zeros((nz, nz)); cka = np.zeros((nz, nz))
+    maxr = 0.0
+    for i in range(nz):
+        for j in range(nz):
+            c = spec.contact[(min(i, j), max(i, j))]
+            crc[i, j] = c.radius_factor * hmin
+            maxr = max(maxr, crc[i, j])
+            cka[i, j] = 2. * zone_K[i] * zone_K[j] / (zone_K[i] + zone_K[j])
+            ckn[i, j] = c.kn * c.kn_factor
+            bf = c.betan_factor if c.damping_on else 0.0
+            le = math.log(c.epsilon)
+            cbn[i, j] = bf * (-2. * le * math.sqrt(1. / (math.pi * math.pi + le * le)))
+            cmu[i, j] = c.friction_coeff if c.friction_on else 0.0
+    # boundary conditions: particle-list selections (particleULoading.cpp:38-88)
+    fix = np.zeros(N, dtype=np.uint8)
+
+    def mk(bcs, disp):
+        out = []
+        for b in bcs:
+            psel = np.zeros(Np, dtype=np.uint8)
+            psel[b.particles] = 1
+            nsel = np.zeros(N, dtype=np.uint8)
+            for p in b.particles:
+                nsel[parts[p]["start"]:parts[p]["end"]] = 1
+            mask = 0
+            for d in b.directions:
+                mask |= 1 << (d - 1)
+            if disp:
+                for p in b.particles:
+                    fix[parts[p]["start"]:parts[p]["end"]] |= np.uint8(mask)
+            tp = np.zeros(4)
+            if not b.zero:
+                tp[:len(b.time_params)] = b.time_params
+            sp = np.zeros(2)
+            sp[:len(b.spatial_params)] = b.spatial_params
+            box = np.zeros((Np, 6))
+            tcode = TIME_CODE.get(b.time_fn, 99) if not b.zero else 99
+            out.append(BCSet(time_fn=tcode, spatial_fn=SPATIAL_CODE.get(b.spatial_fn, 0),
+                             dir_mask=mask, zero=b.zero, time_params=tp, spatial_params=sp,
+                             particle_sel=psel, node_sel=nsel, particle_box=box))
+        return out
+
+    ubc = mk(spec.ubc, True)
+    fbc = mk(spec.fbc, False)
+    T = float(_f(spec.dt * spec.nt))
+    dt = T / spec.nt   # input.cpp:281
+    test = {"two_particle": 1, "compressive_test": 2}.get(spec.test_name, 0)
+    return Scene(
+        dim=dim, dt=dt, nt=spec.nt, xref=xref, vol=vol, fix=fix, ptid=ptid,
+        p_start=P["start"], p_end=P["end"], p_center=P["center"], p_type=P["type"],
+        p_zone=P["zone"], p_compute_force=P["compute_force"], p_all_fixed=P["all_fixed"],
+        p_material=P["material"], p_horizon=P["horizon"], p_h=P["h"], p_density=P["density"],
+        p_rc=P["rc"], p_kn=P["kn"], p_bound_r=P["bound_r"], p_mat=pmat,
+        inf_type=inf_type, inf_params=inf, gravity=np.array(spec.gravity, dtype=float),
+        time_scheme=1 if spec.time_scheme == "velocity_verlet" else 0,
+        multi_particle=True, n_zones=nz, c_rc=crc.ravel(), c_kn=ckn.ravel(),
+        c_mu=cmu.ravel(), c_betan=cbn.ravel(), c_kappa=cka.ravel(), max_contact_r=maxr,
+        search_factor=spec.search_factor, search_interval=spec.search_interval,
+        test=test, test_wall=spec.compressive_wall if test == 2 else 0,
+        test_dir=spec.compressive_dir - 1 if test == 2 else 0,
+        test_interval=spec.test_output_interval,
+        x=xref.copy(), u=np.zeros_like(xref), v=np.zeros_like(xref),
+        ubc=ubc, fbc=fbc,
+        ic_velocity=np.array(spec.ic_velocity) if spec.ic_velocity is not None else None,
+        ic_particles=np.array(spec.ic_particles, dtype=np.uint64), name=spec.name)
