@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark: node-steps/s of the PeriDEM explicit step on B200.
+
+Workload (default): the 2-D compressive test — 502 discs and hexagons
+(50/50), radius U[1, 1.5] mm, random orientation, h = R/15 scaled per
+particle, horizon 3h, RNPBond (E = 2 GPa, nu = 0.25, rho = 1200, Gc = 500),
+fixed frame plus a top wall pressing at 0.1 m/s, seeded synthetic packing.
+
+A step is one DEMModel::integrateStep over the whole scene (integrate,
+displacement BC, peridynamic bond loop, contact-list control and rebuilds,
+contact forces, particle damping, external forces, post-processing).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
+                  [--impl ours|reference]
+
+Timing: W untimed steps, then K steps each timed with CUDA events on the
+model's stream, with a 512 MiB buffer written between steps to flush the
+126 MB L2; max over ranks.  N > 1 runs N independent replicas (one scene per
+GPU, no collective), so scaling is weak.
+"""
+import argparse
+import glob
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "node-steps/s on 1 B200: mixed+surrogate vs plain FP64 at ≤1e-3 wall-force err"
+UNIT = "node-steps/s"
+
+
+def workload_spec(args):
+    from peridem_b200 import scene as scn
+    return scn.compressive_2d(n_particles=args.particles, r_range=(1e-3, 1.5e-3), h_div=15,
+                              width=40e-3, seed=args.seed, material="RNPBond", wall_speed=-0.1,
+                              nt=50000)
+
+
+def workload_config(args, sc):
+    return {"workload": "2-D compressive test, %d discs/hexagons R~U[1,1.5] mm, h=R/15, "
+                        "horizon 3h, RNPBond, top wall 0.1 m/s" % args.particles,
+            "nodes": int(sc.n_nodes) if sc is not None else None,
+            "particles": args.particles, "dt": sc.dt if sc is not None else None,
+            "precision": args.precision, "l2": "flushed between timed steps (512 MiB write)",
+            "graph": args.graph_steps > 0}
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device),
+                                          "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel):
+    """dram bytes per launch recorded by an ncu capture summary in profiles/."""
+    for p in glob.glob(os.path.join(ROOT, "profiles", "*.md")):
+        with open(p) as fh:
+            for line in fh:
+                if line.startswith(f"traffic_bytes_per_launch[{kernel}]:"):
+                    try:
+                        return float(line.split(":", 1)[1].split()[0])
+                    except ValueError:
+                        pass
+    return None
+
+
+def algorithmic_bytes(kernel, sc, precision):
+    """Bytes one launch must move at minimum (per bond: neighbour index and
+    broken bit; per active node: its own coordinates, displacement, volume,
+    row offset, force and damage; neighbour data are re-read from cache)."""
+    import numpy as np
+    dim = sc.dim
+    active = np.zeros(sc.n_nodes, dtype=bool)
+    for p in range(sc.n_particles):
+        if sc.p_compute_force[p]:
+            active[sc.p_start[p]:sc.p_end[p]] = True
+    rp = np.asarray(sc.pd_rowptr, dtype=np.int64)
+    bonds = int((rp[1:] - rp[:-1])[active].sum())
+    nodes = int(active.sum())
+    if kernel == "pd_force":
+        per_bond, per_node = 4 + 1 / 8, 8 * dim * 3 + 8 + 8 + 4
+    elif kernel == "pd_force_mixed":
+        per_bond, per_node = 2 + 1 / 8, 4 * dim + 8 * dim + 4 + 8 + 8 * dim + 4
+    else:
+        return None, None
+    return bonds * per_bond + nodes * per_node, {"bonds": bonds, "nodes": nodes,
+                                                  "bytes_per_bond": per_bond,
+                                                  "bytes_per_node": per_node}
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    from peridem_b200 import scene as scn
+    from peridem_b200.model import GpuDEMModel, PREC_FP64, PREC_MIXED
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    spec = workload_spec(args)
+    sc = scn.build_scene(spec)
+    prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
+    model = GpuDEMModel(sc, precision=prec, device=dev, build_neighbors=True, compute_mx=True)
+    rp, col = model.pd_neighbors()
+    sc.pd_rowptr, sc.pd_col = rp, col
+    model.integrate_begin()
+    stream = torch.cuda.ExternalStream(model.stream_handle(), device=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        if args.graph_steps:
+            model.integrate_step(1, graph_steps=1)
+        else:
+            model.integrate_step(1)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        model.sync()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        with ClockSampler(dev) as clk:
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                ev[k][0].record(stream)
+                step()
+                ev[k][1].record(stream)
+            model.sync()
+            torch.cuda.synchronize()
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    nodes = sc.n_nodes
+    value = nodes * args.steps * world / (total_ms * 1e-3)
+
+    # per-kernel device times over a second timed pass (same flush)
+    model.enable_timing(True)
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            model.integrate_step(1)
+        model.sync()
+    ktimes = model.kernel_times()
+    model.enable_timing(False)
+    sc_vals = model.scalars()
+
+    # end to end through the host-buffer call: H2D of u, v, x and D2H of
+    # u, v, x, f every step (pinned buffers)
+    N = sc.n_nodes
+    bufs = [torch.empty((N, 3), dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
+    u_h, v_h, x_h, f_h = bufs
+    u_h[:] = model.field("u")
+    v_h[:] = model.field("v")
+    x_h[:] = model.field("x")
+    for _ in range(3):
+        model.step_host(u_h, v_h, x_h, f_h, 1)
+    e2e_steps = max(10, min(args.steps, 200))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        model.step_host(u_h, v_h, x_h, f_h, 1)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": nodes * e2e_steps * world / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": 3 * N * 3 * 8, "d2h_bytes_per_step": 4 * N * 3 * 8,
+           "call": "pdgpu_step_host (host u,v,x in; u,v,x,f out; 1 step per call)"}
+
+    # roofline of the dominant kernel
+    dom = max(ktimes.items(), key=lambda kv: kv[1][0]) if ktimes else None
+    roof = None
+    gpu_launches = model.step_kernel_count() * args.steps
+    if dom:
+        name, (ms, launches) = dom
+        bytes_, units = algorithmic_bytes(name, sc, args.precision)
+        peak, kind = measured_peak()
+        avg_s = ms / launches * 1e-3
+        if bytes_:
+            ach = bytes_ / avg_s / 1e9
+            roof = {"kernel": name, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(ach / peak, 4), "peak_source": kind,
+                    "traffic": traffic_from_profiles(name), "avg_launch_us": round(avg_s * 1e6, 2),
+                    "algorithmic_bytes_per_launch": int(bytes_), "units": units}
+        else:
+            roof = {"kernel": name, "bound": "hbm", "achieved": None, "peak": peak,
+                    "unit": "GB/s", "frac": None, "avg_launch_us": round(avg_s * 1e6, 2)}
+    kt = {k: {"ms_total": round(v[0], 4), "launches": v[1], "us_avg": round(1e3 * v[0] / max(v[1], 1), 2)}
+          for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1][0])}
+    model.close()
+    return {"value": value, "ms_per_step": total_ms / args.steps, "e2e": e2e, "roofline": roof,
+            "kernels": kt, "clocks": clk.summary(), "gpu_launches": gpu_launches,
+            "scalars": {k: sc_vals[k] for k in ("n", "contact_updates", "contact_entries",
+                                                 "contact_update_interval", "broken_bonds",
+                                                 "reaction", "contact_reaction")},
+            "sc": sc}
+
+
+def cpu_reference(args, steps, warmup):
+    """The reference's own CPU step (oracle/_ref/peridem_ref, Taskflow on all
+    host threads) on the same workload deck; returns the parsed JSON line."""
+    from peridem_b200 import scene as scn
+    ref = os.path.join(ROOT, "oracle", "_ref", "peridem_ref")
+    if not os.path.exists(ref):
+        return None
+    spec = workload_spec(args)
+    d = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "_work",
+                     "bench_deck")
+    scn.write_deck(spec, d)
+    threads = os.cpu_count() or 1
+    r = subprocess.run([ref, "-i", "deck.yaml", "-nThreads", str(threads), "-time", str(steps)],
+                       cwd=d, capture_output=True, text=True, timeout=1800)
+    for line in r.stdout.splitlines()[::-1]:
+        if line.startswith("{"):
+            out = json.loads(line)
+            out["threads"] = threads
+            return out
+    raise RuntimeError("reference timing failed: " + r.stdout[-500:] + r.stderr[-500:])
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--particles", type=int, default=502)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--graph-steps", type=int, default=0)
+    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import torch
+        import datetime
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        t0 = time.perf_counter()
+        res = cpu_reference(args, args.steps, args.warmup)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference binary oracle/_ref/peridem_ref not built"}))
+            return
+        v = res["node_steps_per_s"]
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * res["seconds"] / res["steps"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": workload_config(args, None) | {"nodes": int(res["nodes"])},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": res["threads"], "kind": "reference",
+                                 "sample": f"{res['steps']} steps of the full scene after one warm-up step "
+                                           f"(init {res['init_seconds']:.1f} s excluded)"},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "wall_s": time.perf_counter() - t0}
+        print(json.dumps(line))
+        return
+
+    res = run_ours(args, rank, world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            r = cpu_reference(args, args.cpu_steps, 1)
+            if r is not None:
+                cpu = {"value": r["node_steps_per_s"], "unit": UNIT, "cores": r["threads"],
+                       "kind": "reference",
+                       "sample": f"{r['steps']} steps of the same scene after one warm-up step "
+                                 f"(init {r['init_seconds']:.1f} s excluded)"}
+        except Exception as e:  # report, do not hide
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"}
+    if rank == 0:
+        sc = res.pop("sc")
+        line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32-bond/f64" if args.precision == "mixed" else "f64",
+                "data": "synthetic", "config": workload_config(args, sc),
+                "e2e": res["e2e"], "roofline": res["roofline"], "cpu_baseline": cpu,
+                "clocks": res["clocks"], "gpu_launches": res["gpu_launches"],
+                "kernels": res["kernels"], "scalars": res["scalars"]}
+        print(json.dumps(line))
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -252,6 +252,10 @@ PDGPU_API int pdgpu_step(pdgpu_ctx *ctx, int64_t nsteps);
  * steps captured on first use (kernels only; no host work per step). */
 PDGPU_API int pdgpu_step_graph(pdgpu_ctx *ctx, int64_t nsteps, int32_t graph_steps);
 
+/* Number of kernels one pdgpu_step step launches (counted from a captured
+ * graph of one step; nothing runs). */
+PDGPU_API int pdgpu_step_kernel_count(pdgpu_ctx *ctx, int64_t *count);
+
 /* Waits for the context stream and reports device-side errors. */
 PDGPU_API int pdgpu_sync(pdgpu_ctx *ctx);
 

@@ -76,6 +76,7 @@ SIGNATURES = {
     "pdgpu_step": [c_vp, c_i64],
     "pdgpu_step_graph": [c_vp, c_i64, c_i32],
     "pdgpu_sync": [c_vp],
+    "pdgpu_step_kernel_count": [c_vp, P(c_i64)],
     "pdgpu_download": [c_vp, c_i32, c_vp],
     "pdgpu_upload_field": [c_vp, c_i32, c_vp],
     "pdgpu_step_host": [c_vp, P(c_d), P(c_d), P(c_d), P(c_d), c_i64, P(Scalars)],

@@ -195,6 +195,9 @@ void launch_mixed_setup(const DevData &d, cudaStream_t s);
 void launch_contact_update(const DevData &d, void *scan_tmp, size_t scan_tmp_bytes, int lanes,
                            int init, cudaStream_t s);
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s);
+int rebuild_grid_blocks(const DevData &d, int lanes);
+cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, int lanes, int init,
+                                   cudaStream_t s);
 void launch_damping(const DevData &d, cudaStream_t s);
 void launch_external(const DevData &d, cudaStream_t s);
 void launch_postprocess(const DevData &d, cudaStream_t s);

@@ -8,6 +8,7 @@
 // (double2) and 4 doubles in 3-D (double4, last lane unused), so one node is
 // one aligned 16- or 32-byte access; peridynamic bonds are CSR (int64 row
 // offsets, int32 columns) with one broken-bit per bond in a uint32 bitmap.
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 
 #include <cfloat>
@@ -693,6 +694,186 @@ __global__ void k_cand_check(DevData d) {
 }
 
 // ---------------------------------------------------------------------------
+// The whole contact-list rebuild as one cooperative launch: every phase is
+// separated by a grid-wide barrier of the cooperative launch (all blocks are
+// co-resident by construction).  On steps without a rebuild every block
+// returns after reading the control word, so the rebuild costs one launch.
+// ---------------------------------------------------------------------------
+namespace cg = cooperative_groups;
+constexpr int kCoopBlock = 256;
+
+// exclusive scan over the whole grid: out[i] = sum_{k<i} in(k) for
+// i = 0..n, each block scanning one contiguous chunk
+template <class Tout, class F>
+__device__ void grid_scan(cg::grid_group &g, F in, Tout *out, int64_t n, int64_t *bsum) {
+  __shared__ int64_t wsum[kCoopBlock / 32];
+  __shared__ int64_t carry;
+  const int64_t nb = gridDim.x;
+  const int64_t chunk = (n + nb - 1) / nb;
+  const int64_t b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // block totals
+  int64_t t = 0;
+  for (int64_t k = b0 + threadIdx.x; k < b1; k += blockDim.x) t += (int64_t)in(k);
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (lane == 0) wsum[warp] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t s = 0;
+    for (int w = 0; w < kCoopBlock / 32; w++) s += wsum[w];
+    bsum[blockIdx.x] = s;
+  }
+  g.sync();
+  if (threadIdx.x == 0) {
+    int64_t s = 0;
+    for (int64_t b = 0; b < blockIdx.x; b++) s += bsum[b];
+    carry = s;
+  }
+  __syncthreads();
+  for (int64_t base = b0; base < b1; base += blockDim.x) {
+    const int64_t k = base + threadIdx.x;
+    const int64_t v = k < b1 ? (int64_t)in(k) : 0;
+    int64_t incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int64_t woff = 0;
+    for (int w = 0; w < warp; w++) woff += wsum[w];
+    if (k < b1) out[k] = (Tout)(carry + woff + incl - v);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int64_t s = 0;
+      for (int w = 0; w < kCoopBlock / 32; w++) s += wsum[w];
+      carry += s;
+    }
+    __syncthreads();
+  }
+  if (blockIdx.x == nb - 1 && threadIdx.x == 0) out[n] = (Tout)carry;
+  g.sync();
+}
+
+template <int DIM, int LPN>
+__device__ __forceinline__ int64_t cand_node(const DevData &d, int64_t i, int lane, unsigned gm,
+                                             unsigned lane_base, bool fill) {
+  const Grid g = d.grid;
+  double q[3];
+  ldv<DIM>(d.x, i, q);
+  const int32_t pi = d.ptid[i];
+  const double r = d.ctrl->radius;
+  const double r2 = r * r;
+  int c[3] = {cell_coord<DIM>(q[0], g, 0), cell_coord<DIM>(q[1], g, 1),
+              DIM == 3 ? cell_coord<DIM>(q[2], g, 2) : 0};
+  int64_t out = fill ? d.c_row[i] : 0;
+  const int64_t out_end = fill ? d.c_row[i + 1] : 0;
+  int64_t count = 0;
+  const int zlo = DIM == 3 ? max(c[2] - 1, 0) : 0;
+  const int zhi = DIM == 3 ? min(c[2] + 1, g.dims[2] - 1) : 0;
+  for (int cz = zlo; cz <= zhi; cz++)
+    for (int cy = max(c[1] - 1, 0); cy <= min(c[1] + 1, g.dims[1] - 1); cy++)
+      for (int cx = max(c[0] - 1, 0); cx <= min(c[0] + 1, g.dims[0] - 1); cx++) {
+        const int cell = cx + g.dims[0] * (cy + g.dims[1] * cz);
+        const int s = d.cell_start[cell], e = d.cell_start[cell + 1];
+        for (int base = s; base < e; base += LPN) {
+          const int a = base + lane;
+          bool hit = false;
+          int32_t j = -1;
+          if (a < e) {
+            j = d.cell_nodes[a];
+            if (d.ptid[j] != pi) {
+              double p[3];
+              ldv<DIM>(d.x, j, p);
+              double dd = 0.0;
+#pragma unroll
+              for (int t = 0; t < DIM; t++) {
+                const double df = q[t] - p[t];
+                dd += df * df;
+              }
+              hit = dd < r2;
+            }
+          }
+          const unsigned bal = (__ballot_sync(gm, hit) & gm) >> lane_base;
+          if (fill) {
+            if (hit) {
+              const int64_t at = out + __popc(bal & ((1u << lane) - 1u));
+              if (at < out_end && at < d.contact_cap) d.c_col[at] = j;
+            }
+            out += __popc(bal);
+          } else {
+            count += __popc(bal);
+          }
+        }
+      }
+  return count;
+}
+
+template <int DIM, int LPN>
+__global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8_t search_bit,
+                                                               int64_t *bsum) {
+  if (d.ctrl->error || !d.ctrl->update) return;
+  cg::grid_group g = cg::this_grid();
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+  const int64_t N = d.n_nodes;
+  const Grid G = d.grid;
+  for (int64_t c = tid; c <= G.ncells; c += nth) {
+    d.cell_cnt[c] = 0;
+    d.cell_fill[c] = 0;
+  }
+  g.sync();
+  for (int64_t i = tid; i < N; i += nth) {
+    double p[3];
+    ldv<DIM>(d.x, i, p);
+    const int c = cell_index<DIM>(p, G);
+    d.cell_of[i] = c;
+    atomicAdd(d.cell_cnt + c, 1);
+  }
+  g.sync();
+  const int32_t *cc = d.cell_cnt;
+  grid_scan<int32_t>(g, [cc](int64_t k) { return cc[k]; }, d.cell_start, G.ncells, bsum);
+  for (int64_t i = tid; i < N; i += nth) {
+    const int c = d.cell_of[i];
+    d.cell_tmp[d.cell_start[c] + atomicAdd(d.cell_fill + c, 1)] = (int32_t)i;
+  }
+  g.sync();
+  {
+    const int lane = threadIdx.x & 31;
+    for (int64_t c = tid >> 5; c < G.ncells; c += nth >> 5) {
+      const int s = d.cell_start[c], e = d.cell_start[c + 1];
+      for (int a = s + lane; a < e; a += 32) {
+        const int32_t va = d.cell_tmp[a];
+        int rank = 0;
+        for (int b = s; b < e; b++) rank += d.cell_tmp[b] < va;
+        d.cell_nodes[s + rank] = va;
+      }
+    }
+  }
+  g.sync();
+  const int lane = threadIdx.x % LPN;
+  const unsigned gm = group_mask<LPN>();
+  const unsigned lane_base = (threadIdx.x & 31u) / LPN * LPN;
+  for (int64_t i = tid / LPN; i < N; i += nth / LPN) {
+    int64_t cnt = 0;
+    if (d.flags[i] & search_bit) cnt = cand_node<DIM, LPN>(d, i, lane, gm, lane_base, false);
+    if (lane == 0) d.c_cnt[i] = cnt;
+  }
+  g.sync();
+  const int64_t *cn = d.c_cnt;
+  grid_scan<int64_t>(g, [cn](int64_t k) { return cn[k]; }, d.c_row, N, bsum);
+  for (int64_t i = tid / LPN; i < N; i += nth / LPN)
+    if ((d.flags[i] & search_bit) && d.c_row[i + 1] > d.c_row[i])
+      cand_node<DIM, LPN>(d, i, lane, gm, lane_base, true);
+  if (tid == 0) {
+    const int64_t total = d.c_row[N];
+    d.ctrl->entries = total;
+    d.ctrl->updates += 1;
+    if (total > d.contact_cap) set_error(d.ctrl, DEV_ERR_CONTACT_OVERFLOW, total);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Node pass of DEMModel::computeContactForces (demModel.cpp:832-934):
 // penalty normal force + Coulomb-type friction for candidates inside the
 // zone-pair contact radius; f_i += sum.  Particle-wall pairs inside the
@@ -705,7 +886,13 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
   const int lane = threadIdx.x % LPN;
   double crd = 0.0;
-  const bool live = i < d.n_nodes && (d.flags[i] & NODE_SEARCH) && !d.ctrl->error;
+  int64_t k0 = 0, k1 = 0;
+  if (i < d.n_nodes && (d.flags[i] & NODE_SEARCH) && !d.ctrl->error) {
+    k0 = d.c_row[i];
+    k1 = d.c_row[i + 1];
+  }
+  // nodes without candidates (most of each particle) leave f untouched
+  const bool live = k1 > k0;
   if (live) {
     const unsigned gm = group_mask<LPN>();
     const int32_t pi = d.ptid[i];
@@ -714,7 +901,6 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
     ldv<DIM>(d.x, i, yi);
     ldv<DIM>(d.v, i, vi);
     double fx = 0.0, fy = 0.0, fz = 0.0;
-    const int64_t k0 = d.c_row[i], k1 = d.c_row[i + 1];
     for (int64_t k = k0 + lane; k < k1; k += LPN) {
       const int32_t j = d.c_col[k];
       double yj[3];
@@ -761,8 +947,8 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
           else set_error(d.ctrl, DEV_ERR_WALLPAIR_OVERFLOW, pi);
         }
         if (pj == d.test_wall) {
-          const double c3[3] = {cx + mf * et[0], cy + mf * et[1], cz + mf * et[2]};
-          crd += c3[d.test_dir];
+          const int td = d.test_dir;
+          crd += td == 0 ? cx + mf * et[0] : (td == 1 ? cy + mf * et[1] : cz + mf * et[2]);
         }
       }
     }
@@ -1256,6 +1442,33 @@ void launch_contact_update(const DevData &d, void *tmp, size_t bytes, int lanes,
     else cand_dim<3, 32>(d, bit, s, tmp, bytes);
   }
   k_cand_check<<<1, 1, 0, s>>>(d);
+}
+
+template <int DIM, int LPN>
+static cudaError_t rebuild_dim(const DevData &d, uint8_t bit, int64_t *bsum, int grid,
+                               cudaStream_t s) {
+  DevData dd = d;
+  void *args[] = {(void *)&dd, (void *)&bit, (void *)&bsum};
+  return cudaLaunchCooperativeKernel((const void *)k_contact_rebuild<DIM, LPN>, dim3(grid),
+                                     dim3(kCoopBlock), args, 0, s);
+}
+
+int rebuild_grid_blocks(const DevData &d, int lanes) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const void *f;
+  if (d.dim == 2) f = lanes <= 8 ? (const void *)k_contact_rebuild<2, 8> : (const void *)k_contact_rebuild<2, 32>;
+  else f = lanes <= 8 ? (const void *)k_contact_rebuild<3, 8> : (const void *)k_contact_rebuild<3, 32>;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, kCoopBlock, 0);
+  return sms * (per > 0 ? per : 1);
+}
+
+cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, int lanes, int init,
+                                   cudaStream_t s) {
+  const uint8_t bit = init ? NODE_SEARCH0 : NODE_SEARCH;
+  if (d.dim == 2) return lanes <= 8 ? rebuild_dim<2, 8>(d, bit, bsum, grid, s) : rebuild_dim<2, 32>(d, bit, bsum, grid, s);
+  return lanes <= 8 ? rebuild_dim<3, 8>(d, bit, bsum, grid, s) : rebuild_dim<3, 32>(d, bit, bsum, grid, s);
 }
 
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s) {

@@ -57,6 +57,8 @@ struct pdgpu_ctx {
   void *scan_tmp = nullptr;
   size_t scan_bytes = 0;
   int pd_lanes = 0, contact_lanes = 8;
+  int64_t *rebuild_bsum = nullptr;
+  int rebuild_grid = 0;
   bool state_prepass = false;
 
   // graph replay
@@ -542,6 +544,8 @@ int prepare(pdgpu_ctx *ctx) {
     if (!(cell > 0)) return fail(ctx, PDGPU_ERR_ARG, "max_contact_r must be positive");
     TRY(make_grid(ctx, cell, &g));
     TRY(ensure_cells(ctx, g));
+    ctx->rebuild_grid = rebuild_grid_blocks(d, ctx->contact_lanes);
+    TRY(dalloc(ctx, &ctx->rebuild_bsum, (size_t)ctx->rebuild_grid + 1));
   }
   // step control
   CtrlState c{};
@@ -573,7 +577,7 @@ void compute_forces(pdgpu_ctx *ctx) {
     run(ctx, "pd_force", [&] { launch_pd_force(d, ctx->pd_lanes, s); });
   if (ctx->desc.multi_particle) {
     run(ctx, "contact_update", [&] {
-      launch_contact_update(d, ctx->scan_tmp, ctx->scan_bytes, ctx->contact_lanes, 0, s);
+      launch_contact_rebuild(d, ctx->rebuild_bsum, ctx->rebuild_grid, ctx->contact_lanes, 0, s);
     });
     run(ctx, "contact_force", [&] { launch_contact_force(d, ctx->contact_lanes, s); });
     run(ctx, "damping", [&] { launch_damping(d, s); });
@@ -942,8 +946,8 @@ int pdgpu_init_contact(pdgpu_ctx *ctx) {
   if (!ctx->desc.multi_particle) return PDGPU_OK;
   if (ctx->contact_init) return fail(ctx, PDGPU_ERR_STATE, "contact lists already initialised");
   launch_ctrl(ctx->d, 2, ctx->stream);
-  launch_contact_update(ctx->d, ctx->scan_tmp, ctx->scan_bytes, ctx->contact_lanes, 1, ctx->stream);
-  CK(cudaGetLastError());
+  CK(launch_contact_rebuild(ctx->d, ctx->rebuild_bsum, ctx->rebuild_grid, ctx->contact_lanes, 1,
+                            ctx->stream));
   TRY(device_error(ctx));
   ctx->contact_init = true;
   return PDGPU_OK;
@@ -1000,6 +1004,31 @@ int pdgpu_step_graph(pdgpu_ctx *ctx, int64_t nsteps, int32_t graph_steps) {
   }
   for (int64_t k = 0; k < left; k++) one_step(ctx);
   CK(cudaGetLastError());
+  return PDGPU_OK;
+}
+
+int pdgpu_step_kernel_count(pdgpu_ctx *ctx, int64_t *count) {
+  if (!ctx || !count) return PDGPU_ERR_ARG;
+  if (!ctx->begun) return fail(ctx, PDGPU_ERR_STATE, "call pdgpu_integrate_begin first");
+  const bool was_timing = ctx->timing;
+  ctx->timing = false;
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  one_step(ctx);
+  CK(cudaStreamEndCapture(ctx->stream, &g));
+  ctx->timing = was_timing;
+  size_t n = 0;
+  CK(cudaGraphGetNodes(g, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n);
+  CK(cudaGraphGetNodes(g, nodes.data(), &n));
+  int64_t k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    CK(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) k++;
+  }
+  cudaGraphDestroy(g);
+  *count = k;
   return PDGPU_OK;
 }
 

@@ -314,6 +314,11 @@ class GpuDEMModel:
                                                          _ptr(col, ctypes.c_uint64)))
         return rp, col
 
+    def step_kernel_count(self) -> int:
+        n = ctypes.c_int64()
+        self._check(self.lib.pdgpu_step_kernel_count(self.ctx, ctypes.byref(n)))
+        return n.value
+
     def stream_handle(self) -> int:
         p = ctypes.c_void_p()
         self._check(self.lib.pdgpu_get_stream(self.ctx, ctypes.byref(p)))

@@ -1,0 +1,52 @@
+"""The C ABI: every entry point declared in include/pdgpu.h is exported by
+the built library and bound by peridem_b200.api with a signature; no
+compute call is made (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from peridem_b200 import api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    text = open(os.path.join(ROOT, "include", "pdgpu.h")).read()
+    return sorted(set(re.findall(r"PDGPU_API\s+(?:int|void)\s+(pdgpu_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_abi():
+    names = _declared()
+    assert len(names) >= 30
+    assert "pdgpu_step" in names and "pdgpu_create" in names
+
+
+def test_binding_covers_every_declared_entry_point():
+    assert sorted(api.SIGNATURES) == _declared()
+
+
+@pytest.mark.skipif(not os.path.exists(api.LIB_PATH), reason="libpdgpu.so not built")
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(api.LIB_PATH)
+    for name in _declared():
+        assert hasattr(lib, name), name
+
+
+@pytest.mark.skipif(not os.path.exists(api.LIB_PATH), reason="libpdgpu.so not built")
+def test_create_fails_loudly_without_a_b200():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    from peridem_b200 import scene as scn
+    from peridem_b200.model import GpuDEMModel
+    sc = scn.build_scene(scn.two_particle(h_div=4, nt=10))
+    with pytest.raises(api.PdgpuError):
+        GpuDEMModel(sc)
+
+
+def test_struct_layouts_match_header():
+    # sizes of the ABI structs as the C compiler lays them out
+    assert ctypes.sizeof(api.Particle) == 3 * 8 + 6 * 4 + 6 * 8 + 6 * 8
+    assert ctypes.sizeof(api.BcSet) == 4 * 4 + 6 * 8
