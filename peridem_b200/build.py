@@ -20,6 +20,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 
 UNITS = [
     ("pdgpu_kernels.cu", ["--fmad=false"]),
+    ("pdgpu_bonds_fp64.cu", ["--fmad=false"]),
+    ("pdgpu_bonds_mixed.cu", []),
     ("pdgpu_mixed.cu", []),
     ("pdgpu_runtime.cu", []),
 ]
@@ -32,7 +34,8 @@ def _nvcc():
 
 def sources():
     return [os.path.join(CSRC, u) for u, _ in UNITS] + [
-        os.path.join(CSRC, "pdgpu_internal.h"), os.path.join(ROOT, "include", "pdgpu.h")]
+        os.path.join(CSRC, "pdgpu_internal.h"), os.path.join(CSRC, "pdgpu_bonds.cuh"),
+        os.path.join(ROOT, "include", "pdgpu.h")]
 
 
 def up_to_date():

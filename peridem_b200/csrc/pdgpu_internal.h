@@ -97,6 +97,14 @@ struct MixParticle {
   float K, G;
 };
 
+// One CTA of the tiled bond loop: nodes [node_begin, node_end) of one
+// particle, whose bonds reach node indices inside [win_begin, win_end).
+struct BondTile {
+  int32_t particle;
+  int32_t pad;
+  int64_t node_begin, node_end, win_begin, win_end;
+};
+
 struct DevData {
   int32_t dim;
   int32_t precision;
@@ -171,8 +179,6 @@ struct DevData {
 
   // mixed-precision bond loop: particle-local FP32 reference coordinates,
   // FP32 volumes, particle-local 16-bit neighbour offsets when they fit
-  float *xl;
-  float *volf;
   uint16_t *pd_col16;
   MixParticle *mixp;
   int32_t use16;
@@ -187,11 +193,21 @@ void launch_integrate(const DevData &d, int half_kick_only, cudaStream_t s);  //
 void launch_verlet_second(const DevData &d, cudaStream_t s);
 void launch_ctrl(const DevData &d, int mode, cudaStream_t s);  // mode 0 step, 1 prelude, 2 init list
 void launch_bc(const DevData &d, cudaStream_t s);
-void launch_pd_prepass(const DevData &d, cudaStream_t s);
-void launch_pd_force(const DevData &d, int lanes, cudaStream_t s);
-void launch_pd_force_mixed(const DevData &d, int lanes, cudaStream_t s);
-void launch_pd_prepass_mixed(const DevData &d, int lanes, cudaStream_t s);
 void launch_mixed_setup(const DevData &d, cudaStream_t s);
+void launch_tile_windows(const DevData &d, BondTile *tiles, int n_tiles, cudaStream_t s);
+// tiled bond loop (pdgpu_bonds_fp64.cu / pdgpu_bonds_mixed.cu)
+void launch_pd_tiled_fp64(const DevData &d, const BondTile *tiles, int n_tiles, int lanes,
+                          size_t smem, cudaStream_t s);
+void launch_prepass_tiled_fp64(const DevData &d, const BondTile *tiles, int n_tiles, int lanes,
+                               size_t smem, cudaStream_t s);
+void launch_pd_tiled_mixed(const DevData &d, const BondTile *tiles, int n_tiles, int lanes,
+                           size_t smem, cudaStream_t s);
+void launch_prepass_tiled_mixed(const DevData &d, const BondTile *tiles, int n_tiles, int lanes,
+                                size_t smem, cudaStream_t s);
+size_t tile_smem_fp64(int dim, bool state, int64_t window);
+size_t tile_smem_mixed(int dim, bool state, int64_t window);
+int set_tile_smem_limit_fp64(int dim, size_t bytes);
+int set_tile_smem_limit_mixed(int dim, size_t bytes);
 void launch_contact_update(const DevData &d, void *scan_tmp, size_t scan_tmp_bytes, int lanes,
                            int init, cudaStream_t s);
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s);

@@ -392,182 +392,6 @@ __global__ void k_bc(DevData d) {
 }
 
 // ---------------------------------------------------------------------------
-// State-based pre-pass of DEMModel::computePeridynamicForces
-// (demModel.cpp:610-679): bond breaking and dilatation theta_i.
-// LPN lanes per node, lane-strided over the node's bonds.
-// ---------------------------------------------------------------------------
-template <int DIM, int LPN>
-__global__ void __launch_bounds__(kBlock) k_pd_prepass(DevData d) {
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
-  const int lane = threadIdx.x % LPN;
-  if (i >= d.n_nodes) return;
-  if (!(d.flags[i] & NODE_ACTIVE) || d.ctrl->error) return;
-  const DevParticle &P = d.particles[d.ptid[i]];
-  if (P.material != PDGPU_MAT_PDSTATE) return;
-  const unsigned gm = group_mask<LPN>();
-  double xi[3], ui[3];
-  ldg_v<DIM>(d.xref, i, xi);
-  ldg_v<DIM>(d.u, i, ui);
-  const double sc = P.mat[2];
-  double theta = 0.0;
-  const int64_t k0 = d.pd_row[i], k1 = d.pd_row[i + 1];
-  for (int64_t k = k0 + lane; k < k1; k += LPN) {
-    const int32_t j = __ldg(d.pd_col + k);
-    double xj[3], uj[3];
-    ldg_v<DIM>(d.xref, j, xj);
-    ldg_v<DIM>(d.u, j, uj);
-    double dx[3], y[3];
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      dx[q] = xj[q] - xi[q];
-      y[q] = dx[q] + uj[q] - ui[q];  // (xj - xi + uj - ui), left to right
-    }
-    const double rji = len3<DIM>(dx);
-    const double cl = len3<DIM>(y) - rji;
-    const double s = cl / rji;
-    const uint32_t bit = 1u << (k & 31);
-    bool fs = (d.bond_bits[k >> 5] & bit) != 0;
-    if (!fs && is_greater(fabs(s), sc + 1.0e-10)) {
-      fs = true;
-      atomicOr(d.bond_bits + (k >> 5), bit);
-    }
-    if (!fs) {
-      double volj = __ldg(d.vol + j);
-      if (is_greater(rji, P.check_low)) volj *= (P.check_up - rji) / P.h;
-      theta += rji * cl * influence(d.inf, rji, P.horizon) * volj;
-    }
-  }
-  theta = group_sum<LPN>(theta, gm);
-  if (lane == 0) d.theta[i] = 3.0 * theta / d.mx[i];
-}
-
-// ---------------------------------------------------------------------------
-// Main bond loop of DEMModel::computePeridynamicForces (demModel.cpp:681-789)
-// with the bond laws of RnpMaterial (material.h:342-417), PmbMaterial
-// (:732-801), PdElastic (:1090-1144) and PdState (:1415-1459).  Overwrites
-// f_i (the reference zeroes f then sets d_f[i] = force_i) and Z_i.
-// ---------------------------------------------------------------------------
-template <int DIM, int LPN>
-__global__ void __launch_bounds__(kBlock) k_pd_force(DevData d) {
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
-  const int lane = threadIdx.x % LPN;
-  if (i >= d.n_nodes) return;
-  if (d.ctrl->error) return;
-  if (!(d.flags[i] & NODE_ACTIVE)) {
-    if (lane == 0) {
-      const double z[3] = {0.0, 0.0, 0.0};
-      stv<DIM>(d.f, i, z);
-    }
-    return;
-  }
-  const unsigned gm = group_mask<LPN>();
-  const DevParticle &P = d.particles[d.ptid[i]];
-  const int mat = P.material;
-  double xi[3], ui[3];
-  ldg_v<DIM>(d.xref, i, xi);
-  ldg_v<DIM>(d.u, i, ui);
-  const double mi = d.mx[i];
-  const double thi = d.theta[i];
-  double fx = 0.0, fy = 0.0, fz = 0.0;
-  double zmax = 0.0;
-  const int64_t k0 = d.pd_row[i], k1 = d.pd_row[i + 1];
-  for (int64_t k = k0 + lane; k < k1; k += LPN) {
-    const int32_t j = __ldg(d.pd_col + k);
-    const uint32_t bit = 1u << (k & 31);
-    bool fs = (d.bond_bits[k >> 5] & bit) != 0;
-    double xj[3], uj[3];
-    ldg_v<DIM>(d.xref, j, xj);
-    ldg_v<DIM>(d.u, j, uj);
-    double volj = __ldg(d.vol + j);
-    double dx[3], du[3];
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      dx[q] = xj[q] - xi[q];
-      du[q] = uj[q] - ui[q];
-    }
-    const double rji = len3<DIM>(dx);
-    double S, dpl[3], ldpl = 0.0;
-    if (mat == PDGPU_MAT_RNP) {
-      S = dot3<DIM>(dx, du) / dot3<DIM>(dx, dx);  // material.h:405-407
-    } else {
-#pragma unroll
-      for (int q = 0; q < 3; q++) dpl[q] = dx[q] + du[q];
-      ldpl = len3<DIM>(dpl);
-      S = (ldpl - rji) / rji;  // material.h:791-793
-    }
-    double sc;
-    if (mat == PDGPU_MAT_RNP) sc = P.mat[2] / sqrt(rji);
-    else if (mat == PDGPU_MAT_PDELASTIC) sc = DBL_MAX;
-    else if (mat == PDGPU_MAT_PMB) sc = P.mat[1];
-    else sc = P.mat[2];
-    if (!fs) {
-      if (is_greater(rji, P.check_low)) volj *= (P.check_up - rji) / P.h;
-      double ef = 0.0;
-      const double J = influence(d.inf, rji, P.horizon);
-      if (mat == PDGPU_MAT_PDSTATE) {
-        const double mj = __ldg(d.mx + j), thj = __ldg(d.theta + j);
-        const double K = P.mat[0], G = P.mat[1];
-        const double cl = S * rji;
-        const double ai = 15. * G / mi, aj = 15. * G / mj;
-        const double fi = (3. * K / mi) - ai / 3., fj = (3. * K / mj) - aj / 3.;
-        const double efi = J * (rji * thi * fi + cl * ai);
-        const double efj = J * (rji * thj * fj + cl * aj);
-        const double sf = (efi + efj) * volj;
-        const double inv = ldpl;
-        fx += sf * (dpl[0] / inv);
-        fy += sf * (dpl[1] / inv);
-        if constexpr (DIM == 3) fz += sf * (dpl[2] / inv);
-      } else {
-        if (mat == PDGPU_MAT_RNP) {
-          if (P.mat[5] != 0.0 && !fs && is_greater(fabs(S), P.mat[4] * sc)) {
-            fs = true;
-            atomicOr(d.bond_bits + (k >> 5), bit);
-          }
-          if (!fs)
-            ef = J * 4. * S * P.mat[0] * P.mat[1] * exp(-P.mat[1] * rji * S * S) / P.mat[3];
-          const double sf = ef * volj;
-          fx += sf * (dx[0] / rji);
-          fy += sf * (dx[1] / rji);
-          if constexpr (DIM == 3) fz += sf * (dx[2] / rji);
-        } else {
-          if (mat == PDGPU_MAT_PMB && !fs && is_greater(fabs(S), P.mat[1] + 1.0e-10)) {
-            fs = true;
-            atomicOr(d.bond_bits + (k >> 5), bit);
-          }
-          if (!fs) ef = J * P.mat[0] * S;
-          const double sf = ef * volj;
-          fx += sf * (dpl[0] / ldpl);
-          fy += sf * (dpl[1] / ldpl);
-          if constexpr (DIM == 3) fz += sf * (dpl[2] / ldpl);
-        }
-      }
-    } else {
-      // broken bond: internal normal contact (demModel.cpp:760-768)
-      double y[3];
-#pragma unroll
-      for (int q = 0; q < 3; q++) y[q] = (xj[q] + uj[q]) - (xi[q] + ui[q]);
-      const double R = len3<DIM>(y);
-      double sf = P.kn * volj * (R - P.rc) / R;
-      if (sf > 0.) sf = 0.;
-      fx += sf * y[0];
-      fy += sf * y[1];
-      if constexpr (DIM == 3) fz += sf * y[2];
-    }
-    // damage Z = max |S / Sc| (demModel.cpp:770-773)
-    zmax = fmax(zmax, fabs(S / sc));
-  }
-  fx = group_sum<LPN>(fx, gm);
-  fy = group_sum<LPN>(fy, gm);
-  if constexpr (DIM == 3) fz = group_sum<LPN>(fz, gm);
-  zmax = group_max<LPN>(zmax, gm);
-  if (lane == 0) {
-    const double o[3] = {fx, fy, fz};
-    stv<DIM>(d.f, i, o);
-    d.Z[i] = (float)zmax;
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Contact candidate lists: DEMModel::updateContactNeighborlist
 // (demModel.cpp:1696-1756) with the kd-tree exclude-tag radius search
 // (nsearch.h:278-301; strict  sum_d (q_d - p_d)^2 < r*r  of
@@ -1098,8 +922,10 @@ template <int DIM>
 __global__ void k_external(DevData d) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n_nodes || d.ctrl->error) return;
-  double f[3];
-  ldv<DIM>(d.f, i, f);
+  // nodes outside d_fPdCompNodes carry no peridynamic or contact force: the
+  // reference zeroes f for all nodes at the start of computeForces (:473-478)
+  double f[3] = {0.0, 0.0, 0.0};
+  if (d.flags[i] & NODE_ACTIVE) ldv<DIM>(d.f, i, f);
   const int32_t p = d.ptid[i];
   if (d.flags[i] & NODE_PARTICLE) {
 #pragma unroll
@@ -1373,39 +1199,6 @@ void launch_ctrl(const DevData &d, int mode, cudaStream_t s) { k_ctrl<<<1, 1, 0,
 void launch_bc(const DevData &d, cudaStream_t s) {
   if (!d.n_ubc_nodes) return;
   PDGPU_DIM_DISPATCH(d, k_bc, <<<blocks_for(d.n_ubc_nodes, 128), 128, 0, s>>>(d));
-}
-
-template <int DIM>
-static void pd_prepass_dim(const DevData &d, int lanes, cudaStream_t s) {
-  const int64_t threads = d.n_nodes * lanes;
-  const unsigned g = blocks_for(threads, kBlock);
-  switch (lanes) {
-    case 4: k_pd_prepass<DIM, 4><<<g, kBlock, 0, s>>>(d); break;
-    case 8: k_pd_prepass<DIM, 8><<<g, kBlock, 0, s>>>(d); break;
-    case 16: k_pd_prepass<DIM, 16><<<g, kBlock, 0, s>>>(d); break;
-    default: k_pd_prepass<DIM, 32><<<g, kBlock, 0, s>>>(d); break;
-  }
-}
-void launch_pd_prepass(const DevData &d, cudaStream_t s) {
-  const int lanes = d.dim == 2 ? 8 : 32;
-  if (d.dim == 2) pd_prepass_dim<2>(d, lanes, s);
-  else pd_prepass_dim<3>(d, lanes, s);
-}
-
-template <int DIM>
-static void pd_force_dim(const DevData &d, int lanes, cudaStream_t s) {
-  const int64_t threads = d.n_nodes * lanes;
-  const unsigned g = blocks_for(threads, kBlock);
-  switch (lanes) {
-    case 4: k_pd_force<DIM, 4><<<g, kBlock, 0, s>>>(d); break;
-    case 8: k_pd_force<DIM, 8><<<g, kBlock, 0, s>>>(d); break;
-    case 16: k_pd_force<DIM, 16><<<g, kBlock, 0, s>>>(d); break;
-    default: k_pd_force<DIM, 32><<<g, kBlock, 0, s>>>(d); break;
-  }
-}
-void launch_pd_force(const DevData &d, int lanes, cudaStream_t s) {
-  if (d.dim == 2) pd_force_dim<2>(d, lanes, s);
-  else pd_force_dim<3>(d, lanes, s);
 }
 
 size_t scan_temp_bytes(int64_t n) {

@@ -59,6 +59,11 @@ struct pdgpu_ctx {
   int pd_lanes = 0, contact_lanes = 8;
   int64_t *rebuild_bsum = nullptr;
   int rebuild_grid = 0;
+  // tiled bond loop
+  BondTile *tiles = nullptr;
+  int n_tiles = 0;
+  size_t tile_smem = 0, tile_smem_state = 0;
+  int64_t tile_nodes = 0;  // nodes per tile (0 = chosen at set-up)
   bool state_prepass = false;
 
   // graph replay
@@ -461,8 +466,7 @@ int prepare_mixed(pdgpu_ctx *ctx) {
   }
   TRY(dalloc(ctx, &d.mixp, mp.size()));
   CK(cudaMemcpy(d.mixp, mp.data(), mp.size() * sizeof(MixParticle), cudaMemcpyHostToDevice));
-  TRY(dalloc(ctx, &d.xl, (size_t)(d.dim == 2 ? 2 : 4) * N));
-  TRY(dalloc(ctx, &d.volf, N));
+  (void)N;
   d.use16 = fits16 ? 1 : 0;
   if (fits16) TRY(dalloc(ctx, &d.pd_col16, d.n_bonds));
   d.inf_p0 = (float)d.inf.p0;
@@ -471,6 +475,65 @@ int prepare_mixed(pdgpu_ctx *ctx) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   return PDGPU_OK;
+}
+
+// Tiles of the bond loop: every force-computing particle is cut into runs of
+// tile_nodes consecutive nodes; the device finds each tile's neighbour window
+// and the largest window fixes the shared-memory stage.
+int prepare_tiles(pdgpu_ctx *ctx) {
+  DevData &d = ctx->d;
+  const bool mixed = d.precision == PDGPU_PREC_MIXED;
+  const size_t limit = 227 * 1024;
+  for (int64_t tn : {ctx->tile_nodes > 0 ? ctx->tile_nodes : (int64_t)(d.dim == 2 ? 128 : 96),
+                     (int64_t)64, (int64_t)32, (int64_t)16}) {
+    std::vector<BondTile> t;
+    for (size_t p = 0; p < ctx->hp.size(); p++) {
+      const DevParticle &P = ctx->hp[p];
+      if (!P.compute_force) continue;
+      for (int64_t a = P.start; a < P.end; a += tn) {
+        BondTile b{};
+        b.particle = (int32_t)p;
+        b.node_begin = a;
+        b.node_end = std::min(P.end, a + tn);
+        t.push_back(b);
+      }
+    }
+    if (ctx->tiles) dfree(ctx, ctx->tiles);
+    ctx->n_tiles = (int)t.size();
+    if (t.empty()) return PDGPU_OK;
+    TRY(dalloc(ctx, &ctx->tiles, t.size()));
+    CK(cudaMemcpyAsync(ctx->tiles, t.data(), t.size() * sizeof(BondTile), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    launch_tile_windows(d, ctx->tiles, ctx->n_tiles, ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(t.data(), ctx->tiles, t.size() * sizeof(BondTile), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // every tile's window must hold its own nodes and fit the stage
+    int64_t wmax = 0;
+    for (auto &b : t) {
+      const DevParticle &P = ctx->hp[b.particle];
+      if (b.win_begin < 0 || b.win_end > d.n_nodes || b.win_begin > b.node_begin ||
+          b.win_end < b.node_end || b.win_begin < P.start || b.win_end > P.end)
+        return fail(ctx, PDGPU_ERR_STATE, "bond tile window [%lld, %lld) inconsistent with nodes [%lld, %lld)",
+                    (long long)b.win_begin, (long long)b.win_end, (long long)b.node_begin,
+                    (long long)b.node_end);
+      wmax = std::max(wmax, b.win_end - b.win_begin);
+    }
+    const size_t sm = mixed ? tile_smem_mixed(d.dim, false, wmax) : tile_smem_fp64(d.dim, false, wmax);
+    const size_t ss = mixed ? tile_smem_mixed(d.dim, true, wmax) : tile_smem_fp64(d.dim, true, wmax);
+    const size_t need = ctx->state_prepass ? ss : sm;
+    if (need > limit) continue;
+    const int rc = mixed ? set_tile_smem_limit_mixed(d.dim, need) : set_tile_smem_limit_fp64(d.dim, need);
+    if (rc != 0) return fail(ctx, PDGPU_ERR_CUDA, "cannot raise the shared-memory limit to %zu bytes", need);
+    ctx->tile_smem = sm;
+    ctx->tile_smem_state = ss;
+    ctx->tile_nodes = tn;
+    return PDGPU_OK;
+  }
+  return fail(ctx, PDGPU_ERR_ARG,
+              "a particle's bonds reach too far in node order for the shared-memory stage; "
+              "order each particle's nodes spatially");
 }
 
 // flags, BC tables, grid and contact buffers: done once before stepping
@@ -557,6 +620,7 @@ int prepare(pdgpu_ctx *ctx) {
   // the state pre-pass runs when particle 0 is state-based (demModel.cpp:607-610)
   ctx->state_prepass = !ctx->hp.empty() && ctx->hp[0].material == PDGPU_MAT_PDSTATE;
   if (d.precision == PDGPU_PREC_MIXED) TRY(prepare_mixed(ctx));
+  TRY(prepare_tiles(ctx));
   ctx->prepared = true;
   return PDGPU_OK;
 }
@@ -565,16 +629,26 @@ int prepare(pdgpu_ctx *ctx) {
 void compute_forces(pdgpu_ctx *ctx) {
   DevData &d = ctx->d;
   cudaStream_t s = ctx->stream;
+  const bool mixed = d.precision == PDGPU_PREC_MIXED;
   if (ctx->state_prepass) {
-    if (d.precision == PDGPU_PREC_MIXED)
-      run(ctx, "pd_prepass_mixed", [&] { launch_pd_prepass_mixed(d, ctx->pd_lanes, s); });
+    if (mixed)
+      run(ctx, "pd_prepass_mixed", [&] {
+        launch_prepass_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
+      });
     else
-      run(ctx, "pd_prepass", [&] { launch_pd_prepass(d, s); });
+      run(ctx, "pd_prepass", [&] {
+        launch_prepass_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
+      });
   }
-  if (d.precision == PDGPU_PREC_MIXED)
-    run(ctx, "pd_force_mixed", [&] { launch_pd_force_mixed(d, ctx->pd_lanes, s); });
+  const size_t smem = ctx->state_prepass ? ctx->tile_smem_state : ctx->tile_smem;
+  if (mixed)
+    run(ctx, "pd_force_mixed", [&] {
+      launch_pd_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
+    });
   else
-    run(ctx, "pd_force", [&] { launch_pd_force(d, ctx->pd_lanes, s); });
+    run(ctx, "pd_force", [&] {
+      launch_pd_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
+    });
   if (ctx->desc.multi_particle) {
     run(ctx, "contact_update", [&] {
       launch_contact_rebuild(d, ctx->rebuild_bsum, ctx->rebuild_grid, ctx->contact_lanes, 0, s);
@@ -641,7 +715,9 @@ int pdgpu_create(const pdgpu_desc *desc, pdgpu_ctx **out) {
   if (rc != PDGPU_OK) return rc;
   auto *ctx = new pdgpu_ctx();
   ctx->desc = *desc;
-  if (cudaSetDevice(desc->device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  // a blocking stream: ordered with the legacy default stream, so plain
+  // cudaMemcpy/cudaMemset calls of the set-up path never race the kernels
+  if (cudaSetDevice(desc->device) != cudaSuccess || cudaStreamCreate(&ctx->stream) != cudaSuccess) {
     delete ctx;
     return PDGPU_ERR_CUDA;
   }
