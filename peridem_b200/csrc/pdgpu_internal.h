@@ -69,6 +69,7 @@ struct CtrlState {
   double reaction, contact_reaction, penetration;
   double pen_dist, max_y, contact_area_radius;
   int64_t history_count;
+  int64_t c_nnodes;  // nodes with a non-empty contact candidate list
 };
 
 // Cell grid fixed at set-up; nodes outside are clamped to the border cells,
@@ -141,6 +142,9 @@ struct DevData {
   int64_t *c_row;
   int32_t *c_col;
   int64_t *c_cnt;  // per-node candidate counts of the last rebuild
+  int64_t *c_tmp;  // N+1 scratch for the compaction scan
+  int32_t *c_nodes;  // nodes with candidates, ascending
+  int32_t contact_grid;  // blocks of the contact node pass
   Grid grid;
   int32_t *cell_of, *cell_cnt, *cell_start, *cell_fill, *cell_tmp, *cell_nodes;
   int64_t cell_cap;  // max nodes in one cell handled by the in-cell sort
@@ -192,6 +196,7 @@ void launch_apply_ic(const DevData &d, cudaStream_t s);
 void launch_integrate(const DevData &d, int half_kick_only, cudaStream_t s);  // CD or Verlet first half
 void launch_verlet_second(const DevData &d, cudaStream_t s);
 void launch_ctrl(const DevData &d, int mode, cudaStream_t s);  // mode 0 step, 1 prelude, 2 init list
+void launch_ctrl_cond(const DevData &d, int mode, cudaGraphConditionalHandle h, cudaStream_t s);
 void launch_bc(const DevData &d, cudaStream_t s);
 void launch_mixed_setup(const DevData &d, cudaStream_t s);
 void launch_tile_windows(const DevData &d, BondTile *tiles, int n_tiles, cudaStream_t s);

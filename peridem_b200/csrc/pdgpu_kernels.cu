@@ -260,7 +260,7 @@ __global__ void k_verlet_second(DevData d) {
 // mode 0: a time step; 1: the computeForces call of the integrate() prelude;
 // 2: the contact list build of DEMModel::init.
 // ---------------------------------------------------------------------------
-__global__ void k_ctrl(DevData d, int mode) {
+__device__ void ctrl_step(const DevData &d, int mode) {
   CtrlState *c = d.ctrl;
   if (c->error) return;
   if (mode == 0) {
@@ -319,6 +319,15 @@ __global__ void k_ctrl(DevData d, int mode) {
   c->counter += 1;
   upd = ((c->counter - 1) % c->interval) == 0;
   c->update = upd;
+}
+
+__global__ void k_ctrl(DevData d, int mode) { ctrl_step(d, mode); }
+
+// same, inside a CUDA graph: the rebuild decision also drives the graph's
+// conditional node that holds the contact-list rebuild
+__global__ void k_ctrl_cond(DevData d, int mode, cudaGraphConditionalHandle h) {
+  ctrl_step(d, mode);
+  cudaGraphSetConditional(h, (d.ctrl->update && !d.ctrl->error) ? 1u : 0u);
 }
 
 // ---------------------------------------------------------------------------
@@ -509,6 +518,20 @@ __global__ void __launch_bounds__(kBlock) k_cand(DevData d, uint8_t search_bit) 
   if (!FILL && lane == 0) d.c_cnt[i] = count;
 }
 
+__global__ void k_compact_flag(DevData d) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_nodes || d.ctrl->error || !d.ctrl->update) return;
+  d.c_tmp[i] = d.c_cnt[i] > 0 ? 1 : 0;
+}
+
+__global__ void k_compact_scatter(DevData d) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_nodes || d.ctrl->error || !d.ctrl->update) return;
+  // c_tmp holds the inclusive scan of the flags
+  if (d.c_cnt[i] > 0) d.c_nodes[d.c_tmp[i] - 1] = (int32_t)i;
+  if (i == d.n_nodes - 1) d.ctrl->c_nnodes = d.c_tmp[i];
+}
+
 __global__ void k_cand_check(DevData d) {
   if (d.ctrl->error || !d.ctrl->update) return;
   const int64_t total = d.c_row[d.n_nodes];
@@ -686,6 +709,10 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
   g.sync();
   const int64_t *cn = d.c_cnt;
   grid_scan<int64_t>(g, [cn](int64_t k) { return cn[k]; }, d.c_row, N, bsum);
+  grid_scan<int64_t>(g, [cn](int64_t k) { return (int64_t)(cn[k] > 0); }, d.c_tmp, N, bsum);
+  for (int64_t i = tid; i < N; i += nth)
+    if (cn[i] > 0) d.c_nodes[d.c_tmp[i]] = (int32_t)i;
+  if (tid == 0) d.ctrl->c_nnodes = d.c_tmp[N];
   for (int64_t i = tid / LPN; i < N; i += nth / LPN)
     if ((d.flags[i] & search_bit) && d.c_row[i + 1] > d.c_row[i])
       cand_node<DIM, LPN>(d, i, lane, gm, lane_base, true);
@@ -707,24 +734,21 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
 template <int DIM, int LPN>
 __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
   __shared__ double scr[kBlock / LPN];
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
   const int lane = threadIdx.x % LPN;
-  double crd = 0.0;
-  int64_t k0 = 0, k1 = 0;
-  if (i < d.n_nodes && (d.flags[i] & NODE_SEARCH) && !d.ctrl->error) {
-    k0 = d.c_row[i];
-    k1 = d.c_row[i + 1];
-  }
-  // nodes without candidates (most of each particle) leave f untouched
-  const bool live = k1 > k0;
-  if (live) {
+  const int64_t nn = d.ctrl->error ? 0 : d.ctrl->c_nnodes;
+  double crd_acc = 0.0;
+  // grid-stride over the nodes that have candidates (compacted at rebuild)
+  for (int64_t t = (int64_t)blockIdx.x * (kBlock / LPN) + threadIdx.x / LPN; t < nn;
+       t += (int64_t)gridDim.x * (kBlock / LPN)) {
+    const int64_t i = d.c_nodes[t];
+    const int64_t k0 = d.c_row[i], k1 = d.c_row[i + 1];
     const unsigned gm = group_mask<LPN>();
     const int32_t pi = d.ptid[i];
     const int zi = d.particles[pi].zone;
     double yi[3], vi[3];
     ldv<DIM>(d.x, i, yi);
     ldv<DIM>(d.v, i, vi);
-    double fx = 0.0, fy = 0.0, fz = 0.0;
+    double fx = 0.0, fy = 0.0, fz = 0.0, crd = 0.0;
     for (int64_t k = k0 + lane; k < k1; k += LPN) {
       const int32_t j = d.c_col[k];
       double yj[3];
@@ -787,16 +811,16 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
       f[1] += fy;
       f[2] += fz;
       stv<DIM>(d.f, i, f);
-      crd *= d.vol[i];
+      crd_acc += crd * d.vol[i];
     }
   }
   // deterministic per-block partial of the test wall's contact reaction
-  if (lane == 0) scr[threadIdx.x / LPN] = live ? crd : 0.0;
+  if (lane == 0) scr[threadIdx.x / LPN] = crd_acc;
   __syncthreads();
   if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int g = 0; g < kBlock / LPN; g++) s += scr[g];
-    d.cr_partial[blockIdx.x] = s;
+    double sum = 0.0;
+    for (int g = 0; g < kBlock / LPN; g++) sum += scr[g];
+    d.cr_partial[blockIdx.x] = sum;
   }
 }
 
@@ -1196,6 +1220,9 @@ void launch_verlet_second(const DevData &d, cudaStream_t s) {
   PDGPU_DIM_DISPATCH(d, k_verlet_second, <<<blocks_for(d.n_nodes, kBlock), kBlock, 0, s>>>(d));
 }
 void launch_ctrl(const DevData &d, int mode, cudaStream_t s) { k_ctrl<<<1, 1, 0, s>>>(d, mode); }
+void launch_ctrl_cond(const DevData &d, int mode, cudaGraphConditionalHandle h, cudaStream_t s) {
+  k_ctrl_cond<<<1, 1, 0, s>>>(d, mode, h);
+}
 void launch_bc(const DevData &d, cudaStream_t s) {
   if (!d.n_ubc_nodes) return;
   PDGPU_DIM_DISPATCH(d, k_bc, <<<blocks_for(d.n_ubc_nodes, 128), 128, 0, s>>>(d));
@@ -1214,6 +1241,10 @@ static void cand_dim(const DevData &d, uint8_t bit, cudaStream_t s, void *tmp, s
   k_cand<DIM, LPN, false><<<g, kBlock, 0, s>>>(d, bit);
   cub::DeviceScan::InclusiveSum(tmp, bytes, d.c_cnt, d.c_row + 1, d.n_nodes, s);
   k_cand<DIM, LPN, true><<<g, kBlock, 0, s>>>(d, bit);
+  const unsigned gn = blocks_for(d.n_nodes, kBlock);
+  k_compact_flag<<<gn, kBlock, 0, s>>>(d);
+  cub::DeviceScan::InclusiveSum(tmp, bytes, d.c_tmp, d.c_tmp, d.n_nodes, s);
+  k_compact_scatter<<<gn, kBlock, 0, s>>>(d);
 }
 
 void launch_contact_update(const DevData &d, void *tmp, size_t bytes, int lanes, int init,
@@ -1265,7 +1296,7 @@ cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, in
 }
 
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s) {
-  const unsigned g = blocks_for(d.n_nodes * lanes, kBlock);
+  const unsigned g = (unsigned)d.contact_grid;
   if (d.dim == 2) {
     if (lanes == 4) k_contact<2, 4><<<g, kBlock, 0, s>>>(d);
     else if (lanes == 8) k_contact<2, 8><<<g, kBlock, 0, s>>>(d);

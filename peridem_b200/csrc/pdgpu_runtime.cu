@@ -69,6 +69,7 @@ struct pdgpu_ctx {
   // graph replay
   cudaGraphExec_t gexec = nullptr;
   int graph_steps = 0;
+  cudaStream_t side = nullptr;  // captures the body of the rebuild's conditional node
 
   // timing
   bool timing = false;
@@ -578,8 +579,13 @@ int prepare(pdgpu_ctx *ctx) {
   const double bpn = N ? (double)d.n_bonds / (double)N : 0.0;
   if (ctx->pd_lanes <= 0) ctx->pd_lanes = bpn > 48 ? 32 : (bpn > 20 ? 8 : 4);
   // contact buffers
-  const int64_t lanes_c = ctx->contact_lanes;
-  d.cr_blocks = (int32_t)((N * lanes_c + 255) / 256);
+  {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    d.contact_grid = 4 * (sms > 0 ? sms : 148);
+  }
+  d.cr_blocks = d.contact_grid;
   TRY(dalloc(ctx, &d.cr_partial, (size_t)d.cr_blocks + 1));
   CK(cudaMemset(d.cr_partial, 0, ((size_t)d.cr_blocks + 1) * 8));
   TRY(dalloc(ctx, &d.history, (size_t)kHistoryCap * 4));
@@ -590,6 +596,8 @@ int prepare(pdgpu_ctx *ctx) {
   CK(cudaMemset(d.c_row, 0, ((size_t)N + 1) * 8));
   TRY(dalloc(ctx, &d.c_cnt, (size_t)N));
   CK(cudaMemset(d.c_cnt, 0, (size_t)N * 8));
+  TRY(dalloc(ctx, &d.c_tmp, (size_t)N + 1));
+  TRY(dalloc(ctx, &d.c_nodes, (size_t)N));
   if (ctx->desc.multi_particle) {
     d.contact_cap = ctx->desc.contact_capacity > 0 ? ctx->desc.contact_capacity
                                                    : std::max<int64_t>(64 * nsearch, 1 << 20);
@@ -672,6 +680,106 @@ void one_step(pdgpu_ctx *ctx) {
   run(ctx, "postprocess", [&] { launch_postprocess(d, s); });
 }
 
+// One step inside a graph under capture: like one_step, but the contact-list
+// rebuild sits in a conditional node that the step-control kernel switches
+// on only on rebuild steps, so other steps pay nothing for it.
+cudaError_t graph_step(pdgpu_ctx *ctx, cudaGraphConditionalHandle h, const char **where) {
+  DevData &d = ctx->d;
+  cudaStream_t s = ctx->stream;
+  const bool verlet = ctx->desc.time_scheme == 1;
+  const bool mixed = d.precision == PDGPU_PREC_MIXED;
+  launch_integrate(d, verlet ? 1 : 0, s);
+  launch_ctrl_cond(d, 0, h, s);
+  launch_bc(d, s);
+  if (ctx->state_prepass) {
+    if (mixed) launch_prepass_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
+    else launch_prepass_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
+  }
+  const size_t smem = ctx->state_prepass ? ctx->tile_smem_state : ctx->tile_smem;
+  if (mixed) launch_pd_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
+  else launch_pd_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
+  if (ctx->desc.multi_particle) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    *where = "kernels before the rebuild";
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    *where = "cudaStreamGetCaptureInfo";
+    e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    *where = "cudaGraphAddNode(conditional)";
+    e = cudaGraphAddNode(&node, g, deps, nd, &p);
+    if (e != cudaSuccess) return e;
+    *where = "cudaStreamUpdateCaptureDependencies";
+    e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    *where = "cudaStreamBeginCaptureToGraph(body)";
+    e = cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    launch_contact_update(d, ctx->scan_tmp, ctx->scan_bytes, ctx->contact_lanes, 0, ctx->side);
+    *where = "contact-rebuild body kernels";
+    const cudaError_t eb = cudaGetLastError();
+    e = cudaStreamEndCapture(ctx->side, &body);
+    if (eb != cudaSuccess) return eb;
+    *where = "cudaStreamEndCapture(body)";
+    if (e != cudaSuccess) return e;
+    *where = "kernels after the rebuild";
+    launch_contact_force(d, ctx->contact_lanes, s);
+    launch_damping(d, s);
+  }
+  launch_external(d, s);
+  if (verlet) launch_verlet_second(d, s);
+  launch_postprocess(d, s);
+  return cudaGetLastError();
+}
+
+int build_graph(pdgpu_ctx *ctx, int steps) {
+  if (!ctx->side) CK(cudaStreamCreate(&ctx->side));
+  cudaStream_t s = ctx->stream;
+  // the conditional handle belongs to a graph created up front, which the
+  // stream then captures into
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  // one handle per conditional node (a handle drives exactly one node)
+  std::vector<cudaGraphConditionalHandle> hs(steps);
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < steps && e == cudaSuccess; k++)
+    e = cudaGraphConditionalHandleCreate(&hs[k], g, 0, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(ctx, PDGPU_ERR_CUDA, "cudaGraphConditionalHandleCreate: %s", cudaGetErrorString(e));
+  }
+  e = cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(ctx, PDGPU_ERR_CUDA, "cudaStreamBeginCaptureToGraph: %s", cudaGetErrorString(e));
+  }
+  const char *where = "graph_step";
+  for (int k = 0; k < steps && e == cudaSuccess; k++) e = graph_step(ctx, hs[k], &where);
+  cudaGraph_t done = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(s, &done);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(ctx, PDGPU_ERR_CUDA, "graph capture failed in %s (step %d of %d): %s",
+                e != cudaSuccess ? where : "cudaStreamEndCapture", 0, steps,
+                cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  e = cudaGraphInstantiate(&ctx->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(ctx, PDGPU_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+  ctx->graph_steps = steps;
+  return PDGPU_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -751,6 +859,7 @@ void pdgpu_destroy(pdgpu_ctx *ctx) {
   cudaSetDevice(ctx->desc.device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->side) cudaStreamDestroy(ctx->side);
   for (auto &t : ctx->pending) {
     cudaEventDestroy(t.a);
     cudaEventDestroy(t.b);
@@ -1061,18 +1170,7 @@ int pdgpu_step_graph(pdgpu_ctx *ctx, int64_t nsteps, int32_t graph_steps) {
     cudaGraphExecDestroy(ctx->gexec);
     ctx->gexec = nullptr;
   }
-  if (!ctx->gexec) {
-    const bool was_timing = ctx->timing;
-    ctx->timing = false;
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < graph_steps; k++) one_step(ctx);
-    CK(cudaStreamEndCapture(ctx->stream, &g));
-    ctx->timing = was_timing;
-    CK(cudaGraphInstantiate(&ctx->gexec, g, 0));
-    cudaGraphDestroy(g);
-    ctx->graph_steps = graph_steps;
-  }
+  if (!ctx->gexec) TRY(build_graph(ctx, graph_steps));
   int64_t left = nsteps;
   while (left >= graph_steps) {
     CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
