@@ -303,6 +303,32 @@ PDGPU_API int pdgpu_enable_timing(pdgpu_ctx *ctx, int32_t on);
 PDGPU_API int pdgpu_kernel_times(pdgpu_ctx *ctx, int32_t max_kernels, const char **names, double *ms,
                        int64_t *launches, int32_t *count);
 
+/* Peridynamic neighbour lists built WITHOUT ANY DEVICE ALLOCATION, for
+ * callers that cannot call cudaMalloc: a host whose device memory is held by
+ * another allocator (a framework's caching allocator that owns the GPU), or
+ * code that must not allocate or synchronise the device at that point (a
+ * latency-bound loop, or work that another component is capturing).  No
+ * counterpart in the reference (its kd-tree search is host code).
+ *
+ * Inputs and outputs are caller-owned DEVICE buffers: x (n_nodes*3 doubles,
+ * util::Point layout), particle (n_nodes particle ids), horizon (one per
+ * particle id); rowptr receives n_nodes+1 offsets and col up to col_capacity
+ * neighbour indices.  The sets equal pdgpu_build_pd_neighbors' (same
+ * particle, j != i, strict |x_i - x_j|^2 < horizon^2), rows ascending.
+ * Pass col = NULL to learn the size in *n_bonds.  Work runs on `stream`
+ * (a cudaStream_t, NULL = default stream); the call returns when done.
+ *
+ * Limits: n_nodes <= 262144.  Scratch is a 16 MiB static device array
+ * that every GPU loading this library keeps until the process exits; the
+ * first call on a device looks its address up (make that first call before
+ * any stream capture).  All calls share that array, so calls that overlap on
+ * the GPU race.  Errors come back as a code and a message in err. */
+PDGPU_API int pdgpu_build_neighbors_noalloc(const double *x, const uint32_t *particle,
+                                            const double *horizon, int64_t n_nodes, int32_t dim,
+                                            uint64_t *rowptr, uint32_t *col, int64_t col_capacity,
+                                            int64_t *n_bonds, void *stream, char *err,
+                                            size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,6 +23,7 @@ UNITS = [
     ("pdgpu_bonds_fp64.cu", ["--fmad=false"]),
     ("pdgpu_bonds_mixed.cu", []),
     ("pdgpu_mixed.cu", []),
+    ("pdgpu_noalloc.cu", ["--fmad=false"]),
     ("pdgpu_runtime.cu", []),
 ]
 
