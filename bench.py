@@ -54,32 +54,84 @@ def workload_config(args, sc):
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and throttle reasons polled every 5 ms through NVML while the
+    timed region runs (read-only queries; the device is found by PCI bus id,
+    so CUDA_VISIBLE_DEVICES remapping does not matter).  Falls back to
+    `nvidia-smi -lms 100` when NVML cannot be used."""
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device):
         self.device = device
+        self.samples = []       # (sm_mhz, max_mhz, set of reasons)
         self.proc = None
-        self.lines = []
+        self.nvml = None
+        self.stop = threading.Event()
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device),
-                                          "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
-                                          "-lms", "100"], stdout=subprocess.PIPE,
-                                         stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except OSError:
-            self.proc = None
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            p = torch.cuda.get_device_properties(self.device)
+            bus = "%08x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            self.max = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.nvml = pynvml
+            self.t = threading.Thread(target=self._poll, daemon=True)
+        except Exception:
+            self.nvml = None
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device),
+                                              "--query-gpu=" + self.Q,
+                                              "--format=csv,noheader,nounits", "-lms", "100"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                             text=True)
+                self.t = threading.Thread(target=self._read, daemon=True)
+            except OSError:
+                self.proc = None
+                return self
+        self.t.start()
         return self
 
+    def _poll(self):
+        nv = self.nvml
+        masks = [(n, getattr(nv, m)) for n, m in self.REASONS]
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((float(sm), float(self.max), {n for n, m in masks if r & m}))
+            except Exception:
+                pass
+            self.stop.wait(0.005)
+
     def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+        names = [n for n, _ in self.REASONS]
+        for ln in self.proc.stdout:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                self.samples.append((float(f[1]), float(f[2]),
+                                     {nm for k, nm in enumerate(names)
+                                      if f[5 + k].lower().startswith("active")}))
+            except ValueError:
+                continue
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml:
+            self.t.join(timeout=2)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -88,23 +140,12 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for k, nm in enumerate(names):
-                if f[5 + k].lower().startswith("active"):
-                    reasons.add(nm)
-        sm.sort()
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        sm = sorted(s[0] for s in self.samples)
+        reasons = set().union(*[s[2] for s in self.samples]) if self.samples else set()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None,
+                "sm_max_mhz": self.samples[-1][1] if self.samples else None,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml 5 ms" if self.nvml else "nvidia-smi 100 ms"}
 
 
 # ---------------------------------------------------------------------------

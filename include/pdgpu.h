@@ -262,9 +262,16 @@ PDGPU_API int pdgpu_sync(pdgpu_ctx *ctx);
 /* Copies a field into a caller buffer (blocking). */
 PDGPU_API int pdgpu_download(pdgpu_ctx *ctx, int32_t field, void *dst);
 
-/* Overwrites u, v or x from a caller buffer (blocking); used by the
+/* Overwrites u, v or x (N*3 doubles), or the bond state (PDGPU_FIELD_BONDS,
+ * uint8[B], 1 = broken), from a caller buffer (blocking); used by the
  * host-buffer step below and by restarts. */
 PDGPU_API int pdgpu_upload_field(pdgpu_ctx *ctx, int32_t field, const void *src);
+
+/* DEMModel::computePeridynamicForces (demModel.cpp:602-789) alone on the
+ * current state: the state-based pre-pass and the bond loop write the
+ * peridynamic force density f and damage Z and may break bonds; contact,
+ * damping and external forces are not added.  Blocking. */
+PDGPU_API int pdgpu_compute_pd_forces(pdgpu_ctx *ctx);
 
 /* One reference-facing step on host buffers, as a DEMModel::integrateStep
  * override that keeps ModelData on the host: uploads u, v, x from the caller

@@ -89,6 +89,7 @@ SIGNATURES = {
     "pdgpu_get_stream": [c_vp, P(c_vp)],
     "pdgpu_enable_timing": [c_vp, c_i32],
     "pdgpu_kernel_times": [c_vp, c_i32, P(ctypes.c_char_p), P(c_d), P(c_i64), P(c_i32)],
+    "pdgpu_compute_pd_forces": [c_vp],
     "pdgpu_build_neighbors_noalloc": [c_vp, c_vp, c_vp, c_i64, c_i32, c_vp, c_vp, c_i64, P(c_i64),
                                       c_vp, ctypes.c_char_p, ctypes.c_size_t],
 }

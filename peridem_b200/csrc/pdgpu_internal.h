@@ -26,6 +26,7 @@ enum : int {
   DEV_ERR_WALLPAIR_OVERFLOW = 2,
   DEV_ERR_CELL_OVERFLOW = 3,
   DEV_ERR_NONFINITE = 4,
+  DEV_ERR_STAGE_TIMEOUT = 5,  // a bond tile's bulk copies did not complete
 };
 
 struct DevParticle {
@@ -96,6 +97,13 @@ struct MixParticle {
   float k_force;   // RNP: 4 C beta / invFactor | PMB, PD elastic: c | PD state: unused
   float beta, rbar, factor_sc, s0;
   float K, G;
+  // util::isGreater(a, b) for a, b > 0 is a > b / (1 - 1e-5): thresholds
+  float low_thr;   // volume correction applies beyond it (horizon - h/2)
+  float fsc_thr;   // RNP: bond breaks when |S| sqrt(r) / rbar exceeds it
+  float s0_thr;    // PMB: bond breaks when |S| exceeds it (s0 + 1e-10)
+  float inv_rbar, inv_s0;  // damage Z = |S| / critical stretch
+  float j0, j1;    // influence J(r): j0 + j1 r (constant, linear) | j0 exp(j1 r^2) (Gaussian)
+  float tf_coef, am_coef;  // PD state: 3K - 5G and 15G
 };
 
 // One CTA of the tiled bond loop: nodes [node_begin, node_end) of one
@@ -104,6 +112,7 @@ struct BondTile {
   int32_t particle;
   int32_t pad;
   int64_t node_begin, node_end, win_begin, win_end;
+  int64_t bond_begin, bond_end;  // pd_row[node_begin], pd_row[node_end]
 };
 
 struct DevData {
@@ -210,7 +219,8 @@ void launch_pd_tiled_mixed(const DevData &d, const BondTile *tiles, int n_tiles,
 void launch_prepass_tiled_mixed(const DevData &d, const BondTile *tiles, int n_tiles, int lanes,
                                 size_t smem, cudaStream_t s);
 size_t tile_smem_fp64(int dim, bool state, int64_t window);
-size_t tile_smem_mixed(int dim, bool state, int64_t window);
+size_t tile_smem_mixed(int dim, bool state, int64_t window);       // state pre-pass
+size_t tile_smem_mixed_main(int dim, bool state, bool col16, const BondTile &t);
 int set_tile_smem_limit_fp64(int dim, size_t bytes);
 int set_tile_smem_limit_mixed(int dim, size_t bytes);
 void launch_contact_update(const DevData &d, void *scan_tmp, size_t scan_tmp_bytes, int lanes,

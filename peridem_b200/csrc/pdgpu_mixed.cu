@@ -38,6 +38,8 @@ __global__ void k_tile_windows(DevData d, BondTile *tiles) {
     }
     T.win_begin = lo;
     T.win_end = hi + 1;
+    T.bond_begin = d.pd_row[T.node_begin];
+    T.bond_end = d.pd_row[T.node_end];
   }
 }
 

@@ -20,6 +20,10 @@ namespace {
 
 constexpr int kMaxTimed = 64;
 constexpr int64_t kHistoryCap = 1 << 16;
+// tail padding of the bond arrays: the bond loop copies whole 16-byte
+// blocks of neighbour columns and bitmap words around each tile's range
+constexpr int64_t kBondPad = 16;
+constexpr int64_t kBitPad = 8;
 
 struct TimedLaunch {
   int slot;
@@ -62,7 +66,8 @@ struct pdgpu_ctx {
   // tiled bond loop
   BondTile *tiles = nullptr;
   int n_tiles = 0;
-  size_t tile_smem = 0, tile_smem_state = 0;
+  size_t tile_smem = 0, tile_smem_state = 0;  // pre-pass stage; FP64 bond loop with m_x, theta
+  size_t tile_smem_pd = 0;                     // the bond-loop launch
   int64_t tile_nodes = 0;  // nodes per tile (0 = chosen at set-up)
   bool state_prepass = false;
 
@@ -418,6 +423,9 @@ int device_error(pdgpu_ctx *ctx) {
       return fail(ctx, PDGPU_ERR_OVERFLOW,
                   "particle %lld has more particle-wall pairs than wall_pair_capacity=%d (step %lld)",
                   (long long)c.error_info, ctx->d.wp_cap, (long long)c.n);
+    case DEV_ERR_STAGE_TIMEOUT:
+      return fail(ctx, PDGPU_ERR_CUDA, "bond tile %lld: shared-memory bulk copies did not complete",
+                  (long long)c.error_info);
     case DEV_ERR_NONFINITE:
       return fail(ctx, PDGPU_ERR_NAN, "weighted volume of node %lld is too close to zero",
                   (long long)c.error_info);
@@ -444,6 +452,8 @@ int prepare_mixed(pdgpu_ctx *ctx) {
     M.inv_h = (float)(1.0 / P.h);
     M.rc = (float)P.rc;
     M.kn = (float)P.kn;
+    const double rel = 1.0 - 1.0e-5;  // util::isGreater's relative tolerance
+    M.low_thr = (float)(P.check_low / rel);
     switch (P.material) {
       case PDGPU_MAT_RNP:
         M.k_force = (float)(4.0 * P.mat[0] * P.mat[1] / P.mat[3]);
@@ -451,17 +461,36 @@ int prepare_mixed(pdgpu_ctx *ctx) {
         M.rbar = (float)P.mat[2];
         M.factor_sc = (float)P.mat[4];
         M.irreversible = P.mat[5] != 0.0;
+        M.inv_rbar = (float)(1.0 / P.mat[2]);
+        M.fsc_thr = (float)(P.mat[4] / rel);
         break;
       case PDGPU_MAT_PMB:
         M.k_force = (float)P.mat[0];
         M.s0 = (float)P.mat[1];
+        M.inv_s0 = (float)(1.0 / P.mat[1]);
+        M.s0_thr = (float)((P.mat[1] + 1.0e-10) / rel);
         break;
       case PDGPU_MAT_PDELASTIC: M.k_force = (float)P.mat[0]; break;
       default:
         M.K = (float)P.mat[0];
         M.G = (float)P.mat[1];
         M.s0 = (float)P.mat[2];
+        M.inv_s0 = (float)(1.0 / P.mat[2]);
+        M.tf_coef = (float)(3.0 * P.mat[0] - 5.0 * P.mat[1]);
+        M.am_coef = (float)(15.0 * P.mat[1]);
         break;
+    }
+    // influence function J(r / horizon) (material.h:273-288)
+    const double ih = 1.0 / P.horizon;
+    if (d.inf.type == PDGPU_INF_GAUSSIAN) {
+      M.j0 = (float)d.inf.p0;
+      M.j1 = (float)(-ih * ih / d.inf.p1);
+    } else if (d.inf.type == PDGPU_INF_LINEAR) {
+      M.j0 = (float)d.inf.p0;
+      M.j1 = (float)(d.inf.p1 * ih);
+    } else {
+      M.j0 = (float)d.inf.p0;
+      M.j1 = 0.f;
     }
     if (P.compute_force && P.end - P.start > 65536) fits16 = false;
   }
@@ -469,7 +498,7 @@ int prepare_mixed(pdgpu_ctx *ctx) {
   CK(cudaMemcpy(d.mixp, mp.data(), mp.size() * sizeof(MixParticle), cudaMemcpyHostToDevice));
   (void)N;
   d.use16 = fits16 ? 1 : 0;
-  if (fits16) TRY(dalloc(ctx, &d.pd_col16, d.n_bonds));
+  if (fits16) TRY(dalloc(ctx, &d.pd_col16, d.n_bonds + kBondPad));
   d.inf_p0 = (float)d.inf.p0;
   d.inf_p1 = (float)d.inf.p1;
   launch_mixed_setup(d, ctx->stream);
@@ -484,7 +513,7 @@ int prepare_mixed(pdgpu_ctx *ctx) {
 int prepare_tiles(pdgpu_ctx *ctx) {
   DevData &d = ctx->d;
   const bool mixed = d.precision == PDGPU_PREC_MIXED;
-  const size_t limit = 227 * 1024;
+  const size_t limit = 227 * 1024 - 1024;  // dynamic stage; static shared memory on top
   for (int64_t tn : {ctx->tile_nodes > 0 ? ctx->tile_nodes : (int64_t)(d.dim == 2 ? 128 : 96),
                      (int64_t)64, (int64_t)32, (int64_t)16}) {
     std::vector<BondTile> t;
@@ -519,16 +548,29 @@ int prepare_tiles(pdgpu_ctx *ctx) {
         return fail(ctx, PDGPU_ERR_STATE, "bond tile window [%lld, %lld) inconsistent with nodes [%lld, %lld)",
                     (long long)b.win_begin, (long long)b.win_end, (long long)b.node_begin,
                     (long long)b.node_end);
+      if (b.bond_begin < 0 || b.bond_end < b.bond_begin || b.bond_end > d.n_bonds)
+        return fail(ctx, PDGPU_ERR_STATE, "bond tile bonds [%lld, %lld) outside [0, %lld)",
+                    (long long)b.bond_begin, (long long)b.bond_end, (long long)d.n_bonds);
       wmax = std::max(wmax, b.win_end - b.win_begin);
     }
     const size_t sm = mixed ? tile_smem_mixed(d.dim, false, wmax) : tile_smem_fp64(d.dim, false, wmax);
     const size_t ss = mixed ? tile_smem_mixed(d.dim, true, wmax) : tile_smem_fp64(d.dim, true, wmax);
-    const size_t need = ctx->state_prepass ? ss : sm;
+    // bytes of the bond-loop launch: the FP64 form stages the window only;
+    // the mixed form also holds each tile's columns and bitmap words
+    size_t pd = ctx->state_prepass ? ss : sm;
+    if (mixed) {
+      pd = 0;
+      for (auto &b : t)
+        pd = std::max(pd, tile_smem_mixed_main(d.dim, ctx->hp[b.particle].material == PDGPU_MAT_PDSTATE,
+                                               d.use16 != 0, b));
+    }
+    const size_t need = std::max(pd, ctx->state_prepass ? sm : (size_t)0);
     if (need > limit) continue;
     const int rc = mixed ? set_tile_smem_limit_mixed(d.dim, need) : set_tile_smem_limit_fp64(d.dim, need);
     if (rc != 0) return fail(ctx, PDGPU_ERR_CUDA, "cannot raise the shared-memory limit to %zu bytes", need);
     ctx->tile_smem = sm;
     ctx->tile_smem_state = ss;
+    ctx->tile_smem_pd = pd;
     ctx->tile_nodes = tn;
     return PDGPU_OK;
   }
@@ -634,7 +676,9 @@ int prepare(pdgpu_ctx *ctx) {
 }
 
 // DEMModel::computeForces (demModel.cpp:462-600)
-void compute_forces(pdgpu_ctx *ctx) {
+// DEMModel::computePeridynamicForces (demModel.cpp:602-789): state pre-pass
+// and bond loop; writes f (peridynamic part) and Z, may break bonds
+void pd_forces(pdgpu_ctx *ctx) {
   DevData &d = ctx->d;
   cudaStream_t s = ctx->stream;
   const bool mixed = d.precision == PDGPU_PREC_MIXED;
@@ -648,7 +692,7 @@ void compute_forces(pdgpu_ctx *ctx) {
         launch_prepass_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
       });
   }
-  const size_t smem = ctx->state_prepass ? ctx->tile_smem_state : ctx->tile_smem;
+  const size_t smem = ctx->tile_smem_pd;
   if (mixed)
     run(ctx, "pd_force_mixed", [&] {
       launch_pd_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
@@ -657,6 +701,12 @@ void compute_forces(pdgpu_ctx *ctx) {
     run(ctx, "pd_force", [&] {
       launch_pd_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
     });
+}
+
+void compute_forces(pdgpu_ctx *ctx) {
+  DevData &d = ctx->d;
+  cudaStream_t s = ctx->stream;
+  pd_forces(ctx);
   if (ctx->desc.multi_particle) {
     run(ctx, "contact_update", [&] {
       launch_contact_rebuild(d, ctx->rebuild_bsum, ctx->rebuild_grid, ctx->contact_lanes, 0, s);
@@ -695,7 +745,7 @@ cudaError_t graph_step(pdgpu_ctx *ctx, cudaGraphConditionalHandle h, const char 
     if (mixed) launch_prepass_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
     else launch_prepass_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
   }
-  const size_t smem = ctx->state_prepass ? ctx->tile_smem_state : ctx->tile_smem;
+  const size_t smem = ctx->tile_smem_pd;
   if (mixed) launch_pd_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
   else launch_pd_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
   if (ctx->desc.multi_particle) {
@@ -1024,13 +1074,13 @@ int pdgpu_upload_pd_neighbors(pdgpu_ctx *ctx, const uint64_t *rowptr, const uint
     if (col[k] >= (uint64_t)N) return fail(ctx, PDGPU_ERR_ARG, "neighbour index out of range");
     c32[k] = (int32_t)col[k];
   }
-  std::vector<uint32_t> bits((B + 31) / 32 + 1, 0u);
+  std::vector<uint32_t> bits((B + 31) / 32 + kBitPad, 0u);
   if (bond_state)
     for (int64_t k = 0; k < B; k++)
       if (bond_state[k]) bits[k >> 5] |= 1u << (k & 31);
   d.n_bonds = B;
   TRY(dalloc(ctx, &d.pd_row, N + 1));
-  TRY(dalloc(ctx, &d.pd_col, B));
+  TRY(dalloc(ctx, &d.pd_col, B + kBondPad));
   TRY(dalloc(ctx, &d.bond_bits, bits.size()));
   CK(cudaMemcpy(d.pd_row, row.data(), (N + 1) * 8, cudaMemcpyHostToDevice));
   if (B) CK(cudaMemcpy(d.pd_col, c32.data(), B * 4, cudaMemcpyHostToDevice));
@@ -1066,15 +1116,15 @@ int pdgpu_build_pd_neighbors(pdgpu_ctx *ctx) {
   CK(cudaMemcpyAsync(&B, d.pd_row + N, 8, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   d.n_bonds = B;
-  TRY(dalloc(ctx, &d.pd_col, B));
+  TRY(dalloc(ctx, &d.pd_col, B + kBondPad));
   int32_t *tmp;
   TRY(dalloc(ctx, &tmp, B));
   launch_build_pd(d, hmax, d.pd_row, tmp, ctx->scan_tmp, ctx->scan_bytes, 1, ctx->stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   dfree(ctx, tmp);
-  TRY(dalloc(ctx, &d.bond_bits, (B + 31) / 32 + 1));
-  CK(cudaMemset(d.bond_bits, 0, ((B + 31) / 32 + 1) * 4));
+  TRY(dalloc(ctx, &d.bond_bits, (B + 31) / 32 + kBitPad));
+  CK(cudaMemset(d.bond_bits, 0, ((B + 31) / 32 + kBitPad) * 4));
   CtrlState z{};
   CK(cudaMemcpy(d.ctrl, &z, sizeof z, cudaMemcpyHostToDevice));
   ctx->bonds = true;
@@ -1250,11 +1300,30 @@ int pdgpu_download(pdgpu_ctx *ctx, int32_t field, void *dst) {
   return PDGPU_OK;
 }
 
+int pdgpu_compute_pd_forces(pdgpu_ctx *ctx) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  TRY(prepare(ctx));
+  pd_forces(ctx);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return device_error(ctx);
+}
+
 int pdgpu_upload_field(pdgpu_ctx *ctx, int32_t field, const void *src) {
   if (!ctx || !src) return PDGPU_ERR_ARG;
   DevData &d = ctx->d;
+  if (field == PDGPU_FIELD_BONDS) {
+    if (!ctx->bonds) return fail(ctx, PDGPU_ERR_STATE, "upload the neighbour lists first");
+    const uint8_t *b = static_cast<const uint8_t *>(src);
+    std::vector<uint32_t> bits((d.n_bonds + 31) / 32 + kBitPad, 0u);
+    for (int64_t k = 0; k < d.n_bonds; k++)
+      if (b[k]) bits[k >> 5] |= 1u << (k & 31);
+    CK(cudaMemcpyAsync(d.bond_bits, bits.data(), bits.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PDGPU_OK;
+  }
   double *vec = field == PDGPU_FIELD_X ? d.x : field == PDGPU_FIELD_U ? d.u : field == PDGPU_FIELD_V ? d.v : nullptr;
-  if (!vec) return fail(ctx, PDGPU_ERR_ARG, "upload_field: only x, u, v can be written");
+  if (!vec) return fail(ctx, PDGPU_ERR_ARG, "upload_field: only x, u, v and bonds can be written");
   CK(cudaMemcpyAsync(ctx->stage, src, (size_t)3 * d.n_nodes * 8, cudaMemcpyHostToDevice, ctx->stream));
   launch_pack_vec(d, ctx->stage, vec, ctx->stream);
   CK(cudaGetLastError());

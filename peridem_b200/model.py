@@ -335,6 +335,22 @@ class GpuDEMModel:
         self._check(self.lib.pdgpu_kernel_times(self.ctx, 64, names, ms, cnt, ctypes.byref(n)))
         return {names[i].decode(): (ms[i], cnt[i]) for i in range(n.value)}
 
+    def set_field(self, name: str, values: np.ndarray) -> None:
+        """Overwrite x, u, v ([N, 3] float64) or the bond state ("bonds",
+        uint8 per bond, 1 = broken) (pdgpu_upload_field)."""
+        if name == "bonds":
+            a = np.ascontiguousarray(values, dtype=np.uint8)
+            ptr = a.ctypes.data_as(ctypes.c_void_p)
+        else:
+            a = np.ascontiguousarray(values, dtype=np.float64).reshape(self.scene.n_nodes, 3)
+            ptr = a.ctypes.data_as(ctypes.c_void_p)
+        self._check(self.lib.pdgpu_upload_field(self.ctx, FIELD[name], ptr))
+
+    def compute_pd_forces(self) -> None:
+        """DEMModel::computePeridynamicForces alone on the current state
+        (pdgpu_compute_pd_forces): peridynamic f and Z, bonds may break."""
+        self._check(self.lib.pdgpu_compute_pd_forces(self.ctx))
+
     def step_host(self, u: np.ndarray, v: np.ndarray, x: np.ndarray, f: np.ndarray,
                   nsteps: int = 1) -> None:
         """One reference-facing step on host buffers (pdgpu_step_host)."""
