@@ -47,7 +47,8 @@ def workload_config(args, sc):
             "nodes": int(sc.n_nodes) if sc is not None else None,
             "particles": args.particles, "dt": sc.dt if sc is not None else None,
             "precision": args.precision, "l2": "flushed between timed steps (512 MiB write)",
-            "graph_steps_per_launch": args.graph_steps}
+            "graph_steps_per_launch": args.graph_steps,
+            "pd_lanes": args.pd_lanes or "auto", "tile_nodes": args.tile_nodes or "auto"}
 
 
 # ---------------------------------------------------------------------------
@@ -206,7 +207,8 @@ def run_ours(args, rank, world):
     spec = workload_spec(args)
     sc = scn.build_scene(spec)
     prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
-    model = GpuDEMModel(sc, precision=prec, device=dev, build_neighbors=True, compute_mx=True)
+    model = GpuDEMModel(sc, precision=prec, device=dev, build_neighbors=True, compute_mx=True,
+                        pd_lanes=args.pd_lanes, tile_nodes=args.tile_nodes)
     rp, col = model.pd_neighbors()
     sc.pd_rowptr, sc.pd_col = rp, col
     model.integrate_begin()
@@ -343,6 +345,8 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--graph-steps", type=int, default=1)
     ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--pd-lanes", type=int, default=0, help="lanes per node in the bond loop (0 = auto)")
+    ap.add_argument("--tile-nodes", type=int, default=0, help="nodes per bond-loop tile (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 

@@ -297,9 +297,14 @@ PDGPU_API int pdgpu_num_bonds(pdgpu_ctx *ctx, int64_t *n_bonds);
 PDGPU_API int pdgpu_download_pd_neighbors(pdgpu_ctx *ctx, uint64_t *rowptr, uint64_t *col);
 
 /* Launch shape of the bond loop and the contact kernel: lanes per node
- * (4, 8, 16 or 32 for the bond loop; 4, 8 or 32 for contact); 0 keeps the
- * current choice.  Set before the first step. */
+ * (4, 8, 16 or 32 for the bond loop, also 1 or 2 in the mixed form; 4, 8 or
+ * 32 for contact); 0 keeps the current choice.  Set before the first step. */
 PDGPU_API int pdgpu_set_tuning(pdgpu_ctx *ctx, int32_t pd_lanes, int32_t contact_lanes);
+
+/* Nodes per bond-loop tile (one CTA each); 0 = automatic.  Set before the
+ * first step; tiles shrink by themselves when a window outgrows shared
+ * memory. */
+PDGPU_API int pdgpu_set_tile_nodes(pdgpu_ctx *ctx, int32_t nodes);
 
 /* The context's CUDA stream (a cudaStream_t) for callers that time work. */
 PDGPU_API int pdgpu_get_stream(pdgpu_ctx *ctx, void **stream);

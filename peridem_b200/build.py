@@ -21,7 +21,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("pdgpu_kernels.cu", ["--fmad=false"]),
     ("pdgpu_bonds_fp64.cu", ["--fmad=false"]),
-    ("pdgpu_bonds_mixed.cu", []),
+    ("pdgpu_bonds_mixed.cu", ["-ftz=true"]),
     ("pdgpu_mixed.cu", []),
     ("pdgpu_noalloc.cu", ["--fmad=false"]),
     ("pdgpu_runtime.cu", []),

@@ -73,28 +73,33 @@ __device__ __forceinline__ bool bar_wait(uint64_t *bar) {
 }
 
 // Shared-memory plan of one tile (byte offsets into the dynamic stage);
-// identical on host and device.
+// identical on host and device.  Bulk-copied regions start and end on 16-byte
+// boundaries of the global arrays, which carry tail padding for that.
 struct Plan {
-  int64_t col0;      // first column entry copied (16-byte aligned)
-  int64_t word0;     // first bitmap word copied (16-byte aligned)
-  uint32_t col_bytes, bit_bytes;
-  uint32_t off_a, off_b, off_m, total;
+  int64_t col0;   // first column entry copied
+  int64_t word0;  // first bitmap word copied
+  int64_t row0;   // first row offset copied (pd_row)
+  uint32_t col_bytes, bit_bytes, row_bytes;
+  uint32_t off_row, off_xv, off_u, off_m, total;
 };
 
 __host__ __device__ inline Plan plan(int dim, bool state, int col_size, int64_t kb, int64_t ke,
-                                     int64_t w) {
+                                     int64_t nb, int64_t ne, int64_t w) {
   Plan p;
   const int64_t per16 = 16 / col_size;
   p.col0 = kb / per16 * per16;
   const int64_t col1 = (ke + per16 - 1) / per16 * per16;
   p.word0 = (kb >> 5) / 4 * 4;
   const int64_t word1 = (((ke + 31) >> 5) + 3) / 4 * 4;
+  p.row0 = nb / 2 * 2;
+  const int64_t row1 = (ne + 1 + 1) / 2 * 2;  // rows nb .. ne inclusive
   p.col_bytes = (uint32_t)((col1 - p.col0) * col_size);
   p.bit_bytes = (uint32_t)((word1 - p.word0) * 4);
-  p.off_a = p.col_bytes + p.bit_bytes;                       // float4 records
-  p.off_b = p.off_a + (uint32_t)(16 * w);                    // 2-D: float vol | 3-D: float4 u
-  p.off_m = p.off_b + (uint32_t)((dim == 2 ? 4 : 16) * w);   // state: float2 per node
-  p.off_m = (p.off_m + 15) / 16 * 16;
+  p.row_bytes = (uint32_t)((row1 - p.row0) * 8);
+  p.off_row = p.col_bytes + p.bit_bytes;
+  p.off_xv = p.off_row + p.row_bytes;                        // float4 {x, y, z, vol}
+  p.off_u = p.off_xv + (uint32_t)(16 * w);                   // 2-D float2 | 3-D float4 u
+  p.off_m = p.off_u + (uint32_t)((dim == 2 ? 8 : 16) * w);   // state: float2 per node
   p.total = p.off_m + (state ? (uint32_t)(8 * w) : 0u);
   p.total = (p.total + 15) / 16 * 16;
   return p;
@@ -105,22 +110,21 @@ enum { LAW_RNP = 0, LAW_PMB = 1, LAW_ELASTIC = 2, LAW_STATE = 3 };
 // node-side view of the stage
 template <int DIM>
 struct View {
-  const float4 *a;   // 2-D {x, y, ux, uy} | 3-D {x, y, z, vol}
-  const float *vol;  // 2-D volumes
-  const float4 *b;   // 3-D {ux, uy, uz, 0}
+  const float4 *xv;  // {x, y, z, vol}, reference coordinates relative to the particle centre
+  const float2 *u2;  // 2-D displacement relative to the centre's
+  const float4 *u4;  // 3-D displacement relative to the centre's
   const float2 *m;   // state: {theta (3K - 5G) / m_x, 15 G / m_x}
 
   __device__ __forceinline__ void node(int l, float (&x)[3], float (&u)[3], float &v) const {
-    const float4 p = a[l];
+    const float4 p = xv[l];
+    x[0] = p.x, x[1] = p.y, x[2] = p.z;
+    v = p.w;
     if constexpr (DIM == 2) {
-      x[0] = p.x, x[1] = p.y, x[2] = 0.f;
-      u[0] = p.z, u[1] = p.w, u[2] = 0.f;
-      v = vol[l];
+      const float2 q = u2[l];
+      u[0] = q.x, u[1] = q.y, u[2] = 0.f;
     } else {
-      const float4 q = b[l];
-      x[0] = p.x, x[1] = p.y, x[2] = p.z;
+      const float4 q = u4[l];
       u[0] = q.x, u[1] = q.y, u[2] = q.z;
-      v = p.w;
     }
   }
 };
@@ -132,90 +136,97 @@ __device__ __forceinline__ float dot(const float (&a)[3], const float (&b)[3]) {
   return s;
 }
 
-// the bond loop of one node for one material law; returns the force sum of
-// this lane's bonds and their largest |stretch / critical stretch|
-template <int DIM, int LPN, int LAW, typename CT>
-__device__ __forceinline__ void node_bonds(const DevData &d, const MixParticle &M, const View<DIM> &V,
-                                           const CT *s_col, const uint32_t *s_bits, int k0, int k1,
-                                           int col_off, int bit_off, int shift, int64_t kb, int li,
-                                           float (&F)[3], float &zmax) {
-  const int lane = threadIdx.x % LPN;
-  float xi[3], ui[3], vi;
-  V.node(li, xi, ui, vi);
-  float2 mi = make_float2(0.f, 0.f);
-  if constexpr (LAW == LAW_STATE) mi = V.m[li];
-  const bool gauss = d.inf.type == PDGPU_INF_GAUSSIAN;
-#pragma unroll 2
-  for (int k = k0 + lane; k < k1; k += LPN) {
-    const int lj = (int)s_col[k + col_off] + shift;
-    const int b = k + bit_off;
-    const bool broken = (s_bits[b >> 5] >> (b & 31)) & 1u;
-    float xj[3], uj[3], volj;
-    V.node(lj, xj, uj, volj);
-    float dx[3], du[3], y[3];
+__device__ __forceinline__ float ex2(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// One bond (i, j) of node i for one material law.  zq tracks the damage
+// measure in a monotone form: RNP S^2 r (Z = sqrt(zq) / rbar), the others
+// |S| (Z = zq / s0).  `broken` is the bond's state before this step.
+template <int DIM, int LAW, bool BROKEN_KNOWN_CLEAR>
+__device__ __forceinline__ void bond(const DevData &d, const MixParticle &M, const View<DIM> &V,
+                                     const float (&xi)[3], const float (&ui)[3], float2 mi, int lj,
+                                     bool broken, bool gauss, int64_t kglob, float (&F)[3],
+                                     float &zmax) {
+  float xj[3], uj[3], volj;
+  V.node(lj, xj, uj, volj);
+  float dx[3], du[3], y[3];
 #pragma unroll
-    for (int q = 0; q < 3; q++) {
-      dx[q] = xj[q] - xi[q];
-      du[q] = uj[q] - ui[q];
-      y[q] = dx[q] + du[q];
-    }
-    const float r2 = dot<DIM>(dx, dx);
-    const float inv_r = rsqrtf(r2);
-    const float rji = r2 * inv_r;
-    const float dxdu = dot<DIM>(dx, du);
-    float S, z, inv_ly = 0.f;
-    if constexpr (LAW == LAW_RNP) {
-      // linearised stretch; critical stretch rbar / sqrt(r)
-      S = dxdu * inv_r * inv_r;
-      z = fabsf(S) * rsqrtf(inv_r) * M.inv_rbar;
-    } else {
-      const float y2 = dot<DIM>(y, y);
-      inv_ly = rsqrtf(y2);
-      const float ly = y2 * inv_ly;
-      // (|y| - r) / r without cancellation
-      S = __fdividef(2.f * dxdu + dot<DIM>(du, du), rji * (ly + rji));
-      z = fabsf(S) * M.inv_s0;
-    }
-    zmax = fmaxf(zmax, z);
-    if (!broken) {
-      const float vol = rji > M.low_thr ? volj * (M.check_up - rji) * M.inv_h : volj;
-      const float J = gauss ? M.j0 * __expf(rji * rji * M.j1) : M.j0 + M.j1 * rji;
-      float sf = 0.f;
-      if constexpr (LAW == LAW_RNP) {
-        if (M.irreversible && z > M.fsc_thr) {
-          atomicOr(d.bond_bits + ((kb + k) >> 5), 1u << ((kb + k) & 31));
-        } else {
-          sf = J * M.k_force * S * __expf(-M.beta * rji * S * S) * vol * inv_r;
-        }
-      } else if constexpr (LAW == LAW_PMB) {
-        if (fabsf(S) > M.s0_thr) {
-          atomicOr(d.bond_bits + ((kb + k) >> 5), 1u << ((kb + k) & 31));
-        } else {
-          sf = J * M.k_force * S * vol * inv_ly;
-        }
-      } else if constexpr (LAW == LAW_ELASTIC) {
-        sf = J * M.k_force * S * vol * inv_ly;
-      } else {
-        const float2 mj = V.m[lj];
-        sf = J * rji * ((mi.x + mj.x) + S * (mi.y + mj.y)) * vol * inv_ly;
-      }
-      // bond-based RNP acts along the reference bond, the others along y
-#pragma unroll
-      for (int q = 0; q < DIM; q++) F[q] += sf * (LAW == LAW_RNP ? dx[q] : y[q]);
-    } else {
-      // broken bond: short-range repulsion between the two nodes
-      const float inv_R = rsqrtf(dot<DIM>(y, y));
-      const float sf = fminf(M.kn * volj * (1.f - M.rc * inv_R), 0.f);
-#pragma unroll
-      for (int q = 0; q < DIM; q++) F[q] += sf * y[q];
-    }
+  for (int q = 0; q < 3; q++) {
+    dx[q] = xj[q] - xi[q];
+    du[q] = uj[q] - ui[q];
+    y[q] = dx[q] + du[q];
   }
+  const float r2 = dot<DIM>(dx, dx);
+  const float inv_r = rsqrtf(r2);
+  const float rji = r2 * inv_r;
+  const float dxdu = dot<DIM>(dx, du);
+  float S, zq, inv_ly = 0.f;
+  if constexpr (LAW == LAW_RNP) {
+    S = dxdu * (inv_r * inv_r);  // linearised stretch
+    zq = S * S * rji;
+  } else {
+    const float y2 = dot<DIM>(y, y);
+    inv_ly = rsqrtf(y2);
+    const float ly = y2 * inv_ly;
+    S = __fdividef(2.f * dxdu + dot<DIM>(du, du), rji * (ly + rji));  // (|y| - r) / r
+    zq = fabsf(S);
+  }
+  zmax = fmaxf(zmax, zq);
+  if (BROKEN_KNOWN_CLEAR || !broken) {
+    const float vol = volj * (rji > M.low_thr ? fmaf(-rji, M.inv_h, M.cu_h) : 1.f);
+    // influence times the law's constant
+    const float kJ = gauss ? M.kj0 * ex2(rji * rji * M.j1) : fmaf(M.kj1, rji, M.kj0);
+    float sf = 0.f;
+    if constexpr (LAW == LAW_RNP) {
+      if (M.irreversible && zq > M.fsc_q)
+        atomicOr(d.bond_bits + (kglob >> 5), 1u << (kglob & 31));
+      else
+        sf = kJ * S * ex2(M.nbeta_l2e * zq) * vol * inv_r;
+    } else if constexpr (LAW == LAW_PMB) {
+      if (zq > M.s0_thr)
+        atomicOr(d.bond_bits + (kglob >> 5), 1u << (kglob & 31));
+      else
+        sf = kJ * S * vol * inv_ly;
+    } else if constexpr (LAW == LAW_ELASTIC) {
+      sf = kJ * S * vol * inv_ly;
+    } else {
+      const float2 mj = V.m[lj];
+      sf = kJ * rji * ((mi.x + mj.x) + S * (mi.y + mj.y)) * vol * inv_ly;
+    }
+    // bond-based RNP acts along the reference bond, the others along y
+#pragma unroll
+    for (int q = 0; q < DIM; q++) F[q] += sf * (LAW == LAW_RNP ? dx[q] : y[q]);
+  } else {
+    // broken bond: short-range repulsion between the two nodes
+    const float inv_R = rsqrtf(dot<DIM>(y, y));
+    const float sf = fminf(M.kn * volj * (1.f - M.rc * inv_R), 0.f);
+#pragma unroll
+    for (int q = 0; q < DIM; q++) F[q] += sf * y[q];
+  }
+}
+
+// does any bond of [b0, b1) (bit positions in the staged bitmap) start broken?
+template <int LPN>
+__device__ __forceinline__ bool any_broken(const uint32_t *s_bits, int b0, int b1, unsigned gm) {
+  const int lane = threadIdx.x % LPN;
+  const int w0 = b0 >> 5, w1 = (b1 - 1) >> 5;
+  bool hit = false;
+  for (int w = w0 + lane; w <= w1; w += LPN) {
+    uint32_t m = s_bits[w];
+    if (w == w0) m &= ~0u << (b0 & 31);
+    if (w == w1) m &= ~0u >> (31 - ((b1 - 1) & 31));
+    hit |= m != 0u;
+  }
+  return __any_sync(gm, hit);
 }
 
 template <int DIM, int LPN, int LAW, typename CT>
 __device__ __forceinline__ void tile_nodes(const DevData &d, const BondTile &T, const MixParticle &M,
                                            const View<DIM> &V, const CT *s_col, const uint32_t *s_bits,
-                                           const Plan &p) {
+                                           const int64_t *s_row, const Plan &p) {
   const int lane = threadIdx.x % LPN;
   const unsigned gm = gmask<LPN>();
   const int st = DIM == 2 ? 2 : 4;
@@ -223,84 +234,92 @@ __device__ __forceinline__ void tile_nodes(const DevData &d, const BondTile &T, 
   const int col_off = (int)(kb - p.col0);
   const int bit_off = (int)(kb - 32 * p.word0);
   const int shift = sizeof(CT) == 2 ? (int)(M.start - T.win_begin) : (int)(-T.win_begin);
+  const bool gauss = d.inf.type == PDGPU_INF_GAUSSIAN;
+  // every node of a tile computes forces (tiles cover force-computing particles only)
   for (int64_t i = T.node_begin + threadIdx.x / LPN; i < T.node_end; i += kThreads / LPN) {
-    if (!(d.flags[i] & NODE_ACTIVE)) {
-      if (lane == 0)
-        for (int q = 0; q < DIM; q++) d.f[st * i + q] = 0.0;
-      continue;
-    }
-    const int k0 = (int)(d.pd_row[i] - kb), k1 = (int)(d.pd_row[i + 1] - kb);
+    const int k0 = (int)(s_row[i - p.row0] - kb), k1 = (int)(s_row[i + 1 - p.row0] - kb);
+    const int li = (int)(i - T.win_begin);
+    float xi[3], ui[3], vi;
+    V.node(li, xi, ui, vi);
+    float2 mi = make_float2(0.f, 0.f);
+    if constexpr (LAW == LAW_STATE) mi = V.m[li];
     float F[3] = {0.f, 0.f, 0.f};
     float zmax = 0.f;
-    node_bonds<DIM, LPN, LAW, CT>(d, M, V, s_col, s_bits, k0, k1, col_off, bit_off, shift, kb,
-                                  (int)(i - T.win_begin), F, zmax);
+    if (!any_broken<LPN>(s_bits, k0 + bit_off, k1 + bit_off, gm)) {
+      // no bond of this node starts broken: no per-bond state test
+#pragma unroll 2
+      for (int k = k0 + lane; k < k1; k += LPN)
+        bond<DIM, LAW, true>(d, M, V, xi, ui, mi, (int)s_col[k + col_off] + shift, false, gauss,
+                             kb + k, F, zmax);
+    } else {
+      for (int k = k0 + lane; k < k1; k += LPN) {
+        const int b = k + bit_off;
+        const bool broken = (s_bits[b >> 5] >> (b & 31)) & 1u;
+        bond<DIM, LAW, false>(d, M, V, xi, ui, mi, (int)s_col[k + col_off] + shift, broken, gauss,
+                              kb + k, F, zmax);
+      }
+    }
     const double Fx = gsum<LPN>((double)F[0], gm);
     const double Fy = gsum<LPN>((double)F[1], gm);
     const double Fz = DIM == 3 ? gsum<LPN>((double)F[2], gm) : 0.0;
-    const float Z = gmax<LPN>(zmax, gm);
+    const float zq = gmax<LPN>(zmax, gm);
     if (lane == 0) {
       d.f[st * i] = Fx;
       d.f[st * i + 1] = Fy;
       if constexpr (DIM == 3) d.f[st * i + 2] = Fz;
-      d.Z[i] = Z;
+      d.Z[i] = LAW == LAW_RNP ? sqrtf(zq) * M.inv_rbar : zq * M.inv_s0;
     }
   }
 }
 
-template <int DIM, int LPN, typename CT>
+template <int DIM, int LPN, int LAW, typename CT>
 __global__ void __launch_bounds__(kThreads) k_bonds_mixed(DevData d, const BondTile *tiles, const CT *col) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   if (d.ctrl->error) return;
   const BondTile T = tiles[blockIdx.x];
-  const MixParticle M = d.mixp[T.particle];
-  const bool state = M.material == PDGPU_MAT_PDSTATE;
+  constexpr bool state = LAW == LAW_STATE;
   const int w = (int)(T.win_end - T.win_begin);
-  const Plan p = plan(DIM, state, (int)sizeof(CT), T.bond_begin, T.bond_end, w);
+  const Plan p = plan(DIM, state, (int)sizeof(CT), T.bond_begin, T.bond_end, T.node_begin, T.node_end, w);
   CT *s_col = reinterpret_cast<CT *>(smem);
   uint32_t *s_bits = reinterpret_cast<uint32_t *>(smem + p.col_bytes);
+  int64_t *s_row = reinterpret_cast<int64_t *>(smem + p.off_row);
+  float4 *s_xv = reinterpret_cast<float4 *>(smem + p.off_xv);
+  float2 *s_u2 = reinterpret_cast<float2 *>(smem + p.off_u);
+  float4 *s_u4 = reinterpret_cast<float4 *>(smem + p.off_u);
+  float2 *s_m = reinterpret_cast<float2 *>(smem + p.off_m);
 
-  // columns and bitmap words of the tile's bonds: bulk copies
+  // columns, bitmap words, row offsets and constant node records of the
+  // tile: bulk copies
   if (threadIdx.x == 0) {
     bar_init(&bar);
-    bar_arrive_tx(&bar, p.col_bytes + p.bit_bytes);
+    bar_arrive_tx(&bar, p.col_bytes + p.bit_bytes + p.row_bytes + 16u * (uint32_t)w);
     if (p.col_bytes) bulk_load(s_col, col + p.col0, p.col_bytes, &bar);
     if (p.bit_bytes) bulk_load(s_bits, d.bond_bits + p.word0, p.bit_bytes, &bar);
+    bulk_load(s_row, d.pd_row + p.row0, p.row_bytes, &bar);
+    bulk_load(s_xv, d.xv_mixed + T.win_begin, 16u * (uint32_t)w, &bar);
   }
+  const MixParticle M = d.mixp[T.particle];
 
-  // neighbour window: packed FP32 records relative to the particle centre
-  float4 *sa4 = reinterpret_cast<float4 *>(smem + p.off_a);
-  float *svol = reinterpret_cast<float *>(smem + p.off_b);
-  float4 *sb4 = reinterpret_cast<float4 *>(smem + p.off_b);
-  float2 *sm2 = reinterpret_cast<float2 *>(smem + p.off_m);
+  // displacements of the window relative to the particle centre's
   {
     const int st = DIM == 2 ? 2 : 4;
-    const DevParticle &P = d.particles[T.particle];
-    double xc[DIM], uc[DIM];
+    double uc[DIM];
 #pragma unroll
-    for (int q = 0; q < DIM; q++) {
-      xc[q] = d.xref[st * P.center + q];
-      uc[q] = d.u[st * P.center + q];
-    }
+    for (int q = 0; q < DIM; q++) uc[q] = d.u[st * T.center + q];
     for (int a = threadIdx.x; a < w; a += kThreads) {
       const int64_t j = T.win_begin + a;
-      float xr[DIM], ur[DIM];
-#pragma unroll
-      for (int q = 0; q < DIM; q++) {
-        xr[q] = (float)(__ldg(d.xref + st * j + q) - xc[q]);
-        ur[q] = (float)(d.u[st * j + q] - uc[q]);
-      }
-      const float vj = (float)__ldg(d.vol + j);
       if constexpr (DIM == 2) {
-        sa4[a] = make_float4(xr[0], xr[1], ur[0], ur[1]);
-        svol[a] = vj;
+        const double2 uj = *reinterpret_cast<const double2 *>(d.u + 2 * j);
+        s_u2[a] = make_float2((float)(uj.x - uc[0]), (float)(uj.y - uc[1]));
       } else {
-        sa4[a] = make_float4(xr[0], xr[1], xr[2], vj);
-        sb4[a] = make_float4(ur[0], ur[1], ur[2], 0.f);
+        const double2 u01 = *reinterpret_cast<const double2 *>(d.u + 4 * j);
+        const double u2 = d.u[4 * j + 2];
+        s_u4[a] = make_float4((float)(u01.x - uc[0]), (float)(u01.y - uc[1]), (float)(u2 - uc[2]), 0.f);
       }
       if (state) {
         const double inv_m = 1.0 / d.mx[j];
-        sm2[a] = make_float2((float)(d.theta[j] * M.tf_coef * inv_m), (float)(M.am_coef * inv_m));
+        s_m[a] = make_float2((float)(d.theta[j] * M.tf_coef * inv_m), (float)(M.am_coef * inv_m));
       }
     }
   }
@@ -314,23 +333,37 @@ __global__ void __launch_bounds__(kThreads) k_bonds_mixed(DevData d, const BondT
     return;
   }
 
-  View<DIM> V{sa4, svol, sb4, sm2};
-  switch (M.material) {
-    case PDGPU_MAT_RNP: tile_nodes<DIM, LPN, LAW_RNP, CT>(d, T, M, V, s_col, s_bits, p); break;
-    case PDGPU_MAT_PMB: tile_nodes<DIM, LPN, LAW_PMB, CT>(d, T, M, V, s_col, s_bits, p); break;
-    case PDGPU_MAT_PDELASTIC: tile_nodes<DIM, LPN, LAW_ELASTIC, CT>(d, T, M, V, s_col, s_bits, p); break;
-    default: tile_nodes<DIM, LPN, LAW_STATE, CT>(d, T, M, V, s_col, s_bits, p); break;
+  View<DIM> V{s_xv, s_u2, s_u4, s_m};
+  tile_nodes<DIM, LPN, LAW, CT>(d, T, M, V, s_col, s_bits, s_row, p);
+}
+
+template <int DIM, int LAW, typename CT>
+void launch_law(const DevData &d, const CT *col, const BondTile *t, int n, int lanes, size_t smem,
+                cudaStream_t s) {
+  switch (lanes) {
+    case 1: k_bonds_mixed<DIM, 1, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
+    case 2: k_bonds_mixed<DIM, 2, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
+    case 4: k_bonds_mixed<DIM, 4, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
+    case 8: k_bonds_mixed<DIM, 8, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
+    case 16: k_bonds_mixed<DIM, 16, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
+    default: k_bonds_mixed<DIM, 32, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
   }
 }
 
+// one launch per material law present, each over its run of the tile list
+// (the tiles are ordered by law)
 template <int DIM, typename CT>
-void launch_dim(const DevData &d, const CT *col, const BondTile *t, int n, int lanes, size_t smem,
-                cudaStream_t s) {
-  switch (lanes) {
-    case 4: k_bonds_mixed<DIM, 4, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
-    case 8: k_bonds_mixed<DIM, 8, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
-    case 16: k_bonds_mixed<DIM, 16, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
-    default: k_bonds_mixed<DIM, 32, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
+void launch_dim(const DevData &d, const CT *col, const BondTile *t, const int *law_begin, int lanes,
+                size_t smem, cudaStream_t s) {
+  for (int law = 0; law < 4; law++) {
+    const int b = law_begin[law], n = law_begin[law + 1] - b;
+    if (n <= 0) continue;
+    switch (law) {
+      case PDGPU_MAT_RNP: launch_law<DIM, LAW_RNP>(d, col, t + b, n, lanes, smem, s); break;
+      case PDGPU_MAT_PMB: launch_law<DIM, LAW_PMB>(d, col, t + b, n, lanes, smem, s); break;
+      case PDGPU_MAT_PDELASTIC: launch_law<DIM, LAW_ELASTIC>(d, col, t + b, n, lanes, smem, s); break;
+      default: launch_law<DIM, LAW_STATE>(d, col, t + b, n, lanes, smem, s); break;
+    }
   }
 }
 
@@ -338,6 +371,8 @@ template <int DIM>
 void launch_pre(const DevData &d, const BondTile *t, int n, int lanes, size_t smem, cudaStream_t s) {
   using namespace bonds_mixed;
   switch (lanes) {
+    case 1: k_prepass_tiled<DIM, 1><<<n, kTileThreads, smem, s>>>(d, t); break;
+    case 2: k_prepass_tiled<DIM, 2><<<n, kTileThreads, smem, s>>>(d, t); break;
     case 4: k_prepass_tiled<DIM, 4><<<n, kTileThreads, smem, s>>>(d, t); break;
     case 8: k_prepass_tiled<DIM, 8><<<n, kTileThreads, smem, s>>>(d, t); break;
     case 16: k_prepass_tiled<DIM, 16><<<n, kTileThreads, smem, s>>>(d, t); break;
@@ -345,34 +380,44 @@ void launch_pre(const DevData &d, const BondTile *t, int n, int lanes, size_t sm
   }
 }
 
+template <int DIM, int LAW, typename CT>
+bool set_law_limit(size_t bytes) {
+  const void *fs[] = {(const void *)k_bonds_mixed<DIM, 1, LAW, CT>, (const void *)k_bonds_mixed<DIM, 2, LAW, CT>,
+                      (const void *)k_bonds_mixed<DIM, 4, LAW, CT>, (const void *)k_bonds_mixed<DIM, 8, LAW, CT>,
+                      (const void *)k_bonds_mixed<DIM, 16, LAW, CT>, (const void *)k_bonds_mixed<DIM, 32, LAW, CT>};
+  for (auto f : fs)
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+      return false;
+  return true;
+}
+
 template <int DIM>
 int set_limit(size_t bytes) {
   using bonds_mixed::k_prepass_tiled;
-  const void *fs[] = {
-      (const void *)k_bonds_mixed<DIM, 4, uint16_t>,  (const void *)k_bonds_mixed<DIM, 8, uint16_t>,
-      (const void *)k_bonds_mixed<DIM, 16, uint16_t>, (const void *)k_bonds_mixed<DIM, 32, uint16_t>,
-      (const void *)k_bonds_mixed<DIM, 4, int32_t>,   (const void *)k_bonds_mixed<DIM, 8, int32_t>,
-      (const void *)k_bonds_mixed<DIM, 16, int32_t>,  (const void *)k_bonds_mixed<DIM, 32, int32_t>,
-      (const void *)k_prepass_tiled<DIM, 4>,          (const void *)k_prepass_tiled<DIM, 8>,
-      (const void *)k_prepass_tiled<DIM, 16>,         (const void *)k_prepass_tiled<DIM, 32>};
+  const void *fs[] = {(const void *)k_prepass_tiled<DIM, 1>, (const void *)k_prepass_tiled<DIM, 2>,
+                      (const void *)k_prepass_tiled<DIM, 4>, (const void *)k_prepass_tiled<DIM, 8>,
+                      (const void *)k_prepass_tiled<DIM, 16>, (const void *)k_prepass_tiled<DIM, 32>};
   for (auto f : fs)
     if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
       return -1;
-  return 0;
+  const bool ok = set_law_limit<DIM, LAW_RNP, uint16_t>(bytes) && set_law_limit<DIM, LAW_PMB, uint16_t>(bytes) &&
+                  set_law_limit<DIM, LAW_ELASTIC, uint16_t>(bytes) && set_law_limit<DIM, LAW_STATE, uint16_t>(bytes) &&
+                  set_law_limit<DIM, LAW_RNP, int32_t>(bytes) && set_law_limit<DIM, LAW_PMB, int32_t>(bytes) &&
+                  set_law_limit<DIM, LAW_ELASTIC, int32_t>(bytes) && set_law_limit<DIM, LAW_STATE, int32_t>(bytes);
+  return ok ? 0 : -1;
 }
 
 }  // namespace mixed_loop
 
-void launch_pd_tiled_mixed(const DevData &d, const BondTile *t, int n, int lanes, size_t smem,
-                           cudaStream_t s) {
+void launch_pd_tiled_mixed(const DevData &d, const BondTile *t, const int *law_begin, int lanes,
+                           size_t smem, cudaStream_t s) {
   using namespace mixed_loop;
-  if (n <= 0) return;
   if (d.use16) {
-    if (d.dim == 2) launch_dim<2>(d, d.pd_col16, t, n, lanes, smem, s);
-    else launch_dim<3>(d, d.pd_col16, t, n, lanes, smem, s);
+    if (d.dim == 2) launch_dim<2>(d, d.pd_col16, t, law_begin, lanes, smem, s);
+    else launch_dim<3>(d, d.pd_col16, t, law_begin, lanes, smem, s);
   } else {
-    if (d.dim == 2) launch_dim<2>(d, (const int32_t *)d.pd_col, t, n, lanes, smem, s);
-    else launch_dim<3>(d, (const int32_t *)d.pd_col, t, n, lanes, smem, s);
+    if (d.dim == 2) launch_dim<2>(d, (const int32_t *)d.pd_col, t, law_begin, lanes, smem, s);
+    else launch_dim<3>(d, (const int32_t *)d.pd_col, t, law_begin, lanes, smem, s);
   }
 }
 
@@ -388,8 +433,8 @@ size_t tile_smem_mixed(int dim, bool state, int64_t window) {
 }
 
 size_t tile_smem_mixed_main(int dim, bool state, bool col16, const BondTile &t) {
-  return mixed_loop::plan(dim, state, col16 ? 2 : 4, t.bond_begin, t.bond_end,
-                          t.win_end - t.win_begin)
+  return mixed_loop::plan(dim, state, col16 ? 2 : 4, t.bond_begin, t.bond_end, t.node_begin,
+                          t.node_end, t.win_end - t.win_begin)
       .total;
 }
 

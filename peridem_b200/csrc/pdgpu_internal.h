@@ -102,8 +102,12 @@ struct MixParticle {
   float fsc_thr;   // RNP: bond breaks when |S| sqrt(r) / rbar exceeds it
   float s0_thr;    // PMB: bond breaks when |S| exceeds it (s0 + 1e-10)
   float inv_rbar, inv_s0;  // damage Z = |S| / critical stretch
-  float j0, j1;    // influence J(r): j0 + j1 r (constant, linear) | j0 exp(j1 r^2) (Gaussian)
+  float j0, j1;    // influence J(r): j0 + j1 r (constant, linear) | j0 2^(j1 r^2) (Gaussian)
   float tf_coef, am_coef;  // PD state: 3K - 5G and 15G
+  float cu_h;      // check_up / h: corrected volume factor is cu_h - r / h
+  float kj0, kj1;  // law constant times j0, j1 (PD state: j0, j1)
+  float fsc_q;     // RNP: breaks when S^2 r exceeds (fsc_thr rbar)^2
+  float nbeta_l2e; // RNP: -beta log2(e), exp(-beta r S^2) = 2^(nbeta_l2e S^2 r)
 };
 
 // One CTA of the tiled bond loop: nodes [node_begin, node_end) of one
@@ -113,6 +117,7 @@ struct BondTile {
   int32_t pad;
   int64_t node_begin, node_end, win_begin, win_end;
   int64_t bond_begin, bond_end;  // pd_row[node_begin], pd_row[node_end]
+  int64_t center;                // the particle's centre node
 };
 
 struct DevData {
@@ -194,6 +199,7 @@ struct DevData {
   // FP32 volumes, particle-local 16-bit neighbour offsets when they fit
   uint16_t *pd_col16;
   MixParticle *mixp;
+  float4 *xv_mixed;  // per node {x, y, z, vol}: reference coordinates minus the centre's, FP32
   int32_t use16;
   float inf_p0, inf_p1;
 };
@@ -214,7 +220,8 @@ void launch_pd_tiled_fp64(const DevData &d, const BondTile *tiles, int n_tiles, 
                           size_t smem, cudaStream_t s);
 void launch_prepass_tiled_fp64(const DevData &d, const BondTile *tiles, int n_tiles, int lanes,
                                size_t smem, cudaStream_t s);
-void launch_pd_tiled_mixed(const DevData &d, const BondTile *tiles, int n_tiles, int lanes,
+// law_begin[m] .. law_begin[m + 1]: the tiles of material law m (PDGPU_MAT_*)
+void launch_pd_tiled_mixed(const DevData &d, const BondTile *tiles, const int *law_begin, int lanes,
                            size_t smem, cudaStream_t s);
 void launch_prepass_tiled_mixed(const DevData &d, const BondTile *tiles, int n_tiles, int lanes,
                                 size_t smem, cudaStream_t s);

@@ -45,10 +45,15 @@ __global__ void k_tile_windows(DevData d, BondTile *tiles) {
 
 __global__ void k_mixed_setup(DevData d) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n_nodes || !d.use16) return;
-  const int64_t start = d.particles[d.ptid[i]].start;
+  if (i >= d.n_nodes) return;
+  const DevParticle &P = d.particles[d.ptid[i]];
+  const int st = d.dim == 2 ? 2 : 4;
+  float r[3] = {0.f, 0.f, 0.f};
+  for (int q = 0; q < d.dim; q++) r[q] = (float)(d.xref[st * i + q] - d.xref[st * P.center + q]);
+  d.xv_mixed[i] = make_float4(r[0], r[1], r[2], (float)d.vol[i]);
+  if (!d.use16) return;
   for (int64_t k = d.pd_row[i]; k < d.pd_row[i + 1]; k++)
-    d.pd_col16[k] = (uint16_t)(d.pd_col[k] - start);
+    d.pd_col16[k] = (uint16_t)(d.pd_col[k] - P.start);
 }
 
 }  // namespace

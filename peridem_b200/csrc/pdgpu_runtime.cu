@@ -24,6 +24,7 @@ constexpr int64_t kHistoryCap = 1 << 16;
 // blocks of neighbour columns and bitmap words around each tile's range
 constexpr int64_t kBondPad = 16;
 constexpr int64_t kBitPad = 8;
+constexpr int64_t kRowPad = 2;
 
 struct TimedLaunch {
   int slot;
@@ -68,6 +69,7 @@ struct pdgpu_ctx {
   int n_tiles = 0;
   size_t tile_smem = 0, tile_smem_state = 0;  // pre-pass stage; FP64 bond loop with m_x, theta
   size_t tile_smem_pd = 0;                     // the bond-loop launch
+  int tile_law[5] = {0, 0, 0, 0, 0};           // tiles of law m: [tile_law[m], tile_law[m + 1])
   int64_t tile_nodes = 0;  // nodes per tile (0 = chosen at set-up)
   bool state_prepass = false;
 
@@ -484,7 +486,7 @@ int prepare_mixed(pdgpu_ctx *ctx) {
     const double ih = 1.0 / P.horizon;
     if (d.inf.type == PDGPU_INF_GAUSSIAN) {
       M.j0 = (float)d.inf.p0;
-      M.j1 = (float)(-ih * ih / d.inf.p1);
+      M.j1 = (float)(-ih * ih / d.inf.p1 * 1.4426950408889634);  // exponent in base 2
     } else if (d.inf.type == PDGPU_INF_LINEAR) {
       M.j0 = (float)d.inf.p0;
       M.j1 = (float)(d.inf.p1 * ih);
@@ -492,13 +494,22 @@ int prepare_mixed(pdgpu_ctx *ctx) {
       M.j0 = (float)d.inf.p0;
       M.j1 = 0.f;
     }
+    M.cu_h = (float)(P.check_up / P.h);
+    const double kf = P.material == PDGPU_MAT_PDSTATE ? 1.0 : (double)M.k_force;
+    M.kj0 = (float)(kf * d.inf.p0);
+    M.kj1 = d.inf.type == PDGPU_INF_LINEAR ? (float)(kf * d.inf.p1 * ih) : 0.f;
+    if (P.material == PDGPU_MAT_RNP) {
+      const double t = (P.mat[4] / rel) * P.mat[2];
+      M.fsc_q = (float)(t * t);
+      M.nbeta_l2e = (float)(-P.mat[1] * 1.4426950408889634);
+    }
     if (P.compute_force && P.end - P.start > 65536) fits16 = false;
   }
   TRY(dalloc(ctx, &d.mixp, mp.size()));
   CK(cudaMemcpy(d.mixp, mp.data(), mp.size() * sizeof(MixParticle), cudaMemcpyHostToDevice));
-  (void)N;
   d.use16 = fits16 ? 1 : 0;
   if (fits16) TRY(dalloc(ctx, &d.pd_col16, d.n_bonds + kBondPad));
+  TRY(dalloc(ctx, &d.xv_mixed, N));
   d.inf_p0 = (float)d.inf.p0;
   d.inf_p1 = (float)d.inf.p1;
   launch_mixed_setup(d, ctx->stream);
@@ -514,8 +525,11 @@ int prepare_tiles(pdgpu_ctx *ctx) {
   DevData &d = ctx->d;
   const bool mixed = d.precision == PDGPU_PREC_MIXED;
   const size_t limit = 227 * 1024 - 1024;  // dynamic stage; static shared memory on top
-  for (int64_t tn : {ctx->tile_nodes > 0 ? ctx->tile_nodes : (int64_t)(d.dim == 2 ? 128 : 96),
-                     (int64_t)64, (int64_t)32, (int64_t)16}) {
+  // default: every thread of the 256-thread CTA has a node, and at least
+  // 128 (2-D) or 96 (3-D) nodes per tile
+  const int64_t tn0 = ctx->tile_nodes > 0 ? ctx->tile_nodes
+                                          : std::max<int64_t>(d.dim == 2 ? 128 : 96, 256 / ctx->pd_lanes);
+  for (int64_t tn : {tn0, (int64_t)64, (int64_t)32, (int64_t)16}) {
     std::vector<BondTile> t;
     for (size_t p = 0; p < ctx->hp.size(); p++) {
       const DevParticle &P = ctx->hp[p];
@@ -525,8 +539,17 @@ int prepare_tiles(pdgpu_ctx *ctx) {
         b.particle = (int32_t)p;
         b.node_begin = a;
         b.node_end = std::min(P.end, a + tn);
+        b.center = P.center;
         t.push_back(b);
       }
+    }
+    // ordered by material law: one bond-loop launch per law
+    std::stable_sort(t.begin(), t.end(), [&](const BondTile &a, const BondTile &b) {
+      return ctx->hp[a.particle].material < ctx->hp[b.particle].material;
+    });
+    for (int m = 0; m <= 4; m++) {
+      ctx->tile_law[m] = 0;
+      for (auto &b : t) ctx->tile_law[m] += ctx->hp[b.particle].material < m;
     }
     if (ctx->tiles) dfree(ctx, ctx->tiles);
     ctx->n_tiles = (int)t.size();
@@ -617,9 +640,12 @@ int prepare(pdgpu_ctx *ctx) {
   CK(cudaMemcpy(d.ic_particle, ctx->ic_sel.data(), ctx->hp.size(), cudaMemcpyHostToDevice));
   TRY(upload_bc_tables(ctx, true));
   TRY(upload_bc_tables(ctx, false));
-  // lanes per node: average bonds per node decides (autotuned later)
+  // lanes per node from the average bonds per node (measured on B200: the
+  // FP32 form runs fastest with a thread per node at ~23 bonds per node)
   const double bpn = N ? (double)d.n_bonds / (double)N : 0.0;
-  if (ctx->pd_lanes <= 0) ctx->pd_lanes = bpn > 48 ? 32 : (bpn > 20 ? 8 : 4);
+  if (ctx->pd_lanes <= 0)
+    ctx->pd_lanes = d.precision == PDGPU_PREC_MIXED ? (bpn > 48 ? 4 : 1)
+                                                    : (bpn > 48 ? 32 : (bpn > 20 ? 8 : 4));
   // contact buffers
   {
     int dev = 0, sms = 0;
@@ -695,7 +721,7 @@ void pd_forces(pdgpu_ctx *ctx) {
   const size_t smem = ctx->tile_smem_pd;
   if (mixed)
     run(ctx, "pd_force_mixed", [&] {
-      launch_pd_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
+      launch_pd_tiled_mixed(d, ctx->tiles, ctx->tile_law, ctx->pd_lanes, smem, s);
     });
   else
     run(ctx, "pd_force", [&] {
@@ -746,7 +772,7 @@ cudaError_t graph_step(pdgpu_ctx *ctx, cudaGraphConditionalHandle h, const char 
     else launch_prepass_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
   }
   const size_t smem = ctx->tile_smem_pd;
-  if (mixed) launch_pd_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
+  if (mixed) launch_pd_tiled_mixed(d, ctx->tiles, ctx->tile_law, ctx->pd_lanes, smem, s);
   else launch_pd_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
   if (ctx->desc.multi_particle) {
     cudaStreamCaptureStatus st;
@@ -1079,7 +1105,7 @@ int pdgpu_upload_pd_neighbors(pdgpu_ctx *ctx, const uint64_t *rowptr, const uint
     for (int64_t k = 0; k < B; k++)
       if (bond_state[k]) bits[k >> 5] |= 1u << (k & 31);
   d.n_bonds = B;
-  TRY(dalloc(ctx, &d.pd_row, N + 1));
+  TRY(dalloc(ctx, &d.pd_row, N + 1 + kRowPad));
   TRY(dalloc(ctx, &d.pd_col, B + kBondPad));
   TRY(dalloc(ctx, &d.bond_bits, bits.size()));
   CK(cudaMemcpy(d.pd_row, row.data(), (N + 1) * 8, cudaMemcpyHostToDevice));
@@ -1104,7 +1130,7 @@ int pdgpu_build_pd_neighbors(pdgpu_ctx *ctx) {
   if (!d.cell_tmp) TRY(dalloc(ctx, &d.cell_tmp, N));
   if (!d.cell_nodes) TRY(dalloc(ctx, &d.cell_nodes, N));
   TRY(ensure_cells(ctx, g));
-  TRY(dalloc(ctx, &d.pd_row, N + 1));
+  TRY(dalloc(ctx, &d.pd_row, N + 1 + kRowPad));
   CK(cudaMemset(d.pd_row, 0, (N + 1) * 8));
   // the cell kernels run only when ctrl.update is set
   CtrlState c{};
@@ -1443,8 +1469,11 @@ int pdgpu_download_pd_neighbors(pdgpu_ctx *ctx, uint64_t *rowptr, uint64_t *col)
 int pdgpu_set_tuning(pdgpu_ctx *ctx, int32_t pd_lanes, int32_t contact_lanes) {
   if (!ctx) return PDGPU_ERR_ARG;
   if (ctx->prepared && contact_lanes) return fail(ctx, PDGPU_ERR_STATE, "set_tuning: contact lanes are fixed once stepping starts");
-  if (pd_lanes && pd_lanes != 4 && pd_lanes != 8 && pd_lanes != 16 && pd_lanes != 32)
-    return fail(ctx, PDGPU_ERR_ARG, "set_tuning: pd_lanes must be 4, 8, 16 or 32");
+  const bool mixed = ctx->desc.precision == PDGPU_PREC_MIXED;
+  if (pd_lanes && !((mixed && (pd_lanes == 1 || pd_lanes == 2)) || pd_lanes == 4 || pd_lanes == 8 ||
+                    pd_lanes == 16 || pd_lanes == 32))
+    return fail(ctx, PDGPU_ERR_ARG, "set_tuning: pd_lanes must be 4, 8, 16 or 32 (also 1 or 2 in the mixed form)");
+  if (ctx->prepared && pd_lanes) return fail(ctx, PDGPU_ERR_STATE, "set_tuning: lanes are fixed once stepping starts");
   if (contact_lanes && contact_lanes != 4 && contact_lanes != 8 && contact_lanes != 32)
     return fail(ctx, PDGPU_ERR_ARG, "set_tuning: contact_lanes must be 4, 8 or 32");
   if (pd_lanes) ctx->pd_lanes = pd_lanes;
@@ -1453,6 +1482,13 @@ int pdgpu_set_tuning(pdgpu_ctx *ctx, int32_t pd_lanes, int32_t contact_lanes) {
     cudaGraphExecDestroy(ctx->gexec);
     ctx->gexec = nullptr;
   }
+  return PDGPU_OK;
+}
+
+int pdgpu_set_tile_nodes(pdgpu_ctx *ctx, int32_t nodes) {
+  if (!ctx || nodes < 0 || nodes > 4096) return PDGPU_ERR_ARG;
+  if (ctx->prepared) return fail(ctx, PDGPU_ERR_STATE, "set_tile_nodes: tiles are fixed once stepping starts");
+  ctx->tile_nodes = nodes;
   return PDGPU_OK;
 }
 

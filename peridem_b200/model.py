@@ -132,7 +132,7 @@ class GpuDEMModel:
     def __init__(self, scene: Scene, precision: int = PREC_FP64, device: int = 0,
                  build_neighbors: bool = False, compute_mx: bool = False,
                  contact_capacity: int = 0, wall_pair_capacity: int = 0,
-                 pd_lanes: int = 0):
+                 pd_lanes: int = 0, tile_nodes: int = 0):
         self.lib = api.lib()
         self.scene = scene
         desc = api.Desc()
@@ -164,6 +164,8 @@ class GpuDEMModel:
         self._closed = False
         if pd_lanes:
             api.set_lanes(self, pd_lanes)
+        if tile_nodes:
+            self._check(self.lib.pdgpu_set_tile_nodes(self.ctx, tile_nodes))
         self._upload(build_neighbors, compute_mx)
 
     # ---- DEMModel::init: upload ModelData -----------------------------------
