@@ -17,6 +17,8 @@ enum : uint8_t {
   NODE_WALL = 4,     // node of a wall
   NODE_PARTICLE = 8, // node of a non-wall particle (receives particle damping)
   NODE_SEARCH0 = 16, // searched at DEMModel::init (before the two_particle override)
+  NODE_UBC = 32,     // has displacement boundary-condition entries (ubc_of)
+  NODE_FBC = 64,     // has force boundary-condition entries (fbc_of)
 };
 
 // device error codes (CtrlState::error)
@@ -39,6 +41,11 @@ struct DevParticle {
 
 struct ContactPair {
   double rc, kn, mu, betan, kappa;
+};
+
+struct DampParticle {
+  double bound_r, density;
+  int32_t zone, type;
 };
 
 struct Influence {
@@ -71,6 +78,8 @@ struct CtrlState {
   double pen_dist, max_y, contact_area_radius;
   int64_t history_count;
   int64_t c_nnodes;  // nodes with a non-empty contact candidate list
+  // CTAs finished in the fused step kernels (the last one runs the serial tail)
+  uint32_t begin_done, end_done;
 };
 
 // Cell grid fixed at set-up; nodes outside are clamped to the border cells,
@@ -167,6 +176,15 @@ struct DevData {
   int32_t wp_cap;
   int32_t *wp, *wp_cnt;
   double *fdamp;  // n_particles * 4
+  // contact force sum per node (node-vector layout), written by the contact
+  // pass beside the bond loop and folded into f (then cleared) by the
+  // external-force pass
+  double *fc;
+  // short dependency chains for the contact and damping passes
+  int2 *c_span;          // [c_row[i], c_row[i + 1]) of compacted node t = c_nodes[t]
+  uint8_t *nzone;        // zone of each node's particle
+  DampParticle *dpart;   // per particle: bounding radius, density, zone, type
+  double *pcen;          // per particle: centre position and velocity (8 doubles), this step
 
   // boundary conditions: per BC node, a run of entries applied in set order
   int32_t n_ubc_sets, n_fbc_sets;
@@ -177,6 +195,7 @@ struct DevData {
   uint8_t *ubc_once;
   int32_t *fbc_node, *fbc_row, *fbc_set;
   double *fbc_val;
+  int32_t *ubc_of, *fbc_of;  // per node: its row in the BC tables (valid where NODE_UBC / NODE_FBC)
 
   // initial condition
   int32_t ic_active;
@@ -211,7 +230,10 @@ void launch_apply_ic(const DevData &d, cudaStream_t s);
 void launch_integrate(const DevData &d, int half_kick_only, cudaStream_t s);  // CD or Verlet first half
 void launch_verlet_second(const DevData &d, cudaStream_t s);
 void launch_ctrl(const DevData &d, int mode, cudaStream_t s);  // mode 0 step, 1 prelude, 2 init list
-void launch_ctrl_cond(const DevData &d, int mode, cudaGraphConditionalHandle h, cudaStream_t s);
+// integrate + displacement BC + step control (last CTA)
+void launch_step_begin(const DevData &d, int verlet, cudaStream_t s);
+// external forces + force BC (+ Verlet second half) + post-processing (last CTA)
+void launch_step_end(const DevData &d, int verlet, int post, cudaStream_t s);
 void launch_bc(const DevData &d, cudaStream_t s);
 void launch_mixed_setup(const DevData &d, cudaStream_t s);
 void launch_tile_windows(const DevData &d, BondTile *tiles, int n_tiles, cudaStream_t s);
@@ -230,8 +252,7 @@ size_t tile_smem_mixed(int dim, bool state, int64_t window);       // state pre-
 size_t tile_smem_mixed_main(int dim, bool state, bool col16, const BondTile &t);
 int set_tile_smem_limit_fp64(int dim, size_t bytes);
 int set_tile_smem_limit_mixed(int dim, size_t bytes);
-void launch_contact_update(const DevData &d, void *scan_tmp, size_t scan_tmp_bytes, int lanes,
-                           int init, cudaStream_t s);
+
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s);
 int rebuild_grid_blocks(const DevData &d, int lanes);
 cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, int lanes, int init,

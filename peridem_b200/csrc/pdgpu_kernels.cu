@@ -260,75 +260,87 @@ __global__ void k_verlet_second(DevData d) {
 // mode 0: a time step; 1: the computeForces call of the integrate() prelude;
 // 2: the contact list build of DEMModel::init.
 // ---------------------------------------------------------------------------
-__device__ void ctrl_step(const DevData &d, int mode) {
-  CtrlState *c = d.ctrl;
-  if (c->error) return;
+// the fields the step control changes, written back in one go
+__device__ __forceinline__ void ctrl_commit(CtrlState *dst, const CtrlState &c) {
+  dst->n = c.n;
+  dst->time = c.time;
+  dst->first_bc = c.first_bc;
+  dst->init_calls = c.init_calls;
+  dst->counter = c.counter;
+  dst->interval = c.interval;
+  dst->radius = c.radius;
+  dst->max_velocity = c.max_velocity;
+  dst->update = c.update;
+}
+
+__device__ __noinline__ void ctrl_step(const DevData &d, int mode) {
+  CtrlState *cp = d.ctrl;
+  CtrlState c = *cp;  // one pass over the state instead of a chain of loads
+  if (c.error) return;
   if (mode == 0) {
-    c->n += 1;
-    c->time += d.dt;
-    c->first_bc = 0;
+    c.n += 1;
+    c.time += d.dt;
+    c.first_bc = 0;
   }
+  // read and reset atomically: other CTAs raised it with atomicMax
   const double vmax_now =
-      fmax(__longlong_as_double((long long)c->vmax_bits), c->static_vmax);
-  c->vmax_bits = 0ull;
+      fmax(__longlong_as_double((long long)atomicExch(&cp->vmax_bits, 0ull)), c.static_vmax);
   if (!d.n_zones) {  // single particle: no contact
-    c->update = 0;
+    c.update = 0;
+    ctrl_commit(cp, c);
     return;
   }
-  int upd = 0;
-  const int64_t n = c->n;
+  const int64_t n = c.n;
   if (n == 0) {
-    c->init_calls += 1;
-    if (c->init_calls == 1) {
-      c->update = 1;
+    c.init_calls += 1;
+    if (c.init_calls == 1) {
+      c.update = 1;
+      ctrl_commit(cp, c);
       return;
     }
-    if (c->init_calls == 2) {
-      c->counter += 1;
-      c->update = ((c->counter - 1) % c->interval) == 0;
+    if (c.init_calls == 2) {
+      c.counter += 1;
+      c.update = ((c.counter - 1) % c.interval) == 0;
+      ctrl_commit(cp, c);
       return;
     }
   }
-  if (c->interval == 1) {
-    c->radius = d.max_contact_r;
-    c->counter += 1;
-    c->update = ((c->counter - 1) % c->interval) == 0;
+  if (c.interval == 1) {
+    c.radius = d.max_contact_r;
+    c.counter += 1;
+    c.update = ((c.counter - 1) % c.interval) == 0;
+    ctrl_commit(cp, c);
     return;
   }
-  const int64_t upi = c->interval > 5 ? (int64_t)(0.2 * (double)c->interval) : 1;
-  if (c->counter > 0 && c->counter % upi != 0) {
-    c->counter += 1;
-    c->update = ((c->counter - 1) % c->interval) == 0;
+  const int64_t upi = c.interval > 5 ? (int64_t)(0.2 * (double)c.interval) : 1;
+  if (c.counter > 0 && c.counter % upi != 0) {
+    c.counter += 1;
+    c.update = ((c.counter - 1) % c.interval) == 0;
+    ctrl_commit(cp, c);
     return;
   }
-  c->max_velocity = vmax_now;
+  c.max_velocity = vmax_now;
   const double safety = d.search_factor > 5 ? d.search_factor : 10.0;
   const double r_contact = d.search_factor * d.max_contact_r;
-  const double r_vel = c->max_velocity * d.dt * (double)d.search_interval * safety;
+  const double r_vel = c.max_velocity * d.dt * (double)d.search_interval * safety;
   if (is_greater(r_vel, r_contact)) {
-    c->interval = (int64_t)(d.max_contact_r / (c->max_velocity * d.dt));
-    c->radius = r_contact;
-    c->counter = 0;
-    if (c->interval < 1) {
-      c->interval = 1;
-      c->radius = d.max_contact_r;
+    c.interval = (int64_t)(d.max_contact_r / (c.max_velocity * d.dt));
+    c.radius = r_contact;
+    c.counter = 0;
+    if (c.interval < 1) {
+      c.interval = 1;
+      c.radius = d.max_contact_r;
     }
   } else {
-    c->radius = c->interval < 2 ? d.max_contact_r : r_contact;
+    c.radius = c.interval < 2 ? d.max_contact_r : r_contact;
   }
-  c->counter += 1;
-  upd = ((c->counter - 1) % c->interval) == 0;
-  c->update = upd;
+  c.counter += 1;
+  c.update = ((c.counter - 1) % c.interval) == 0;
+  ctrl_commit(cp, c);
 }
 
-__global__ void k_ctrl(DevData d, int mode) { ctrl_step(d, mode); }
+__global__ void k_ctrl(const __grid_constant__ DevData d, int mode) { ctrl_step(d, mode); }
 
-// same, inside a CUDA graph: the rebuild decision also drives the graph's
-// conditional node that holds the contact-list rebuild
-__global__ void k_ctrl_cond(DevData d, int mode, cudaGraphConditionalHandle h) {
-  ctrl_step(d, mode);
-  cudaGraphSetConditional(h, (d.ctrl->update && !d.ctrl->error) ? 1u : 0u);
-}
 
 // ---------------------------------------------------------------------------
 // DEMModel::computeExternalDisplacementBC -> ParticleULoading::apply
@@ -337,16 +349,9 @@ __global__ void k_ctrl_cond(DevData d, int mode, cudaGraphConditionalHandle h) {
 // on the host from the reference configuration.
 // ---------------------------------------------------------------------------
 template <int DIM>
-__global__ void k_bc(DevData d) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.n_ubc_nodes || d.ctrl->error) return;
-  const int64_t i = d.ubc_node[t];
-  const double time = d.ctrl->time;
-  const int first = d.ctrl->first_bc;
-  double u[3], v[3], x[3], xr[3];
-  ldv<DIM>(d.u, i, u);
-  ldv<DIM>(d.v, i, v);
-  ldv<DIM>(d.x, i, x);
+__device__ __noinline__ void apply_ubc(const DevData &d, int t, int64_t i, double time, int first,
+                                          double (&u)[3], double (&v)[3], double (&x)[3]) {
+  double xr[3];
   ldg_v<DIM>(d.xref, i, xr);
   for (int e = d.ubc_row[t]; e < d.ubc_row[t + 1]; e++) {
     if (d.ubc_once[e] && !first) continue;
@@ -395,9 +400,88 @@ __global__ void k_bc(DevData d) {
         x[q] = ui[q] + xr[q];
       }
   }
+}
+
+template <int DIM>
+__global__ void k_bc(const __grid_constant__ DevData d) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.n_ubc_nodes || d.ctrl->error) return;
+  const int64_t i = d.ubc_node[t];
+  double u[3], v[3], x[3];
+  ldv<DIM>(d.u, i, u);
+  ldv<DIM>(d.v, i, v);
+  ldv<DIM>(d.x, i, x);
+  apply_ubc<DIM>(d, t, i, d.ctrl->time, d.ctrl->first_bc, u, v, x);
   stv<DIM>(d.u, i, u);
   stv<DIM>(d.v, i, v);
   stv<DIM>(d.x, i, x);
+}
+
+// ---------------------------------------------------------------------------
+// First kernel of a step: integrateCD / the first Verlet half (as k_integrate),
+// then the displacement BC of each BC node at the step's new time (as k_bc
+// after k_ctrl: zero-displacement sets are not re-applied), then — in the
+// last CTA to finish — the step control (as k_ctrl, mode 0).
+// ---------------------------------------------------------------------------
+template <int DIM, bool VERLET>
+__global__ void __launch_bounds__(kBlock) k_step_begin(const __grid_constant__ DevData d) {
+  __shared__ double smax[kBlock / 32];
+  __shared__ int last;
+  // CTAs run in reverse node order: the boundary-condition nodes (walls, at
+  // the end of the node array) then start in the first wave
+  const int64_t i = (int64_t)(gridDim.x - 1 - blockIdx.x) * blockDim.x + threadIdx.x;
+  double vm = 0.0;
+  if (i < d.n_nodes && !d.ctrl->error) {
+    const uint8_t fl = d.flags[i];
+    if (fl & (NODE_ACTIVE | NODE_UBC)) {
+      double v[3], u[3], x[3];
+      ldv<DIM>(d.v, i, v);
+      ldv<DIM>(d.u, i, u);
+      ldv<DIM>(d.x, i, x);
+      if (fl & NODE_ACTIVE) {
+        const double rho = d.particles[d.ptid[i]].density;
+        const uint8_t fix = d.fix[i];
+        double f[3];
+        ldv<DIM>(d.f, i, f);
+        const double dt = d.dt;
+        const double k = VERLET ? 0.5 * (dt / rho) : dt / rho;
+#pragma unroll
+        for (int dof = 0; dof < DIM; dof++) {
+          if (!((fix >> dof) & 1u)) {
+            v[dof] += k * f[dof];
+            u[dof] += dt * v[dof];
+            x[dof] += dt * v[dof];
+          }
+        }
+        vm = len3<DIM>(v);
+        d.vmag[i] = vm;
+      }
+      // the step control advances time by dt before the BC pass
+      if (fl & NODE_UBC) apply_ubc<DIM>(d, d.ubc_of[i], i, d.ctrl->time + d.dt, 0, u, v, x);
+      stv<DIM>(d.v, i, v);
+      stv<DIM>(d.u, i, u);
+      stv<DIM>(d.x, i, x);
+    }
+  }
+  // block max of |v| -> one atomic per block
+  for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+  if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = vm;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double m = threadIdx.x < kBlock / 32 ? smax[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) {
+      if (m > 0.0) atomic_max_nonneg(&d.ctrl->vmax_bits, m);
+      __threadfence();
+      last = atomicAdd(&d.ctrl->begin_done, 1u) == gridDim.x - 1;
+    }
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    d.ctrl->begin_done = 0u;
+    ctrl_step(d, 0);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -451,94 +535,9 @@ __global__ void k_zero_cells(DevData d) {
   d.cell_cnt[c] = 0;
 }
 
-// candidate search: COUNT pass writes per-node counts into c_cnt; the scan
-// c_cnt -> c_row[1..N] is out of place, so replaying it on a step without a
-// rebuild reproduces the same offsets.  FILL pass writes the columns in
-// (cell, node index) order.
-template <int DIM, int LPN, bool FILL>
-__global__ void __launch_bounds__(kBlock) k_cand(DevData d, uint8_t search_bit) {
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
-  const int lane = threadIdx.x % LPN;
-  if (i >= d.n_nodes) return;
-  if (d.ctrl->error || !d.ctrl->update) return;
-  const unsigned gm = group_mask<LPN>();
-  const unsigned lane_base = (threadIdx.x & 31u) / LPN * LPN;
-  if (!(d.flags[i] & search_bit)) {
-    if (!FILL && lane == 0) d.c_cnt[i] = 0;
-    return;
-  }
-  const Grid g = d.grid;
-  double q[3];
-  ldv<DIM>(d.x, i, q);
-  const int32_t pi = d.ptid[i];
-  const double r = d.ctrl->radius;
-  const double r2 = r * r;
-  int c[3] = {cell_coord<DIM>(q[0], g, 0), cell_coord<DIM>(q[1], g, 1),
-              DIM == 3 ? cell_coord<DIM>(q[2], g, 2) : 0};
-  int64_t out = FILL ? d.c_row[i] : 0;
-  const int64_t out_end = FILL ? d.c_row[i + 1] : 0;
-  int64_t count = 0;
-  const int zlo = DIM == 3 ? max(c[2] - 1, 0) : 0;
-  const int zhi = DIM == 3 ? min(c[2] + 1, g.dims[2] - 1) : 0;
-  for (int cz = zlo; cz <= zhi; cz++)
-    for (int cy = max(c[1] - 1, 0); cy <= min(c[1] + 1, g.dims[1] - 1); cy++)
-      for (int cx = max(c[0] - 1, 0); cx <= min(c[0] + 1, g.dims[0] - 1); cx++) {
-        const int cell = cx + g.dims[0] * (cy + g.dims[1] * cz);
-        const int s = d.cell_start[cell], e = d.cell_start[cell + 1];
-        for (int base = s; base < e; base += LPN) {
-          const int a = base + lane;
-          bool hit = false;
-          int32_t j = -1;
-          if (a < e) {
-            j = d.cell_nodes[a];
-            if (d.ptid[j] != pi) {
-              double p[3];
-              ldv<DIM>(d.x, j, p);
-              double dd = 0.0;
-#pragma unroll
-              for (int t = 0; t < DIM; t++) {
-                const double df = q[t] - p[t];
-                dd += df * df;
-              }
-              hit = dd < r2;
-            }
-          }
-          const unsigned bal = (__ballot_sync(gm, hit) & gm) >> lane_base;
-          if (FILL) {
-            if (hit) {
-              const int64_t at = out + __popc(bal & ((1u << lane) - 1u));
-              if (at < out_end) d.c_col[at] = j;
-            }
-            out += __popc(bal);
-          } else {
-            count += __popc(bal);
-          }
-        }
-      }
-  if (!FILL && lane == 0) d.c_cnt[i] = count;
-}
 
-__global__ void k_compact_flag(DevData d) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n_nodes || d.ctrl->error || !d.ctrl->update) return;
-  d.c_tmp[i] = d.c_cnt[i] > 0 ? 1 : 0;
-}
 
-__global__ void k_compact_scatter(DevData d) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n_nodes || d.ctrl->error || !d.ctrl->update) return;
-  // c_tmp holds the inclusive scan of the flags
-  if (d.c_cnt[i] > 0) d.c_nodes[d.c_tmp[i] - 1] = (int32_t)i;
-  if (i == d.n_nodes - 1) d.ctrl->c_nnodes = d.c_tmp[i];
-}
 
-__global__ void k_cand_check(DevData d) {
-  if (d.ctrl->error || !d.ctrl->update) return;
-  const int64_t total = d.c_row[d.n_nodes];
-  d.ctrl->entries = total;
-  d.ctrl->updates += 1;
-  if (total > d.contact_cap) set_error(d.ctrl, DEV_ERR_CONTACT_OVERFLOW, total);
-}
 
 // ---------------------------------------------------------------------------
 // The whole contact-list rebuild as one cooperative launch: every phase is
@@ -711,7 +710,10 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
   grid_scan<int64_t>(g, [cn](int64_t k) { return cn[k]; }, d.c_row, N, bsum);
   grid_scan<int64_t>(g, [cn](int64_t k) { return (int64_t)(cn[k] > 0); }, d.c_tmp, N, bsum);
   for (int64_t i = tid; i < N; i += nth)
-    if (cn[i] > 0) d.c_nodes[d.c_tmp[i]] = (int32_t)i;
+    if (cn[i] > 0) {
+      d.c_nodes[d.c_tmp[i]] = (int32_t)i;
+      d.c_span[d.c_tmp[i]] = make_int2((int)d.c_row[i], (int)d.c_row[i + 1]);
+    }
   if (tid == 0) d.ctrl->c_nnodes = d.c_tmp[N];
   for (int64_t i = tid / LPN; i < N; i += nth / LPN)
     if ((d.flags[i] & search_bit) && d.c_row[i + 1] > d.c_row[i])
@@ -731,39 +733,77 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
 // contact radius are recorded for the particle-wall damping (:994-1017),
 // and the test wall's contact reaction is summed per block.
 // ---------------------------------------------------------------------------
+constexpr int kZonePairsSmem = 256;
+
+// Every load a candidate needs is issued together: the compacted node and
+// its candidate span (speculatively, before the node count arrives), then the
+// node's own data with its candidate columns, then all of each candidate's
+// data at once; the zone-pair table sits in shared memory.  The first
+// threads also gather the particle centres for the damping pass.
 template <int DIM, int LPN>
 __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
+  __shared__ ContactPair cps[kZonePairsSmem];
   __shared__ double scr[kBlock / LPN];
   const int lane = threadIdx.x % LPN;
-  const int64_t nn = d.ctrl->error ? 0 : d.ctrl->c_nnodes;
+  const int nz = d.n_zones;
+  const bool tab = nz * nz <= kZonePairsSmem;
+  const int64_t gstride = (int64_t)gridDim.x * (kBlock / LPN);
+  int64_t t = (int64_t)blockIdx.x * (kBlock / LPN) + threadIdx.x / LPN;
+  int32_t i_next = t < d.n_nodes ? d.c_nodes[t] : 0;
+  int2 sp_next = t < d.n_nodes ? d.c_span[t] : make_int2(0, 0);
+  const int64_t nn_raw = d.ctrl->c_nnodes;
+  const int err = d.ctrl->error;
+  if (tab)
+    for (int a = threadIdx.x; a < nz * nz; a += kBlock) cps[a] = d.contact[a];
+  {
+    // particle centres (position, velocity) of this step for the damping pass
+    const int64_t p = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (p < d.n_particles) {
+      const int64_t c = d.particles[p].center;
+      double xc[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
+      ldv<DIM>(d.x, c, xc);
+      ldv<DIM>(d.v, c, vc);
+      double *o = d.pcen + 8 * p;
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        o[q] = xc[q];
+        o[3 + q] = vc[q];
+      }
+    }
+  }
+  __syncthreads();
+  const int64_t nn = err ? 0 : nn_raw;
   double crd_acc = 0.0;
-  // grid-stride over the nodes that have candidates (compacted at rebuild)
-  for (int64_t t = (int64_t)blockIdx.x * (kBlock / LPN) + threadIdx.x / LPN; t < nn;
-       t += (int64_t)gridDim.x * (kBlock / LPN)) {
-    const int64_t i = d.c_nodes[t];
-    const int64_t k0 = d.c_row[i], k1 = d.c_row[i + 1];
+  for (; t < nn; t += gstride) {
+    const int64_t i = i_next;
+    const int2 sp = sp_next;
+    if (t + gstride < nn) {
+      i_next = d.c_nodes[t + gstride];
+      sp_next = d.c_span[t + gstride];
+    }
     const unsigned gm = group_mask<LPN>();
     const int32_t pi = d.ptid[i];
-    const int zi = d.particles[pi].zone;
+    const int zi = d.nzone[i];
     double yi[3], vi[3];
     ldv<DIM>(d.x, i, yi);
     ldv<DIM>(d.v, i, vi);
     double fx = 0.0, fy = 0.0, fz = 0.0, crd = 0.0;
-    for (int64_t k = k0 + lane; k < k1; k += LPN) {
+    for (int k = sp.x + lane; k < sp.y; k += LPN) {
       const int32_t j = d.c_col[k];
-      double yj[3];
+      double yj[3], vj[3];
       ldv<DIM>(d.x, j, yj);
+      ldv<DIM>(d.v, j, vj);
+      const double volj = d.vol[j];
+      const int32_t pj = d.ptid[j];
+      const int zj = d.nzone[j];
+      const bool wall = (d.flags[j] & NODE_WALL) != 0;
       double yji[3];
 #pragma unroll
       for (int q = 0; q < 3; q++) yji[q] = yj[q] - yi[q];
       const double R = len3<DIM>(yji);
-      const int32_t pj = d.ptid[j];
-      const DevParticle &Pj = d.particles[pj];
-      const ContactPair cp = d.contact[zi * d.n_zones + Pj.zone];
+      const ContactPair cp = tab ? cps[zi * nz + zj] : d.contact[zi * nz + zj];
       if (is_less(R, cp.rc)) {
-        double vj[3], vji[3], en[3], et[3];
-        ldv<DIM>(d.v, j, vj);
-        const double volj = d.vol[j];
+        double vji[3], en[3], et[3];
 #pragma unroll
         for (int q = 0; q < 3; q++) {
           vji[q] = vj[q] - vi[q];
@@ -789,7 +829,7 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
         fx += mf * et[0];
         fy += mf * et[1];
         if constexpr (DIM == 3) fz += mf * et[2];
-        if (Pj.type == 1) {
+        if (wall) {
           const int slot = atomicAdd(d.wp_cnt + pi, 1);
           if (slot < d.wp_cap) d.wp[(int64_t)pi * d.wp_cap + slot] = j;
           else set_error(d.ctrl, DEV_ERR_WALLPAIR_OVERFLOW, pi);
@@ -805,12 +845,8 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
     if constexpr (DIM == 3) fz = group_sum<LPN>(fz, gm);
     crd = group_sum<LPN>(crd, gm);
     if (lane == 0) {
-      double f[3];
-      ldv<DIM>(d.f, i, f);
-      f[0] += fx;
-      f[1] += fy;
-      f[2] += fz;
-      stv<DIM>(d.f, i, f);
+      const double f[3] = {fx, fy, fz};
+      stv<DIM>(d.fc, i, f);
       crd_acc += crd * d.vol[i];
     }
   }
@@ -830,40 +866,51 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
 // condensed wall nodes.  One block per particle; the force density is applied
 // to all nodes of the particle by k_external.
 // ---------------------------------------------------------------------------
-constexpr int kDampBlock = 256;
+constexpr int kDampBlock = 128;
 constexpr int kWallSort = 4096;
 
 __global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
   __shared__ int32_t wn[kWallSort];
   __shared__ double red[3][kDampBlock / 32];
+  __shared__ ContactPair cps[kZonePairsSmem];
   const int p = blockIdx.x;
-  const DevParticle P = d.particles[p];
+  const DampParticle P = d.dpart[p];
+  const int nz = d.n_zones;
+  const bool tab = nz * nz <= kZonePairsSmem;
+  int nw = d.wp_cnt[p];
+  if (tab)
+    for (int a = threadIdx.x; a < nz * nz; a += blockDim.x) cps[a] = d.contact[a];
+  __syncthreads();
   if (P.type != 0) return;
   if (d.ctrl->error) return;
   const double Ri = P.bound_r;
   const double vol_pi = kPi * Ri * Ri;
   const double rhoi = P.density;
-  double xc[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
   const int st = dim == 2 ? 2 : 4;
-  for (int q = 0; q < dim; q++) {
-    xc[q] = d.x[st * P.center + q];
-    vc[q] = d.v[st * P.center + q];
+  double xc[3], vc[3];
+  for (int q = 0; q < 3; q++) {
+    xc[q] = d.pcen[8 * p + q];
+    vc[q] = d.pcen[8 * p + 3 + q];
   }
   double acc[3] = {0.0, 0.0, 0.0};
   // particle-particle
   for (int q = threadIdx.x; q < d.n_particles; q += blockDim.x) {
     if (q == p) continue;
-    const DevParticle &Q = d.particles[q];
+    const DampParticle Q = d.dpart[q];
     if (Q.type != 0) continue;
     const double Rj = Q.bound_r;
-    double xcj[3] = {0, 0, 0}, vcj[3] = {0, 0, 0};
-    for (int t = 0; t < dim; t++) {
-      xcj[t] = d.x[st * Q.center + t] - xc[t];
-      vcj[t] = d.v[st * Q.center + t] - vc[t];
+    double xcj[3], vcj[3];
+    for (int t = 0; t < 3; t++) {
+      xcj[t] = d.pcen[8 * q + t] - xc[t];
+      vcj[t] = d.pcen[8 * q + 3 + t] - vc[t];
     }
-    const double dist = sqrt(xcj[0] * xcj[0] + xcj[1] * xcj[1] + xcj[2] * xcj[2]);
-    const ContactPair cp = d.contact[P.zone * d.n_zones + Q.zone];
-    if (is_less(dist, Rj + Ri + 1.01 * cp.rc)) {
+    const double d2 = xcj[0] * xcj[0] + xcj[1] * xcj[1] + xcj[2] * xcj[2];
+    const ContactPair cp = tab ? cps[P.zone * nz + Q.zone] : d.contact[P.zone * nz + Q.zone];
+    const double reach = Rj + Ri + 1.01 * cp.rc;
+    // pairs well beyond the reach cannot pass the relative-tolerance test
+    if (d2 > 1.0625 * reach * reach) continue;
+    const double dist = sqrt(d2);
+    if (is_less(dist, reach)) {
       const double vol_pj = kPi * Rj * Rj;
       const double m1 = rhoi * vol_pi, m2 = Q.density * vol_pj;
       const double meq = 2. * m1 * m2 / (m1 + m2);  // util::equivalentMass
@@ -877,7 +924,6 @@ __global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
     }
   }
   // particle-wall: unique wall nodes within the contact radius of any node
-  int nw = d.wp_cnt[p];
   if (nw > d.wp_cap) nw = d.wp_cap;
   if (nw > kWallSort) nw = kWallSort;  // capacity is validated on the host
   int sz = 1;
@@ -903,8 +949,8 @@ __global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
   for (int a = threadIdx.x; a < nw; a += blockDim.x) {
     const int32_t k = wn[a];
     if (a > 0 && wn[a - 1] == k) continue;
-    const DevParticle &W = d.particles[d.ptid[k]];
-    const ContactPair cp = d.contact[P.zone * d.n_zones + W.zone];
+    const int zk = d.nzone[k];
+    const ContactPair cp = tab ? cps[P.zone * nz + zk] : d.contact[P.zone * nz + zk];
     const double meq = rhoi * vol_pi;
     const double bn = cp.betan * sqrt(cp.kappa * cp.rc * meq);
     double xk[3] = {0, 0, 0}, vk[3] = {0, 0, 0};
@@ -949,7 +995,22 @@ __global__ void k_external(DevData d) {
   // nodes outside d_fPdCompNodes carry no peridynamic or contact force: the
   // reference zeroes f for all nodes at the start of computeForces (:473-478)
   double f[3] = {0.0, 0.0, 0.0};
-  if (d.flags[i] & NODE_ACTIVE) ldv<DIM>(d.f, i, f);
+  const uint8_t fl = d.flags[i];
+  if (fl & NODE_ACTIVE) {
+    ldv<DIM>(d.f, i, f);
+    // contact forces (computeContactForces adds them after the bond loop);
+    // only searching nodes can carry one
+    if (d.fc && (fl & (NODE_SEARCH | NODE_SEARCH0))) {
+      double c[3];
+      ldv<DIM>(d.fc, i, c);
+      if (c[0] != 0.0 || c[1] != 0.0 || (DIM == 3 && c[2] != 0.0)) {
+#pragma unroll
+        for (int q = 0; q < DIM; q++) f[q] += c[q];
+        const double z[3] = {0.0, 0.0, 0.0};
+        stv<DIM>(d.fc, i, z);
+      }
+    }
+  }
   const int32_t p = d.ptid[i];
   if (d.flags[i] & NODE_PARTICLE) {
 #pragma unroll
@@ -964,13 +1025,7 @@ __global__ void k_external(DevData d) {
 }
 
 template <int DIM>
-__global__ void k_force_bc(DevData d) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.n_fbc_nodes || d.ctrl->error) return;
-  const int64_t i = d.fbc_node[t];
-  const double time = d.ctrl->time;
-  double f[3];
-  ldv<DIM>(d.f, i, f);
+__device__ __noinline__ void apply_fbc(const DevData &d, int t, double time, double (&f)[3]) {
   for (int e = d.fbc_row[t]; e < d.fbc_row[t + 1]; e++) {
     const BcSetDev bc = d.fbc_sets[d.fbc_set[e]];
     double fmax = d.fbc_val[e];
@@ -996,6 +1051,16 @@ __global__ void k_force_bc(DevData d) {
     for (int q = 0; q < DIM; q++)
       if ((bc.dir_mask >> q) & 1) f[q] += fmax;
   }
+}
+
+template <int DIM>
+__global__ void k_force_bc(const __grid_constant__ DevData d) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.n_fbc_nodes || d.ctrl->error) return;
+  const int64_t i = d.fbc_node[t];
+  double f[3];
+  ldv<DIM>(d.f, i, f);
+  apply_fbc<DIM>(d, t, d.ctrl->time, f);
   stv<DIM>(d.f, i, f);
 }
 
@@ -1003,9 +1068,15 @@ __global__ void k_force_bc(DevData d) {
 // Post-processing every test_interval steps: DEMModel::ppCompressiveTest
 // (demModel.cpp:2202-2250) or ppTwoParticleTest (:2096-2149).
 // ---------------------------------------------------------------------------
+// The test's post-processing (demModel.cpp ppCompressiveTest / ppTwoParticleTest)
+// run by one 1024-thread block; forces of the current step are read past L1,
+// since other CTAs of the same kernel may have written them.
 template <int DIM>
-__global__ void __launch_bounds__(1024) k_postprocess(DevData d) {
-  __shared__ double red[2][32];
+__device__ __noinline__ void postprocess_block(const DevData &d) {
+  // sums are formed as by a 1024-thread block (per-thread strided partials,
+  // warp butterflies, then the 32 warp sums in order), whatever blockDim is
+  constexpr int kV = 1024;
+  __shared__ double red[2][kV / 32];
   CtrlState *c = d.ctrl;
   if (c->error) return;
   const int64_t n = c->n;
@@ -1014,23 +1085,24 @@ __global__ void __launch_bounds__(1024) k_postprocess(DevData d) {
   if (d.test == PDGPU_TEST_COMPRESSIVE) {
     const DevParticle W = d.particles[d.test_wall];
     const int dir = d.test_dir;
-    double s = 0.0;
-    for (int64_t i = W.start + threadIdx.x; i < W.end; i += blockDim.x)
-      s += d.f[st * i + dir] * d.vol[i];
-    double cr = 0.0;
-    for (int b = threadIdx.x; b < d.cr_blocks; b += blockDim.x) cr += d.cr_partial[b];
-    for (int o = 16; o > 0; o >>= 1) {
-      s += __shfl_xor_sync(0xffffffffu, s, o);
-      cr += __shfl_xor_sync(0xffffffffu, cr, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-      red[0][threadIdx.x >> 5] = s;
-      red[1][threadIdx.x >> 5] = cr;
+    for (int vt = threadIdx.x; vt < kV; vt += blockDim.x) {
+      double s = 0.0;
+      for (int64_t i = W.start + vt; i < W.end; i += kV) s += __ldcg(d.f + st * i + dir) * d.vol[i];
+      double cr = 0.0;
+      for (int b = vt; b < d.cr_blocks; b += kV) cr += d.cr_partial[b];
+      for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        cr += __shfl_xor_sync(0xffffffffu, cr, o);
+      }
+      if ((vt & 31) == 0) {
+        red[0][vt >> 5] = s;
+        red[1][vt >> 5] = cr;
+      }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       double rs = 0.0, rc = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      for (int w = 0; w < kV / 32; w++) {
         rs += red[0][w];
         rc += red[1][w];
       }
@@ -1049,14 +1121,16 @@ __global__ void __launch_bounds__(1024) k_postprocess(DevData d) {
     }
   } else if (d.test == PDGPU_TEST_TWO_PARTICLE && d.n_particles >= 2) {
     const DevParticle P0 = d.particles[0], P1 = d.particles[1];
-    double m = -DBL_MAX;
-    for (int64_t i = P1.start + threadIdx.x; i < P1.end; i += blockDim.x) m = fmax(m, d.x[st * i + 1]);
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) red[0][threadIdx.x >> 5] = m;
+    for (int vt = threadIdx.x; vt < kV; vt += blockDim.x) {
+      double m = -DBL_MAX;
+      for (int64_t i = P1.start + vt; i < P1.end; i += kV) m = fmax(m, d.x[st * i + 1]);
+      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if ((vt & 31) == 0) red[0][vt >> 5] = m;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
       double my = -DBL_MAX;
-      for (int w = 0; w < (int)(blockDim.x >> 5); w++) my = fmax(my, red[0][w]);
+      for (int w = 0; w < kV / 32; w++) my = fmax(my, red[0][w]);
       double dx[3] = {0, 0, 0};
       for (int q = 0; q < DIM; q++) dx[q] = d.x[st * P1.center + q] - d.x[st * P0.center + q];
       const double r = P0.bound_r;
@@ -1073,6 +1147,77 @@ __global__ void __launch_bounds__(1024) k_postprocess(DevData d) {
       c->contact_area_radius = car;
       c->max_y = is_less(0.0, my) ? my : 0.0;
     }
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(1024) k_postprocess(const __grid_constant__ DevData d) {
+  postprocess_block<DIM>(d);
+}
+
+// ---------------------------------------------------------------------------
+// Last kernel of a step: per node, the external-force pass
+// (as k_external: bond forces, then contact forces, damping, gravity), the
+// force BC (as k_force_bc) and, for velocity Verlet, the second half kick (as
+// k_verlet_second); then the last CTA to finish runs the post-processing (as
+// k_postprocess) when `post` is set.
+// ---------------------------------------------------------------------------
+template <int DIM, bool VERLET>
+__global__ void __launch_bounds__(kBlock) k_step_end(const __grid_constant__ DevData d, int post) {
+  __shared__ int last;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < d.n_nodes && !d.ctrl->error) {
+    double f[3] = {0.0, 0.0, 0.0};
+    const uint8_t fl = d.flags[i];
+    if (fl & NODE_ACTIVE) {
+      ldv<DIM>(d.f, i, f);
+      if (d.fc && (fl & (NODE_SEARCH | NODE_SEARCH0))) {
+        double c[3];
+        ldv<DIM>(d.fc, i, c);
+        if (c[0] != 0.0 || c[1] != 0.0 || (DIM == 3 && c[2] != 0.0)) {
+#pragma unroll
+          for (int q = 0; q < DIM; q++) f[q] += c[q];
+          const double z[3] = {0.0, 0.0, 0.0};
+          stv<DIM>(d.fc, i, z);
+        }
+      }
+    }
+    const int32_t p = d.ptid[i];
+    if (fl & NODE_PARTICLE) {
+#pragma unroll
+      for (int q = 0; q < DIM; q++) f[q] += d.fdamp[4 * p + q];
+    }
+    double rho = 0.0;
+    if (d.gravity_on || (VERLET && (fl & NODE_ACTIVE))) rho = d.particles[p].density;
+    if (d.gravity_on) {
+#pragma unroll
+      for (int q = 0; q < DIM; q++) f[q] += rho * d.gravity[q];
+    }
+    if (fl & NODE_FBC) apply_fbc<DIM>(d, d.fbc_of[i], d.ctrl->time, f);
+    stv<DIM>(d.f, i, f);
+    if (VERLET && (fl & NODE_ACTIVE)) {
+      const uint8_t fix = d.fix[i];
+      double v[3];
+      ldv<DIM>(d.v, i, v);
+      const double k = 0.5 * (d.dt / rho);
+#pragma unroll
+      for (int dof = 0; dof < DIM; dof++)
+        if (!((fix >> dof) & 1u)) v[dof] += k * f[dof];
+      stv<DIM>(d.v, i, v);
+      d.vmag[i] = len3<DIM>(v);
+    }
+  }
+  if (!post || d.test == PDGPU_TEST_NONE) return;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&d.ctrl->end_done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    if (threadIdx.x == 0) d.ctrl->end_done = 0u;
+    postprocess_block<DIM>(d);
   }
 }
 
@@ -1220,9 +1365,6 @@ void launch_verlet_second(const DevData &d, cudaStream_t s) {
   PDGPU_DIM_DISPATCH(d, k_verlet_second, <<<blocks_for(d.n_nodes, kBlock), kBlock, 0, s>>>(d));
 }
 void launch_ctrl(const DevData &d, int mode, cudaStream_t s) { k_ctrl<<<1, 1, 0, s>>>(d, mode); }
-void launch_ctrl_cond(const DevData &d, int mode, cudaGraphConditionalHandle h, cudaStream_t s) {
-  k_ctrl_cond<<<1, 1, 0, s>>>(d, mode, h);
-}
 void launch_bc(const DevData &d, cudaStream_t s) {
   if (!d.n_ubc_nodes) return;
   PDGPU_DIM_DISPATCH(d, k_bc, <<<blocks_for(d.n_ubc_nodes, 128), 128, 0, s>>>(d));
@@ -1235,38 +1377,6 @@ size_t scan_temp_bytes(int64_t n) {
   return a > b ? a : b;
 }
 
-template <int DIM, int LPN>
-static void cand_dim(const DevData &d, uint8_t bit, cudaStream_t s, void *tmp, size_t bytes) {
-  const unsigned g = blocks_for(d.n_nodes * LPN, kBlock);
-  k_cand<DIM, LPN, false><<<g, kBlock, 0, s>>>(d, bit);
-  cub::DeviceScan::InclusiveSum(tmp, bytes, d.c_cnt, d.c_row + 1, d.n_nodes, s);
-  k_cand<DIM, LPN, true><<<g, kBlock, 0, s>>>(d, bit);
-  const unsigned gn = blocks_for(d.n_nodes, kBlock);
-  k_compact_flag<<<gn, kBlock, 0, s>>>(d);
-  cub::DeviceScan::InclusiveSum(tmp, bytes, d.c_tmp, d.c_tmp, d.n_nodes, s);
-  k_compact_scatter<<<gn, kBlock, 0, s>>>(d);
-}
-
-void launch_contact_update(const DevData &d, void *tmp, size_t bytes, int lanes, int init,
-                           cudaStream_t s) {
-  // the build of DEMModel::init searches with the flags it had before the
-  // two_particle override switched particle 0's force off
-  const uint8_t bit = init ? NODE_SEARCH0 : NODE_SEARCH;
-  const unsigned gn = blocks_for(d.n_nodes, kBlock);
-  k_zero_cells<<<blocks_for(d.grid.ncells + 1, kBlock), kBlock, 0, s>>>(d);
-  PDGPU_DIM_DISPATCH(d, k_cell_count, <<<gn, kBlock, 0, s>>>(d, d.x, d.grid));
-  cub::DeviceScan::ExclusiveSum(tmp, bytes, d.cell_cnt, d.cell_start, d.grid.ncells + 1, s);
-  k_cell_scatter<<<gn, kBlock, 0, s>>>(d);
-  k_cell_sort<<<blocks_for((int64_t)d.grid.ncells * 32, kBlock), kBlock, 0, s>>>(d);
-  if (d.dim == 2) {
-    if (lanes <= 8) cand_dim<2, 8>(d, bit, s, tmp, bytes);
-    else cand_dim<2, 32>(d, bit, s, tmp, bytes);
-  } else {
-    if (lanes <= 8) cand_dim<3, 8>(d, bit, s, tmp, bytes);
-    else cand_dim<3, 32>(d, bit, s, tmp, bytes);
-  }
-  k_cand_check<<<1, 1, 0, s>>>(d);
-}
 
 template <int DIM, int LPN>
 static cudaError_t rebuild_dim(const DevData &d, uint8_t bit, int64_t *bsum, int grid,
@@ -1317,6 +1427,28 @@ void launch_external(const DevData &d, cudaStream_t s) {
   PDGPU_DIM_DISPATCH(d, k_external, <<<blocks_for(d.n_nodes, kBlock), kBlock, 0, s>>>(d));
   if (d.n_fbc_nodes)
     PDGPU_DIM_DISPATCH(d, k_force_bc, <<<blocks_for(d.n_fbc_nodes, 128), 128, 0, s>>>(d));
+}
+
+void launch_step_begin(const DevData &d, int verlet, cudaStream_t s) {
+  const unsigned g = blocks_for(d.n_nodes, kBlock);
+  if (d.dim == 2) {
+    if (verlet) k_step_begin<2, true><<<g, kBlock, 0, s>>>(d);
+    else k_step_begin<2, false><<<g, kBlock, 0, s>>>(d);
+  } else {
+    if (verlet) k_step_begin<3, true><<<g, kBlock, 0, s>>>(d);
+    else k_step_begin<3, false><<<g, kBlock, 0, s>>>(d);
+  }
+}
+
+void launch_step_end(const DevData &d, int verlet, int post, cudaStream_t s) {
+  const unsigned g = blocks_for(d.n_nodes, kBlock);
+  if (d.dim == 2) {
+    if (verlet) k_step_end<2, true><<<g, kBlock, 0, s>>>(d, post);
+    else k_step_end<2, false><<<g, kBlock, 0, s>>>(d, post);
+  } else {
+    if (verlet) k_step_end<3, true><<<g, kBlock, 0, s>>>(d, post);
+    else k_step_end<3, false><<<g, kBlock, 0, s>>>(d, post);
+  }
 }
 
 void launch_postprocess(const DevData &d, cudaStream_t s) {

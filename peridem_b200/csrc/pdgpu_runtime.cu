@@ -77,6 +77,9 @@ struct pdgpu_ctx {
   cudaGraphExec_t gexec = nullptr;
   int graph_steps = 0;
   cudaStream_t side = nullptr;  // captures the body of the rebuild's conditional node
+  // contact and damping run on `branch` beside the bond loop on `stream`
+  cudaStream_t branch = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
   // timing
   bool timing = false;
@@ -161,17 +164,22 @@ cudaEvent_t take_event(pdgpu_ctx *c) {
 }
 
 template <class F>
-void run(pdgpu_ctx *c, const char *name, F &&f) {
+void run_on(pdgpu_ctx *c, cudaStream_t s, const char *name, F &&f) {
   if (!c->timing) {
     f();
     return;
   }
   const int slot = timed_slot(c, name);
   cudaEvent_t a = take_event(c), b = take_event(c);
-  cudaEventRecord(a, c->stream);
+  cudaEventRecord(a, s);
   f();
-  cudaEventRecord(b, c->stream);
+  cudaEventRecord(b, s);
   c->pending.push_back({slot, a, b});
+}
+
+template <class F>
+void run(pdgpu_ctx *c, const char *name, F &&f) {
+  run_on(c, c->stream, name, f);
 }
 
 void resolve_timing(pdgpu_ctx *c) {
@@ -632,14 +640,29 @@ int prepare(pdgpu_ctx *ctx) {
       if (!(f & NODE_ACTIVE)) svmax = std::max(svmax, ctx->vmag0[i]);
     }
   }
+  // BC tables (entries sorted by node), then the per-node BC rows
+  TRY(upload_bc_tables(ctx, true));
+  TRY(upload_bc_tables(ctx, false));
+  for (int disp = 1; disp >= 0; disp--) {
+    const auto &ent = disp ? ctx->ubc_e : ctx->fbc_e;
+    std::vector<int32_t> of((size_t)N, -1);
+    int32_t t = -1;
+    for (size_t k = 0; k < ent.size(); k++) {
+      if (k == 0 || ent[k].node != ent[k - 1].node) t++;
+      of[ent[k].node] = t;
+      flags[ent[k].node] |= disp ? NODE_UBC : NODE_FBC;
+    }
+    int32_t *dof;
+    TRY(dalloc(ctx, &dof, (size_t)N));
+    CK(cudaMemcpy(dof, of.data(), (size_t)N * 4, cudaMemcpyHostToDevice));
+    (disp ? d.ubc_of : d.fbc_of) = dof;
+  }
   TRY(dalloc(ctx, &d.flags, N));
   CK(cudaMemcpy(d.flags, flags.data(), N, cudaMemcpyHostToDevice));
   // IC particle flags
   TRY(dalloc(ctx, &d.ic_particle, ctx->hp.size()));
   if (ctx->ic_sel.size() != ctx->hp.size()) ctx->ic_sel.assign(ctx->hp.size(), 0);
   CK(cudaMemcpy(d.ic_particle, ctx->ic_sel.data(), ctx->hp.size(), cudaMemcpyHostToDevice));
-  TRY(upload_bc_tables(ctx, true));
-  TRY(upload_bc_tables(ctx, false));
   // lanes per node from the average bonds per node (measured on B200: the
   // FP32 form runs fastest with a thread per node at ~23 bonds per node)
   const double bpn = N ? (double)d.n_bonds / (double)N : 0.0;
@@ -651,7 +674,8 @@ int prepare(pdgpu_ctx *ctx) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    d.contact_grid = 4 * (sms > 0 ? sms : 148);
+    // one CTA per SM: the pass is latency-bound and runs beside the bond loop
+    d.contact_grid = sms > 0 ? sms : 148;
   }
   d.cr_blocks = d.contact_grid;
   TRY(dalloc(ctx, &d.cr_partial, (size_t)d.cr_blocks + 1));
@@ -660,12 +684,45 @@ int prepare(pdgpu_ctx *ctx) {
   d.history_cap = kHistoryCap;
   TRY(dalloc(ctx, &d.fdamp, ctx->hp.size() * 4));
   CK(cudaMemset(d.fdamp, 0, ctx->hp.size() * 4 * 8));
+  if (ctx->desc.multi_particle) {
+    const size_t st = d.dim == 2 ? 2 : 4;
+    TRY(dalloc(ctx, &d.fc, st * (size_t)N));
+    CK(cudaMemset(d.fc, 0, st * (size_t)N * 8));
+    if (!ctx->branch) {
+      // highest priority: the branch's few latency-bound CTAs are scheduled
+      // ahead of the bond loop's remaining tiles
+      int lo = 0, hi = 0;
+      CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      CK(cudaStreamCreateWithPriority(&ctx->branch, cudaStreamDefault, hi));
+    }
+    if (!ctx->ev_fork) CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    if (!ctx->ev_join) CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+  }
   TRY(dalloc(ctx, &d.c_row, (size_t)N + 1));
   CK(cudaMemset(d.c_row, 0, ((size_t)N + 1) * 8));
   TRY(dalloc(ctx, &d.c_cnt, (size_t)N));
   CK(cudaMemset(d.c_cnt, 0, (size_t)N * 8));
   TRY(dalloc(ctx, &d.c_tmp, (size_t)N + 1));
   TRY(dalloc(ctx, &d.c_nodes, (size_t)N));
+  TRY(dalloc(ctx, &d.c_span, (size_t)N));
+  CK(cudaMemset(d.c_span, 0, (size_t)N * sizeof(int2)));
+  {
+    // per-node zone and compact per-particle damping constants
+    if (d.n_zones > 255) return fail(ctx, PDGPU_ERR_ARG, "at most 255 contact zones");
+    std::vector<uint8_t> nz((size_t)N, 0);
+    std::vector<DampParticle> dp(ctx->hp.size());
+    for (size_t p = 0; p < ctx->hp.size(); p++) {
+      const DevParticle &P = ctx->hp[p];
+      for (int64_t i = P.start; i < P.end; i++) nz[i] = (uint8_t)P.zone;
+      dp[p] = DampParticle{P.bound_r, P.density, P.zone, P.type};
+    }
+    TRY(dalloc(ctx, &d.nzone, (size_t)N));
+    CK(cudaMemcpy(d.nzone, nz.data(), (size_t)N, cudaMemcpyHostToDevice));
+    TRY(dalloc(ctx, &d.dpart, dp.size()));
+    CK(cudaMemcpy(d.dpart, dp.data(), dp.size() * sizeof(DampParticle), cudaMemcpyHostToDevice));
+    TRY(dalloc(ctx, &d.pcen, 8 * dp.size()));
+    CK(cudaMemset(d.pcen, 0, 8 * dp.size() * 8));
+  }
   if (ctx->desc.multi_particle) {
     d.contact_cap = ctx->desc.contact_capacity > 0 ? ctx->desc.contact_capacity
                                                    : std::max<int64_t>(64 * nsearch, 1 << 20);
@@ -729,18 +786,31 @@ void pd_forces(pdgpu_ctx *ctx) {
     });
 }
 
-void compute_forces(pdgpu_ctx *ctx) {
+// Contact forces and particle damping depend on positions and velocities
+// only, not on the bond loop's forces: they run on the branch stream while
+// the bond loop runs, and the external-force pass (after the join) adds
+// their results to f in the reference's order: bond forces, contact forces,
+// damping, external forces.
+void compute_forces(pdgpu_ctx *ctx, bool step) {
   DevData &d = ctx->d;
   cudaStream_t s = ctx->stream;
-  pd_forces(ctx);
   if (ctx->desc.multi_particle) {
+    // the cooperative rebuild stays on the main stream, ahead of the fork
     run(ctx, "contact_update", [&] {
       launch_contact_rebuild(d, ctx->rebuild_bsum, ctx->rebuild_grid, ctx->contact_lanes, 0, s);
     });
-    run(ctx, "contact_force", [&] { launch_contact_force(d, ctx->contact_lanes, s); });
-    run(ctx, "damping", [&] { launch_damping(d, s); });
+    cudaEventRecord(ctx->ev_fork, s);
+    cudaStreamWaitEvent(ctx->branch, ctx->ev_fork, 0);
+    run_on(ctx, ctx->branch, "contact_force", [&] { launch_contact_force(d, ctx->contact_lanes, ctx->branch); });
+    run_on(ctx, ctx->branch, "damping", [&] { launch_damping(d, ctx->branch); });
+    cudaEventRecord(ctx->ev_join, ctx->branch);
   }
-  run(ctx, "external", [&] { launch_external(d, s); });
+  pd_forces(ctx);
+  if (ctx->desc.multi_particle) cudaStreamWaitEvent(s, ctx->ev_join, 0);
+  // external forces and force BC; in a step also the Verlet second half and
+  // the post-processing
+  const bool verlet = ctx->desc.time_scheme == 1;
+  run(ctx, "step_end", [&] { launch_step_end(d, step && verlet, step ? 1 : 0, s); });
 }
 
 // DEMModel::integrateStep (demModel.cpp:342-460) + post-processing
@@ -748,25 +818,40 @@ void one_step(pdgpu_ctx *ctx) {
   DevData &d = ctx->d;
   cudaStream_t s = ctx->stream;
   const bool verlet = ctx->desc.time_scheme == 1;
-  run(ctx, "integrate", [&] { launch_integrate(d, verlet ? 1 : 0, s); });
-  run(ctx, "ctrl", [&] { launch_ctrl(d, 0, s); });
-  run(ctx, "displacement_bc", [&] { launch_bc(d, s); });
-  compute_forces(ctx);
-  if (verlet) run(ctx, "integrate_second", [&] { launch_verlet_second(d, s); });
-  run(ctx, "postprocess", [&] { launch_postprocess(d, s); });
+  // integrate, displacement BC, step control
+  run(ctx, "step_begin", [&] { launch_step_begin(d, verlet ? 1 : 0, s); });
+  compute_forces(ctx, true);
 }
 
 // One step inside a graph under capture: like one_step, but the contact-list
 // rebuild sits in a conditional node that the step-control kernel switches
 // on only on rebuild steps, so other steps pay nothing for it.
-cudaError_t graph_step(pdgpu_ctx *ctx, cudaGraphConditionalHandle h, const char **where) {
+cudaError_t graph_step(pdgpu_ctx *ctx, const char **where) {
   DevData &d = ctx->d;
   cudaStream_t s = ctx->stream;
   const bool verlet = ctx->desc.time_scheme == 1;
   const bool mixed = d.precision == PDGPU_PREC_MIXED;
-  launch_integrate(d, verlet ? 1 : 0, s);
-  launch_ctrl_cond(d, 0, h, s);
-  launch_bc(d, s);
+  launch_step_begin(d, verlet ? 1 : 0, s);
+  cudaError_t e = cudaSuccess;
+  if (ctx->desc.multi_particle) {
+    // contact-list rebuild: the single-launch cooperative kernel, which exits
+    // at once on steps without a rebuild; on the main path, where nothing
+    // else runs beside its grid-wide syncs
+    *where = "contact-list rebuild";
+    e = launch_contact_rebuild(d, ctx->rebuild_bsum, ctx->rebuild_grid, ctx->contact_lanes, 0, s);
+    if (e != cudaSuccess) return e;
+    // branch (captured first, so its kernels are dispatched ahead of the bond
+    // loop's tiles): contact forces, then damping
+    *where = "fork";
+    e = cudaEventRecord(ctx->ev_fork, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->branch, ctx->ev_fork, 0);
+    if (e != cudaSuccess) return e;
+    launch_contact_force(d, ctx->contact_lanes, ctx->branch);
+    launch_damping(d, ctx->branch);
+    e = cudaEventRecord(ctx->ev_join, ctx->branch);
+    if (e != cudaSuccess) return e;
+  }
+  // main: bond loop
   if (ctx->state_prepass) {
     if (mixed) launch_prepass_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
     else launch_prepass_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
@@ -775,78 +860,28 @@ cudaError_t graph_step(pdgpu_ctx *ctx, cudaGraphConditionalHandle h, const char 
   if (mixed) launch_pd_tiled_mixed(d, ctx->tiles, ctx->tile_law, ctx->pd_lanes, smem, s);
   else launch_pd_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
   if (ctx->desc.multi_particle) {
-    cudaStreamCaptureStatus st;
-    cudaGraph_t g;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t nd = 0;
-    *where = "kernels before the rebuild";
-    cudaError_t e = cudaGetLastError();
+    *where = "join";
+    e = cudaStreamWaitEvent(s, ctx->ev_join, 0);
     if (e != cudaSuccess) return e;
-    *where = "cudaStreamGetCaptureInfo";
-    e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd);
-    if (e != cudaSuccess) return e;
-    cudaGraphNodeParams p{};
-    p.type = cudaGraphNodeTypeConditional;
-    p.conditional.handle = h;
-    p.conditional.type = cudaGraphCondTypeIf;
-    p.conditional.size = 1;
-    cudaGraphNode_t node;
-    *where = "cudaGraphAddNode(conditional)";
-    e = cudaGraphAddNode(&node, g, deps, nd, &p);
-    if (e != cudaSuccess) return e;
-    *where = "cudaStreamUpdateCaptureDependencies";
-    e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
-    if (e != cudaSuccess) return e;
-    cudaGraph_t body = p.conditional.phGraph_out[0];
-    *where = "cudaStreamBeginCaptureToGraph(body)";
-    e = cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return e;
-    launch_contact_update(d, ctx->scan_tmp, ctx->scan_bytes, ctx->contact_lanes, 0, ctx->side);
-    *where = "contact-rebuild body kernels";
-    const cudaError_t eb = cudaGetLastError();
-    e = cudaStreamEndCapture(ctx->side, &body);
-    if (eb != cudaSuccess) return eb;
-    *where = "cudaStreamEndCapture(body)";
-    if (e != cudaSuccess) return e;
-    *where = "kernels after the rebuild";
-    launch_contact_force(d, ctx->contact_lanes, s);
-    launch_damping(d, s);
   }
-  launch_external(d, s);
-  if (verlet) launch_verlet_second(d, s);
-  launch_postprocess(d, s);
+  *where = "kernels after the join";
+  launch_step_end(d, verlet ? 1 : 0, 1, s);
   return cudaGetLastError();
 }
 
 int build_graph(pdgpu_ctx *ctx, int steps) {
-  if (!ctx->side) CK(cudaStreamCreate(&ctx->side));
   cudaStream_t s = ctx->stream;
-  // the conditional handle belongs to a graph created up front, which the
-  // stream then captures into
   cudaGraph_t g = nullptr;
-  CK(cudaGraphCreate(&g, 0));
-  // one handle per conditional node (a handle drives exactly one node)
-  std::vector<cudaGraphConditionalHandle> hs(steps);
-  cudaError_t e = cudaSuccess;
-  for (int k = 0; k < steps && e == cudaSuccess; k++)
-    e = cudaGraphConditionalHandleCreate(&hs[k], g, 0, cudaGraphCondAssignDefault);
-  if (e != cudaSuccess) {
-    cudaGraphDestroy(g);
-    return fail(ctx, PDGPU_ERR_CUDA, "cudaGraphConditionalHandleCreate: %s", cudaGetErrorString(e));
-  }
-  e = cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) {
-    cudaGraphDestroy(g);
-    return fail(ctx, PDGPU_ERR_CUDA, "cudaStreamBeginCaptureToGraph: %s", cudaGetErrorString(e));
-  }
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   const char *where = "graph_step";
-  for (int k = 0; k < steps && e == cudaSuccess; k++) e = graph_step(ctx, hs[k], &where);
-  cudaGraph_t done = nullptr;
-  const cudaError_t e2 = cudaStreamEndCapture(s, &done);
+  cudaError_t e = cudaSuccess;
+  int k = 0;
+  for (; k < steps && e == cudaSuccess; k++) e = graph_step(ctx, &where);
+  const cudaError_t e2 = cudaStreamEndCapture(s, &g);
   if (e != cudaSuccess || e2 != cudaSuccess) {
-    cudaGraphDestroy(g);
+    if (g) cudaGraphDestroy(g);
     return fail(ctx, PDGPU_ERR_CUDA, "graph capture failed in %s (step %d of %d): %s",
-                e != cudaSuccess ? where : "cudaStreamEndCapture", 0, steps,
+                e != cudaSuccess ? where : "cudaStreamEndCapture", k, steps,
                 cudaGetErrorString(e != cudaSuccess ? e : e2));
   }
   e = cudaGraphInstantiate(&ctx->gexec, g, 0);
@@ -936,6 +971,9 @@ void pdgpu_destroy(pdgpu_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   if (ctx->side) cudaStreamDestroy(ctx->side);
+  if (ctx->branch) cudaStreamDestroy(ctx->branch);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   for (auto &t : ctx->pending) {
     cudaEventDestroy(t.a);
     cudaEventDestroy(t.b);
@@ -1224,7 +1262,7 @@ int pdgpu_integrate_begin(pdgpu_ctx *ctx) {
   if (d.ic_active) run(ctx, "initial_condition", [&] { launch_apply_ic(d, s); });
   run(ctx, "displacement_bc", [&] { launch_bc(d, s); });
   run(ctx, "ctrl", [&] { launch_ctrl(d, 1, s); });
-  compute_forces(ctx);
+  compute_forces(ctx, false);
   CK(cudaGetLastError());
   TRY(device_error(ctx));
   ctx->begun = true;
@@ -1399,7 +1437,8 @@ int pdgpu_step_host(pdgpu_ctx *ctx, double *u, double *v, double *x, double *f, 
     CK(cudaMemcpyAsync(ctx->stage, hosts[k], bytes, cudaMemcpyHostToDevice, s));
     launch_pack_vec(d, ctx->stage, vecs[k], s);
   }
-  for (int64_t k = 0; k < nsteps; k++) one_step(ctx);
+  // replay of the step graph (one step per replay unless a longer graph exists)
+  TRY(pdgpu_step_graph(ctx, nsteps, ctx->gexec ? ctx->graph_steps : 1));
   double *outs[4] = {d.u, d.v, d.x, d.f};
   double *hout[4] = {u, v, x, f};
   for (int k = 0; k < 4; k++) {
