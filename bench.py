@@ -15,8 +15,9 @@ contact forces, particle damping, external forces, post-processing).
 
 Timing: W untimed steps, then K steps each timed with CUDA events on the
 model's stream, with a 512 MiB buffer written and then read back between
-steps to flush the 126 MB L2 (the read leaves it clean); max over ranks.  N > 1 runs N independent replicas (one scene per
-GPU, no collective), so scaling is weak.
+steps to flush the 126 MB L2 (the read leaves it clean); max over ranks.
+N > 1 runs N independent replicas (one scene per GPU, no collective), so
+scaling is weak.
 """
 import argparse
 import glob

@@ -43,6 +43,10 @@ __device__ __forceinline__ void bar_init(uint64_t *bar) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+// orders this CTA's earlier shared-memory accesses before later bulk-copy writes
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 __device__ __forceinline__ void bar_arrive_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sa(bar)), "r"(bytes)
                : "memory");
@@ -65,10 +69,10 @@ __device__ __forceinline__ bool bar_try(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// true once phase 0 completed; false after kWaitTries attempts
-__device__ __forceinline__ bool bar_wait(uint64_t *bar) {
+// true once the phase of the given parity completed; false after kWaitTries attempts
+__device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t parity) {
   for (unsigned t = 0; t < kWaitTries; t++)
-    if (bar_try(bar, 0)) return true;
+    if (bar_try(bar, parity)) return true;
   return false;
 }
 
@@ -272,81 +276,133 @@ __device__ __forceinline__ void tile_nodes(const DevData &d, const BondTile &T, 
   }
 }
 
+// Persistent: a fixed grid (below full occupancy, so that the contact and
+// damping passes running beside it find room) claims tiles from a counter in
+// the step-control state; the claim for the next tile is made while the
+// current one is staged.  The last CTA out resets the counter.
 template <int DIM, int LPN, int LAW, typename CT>
-__global__ void __launch_bounds__(kThreads) k_bonds_mixed(DevData d, const BondTile *tiles, const CT *col) {
+__global__ void __launch_bounds__(kThreads) k_bonds_mixed(DevData d, const BondTile *tiles, int n_tiles,
+                                                         const CT *col) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_tile[2];
   if (d.ctrl->error) return;
-  const BondTile T = tiles[blockIdx.x];
   constexpr bool state = LAW == LAW_STATE;
-  const int w = (int)(T.win_end - T.win_begin);
-  const Plan p = plan(DIM, state, (int)sizeof(CT), T.bond_begin, T.bond_end, T.node_begin, T.node_end, w);
-  CT *s_col = reinterpret_cast<CT *>(smem);
-  uint32_t *s_bits = reinterpret_cast<uint32_t *>(smem + p.col_bytes);
-  int64_t *s_row = reinterpret_cast<int64_t *>(smem + p.off_row);
-  float4 *s_xv = reinterpret_cast<float4 *>(smem + p.off_xv);
-  float2 *s_u2 = reinterpret_cast<float2 *>(smem + p.off_u);
-  float4 *s_u4 = reinterpret_cast<float4 *>(smem + p.off_u);
-  float2 *s_m = reinterpret_cast<float2 *>(smem + p.off_m);
-
-  // columns, bitmap words, row offsets and constant node records of the
-  // tile: bulk copies
   if (threadIdx.x == 0) {
     bar_init(&bar);
-    bar_arrive_tx(&bar, p.col_bytes + p.bit_bytes + p.row_bytes + 16u * (uint32_t)w);
-    if (p.col_bytes) bulk_load(s_col, col + p.col0, p.col_bytes, &bar);
-    if (p.bit_bytes) bulk_load(s_bits, d.bond_bits + p.word0, p.bit_bytes, &bar);
-    bulk_load(s_row, d.pd_row + p.row0, p.row_bytes, &bar);
-    bulk_load(s_xv, d.xv_mixed + T.win_begin, 16u * (uint32_t)w, &bar);
-  }
-  const MixParticle M = d.mixp[T.particle];
-
-  // displacements of the window relative to the particle centre's
-  {
-    const int st = DIM == 2 ? 2 : 4;
-    double uc[DIM];
-#pragma unroll
-    for (int q = 0; q < DIM; q++) uc[q] = d.u[st * T.center + q];
-    for (int a = threadIdx.x; a < w; a += kThreads) {
-      const int64_t j = T.win_begin + a;
-      if constexpr (DIM == 2) {
-        const double2 uj = *reinterpret_cast<const double2 *>(d.u + 2 * j);
-        s_u2[a] = make_float2((float)(uj.x - uc[0]), (float)(uj.y - uc[1]));
-      } else {
-        const double2 u01 = *reinterpret_cast<const double2 *>(d.u + 4 * j);
-        const double u2 = d.u[4 * j + 2];
-        s_u4[a] = make_float4((float)(u01.x - uc[0]), (float)(u01.y - uc[1]), (float)(u2 - uc[2]), 0.f);
-      }
-      if (state) {
-        const double inv_m = 1.0 / d.mx[j];
-        s_m[a] = make_float2((float)(d.theta[j] * M.tf_coef * inv_m), (float)(M.am_coef * inv_m));
-      }
-    }
+    s_tile[0] = (int)atomicAdd(&d.ctrl->tile_next, 1u);
   }
   __syncthreads();
-  if (!bar_wait(&bar)) {
-    // the copies did not land: record it, give them one more bounded wait so
-    // that none is left writing into this CTA's shared memory, and stop
-    if (threadIdx.x == 0 && atomicCAS(&d.ctrl->error, 0, DEV_ERR_STAGE_TIMEOUT) == 0)
-      d.ctrl->error_info = blockIdx.x;
-    bar_wait(&bar);
-    return;
-  }
+  uint32_t parity = 0;
+  int k = 0;
+  int t = s_tile[0];
+  while (t < n_tiles) {
+    const BondTile T = tiles[t];
+    const int w = (int)(T.win_end - T.win_begin);
+    const Plan p = plan(DIM, state, (int)sizeof(CT), T.bond_begin, T.bond_end, T.node_begin, T.node_end, w);
+    CT *s_col = reinterpret_cast<CT *>(smem);
+    uint32_t *s_bits = reinterpret_cast<uint32_t *>(smem + p.col_bytes);
+    int64_t *s_row = reinterpret_cast<int64_t *>(smem + p.off_row);
+    float4 *s_xv = reinterpret_cast<float4 *>(smem + p.off_xv);
+    float2 *s_u2 = reinterpret_cast<float2 *>(smem + p.off_u);
+    float4 *s_u4 = reinterpret_cast<float4 *>(smem + p.off_u);
+    float2 *s_m = reinterpret_cast<float2 *>(smem + p.off_m);
 
-  View<DIM> V{s_xv, s_u2, s_u4, s_m};
-  tile_nodes<DIM, LPN, LAW, CT>(d, T, M, V, s_col, s_bits, s_row, p);
+    // columns, bitmap words, row offsets and constant node records of the
+    // tile: bulk copies; then the claim of the next tile
+    if (threadIdx.x == 0) {
+      fence_async_smem();
+      bar_arrive_tx(&bar, p.col_bytes + p.bit_bytes + p.row_bytes + 16u * (uint32_t)w);
+      if (p.col_bytes) bulk_load(s_col, col + p.col0, p.col_bytes, &bar);
+      if (p.bit_bytes) bulk_load(s_bits, d.bond_bits + p.word0, p.bit_bytes, &bar);
+      bulk_load(s_row, d.pd_row + p.row0, p.row_bytes, &bar);
+      bulk_load(s_xv, d.xv_mixed + T.win_begin, 16u * (uint32_t)w, &bar);
+      s_tile[(k + 1) & 1] = (int)atomicAdd(&d.ctrl->tile_next, 1u);
+    }
+    const MixParticle M = d.mixp[T.particle];
+
+    // displacements of the window relative to the particle centre's
+    {
+      const int st = DIM == 2 ? 2 : 4;
+      double uc[DIM];
+#pragma unroll
+      for (int q = 0; q < DIM; q++) uc[q] = d.u[st * T.center + q];
+      for (int a = threadIdx.x; a < w; a += kThreads) {
+        const int64_t j = T.win_begin + a;
+        if constexpr (DIM == 2) {
+          const double2 uj = *reinterpret_cast<const double2 *>(d.u + 2 * j);
+          s_u2[a] = make_float2((float)(uj.x - uc[0]), (float)(uj.y - uc[1]));
+        } else {
+          const double2 u01 = *reinterpret_cast<const double2 *>(d.u + 4 * j);
+          const double u2 = d.u[4 * j + 2];
+          s_u4[a] = make_float4((float)(u01.x - uc[0]), (float)(u01.y - uc[1]), (float)(u2 - uc[2]), 0.f);
+        }
+        if (state) {
+          const double inv_m = 1.0 / d.mx[j];
+          s_m[a] = make_float2((float)(d.theta[j] * M.tf_coef * inv_m), (float)(M.am_coef * inv_m));
+        }
+      }
+    }
+    __syncthreads();
+    const bool landed = bar_wait(&bar, parity);
+    parity ^= 1u;
+    if (__syncthreads_or(!landed)) {
+      // the copies did not land: record it, give them one more bounded wait
+      // so that none is left writing into this CTA's shared memory, and stop
+      if (threadIdx.x == 0 && atomicCAS(&d.ctrl->error, 0, DEV_ERR_STAGE_TIMEOUT) == 0)
+        d.ctrl->error_info = t;
+      if (!landed) bar_wait(&bar, parity ^ 1u);
+      return;
+    }
+
+    View<DIM> V{s_xv, s_u2, s_u4, s_m};
+    tile_nodes<DIM, LPN, LAW, CT>(d, T, M, V, s_col, s_bits, s_row, p);
+    const int t_next = s_tile[(k + 1) & 1];
+    __syncthreads();  // the stage is free for the next tile's copies
+    t = t_next;
+    k++;
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&d.ctrl->tile_done, 1u) == gridDim.x - 1) {
+      atomicExch(&d.ctrl->tile_next, 0u);
+      atomicExch(&d.ctrl->tile_done, 0u);
+    }
+  }
+}
+
+// CTAs per SM for the persistent bond loop: one below the occupancy limit
+template <class K>
+int bond_grid(K kernel, size_t smem, int n_tiles) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  int per = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, smem);
+  const int g = sms * (per > 1 ? per - 1 : 1);
+  return g < n_tiles ? g : n_tiles;
+}
+
+template <int DIM, int LPN, int LAW, typename CT>
+void launch_one(const DevData &d, const CT *col, const BondTile *t, int n, size_t smem, cudaStream_t s) {
+  auto *k = k_bonds_mixed<DIM, LPN, LAW, CT>;
+  k<<<bond_grid(k, smem, n), kThreads, smem, s>>>(d, t, n, col);
 }
 
 template <int DIM, int LAW, typename CT>
 void launch_law(const DevData &d, const CT *col, const BondTile *t, int n, int lanes, size_t smem,
                 cudaStream_t s) {
   switch (lanes) {
-    case 1: k_bonds_mixed<DIM, 1, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
-    case 2: k_bonds_mixed<DIM, 2, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
-    case 4: k_bonds_mixed<DIM, 4, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
-    case 8: k_bonds_mixed<DIM, 8, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
-    case 16: k_bonds_mixed<DIM, 16, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
-    default: k_bonds_mixed<DIM, 32, LAW, CT><<<n, kThreads, smem, s>>>(d, t, col); break;
+    case 1: launch_one<DIM, 1, LAW, CT>(d, col, t, n, smem, s); break;
+    case 2: launch_one<DIM, 2, LAW, CT>(d, col, t, n, smem, s); break;
+    case 4: launch_one<DIM, 4, LAW, CT>(d, col, t, n, smem, s); break;
+    case 8: launch_one<DIM, 8, LAW, CT>(d, col, t, n, smem, s); break;
+    case 16: launch_one<DIM, 16, LAW, CT>(d, col, t, n, smem, s); break;
+    default: launch_one<DIM, 32, LAW, CT>(d, col, t, n, smem, s); break;
   }
 }
 

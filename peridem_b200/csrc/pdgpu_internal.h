@@ -80,6 +80,8 @@ struct CtrlState {
   int64_t c_nnodes;  // nodes with a non-empty contact candidate list
   // CTAs finished in the fused step kernels (the last one runs the serial tail)
   uint32_t begin_done, end_done;
+  // tile claims and finished CTAs of the persistent bond loop (reset by its last CTA)
+  uint32_t tile_next, tile_done;
 };
 
 // Cell grid fixed at set-up; nodes outside are clamped to the border cells,
