@@ -601,63 +601,229 @@ __device__ void grid_scan(cg::grid_group &g, F in, Tout *out, int64_t n, int64_t
   g.sync();
 }
 
-template <int DIM, int LPN>
-__device__ __forceinline__ int64_t cand_node(const DevData &d, int64_t i, int lane, unsigned gm,
-                                             unsigned lane_base, bool fill) {
-  const Grid g = d.grid;
-  double q[3];
-  ldv<DIM>(d.x, i, q);
-  const int32_t pi = d.ptid[i];
+
+// Candidate pass, cell-centric: a warp takes a centre cell and stages its
+// neighbourhood (the 3^DIM cells around it, z, y, x ascending; each cell's
+// nodes ascending) in its own slice of shared memory, in chunks; every
+// searching node of the centre cell scans the staged list in that order with
+// the strict test sum_d (q_d - p_d)^2 < r^2 (nanoflann's L2 order), skipping
+// nodes of its own particle.  Each node's candidates thus come in (cell, node
+// index) order.  COUNT writes c_cnt for every node; FILL writes the columns.
+// Per-warp staging of the candidate pass, in dynamic shared memory: a chunk
+// of neighbourhood entries (position, node, particle) and the state of up to
+// kCandCentres centre nodes (position, particle, running count / output slot).
+constexpr int kCandChunk = 256;
+constexpr int kCandCentres = 64;
+
+template <int DIM>
+struct CandWarp {
+  double x[DIM][kCandChunk];
+  double q[DIM][kCandCentres];
+  int64_t out[kCandCentres];
+  int32_t j[kCandChunk], p[kCandChunk];
+  int32_t ci[kCandCentres], pi[kCandCentres];
+  int32_t nb_s[DIM == 3 ? 27 : 9], nb_off[(DIM == 3 ? 27 : 9) + 1];
+};
+
+template <int DIM>
+constexpr size_t cand_stage_bytes() {
+  return sizeof(CandWarp<DIM>) * (kCoopBlock / 32);
+}
+
+template <int DIM, int LPN, bool FILL>
+__device__ void cand_cells(const DevData &d, uint8_t search_bit, CandWarp<DIM> *stage) {
+  constexpr int kWarps = kCoopBlock / 32;
+  constexpr int kNb = DIM == 3 ? 27 : 9;
+  const int wl = threadIdx.x >> 5, l32 = threadIdx.x & 31;
+  CandWarp<DIM> &W = stage[wl];
+  const Grid G = d.grid;
   const double r = d.ctrl->radius;
   const double r2 = r * r;
-  int c[3] = {cell_coord<DIM>(q[0], g, 0), cell_coord<DIM>(q[1], g, 1),
-              DIM == 3 ? cell_coord<DIM>(q[2], g, 2) : 0};
-  int64_t out = fill ? d.c_row[i] : 0;
-  const int64_t out_end = fill ? d.c_row[i + 1] : 0;
-  int64_t count = 0;
-  const int zlo = DIM == 3 ? max(c[2] - 1, 0) : 0;
-  const int zhi = DIM == 3 ? min(c[2] + 1, g.dims[2] - 1) : 0;
-  for (int cz = zlo; cz <= zhi; cz++)
-    for (int cy = max(c[1] - 1, 0); cy <= min(c[1] + 1, g.dims[1] - 1); cy++)
-      for (int cx = max(c[0] - 1, 0); cx <= min(c[0] + 1, g.dims[0] - 1); cx++) {
-        const int cell = cx + g.dims[0] * (cy + g.dims[1] * cz);
-        const int s = d.cell_start[cell], e = d.cell_start[cell + 1];
-        for (int base = s; base < e; base += LPN) {
-          const int a = base + lane;
-          bool hit = false;
-          int32_t j = -1;
-          if (a < e) {
-            j = d.cell_nodes[a];
-            if (d.ptid[j] != pi) {
-              double p[3];
-              ldv<DIM>(d.x, j, p);
-              double dd = 0.0;
+  const int lane = threadIdx.x % LPN;
+  const unsigned gm = group_mask<LPN>();
+  const unsigned lane_base = (threadIdx.x & 31u) / LPN * LPN;
+  constexpr int kGroups = 32 / LPN;
+  const int grp = l32 / LPN;
+  const int64_t nwarps = (int64_t)gridDim.x * kWarps;
+  for (int64_t c = (int64_t)blockIdx.x * kWarps + wl; c < G.ncells; c += nwarps) {
+    const int s_c = d.cell_start[c], e_c = d.cell_start[c + 1];
+    if (s_c == e_c) continue;  // warp-uniform
+    {
+      // lane t takes neighbour cell t in traversal order (z, y, x
+      // ascending); cells outside the grid contribute no nodes
+      const int t = l32;
+      const int cx0 = (int)(c % G.dims[0]);
+      const int cy0 = (int)((c / G.dims[0]) % G.dims[1]);
+      const int cz0 = DIM == 3 ? (int)(c / ((int64_t)G.dims[0] * G.dims[1])) : 0;
+      int a = 0, cnt = 0;
+      if (t < kNb) {
+        const int cx = cx0 + t % 3 - 1, cy = cy0 + (t / 3) % 3 - 1, cz = DIM == 3 ? cz0 + t / 9 - 1 : 0;
+        if (cx >= 0 && cx < G.dims[0] && cy >= 0 && cy < G.dims[1] && cz >= 0 &&
+            cz < (DIM == 3 ? G.dims[2] : 1)) {
+          const int cell = cx + G.dims[0] * (cy + G.dims[1] * cz);
+          a = d.cell_start[cell];
+          cnt = d.cell_start[cell + 1] - a;
+        }
+      }
+      int incl = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (t >= o) incl += y;
+      }
+      if (t < kNb) {
+        W.nb_s[t] = a;
+        W.nb_off[t] = incl - cnt;
+      }
+      if (t == kNb - 1) W.nb_off[kNb] = incl;
+    }
+    __syncwarp();
+    const int total = W.nb_off[kNb];
+    // centre nodes in sets of up to kCandCentres (one set unless the cell is crowded)
+    for (int sb = s_c; sb < e_c; sb += kCandCentres) {
+      const int nc = min(kCandCentres, e_c - sb);
+      // particle of the centre cell's first node: a chunk whose entries and
+      // searching centres all belong to it cannot produce a candidate
+      const int32_t pc = d.ptid[d.cell_nodes[sb]];
+      bool mixed_centres = false;
+      for (int a = l32; a < nc; a += 32) {
+        const int32_t i = d.cell_nodes[sb + a];
+        const bool search = (d.flags[i] & search_bit) != 0;
+        double q[3];
+        ldv<DIM>(d.x, i, q);
 #pragma unroll
-              for (int t = 0; t < DIM; t++) {
-                const double df = q[t] - p[t];
-                dd += df * df;
-              }
-              hit = dd < r2;
-            }
+        for (int t = 0; t < DIM; t++) W.q[t][a] = q[t];
+        W.ci[a] = i;
+        W.pi[a] = search ? d.ptid[i] : -2;  // -2: not searching
+        W.out[a] = FILL && search ? d.c_row[i] : 0;
+        if (search && W.pi[a] != pc) mixed_centres = true;
+      }
+      mixed_centres = __any_sync(0xffffffffu, mixed_centres);
+      for (int base = 0; base < total; base += kCandChunk) {
+        const int n = min(kCandChunk, total - base);
+        __syncwarp();  // the previous chunk is no longer read
+        for (int a = l32; a < n; a += 32) {
+          const int g = base + a;
+          int k = 0;
+          while (k + 1 < kNb && W.nb_off[k + 1] <= g) k++;
+          const int32_t j = d.cell_nodes[W.nb_s[k] + (g - W.nb_off[k])];
+          double p[3];
+          ldv<DIM>(d.x, j, p);
+#pragma unroll
+          for (int t = 0; t < DIM; t++) W.x[t][a] = p[t];
+          W.j[a] = j;
+          W.p[a] = d.ptid[j];
+        }
+        __syncwarp();
+        bool other = mixed_centres;
+        for (int a = l32; a < n && !other; a += 32) other = W.p[a] != pc;
+        if (!__any_sync(0xffffffffu, other)) continue;  // one particle only: no candidates here
+        for (int cb = 0; cb < nc; cb += kGroups) {
+          const int cc = cb + grp;
+          const int32_t pi = cc < nc ? W.pi[cc] : -2;
+          const bool search = pi != -2;
+          double q[3] = {0.0, 0.0, 0.0};
+          int64_t out = 0, out_end = 0;
+          if (search) {
+#pragma unroll
+            for (int t = 0; t < DIM; t++) q[t] = W.q[t][cc];
+            out = W.out[cc];
+            if (FILL) out_end = d.c_row[W.ci[cc] + 1];
           }
-          const unsigned bal = (__ballot_sync(gm, hit) & gm) >> lane_base;
-          if (fill) {
-            if (hit) {
+          for (int b0 = 0; b0 < n; b0 += LPN) {
+            const int a = b0 + lane;
+            bool hit = false;
+            int32_t j = -1;
+            if (search && a < n) {
+              j = W.j[a];
+              if (W.p[a] != pi) {
+                double dd = 0.0;
+#pragma unroll
+                for (int t = 0; t < DIM; t++) {
+                  const double df = q[t] - W.x[t][a];
+                  dd += df * df;
+                }
+                hit = dd < r2;
+              }
+            }
+            const unsigned bal = (__ballot_sync(gm, hit) & gm) >> lane_base;
+            if (FILL && hit) {
               const int64_t at = out + __popc(bal & ((1u << lane) - 1u));
               if (at < out_end && at < d.contact_cap) d.c_col[at] = j;
             }
             out += __popc(bal);
-          } else {
-            count += __popc(bal);
           }
+          __syncwarp(gm);
+          if (search && lane == 0) W.out[cc] = out;
         }
       }
-  return count;
+      __syncwarp();
+      if (!FILL)
+        for (int a = l32; a < nc; a += 32) d.c_cnt[W.ci[a]] = W.pi[a] != -2 ? W.out[a] : 0;
+    }
+    __syncwarp();  // the warp's stage is reused by the next cell
+  }
+}
+
+// Fill pass over the nodes that have candidates (c_nodes[0, nn)): a warp per
+// node walks the same neighbourhood in the same order as the count pass and
+// writes the columns.
+template <int DIM>
+__device__ void cand_fill_nodes(const DevData &d, int64_t nn) {
+  constexpr int kNb = DIM == 3 ? 27 : 9;
+  const Grid G = d.grid;
+  const double r = d.ctrl->radius;
+  const double r2 = r * r;
+  const int l32 = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (kCoopBlock / 32);
+  for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nn; t += nwarps) {
+    const int32_t i = d.c_nodes[t];
+    double q[3];
+    ldv<DIM>(d.x, i, q);
+    const int32_t pi = d.ptid[i];
+    int64_t out = d.c_row[i];
+    const int64_t out_end = d.c_row[i + 1];
+    const int cx0 = cell_coord<DIM>(q[0], G, 0), cy0 = cell_coord<DIM>(q[1], G, 1);
+    const int cz0 = DIM == 3 ? cell_coord<DIM>(q[2], G, 2) : 0;
+    for (int nb = 0; nb < kNb; nb++) {
+      const int cx = cx0 + nb % 3 - 1, cy = cy0 + (nb / 3) % 3 - 1, cz = DIM == 3 ? cz0 + nb / 9 - 1 : 0;
+      if (cx < 0 || cx >= G.dims[0] || cy < 0 || cy >= G.dims[1] || cz < 0 || cz >= (DIM == 3 ? G.dims[2] : 1))
+        continue;
+      const int cell = cx + G.dims[0] * (cy + G.dims[1] * cz);
+      const int a0 = d.cell_start[cell], a1 = d.cell_start[cell + 1];
+      for (int base = a0; base < a1; base += 32) {
+        const int a = base + l32;
+        bool hit = false;
+        int32_t j = -1;
+        if (a < a1) {
+          j = d.cell_nodes[a];
+          if (d.ptid[j] != pi) {
+            double p[3];
+            ldv<DIM>(d.x, j, p);
+            double dd = 0.0;
+#pragma unroll
+            for (int u = 0; u < DIM; u++) {
+              const double df = q[u] - p[u];
+              dd += df * df;
+            }
+            hit = dd < r2;
+          }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+          const int64_t at = out + __popc(bal & ((1u << l32) - 1u));
+          if (at < out_end && at < d.contact_cap) d.c_col[at] = j;
+        }
+        out += __popc(bal);
+      }
+    }
+  }
 }
 
 template <int DIM, int LPN>
 __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8_t search_bit,
                                                                int64_t *bsum) {
+  extern __shared__ __align__(16) unsigned char cand_smem[];
+  CandWarp<DIM> *stage = reinterpret_cast<CandWarp<DIM> *>(cand_smem);
   if (d.ctrl->error || !d.ctrl->update) return;
   cg::grid_group g = cg::this_grid();
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -697,14 +863,7 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
     }
   }
   g.sync();
-  const int lane = threadIdx.x % LPN;
-  const unsigned gm = group_mask<LPN>();
-  const unsigned lane_base = (threadIdx.x & 31u) / LPN * LPN;
-  for (int64_t i = tid / LPN; i < N; i += nth / LPN) {
-    int64_t cnt = 0;
-    if (d.flags[i] & search_bit) cnt = cand_node<DIM, LPN>(d, i, lane, gm, lane_base, false);
-    if (lane == 0) d.c_cnt[i] = cnt;
-  }
+  cand_cells<DIM, LPN, false>(d, search_bit, stage);
   g.sync();
   const int64_t *cn = d.c_cnt;
   grid_scan<int64_t>(g, [cn](int64_t k) { return cn[k]; }, d.c_row, N, bsum);
@@ -715,9 +874,8 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
       d.c_span[d.c_tmp[i]] = make_int2((int)d.c_row[i], (int)d.c_row[i + 1]);
     }
   if (tid == 0) d.ctrl->c_nnodes = d.c_tmp[N];
-  for (int64_t i = tid / LPN; i < N; i += nth / LPN)
-    if ((d.flags[i] & search_bit) && d.c_row[i + 1] > d.c_row[i])
-      cand_node<DIM, LPN>(d, i, lane, gm, lane_base, true);
+  g.sync();  // the compacted list is complete
+  cand_fill_nodes<DIM>(d, d.c_tmp[N]);
   if (tid == 0) {
     const int64_t total = d.c_row[N];
     d.ctrl->entries = total;
@@ -1384,7 +1542,7 @@ static cudaError_t rebuild_dim(const DevData &d, uint8_t bit, int64_t *bsum, int
   DevData dd = d;
   void *args[] = {(void *)&dd, (void *)&bit, (void *)&bsum};
   return cudaLaunchCooperativeKernel((const void *)k_contact_rebuild<DIM, LPN>, dim3(grid),
-                                     dim3(kCoopBlock), args, 0, s);
+                                     dim3(kCoopBlock), args, cand_stage_bytes<DIM>(), s);
 }
 
 int rebuild_grid_blocks(const DevData &d, int lanes) {
@@ -1394,7 +1552,9 @@ int rebuild_grid_blocks(const DevData &d, int lanes) {
   const void *f;
   if (d.dim == 2) f = lanes <= 8 ? (const void *)k_contact_rebuild<2, 8> : (const void *)k_contact_rebuild<2, 32>;
   else f = lanes <= 8 ? (const void *)k_contact_rebuild<3, 8> : (const void *)k_contact_rebuild<3, 32>;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, kCoopBlock, 0);
+  const size_t dyn = d.dim == 2 ? cand_stage_bytes<2>() : cand_stage_bytes<3>();
+  cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, kCoopBlock, dyn);
   return sms * (per > 0 ? per : 1);
 }
 
