@@ -315,6 +315,18 @@ PDGPU_API int pdgpu_enable_timing(pdgpu_ctx *ctx, int32_t on);
 PDGPU_API int pdgpu_kernel_times(pdgpu_ctx *ctx, int32_t max_kernels, const char **names, double *ms,
                        int64_t *launches, int32_t *count);
 
+/* Building block of the learned surrogate (no counterpart in the
+ * reference): C = act(A B^T + bias) on the tensor cores (tcgen05, BF16
+ * operands, FP32 accumulation).  A is M x K and B is N x K, both row-major
+ * BF16 device arrays with K contiguous (lda, ldb in elements, multiples of
+ * 8); K and N multiples of 16.  bias (N floats) may be NULL; act 0 = none,
+ * 1 = tanh.  C (ldc) is written as FP32 (Cf) and/or BF16 (Cb).  *err (device
+ * int) is set to 1 if the kernel's bounded waits time out.  Asynchronous on
+ * `stream`. */
+PDGPU_API int pdgpu_tc_gemm(const void *A, int32_t lda, const void *B, int32_t ldb, int32_t M, int32_t N,
+                            int32_t K, const float *bias, int32_t act, float *Cf, void *Cb, int32_t ldc,
+                            int32_t *err, void *stream);
+
 /* Peridynamic neighbour lists built WITHOUT ANY DEVICE ALLOCATION, for
  * callers that cannot call cudaMalloc: a host whose device memory is held by
  * another allocator (a framework's caching allocator that owns the GPU), or

@@ -91,6 +91,8 @@ SIGNATURES = {
     "pdgpu_kernel_times": [c_vp, c_i32, P(ctypes.c_char_p), P(c_d), P(c_i64), P(c_i32)],
     "pdgpu_compute_pd_forces": [c_vp],
     "pdgpu_set_tile_nodes": [c_vp, c_i32],
+    "pdgpu_tc_gemm": [c_vp, c_i32, c_vp, c_i32, c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_vp, c_i32,
+                      c_vp, c_vp],
     "pdgpu_build_neighbors_noalloc": [c_vp, c_vp, c_vp, c_i64, c_i32, c_vp, c_vp, c_i64, P(c_i64),
                                       c_vp, ctypes.c_char_p, ctypes.c_size_t],
 }

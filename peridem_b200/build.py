@@ -24,6 +24,7 @@ UNITS = [
     ("pdgpu_bonds_mixed.cu", ["-ftz=true"]),
     ("pdgpu_mixed.cu", []),
     ("pdgpu_noalloc.cu", ["--fmad=false"]),
+    ("pdgpu_tc.cu", []),
     ("pdgpu_runtime.cu", []),
 ]
 

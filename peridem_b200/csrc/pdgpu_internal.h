@@ -226,6 +226,9 @@ struct DevData {
 };
 
 // ---- launchers (all asynchronous on `s`) ----
+// tensor-core GEMM of the surrogate: C = act(A B^T + bias) (pdgpu_tc.cu)
+int launch_tc_gemm(const void *A, int lda, const void *B, int ldb, int M, int N, int K, const float *bias,
+                   int act, float *Cf, void *Cb, int ldc, int *err, cudaStream_t s);
 void launch_pack_vec(const DevData &d, const double *aos3, double *dst, cudaStream_t s);
 void launch_unpack_vec(const DevData &d, const double *src, double *aos3, cudaStream_t s);
 void launch_apply_ic(const DevData &d, cudaStream_t s);

@@ -1,0 +1,233 @@
+// Tensor-core GEMM of the learned surrogate: C = act(A B^T + bias), BF16
+// operands, FP32 accumulation in tensor memory (tcgen05.mma, kind::f16,
+// cta_group::1), one 128-row tile of C per CTA and up to 256 columns per
+// tile (blockIdx.y walks wider outputs).
+//
+//   A: M x K, row-major (K contiguous), BF16
+//   B: N x K, row-major (K contiguous), BF16   (a weight matrix W[out][in])
+//   C: M x N, row-major, FP32 and/or BF16; act: 0 none, 1 tanh
+//
+// Operand tiles are written by the CTA's threads into shared memory in the
+// canonical no-swizzle K-major layout of the tensor core (8-row x 16-byte
+// core matrices; the next core along K is LBO bytes on, the next along M/N
+// SBO bytes on); one elected thread issues the MMAs and commits them to an
+// mbarrier; the accumulator is read back with tcgen05.ld (warp w owns TMEM
+// lanes 32w..32w+31 = rows 32w..32w+31 of the tile).
+//
+// Limits: K a multiple of 16, N a multiple of 16, lda/ldb multiples of 8
+// elements (16-byte rows).  Waits are bounded: on timeout the kernel sets
+// *err and returns after a further bounded wait for its own MMAs.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pdgpu_internal.h"
+
+namespace pdgpu {
+namespace tc {
+
+constexpr int kRows = 128;     // tile rows (MMA M)
+// K per shared-memory stage: 64, or 32 for 256-column tiles (48 KB static limit)
+constexpr int kThreads = 128;  // 4 warps: one per 32 TMEM lanes
+constexpr unsigned kTries = 1u << 24;
+
+__device__ __forceinline__ uint32_t sa(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start, LBO, SBO (all >> 4), version 1, no swizzle
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version (sm100)
+  return d;                // base offset 0, layout type 0 (no swizzle)
+}
+
+// instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N
+__host__ __device__ constexpr uint32_t idesc(int n) {
+  return (1u << 4)                    // D format F32
+         | (1u << 7)                  // A format BF16
+         | (1u << 10)                 // B format BF16
+         | ((uint32_t)(n >> 3) << 17)  // N / 8
+         | ((uint32_t)(kRows >> 4) << 24);  // M / 16
+}
+
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(id), "r"(acc));
+}
+
+__device__ __forceinline__ void commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   sa(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool bar_try(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(sa(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t parity) {
+  for (unsigned t = 0; t < kTries; t++)
+    if (bar_try(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void ld8(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int q = 0; q < 8; q++) v[q] = __uint_as_float(r[q]);
+}
+
+// byte offset of element (r, k) of an R-row tile in the canonical layout:
+// core (r / 8, k / 8) at ((k / 8) * (R / 8) + r / 8) * 128, row r % 8 at 16 B
+__device__ __forceinline__ uint32_t tile_off(int r, int k8, int R) {
+  return (uint32_t)((k8 * (R / 8) + (r >> 3)) * 128 + (r & 7) * 16);
+}
+
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *__restrict__ A, int lda,
+                                                   const __nv_bfloat16 *__restrict__ B, int ldb, int M,
+                                                   int Ntot, int K, const float *__restrict__ bias, int act,
+                                                   float *__restrict__ Cf, __nv_bfloat16 *__restrict__ Cb,
+                                                   int ldc, int *err) {
+  constexpr uint32_t kCols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+  constexpr int kKc = N >= 256 ? 32 : 64;
+  __shared__ __align__(128) unsigned char sA[kRows * kKc * 2];
+  __shared__ __align__(128) unsigned char sB[N * kKc * 2];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row0 = blockIdx.x * kRows;
+  const int col0 = blockIdx.y * N;  // this CTA's columns of C (rows of B)
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa(&tmem_base)),
+                 "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sa(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const uint32_t id = idesc(N);
+  bool ok = true;
+  uint32_t parity = 0;
+  for (int k0 = 0; k0 < K; k0 += kKc) {
+    const int kc = min(kKc, K - k0);  // a multiple of 16
+    const int k8n = kc >> 3;          // 16-byte vectors per row in this stage
+    // A tile: 128 rows x kc (rows past M are zero)
+    for (int v = threadIdx.x; v < kRows * k8n; v += kThreads) {
+      const int r = v / k8n, k8 = v % k8n;
+      uint4 val = make_uint4(0, 0, 0, 0);
+      if (row0 + r < M) val = *reinterpret_cast<const uint4 *>(A + (size_t)(row0 + r) * lda + k0 + 8 * k8);
+      *reinterpret_cast<uint4 *>(sA + tile_off(r, k8, kRows)) = val;
+    }
+    // B tile: N rows x kc (rows past Ntot are zero)
+    for (int v = threadIdx.x; v < N * k8n; v += kThreads) {
+      const int r = v / k8n, k8 = v % k8n;
+      uint4 val = make_uint4(0, 0, 0, 0);
+      if (col0 + r < Ntot) val = *reinterpret_cast<const uint4 *>(B + (size_t)(col0 + r) * ldb + k0 + 8 * k8);
+      *reinterpret_cast<uint4 *>(sB + tile_off(r, k8, N)) = val;
+    }
+    // generic-proxy writes become visible to the tensor core
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (threadIdx.x == 0) {
+      const uint32_t lboA = (kRows / 8) * 128, lboB = (N / 8) * 128;
+      for (int s = 0; s < kc / 16; s++) {
+        const uint64_t da = sdesc(sa(sA) + 2 * s * lboA, lboA, 128);
+        const uint64_t db = sdesc(sa(sB) + 2 * s * lboB, lboB, 128);
+        mma(tmem, da, db, id, (k0 > 0 || s > 0) ? 1u : 0u);
+      }
+      commit(&bar);
+    }
+    // the stage is reused only after the MMAs that read it completed
+    const bool landed = bar_wait(&bar, parity);
+    parity ^= 1u;
+    if (__syncthreads_or(!landed)) {
+      ok = false;
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  if (ok) {
+    // epilogue: warp w reads rows 32w + lane, 8 columns at a time
+    const int r = row0 + warp * 32 + lane;
+    for (int c = 0; c < N; c += 8) {
+      float v[8];
+      ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+      if (r < M) {
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const int col = col0 + c + q;
+          if (col >= Ntot) continue;
+          float x = v[q] + (bias ? bias[col] : 0.f);
+          if (act == 1) x = tanhf(x);
+          if (Cf) Cf[(size_t)r * ldc + col] = x;
+          if (Cb) Cb[(size_t)r * ldc + col] = __float2bfloat16(x);
+        }
+      }
+    }
+  } else if (threadIdx.x == 0) {
+    atomicExch(err, 1);
+    bar_wait(&bar, parity ^ 1u);  // let the committed MMAs finish before TMEM is freed
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+  }
+}
+
+}  // namespace tc
+
+// C = act(A B^T + bias) on `stream`; returns a CUDA error code of the launch
+int launch_tc_gemm(const void *A, int lda, const void *B, int ldb, int M, int N, int K, const float *bias,
+                   int act, float *Cf, void *Cb, int ldc, int *err, cudaStream_t s) {
+  using namespace tc;
+  if (M <= 0 || N <= 0 || K <= 0 || K % 16 || N % 16 || lda % 8 || ldb % 8) return (int)cudaErrorInvalidValue;
+  const auto *a = static_cast<const __nv_bfloat16 *>(A);
+  const auto *b = static_cast<const __nv_bfloat16 *>(B);
+  auto *cb = static_cast<__nv_bfloat16 *>(Cb);
+  const unsigned gx = (unsigned)((M + kRows - 1) / kRows);
+  if (N <= 32) k_gemm<32><<<dim3(gx, 1), kThreads, 0, s>>>(a, lda, b, ldb, M, N, K, bias, act, Cf, cb, ldc, err);
+  else if (N <= 64) k_gemm<64><<<dim3(gx, 1), kThreads, 0, s>>>(a, lda, b, ldb, M, N, K, bias, act, Cf, cb, ldc, err);
+  else if (N <= 128) k_gemm<128><<<dim3(gx, 1), kThreads, 0, s>>>(a, lda, b, ldb, M, N, K, bias, act, Cf, cb, ldc, err);
+  else k_gemm<256><<<dim3(gx, (unsigned)((N + 255) / 256)), kThreads, 0, s>>>(a, lda, b, ldb, M, N, K, bias, act, Cf, cb, ldc, err);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace pdgpu
+
+extern "C" PDGPU_API int pdgpu_tc_gemm(const void *A, int32_t lda, const void *B, int32_t ldb, int32_t M,
+                                      int32_t N, int32_t K, const float *bias, int32_t act, float *Cf,
+                                      void *Cb, int32_t ldc, int32_t *err, void *stream) {
+  if (!A || !B || !err || (!Cf && !Cb)) return PDGPU_ERR_ARG;
+  const int rc = pdgpu::launch_tc_gemm(A, lda, B, ldb, M, N, K, bias, act, Cf, Cb, ldc, err,
+                                       (cudaStream_t)stream);
+  return rc == 0 ? PDGPU_OK : (rc == (int)cudaErrorInvalidValue ? PDGPU_ERR_ARG : PDGPU_ERR_CUDA);
+}
