@@ -327,6 +327,67 @@ PDGPU_API int pdgpu_tc_gemm(const void *A, int32_t lda, const void *B, int32_t l
                             int32_t K, const float *bias, int32_t act, float *Cf, void *Cb, int32_t ldc,
                             int32_t *err, void *stream);
 
+/* The learned surrogate of the bond loop (no counterpart in the reference;
+ * mixed-precision form, 2-D).  Per zone ("shape": particles sharing a
+ * reference mesh, scaled and rotated), a particle's displacement in its body
+ * frame, u_b = R(-orient) (u_i - u_centre) / scale (2 n_nodes values in the
+ * particle's node order), is projected on 32 displacement modes (phi_t,
+ * 32 x 2 n_nodes) to x, mapped by an MLP 32-256-256-32 (tanh, tanh, linear;
+ * weights W[out][in]) to y, and [y, x] is lifted (psi, 2 n_nodes x 64: the
+ * force modes of the network's output, then the tangent force of each
+ * displacement mode) to the body-frame force f_b; f_i = fscale R(orient) f_b.
+ * Zero deformation gives exactly zero force (the chain's output for a zero
+ * input is subtracted).  Every check_interval steps the bond loop runs for
+ * all particles; a particle then keeps the surrogate until the next check
+ * only if none of its bonds is broken, its damage Z stays below z_gate
+ * (0.5 = half the critical stretch) and |f_surrogate - f| < err_gate
+ * max(|f|, floor).  With near_gate != 0 a particle also stays on the bond
+ * loop while the last contact-list rebuild found contact candidates of its
+ * nodes (within contact radius plus skin, so no contact starts on a
+ * surrogate particle).  Per-particle arrays fscale, floor, orient, scale are
+ * indexed by particle.  All arrays are host FP32/FP64 and are copied
+ * (weights to BF16).  Call once, before pdgpu_integrate_begin. */
+typedef struct {
+  int32_t zone, n_nodes;
+  const float *phi_t, *psi;
+  const float *w1, *b1; /* 256 x 32, 256 */
+  const float *w2, *b2; /* 256 x 256, 256 */
+  const float *w3, *b3; /* 32 x 256, 32 */
+} pdgpu_sur_shape;
+
+PDGPU_API int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape *shapes,
+                                  const double *fscale, const double *floor, const double *orient,
+                                  const double *scale, int32_t check_interval, double z_gate,
+                                  double err_gate, int32_t near_gate);
+
+/* Particles on the surrogate now and particles it covers; and, summed over
+ * the steps so far, particle-steps whose force came from the surrogate and
+ * particle-steps of the particles it covers. */
+PDGPU_API int pdgpu_surrogate_stats(pdgpu_ctx *ctx, int64_t *n_on, int64_t *n_total, int64_t *steps_on,
+                                    int64_t *steps_total);
+
+/* The last check step's comparison per particle: err2[2p] = sum over the
+ * particle's nodes of |f_surrogate - f|^2, err2[2p + 1] = sum of |f|^2 (f the
+ * bond loop's force density); zeros outside the surrogate's zones.
+ * n = 2 x number of particles. */
+PDGPU_API int pdgpu_surrogate_errors(pdgpu_ctx *ctx, double *err2, int64_t n);
+
+/* Training building blocks of the surrogate on caller-owned device arrays
+ * (no counterpart in the reference), asynchronous on `stream`:
+ *   mse_grad:   dY = scale (Y - T) as FP32 and BF16; *loss += sum (Y - T)^2
+ *   tanh_back:  dZ = dH (1 - H^2) as FP32 and BF16 (H = tanh of the layer)
+ *   colsum:     out[c] = sum_r X[r][c] (bias gradients; X rows x cols FP32)
+ *   transpose:  out (cols x rows) = in (rows x cols)^T, BF16
+ *   adam:       Adam step `step` (1-based) on FP32 p with moments m, v;
+ *               wb (may be NULL) receives p as BF16 */
+PDGPU_API int pdgpu_sur_mse_grad(const float *Y, const float *T, int64_t n, float scale, float *dY, void *dYb,
+                                 double *loss, void *stream);
+PDGPU_API int pdgpu_sur_tanh_back(const float *dH, const float *H, int64_t n, float *dZ, void *dZb, void *stream);
+PDGPU_API int pdgpu_sur_colsum(const float *X, int32_t rows, int32_t cols, float *out, void *stream);
+PDGPU_API int pdgpu_sur_transpose(const void *in, int32_t rows, int32_t cols, void *out, void *stream);
+PDGPU_API int pdgpu_sur_adam(float *p, float *m, float *v, const float *g, int64_t n, float lr, float beta1,
+                             float beta2, float eps, int32_t step, void *wb, void *stream);
+
 /* Peridynamic neighbour lists built WITHOUT ANY DEVICE ALLOCATION, for
  * callers that cannot call cudaMalloc: a host whose device memory is held by
  * another allocator (a framework's caching allocator that owns the GPU), or

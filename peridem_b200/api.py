@@ -95,7 +95,25 @@ SIGNATURES = {
                       c_vp, c_vp],
     "pdgpu_build_neighbors_noalloc": [c_vp, c_vp, c_vp, c_i64, c_i32, c_vp, c_vp, c_i64, P(c_i64),
                                       c_vp, ctypes.c_char_p, ctypes.c_size_t],
+    "pdgpu_set_surrogate": [c_vp, c_i32, c_vp, P(c_d), P(c_d), P(c_d), P(c_d), c_i32, c_d, c_d, c_i32],
+    "pdgpu_surrogate_stats": [c_vp, P(c_i64), P(c_i64), P(c_i64), P(c_i64)],
+    "pdgpu_surrogate_errors": [c_vp, P(c_d), c_i64],
+    "pdgpu_sur_mse_grad": [c_vp, c_vp, c_i64, ctypes.c_float, c_vp, c_vp, c_vp, c_vp],
+    "pdgpu_sur_tanh_back": [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp],
+    "pdgpu_sur_colsum": [c_vp, c_i32, c_i32, c_vp, c_vp],
+    "pdgpu_sur_transpose": [c_vp, c_i32, c_i32, c_vp, c_vp],
+    "pdgpu_sur_adam": [c_vp, c_vp, c_vp, c_vp, c_i64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                       ctypes.c_float, c_i32, c_vp, c_vp],
 }
+
+
+class SurShape(ctypes.Structure):
+    """pdgpu_sur_shape: one reference shape of the learned surrogate."""
+    _fields_ = [("zone", c_i32), ("n_nodes", c_i32),
+                ("phi_t", P(ctypes.c_float)), ("psi", P(ctypes.c_float)),
+                ("w1", P(ctypes.c_float)), ("b1", P(ctypes.c_float)),
+                ("w2", P(ctypes.c_float)), ("b2", P(ctypes.c_float)),
+                ("w3", P(ctypes.c_float)), ("b3", P(ctypes.c_float))]
 
 
 def lib(path: str = LIB_PATH):

@@ -25,6 +25,7 @@ UNITS = [
     ("pdgpu_mixed.cu", []),
     ("pdgpu_noalloc.cu", ["--fmad=false"]),
     ("pdgpu_tc.cu", []),
+    ("pdgpu_surrogate.cu", []),
     ("pdgpu_runtime.cu", []),
 ]
 

@@ -296,8 +296,17 @@ __global__ void __launch_bounds__(kThreads) k_bonds_mixed(DevData d, const BondT
   uint32_t parity = 0;
   int k = 0;
   int t = s_tile[0];
+  // learned surrogate: off check steps, its particles' tiles are skipped
+  const bool sur_step = d.sur_on != nullptr && !d.ctrl->sur_check;
   while (t < n_tiles) {
     const BondTile T = tiles[t];
+    if (sur_step && d.sur_on[T.particle] && !d.sur_near[T.particle]) {
+      if (threadIdx.x == 0) s_tile[(k + 1) & 1] = (int)atomicAdd(&d.ctrl->tile_next, 1u);
+      __syncthreads();
+      t = s_tile[(k + 1) & 1];
+      k++;
+      continue;
+    }
     const int w = (int)(T.win_end - T.win_begin);
     const Plan p = plan(DIM, state, (int)sizeof(CT), T.bond_begin, T.bond_end, T.node_begin, T.node_end, w);
     CT *s_col = reinterpret_cast<CT *>(smem);

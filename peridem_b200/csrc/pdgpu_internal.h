@@ -82,6 +82,10 @@ struct CtrlState {
   uint32_t begin_done, end_done;
   // tile claims and finished CTAs of the persistent bond loop (reset by its last CTA)
   uint32_t tile_next, tile_done;
+  // learned surrogate: this step the bond loop runs for every particle and
+  // the surrogate is judged against it (every sur_interval-th step)
+  int32_t sur_check;
+  int32_t pad2;
 };
 
 // Cell grid fixed at set-up; nodes outside are clamped to the border cells,
@@ -129,6 +133,24 @@ struct BondTile {
   int64_t node_begin, node_end, win_begin, win_end;
   int64_t bond_begin, bond_end;  // pd_row[node_begin], pd_row[node_end]
   int64_t center;                // the particle's centre node
+};
+
+// one problem of a grouped tensor-core GEMM: C = act(A B^T + bias), A M x K
+// and B N x K BF16 row-major, C FP32 (Cf) and/or BF16 (Cb)
+struct GemmProblem {
+  const void *A, *B;
+  const float *bias;
+  float *Cf;
+  void *Cb;
+  int32_t lda, ldb, ldc, M, N, K, act, pad;
+};
+
+// a particle of a surrogate zone: first node, centre node, orientation
+// (cos, sin), 1 / scale, force scale, squared gate floor
+struct SurPart {
+  int64_t start, center;
+  int32_t particle, pad;
+  double c, s, inv_scale, fscale, floor2;
 };
 
 struct DevData {
@@ -223,12 +245,33 @@ struct DevData {
   float4 *xv_mixed;  // per node {x, y, z, vol}: reference coordinates minus the centre's, FP32
   int32_t use16;
   float inf_p0, inf_p1;
+
+  // learned surrogate (pdgpu_set_surrogate): per particle the gate's verdict
+  // at the last check, and whether the last contact-list rebuild found
+  // contact candidates of its nodes (within contact radius plus skin, so no
+  // contact can start before the next rebuild); the check interval (0 = no
+  // surrogate) and whether the proximity flags are kept.  A particle is on
+  // the surrogate when sur_on && !sur_near.
+  uint8_t *sur_on;
+  uint8_t *sur_near;
+  int32_t sur_interval;
+  int32_t sur_near_gate;
 };
 
 // ---- launchers (all asynchronous on `s`) ----
 // tensor-core GEMM of the surrogate: C = act(A B^T + bias) (pdgpu_tc.cu)
 int launch_tc_gemm(const void *A, int lda, const void *B, int ldb, int M, int N, int K, const float *bias,
                    int act, float *Cf, void *Cb, int ldc, int *err, cudaStream_t s);
+int launch_tc_gemm_grouped(const GemmProblem *probs, int n_probs, int max_m, int max_n, int ncol, int *err,
+                           cudaStream_t s);
+// learned surrogate around the GEMMs (pdgpu_surrogate.cu)
+void launch_sur_gather(const double *u, const SurPart *parts, int P, int n_nodes, void *A, int lda, float *Af,
+                       cudaStream_t s);
+void launch_sur_scatter(double *f, const SurPart *parts, int P, int n_nodes, const float *F, int ldf,
+                        const uint8_t *on, const uint8_t *near, const CtrlState *ctrl, double *err2,
+                        unsigned long long *count, cudaStream_t s);
+void launch_sur_gate(const DevData &d, const SurPart *parts, int P, const double *err2, float z_gate,
+                     double err_gate, cudaStream_t s);
 void launch_pack_vec(const DevData &d, const double *aos3, double *dst, cudaStream_t s);
 void launch_unpack_vec(const DevData &d, const double *src, double *aos3, cudaStream_t s);
 void launch_apply_ic(const DevData &d, cudaStream_t s);

@@ -271,6 +271,7 @@ __device__ __forceinline__ void ctrl_commit(CtrlState *dst, const CtrlState &c) 
   dst->radius = c.radius;
   dst->max_velocity = c.max_velocity;
   dst->update = c.update;
+  dst->sur_check = c.sur_check;
 }
 
 __device__ __noinline__ void ctrl_step(const DevData &d, int mode) {
@@ -282,6 +283,9 @@ __device__ __noinline__ void ctrl_step(const DevData &d, int mode) {
     c.time += d.dt;
     c.first_bc = 0;
   }
+  // learned surrogate: every sur_interval-th step (and the first) re-judges
+  // it with the full bond loop
+  c.sur_check = d.sur_interval > 0 && (c.n % d.sur_interval == 0 || c.n <= 1);
   // read and reset atomically: other CTAs raised it with atomicMax
   const double vmax_now =
       fmax(__longlong_as_double((long long)atomicExch(&cp->vmax_bits, 0ull)), c.static_vmax);
@@ -834,6 +838,8 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
     d.cell_cnt[c] = 0;
     d.cell_fill[c] = 0;
   }
+  if (d.sur_near_gate)
+    for (int64_t p = tid; p < d.n_particles; p += nth) d.sur_near[p] = 0;
   g.sync();
   for (int64_t i = tid; i < N; i += nth) {
     double p[3];
@@ -872,6 +878,7 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
     if (cn[i] > 0) {
       d.c_nodes[d.c_tmp[i]] = (int32_t)i;
       d.c_span[d.c_tmp[i]] = make_int2((int)d.c_row[i], (int)d.c_row[i + 1]);
+      if (d.sur_near_gate) d.sur_near[d.ptid[i]] = 1;  // every writer stores the same value
     }
   if (tid == 0) d.ctrl->c_nnodes = d.c_tmp[N];
   g.sync();  // the compacted list is complete

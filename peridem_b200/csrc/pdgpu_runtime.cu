@@ -1,6 +1,7 @@
 // Host runtime of the pdgpu C ABI: context, uploads, the step sequence of
 // DEMModel::integrate / integrateStep / computeForces, CUDA-graph replay,
 // downloads and per-kernel timing.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -80,6 +81,28 @@ struct pdgpu_ctx {
   // contact and damping run on `branch` beside the bond loop on `stream`
   cudaStream_t branch = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+
+  // learned surrogate (pdgpu_set_surrogate): per shape its particles, BF16
+  // weights and the activations of the chain (P + 1 rows: row P is a zero
+  // input, whose output the scatter subtracts)
+  struct SurShape {
+    int n_nodes = 0, kpad = 0, P = 0;
+    SurPart *parts = nullptr;
+    void *phiT = nullptr, *lift = nullptr, *w1 = nullptr, *w2 = nullptr, *w3 = nullptr;
+    float *b1 = nullptr, *b2 = nullptr, *b3 = nullptr;
+    void *A = nullptr, *xy = nullptr, *h1 = nullptr, *h2 = nullptr;
+    float *F = nullptr;
+  };
+  std::vector<SurShape> sur;
+  GemmProblem *sur_probs = nullptr;  // device: 5 stages x shapes
+  int sur_max_p = 0, sur_max_k = 0;
+  double *sur_err2 = nullptr;        // per particle: squared error, squared norm (last check)
+  int32_t *sur_errflag = nullptr;    // a tensor-core wait timed out
+  unsigned long long *sur_count = nullptr;  // particle-steps on the surrogate, covered
+  float sur_z_gate = 0.5f;
+  double sur_err_gate = 0.05;
+  cudaStream_t sur_stream = nullptr;
+  cudaEvent_t ev_sur0 = nullptr, ev_sur1 = nullptr;
 
   // timing
   bool timing = false;
@@ -786,6 +809,34 @@ void pd_forces(pdgpu_ctx *ctx) {
     });
 }
 
+// The learned surrogate's chain for every particle of its zones, on its own
+// stream beside the bond loop: gather the body-frame displacements, project
+// (x = A phi^T), the three layers (y), and lift [y | x] to body-frame forces.
+void sur_forward(pdgpu_ctx *ctx, cudaStream_t s) {
+  const DevData &d = ctx->d;
+  const int ns = (int)ctx->sur.size();
+  for (auto &S : ctx->sur) launch_sur_gather(d.u, S.parts, S.P, S.n_nodes, S.A, S.kpad, nullptr, s);
+  const int pm = ctx->sur_max_p, km = ctx->sur_max_k;
+  launch_tc_gemm_grouped(ctx->sur_probs + 0 * ns, ns, pm, 32, 32, ctx->sur_errflag, s);    // projection
+  launch_tc_gemm_grouped(ctx->sur_probs + 1 * ns, ns, pm, 256, 256, ctx->sur_errflag, s);  // layer 1
+  launch_tc_gemm_grouped(ctx->sur_probs + 2 * ns, ns, pm, 256, 256, ctx->sur_errflag, s);  // layer 2
+  launch_tc_gemm_grouped(ctx->sur_probs + 3 * ns, ns, pm, 32, 32, ctx->sur_errflag, s);    // layer 3
+  launch_tc_gemm_grouped(ctx->sur_probs + 4 * ns, ns, pm, km, 256, ctx->sur_errflag, s);   // lift
+}
+
+// After the bond loop: surrogate forces into f (ordinary steps) or, on check
+// steps, the comparison with the bond loop and the gate.
+void sur_apply(pdgpu_ctx *ctx, cudaStream_t s) {
+  const DevData &d = ctx->d;
+  for (auto &S : ctx->sur) {
+    launch_sur_scatter(d.f, S.parts, S.P, S.n_nodes, S.F, S.kpad, d.sur_on, d.sur_near, d.ctrl, nullptr,
+                       ctx->sur_count, s);
+    launch_sur_scatter(d.f, S.parts, S.P, S.n_nodes, S.F, S.kpad, d.sur_on, d.sur_near, d.ctrl, ctx->sur_err2,
+                       ctx->sur_count, s);
+    launch_sur_gate(d, S.parts, S.P, ctx->sur_err2, ctx->sur_z_gate, ctx->sur_err_gate, s);
+  }
+}
+
 // Contact forces and particle damping depend on positions and velocities
 // only, not on the bond loop's forces: they run on the branch stream while
 // the bond loop runs, and the external-force pass (after the join) adds
@@ -805,7 +856,18 @@ void compute_forces(pdgpu_ctx *ctx, bool step) {
     run_on(ctx, ctx->branch, "damping", [&] { launch_damping(d, ctx->branch); });
     cudaEventRecord(ctx->ev_join, ctx->branch);
   }
+  const bool sur = step && !ctx->sur.empty();
+  if (sur) {
+    cudaEventRecord(ctx->ev_sur0, s);
+    cudaStreamWaitEvent(ctx->sur_stream, ctx->ev_sur0, 0);
+    run_on(ctx, ctx->sur_stream, "surrogate", [&] { sur_forward(ctx, ctx->sur_stream); });
+    cudaEventRecord(ctx->ev_sur1, ctx->sur_stream);
+  }
   pd_forces(ctx);
+  if (sur) {
+    cudaStreamWaitEvent(s, ctx->ev_sur1, 0);
+    run(ctx, "surrogate_apply", [&] { sur_apply(ctx, s); });
+  }
   if (ctx->desc.multi_particle) cudaStreamWaitEvent(s, ctx->ev_join, 0);
   // external forces and force BC; in a step also the Verlet second half and
   // the post-processing
@@ -823,9 +885,8 @@ void one_step(pdgpu_ctx *ctx) {
   compute_forces(ctx, true);
 }
 
-// One step inside a graph under capture: like one_step, but the contact-list
-// rebuild sits in a conditional node that the step-control kernel switches
-// on only on rebuild steps, so other steps pay nothing for it.
+// One step inside a graph under capture: the same kernels as one_step,
+// captured without the timing events.
 cudaError_t graph_step(pdgpu_ctx *ctx, const char **where) {
   DevData &d = ctx->d;
   cudaStream_t s = ctx->stream;
@@ -851,6 +912,17 @@ cudaError_t graph_step(pdgpu_ctx *ctx, const char **where) {
     e = cudaEventRecord(ctx->ev_join, ctx->branch);
     if (e != cudaSuccess) return e;
   }
+  // surrogate chain beside the bond loop
+  const bool sur = !ctx->sur.empty();
+  if (sur) {
+    *where = "surrogate fork";
+    e = cudaEventRecord(ctx->ev_sur0, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->sur_stream, ctx->ev_sur0, 0);
+    if (e != cudaSuccess) return e;
+    sur_forward(ctx, ctx->sur_stream);
+    e = cudaEventRecord(ctx->ev_sur1, ctx->sur_stream);
+    if (e != cudaSuccess) return e;
+  }
   // main: bond loop
   if (ctx->state_prepass) {
     if (mixed) launch_prepass_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
@@ -859,6 +931,12 @@ cudaError_t graph_step(pdgpu_ctx *ctx, const char **where) {
   const size_t smem = ctx->tile_smem_pd;
   if (mixed) launch_pd_tiled_mixed(d, ctx->tiles, ctx->tile_law, ctx->pd_lanes, smem, s);
   else launch_pd_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
+  if (sur) {
+    *where = "surrogate join";
+    e = cudaStreamWaitEvent(s, ctx->ev_sur1, 0);
+    if (e != cudaSuccess) return e;
+    sur_apply(ctx, s);
+  }
   if (ctx->desc.multi_particle) {
     *where = "join";
     e = cudaStreamWaitEvent(s, ctx->ev_join, 0);
@@ -974,6 +1052,9 @@ void pdgpu_destroy(pdgpu_ctx *ctx) {
   if (ctx->branch) cudaStreamDestroy(ctx->branch);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->sur_stream) cudaStreamDestroy(ctx->sur_stream);
+  if (ctx->ev_sur0) cudaEventDestroy(ctx->ev_sur0);
+  if (ctx->ev_sur1) cudaEventDestroy(ctx->ev_sur1);
   for (auto &t : ctx->pending) {
     cudaEventDestroy(t.a);
     cudaEventDestroy(t.b);
@@ -1361,6 +1442,149 @@ int pdgpu_download(pdgpu_ctx *ctx, int32_t field, void *dst) {
     CK(cudaMemcpyAsync(dst, ctx->stage, (size_t)3 * N * 8, cudaMemcpyDeviceToHost, s));
   }
   CK(cudaStreamSynchronize(s));
+  return PDGPU_OK;
+}
+
+int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape *shapes, const double *fscale,
+                        const double *floor, const double *orient, const double *scale, int32_t check_interval,
+                        double z_gate, double err_gate, int32_t near_gate) {
+  if (!ctx || n_shapes <= 0 || !shapes || !fscale || !floor || !orient || !scale || check_interval <= 0)
+    return PDGPU_ERR_ARG;
+  if (ctx->desc.precision != PDGPU_PREC_MIXED || ctx->desc.dim != 2)
+    return fail(ctx, PDGPU_ERR_ARG, "the learned surrogate needs the mixed-precision form in 2-D");
+  if (ctx->begun || !ctx->sur.empty())
+    return fail(ctx, PDGPU_ERR_STATE, "set the surrogate once, before integrate_begin");
+  if (!ctx->particles) return fail(ctx, PDGPU_ERR_STATE, "upload particles first");
+  DevData &d = ctx->d;
+  // FP32 rows x cols -> BF16 rows_out x ld_out on the device (zero padded)
+  auto bf = [&](const float *src, size_t rows, size_t cols, size_t ld_out, size_t rows_out, void **dst) -> int {
+    std::vector<__nv_bfloat16> h(rows_out * ld_out, __float2bfloat16(0.f));
+    for (size_t r = 0; r < rows; r++)
+      for (size_t c = 0; c < cols; c++) h[r * ld_out + c] = __float2bfloat16(src[r * cols + c]);
+    __nv_bfloat16 *p;
+    TRY(dalloc(ctx, &p, h.size()));
+    CK(cudaMemcpy(p, h.data(), h.size() * 2, cudaMemcpyHostToDevice));
+    *dst = p;
+    return PDGPU_OK;
+  };
+  auto f32 = [&](const float *src, size_t n, float **dst) -> int {
+    TRY(dalloc(ctx, dst, n));
+    CK(cudaMemcpy(*dst, src, n * 4, cudaMemcpyHostToDevice));
+    return PDGPU_OK;
+  };
+  std::vector<GemmProblem> probs(5 * (size_t)n_shapes);
+  for (int k = 0; k < n_shapes; k++) {
+    const pdgpu_sur_shape &in = shapes[k];
+    if (in.n_nodes <= 0 || !in.phi_t || !in.psi || !in.w1 || !in.b1 || !in.w2 || !in.b2 || !in.w3 || !in.b3)
+      return fail(ctx, PDGPU_ERR_ARG, "surrogate shape %d incomplete", k);
+    pdgpu_ctx::SurShape S;
+    S.n_nodes = in.n_nodes;
+    const int K = 2 * in.n_nodes;
+    S.kpad = (K + 15) / 16 * 16;
+    std::vector<SurPart> parts;
+    for (size_t p = 0; p < ctx->hp.size(); p++) {
+      const DevParticle &P = ctx->hp[p];
+      if (P.zone != in.zone || P.type != 0 || !P.compute_force) continue;
+      if (P.end - P.start != in.n_nodes)
+        return fail(ctx, PDGPU_ERR_ARG, "particle %zu of zone %d has %lld nodes, the surrogate %d", p, in.zone,
+                    (long long)(P.end - P.start), in.n_nodes);
+      SurPart q{};
+      q.start = P.start;
+      q.center = P.center;
+      q.particle = (int32_t)p;
+      q.c = std::cos(orient[p]);
+      q.s = std::sin(orient[p]);
+      q.inv_scale = 1.0 / scale[p];
+      q.fscale = fscale[p];
+      q.floor2 = floor[p] * floor[p];
+      parts.push_back(q);
+    }
+    S.P = (int)parts.size();
+    if (S.P == 0) return fail(ctx, PDGPU_ERR_ARG, "no force-computing particle in surrogate zone %d", in.zone);
+    TRY(dalloc(ctx, &S.parts, parts.size()));
+    CK(cudaMemcpy(S.parts, parts.data(), parts.size() * sizeof(SurPart), cudaMemcpyHostToDevice));
+    TRY(bf(in.phi_t, 32, K, S.kpad, 32, &S.phiT));
+    TRY(bf(in.psi, K, 64, 64, S.kpad, &S.lift));
+    TRY(bf(in.w1, 256, 32, 32, 256, &S.w1));
+    TRY(bf(in.w2, 256, 256, 256, 256, &S.w2));
+    TRY(bf(in.w3, 32, 256, 256, 32, &S.w3));
+    TRY(f32(in.b1, 256, &S.b1));
+    TRY(f32(in.b2, 256, &S.b2));
+    TRY(f32(in.b3, 32, &S.b3));
+    const int M = S.P + 1;  // row P: the zero input
+    __nv_bfloat16 *A, *xy, *h1, *h2;
+    TRY(dalloc(ctx, &A, (size_t)M * S.kpad));
+    CK(cudaMemset(A, 0, (size_t)M * S.kpad * 2));
+    TRY(dalloc(ctx, &xy, (size_t)M * 64));  // [network output | projected input]
+    TRY(dalloc(ctx, &h1, (size_t)M * 256));
+    TRY(dalloc(ctx, &h2, (size_t)M * 256));
+    TRY(dalloc(ctx, &S.F, (size_t)M * S.kpad));
+    S.A = A, S.xy = xy, S.h1 = h1, S.h2 = h2;
+    // x = A phi^T -> xy[:, 32:64]; h1 = tanh(x W1^T + b1); h2 = tanh(h1 W2^T + b2);
+    // y = h2 W3^T + b3 -> xy[:, 0:32]; F = xy lift^T
+    probs[0 * n_shapes + k] = GemmProblem{A, S.phiT, nullptr, nullptr, xy + 32, S.kpad, S.kpad, 64, M, 32, S.kpad, 0, 0};
+    probs[1 * n_shapes + k] = GemmProblem{xy + 32, S.w1, S.b1, nullptr, h1, 64, 32, 256, M, 256, 32, 1, 0};
+    probs[2 * n_shapes + k] = GemmProblem{h1, S.w2, S.b2, nullptr, h2, 256, 256, 256, M, 256, 256, 1, 0};
+    probs[3 * n_shapes + k] = GemmProblem{h2, S.w3, S.b3, nullptr, xy, 256, 256, 64, M, 32, 256, 0, 0};
+    probs[4 * n_shapes + k] = GemmProblem{xy, S.lift, nullptr, S.F, nullptr, 64, 64, S.kpad, M, S.kpad, 64, 0, 0};
+    ctx->sur_max_p = std::max(ctx->sur_max_p, M);
+    ctx->sur_max_k = std::max(ctx->sur_max_k, S.kpad);
+    ctx->sur.push_back(S);
+  }
+  TRY(dalloc(ctx, &ctx->sur_probs, probs.size()));
+  CK(cudaMemcpy(ctx->sur_probs, probs.data(), probs.size() * sizeof(GemmProblem), cudaMemcpyHostToDevice));
+  TRY(dalloc(ctx, &ctx->sur_err2, 2 * ctx->hp.size()));
+  CK(cudaMemset(ctx->sur_err2, 0, 2 * ctx->hp.size() * 8));
+  TRY(dalloc(ctx, &ctx->sur_errflag, 1));
+  CK(cudaMemset(ctx->sur_errflag, 0, 4));
+  TRY(dalloc(ctx, &ctx->sur_count, 2));
+  CK(cudaMemset(ctx->sur_count, 0, 16));
+  TRY(dalloc(ctx, &d.sur_on, ctx->hp.size()));
+  CK(cudaMemset(d.sur_on, 0, ctx->hp.size()));  // on only after a check step passes the gate
+  TRY(dalloc(ctx, &d.sur_near, ctx->hp.size()));
+  // with the proximity gate: near until the first contact-list rebuild
+  CK(cudaMemset(d.sur_near, near_gate ? 1 : 0, ctx->hp.size()));
+  d.sur_near_gate = near_gate ? 1 : 0;
+  d.sur_interval = check_interval;
+  ctx->sur_z_gate = (float)z_gate;
+  ctx->sur_err_gate = err_gate;
+  CK(cudaStreamCreateWithFlags(&ctx->sur_stream, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&ctx->ev_sur0, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&ctx->ev_sur1, cudaEventDisableTiming));
+  if (ctx->gexec) {
+    cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_surrogate_stats(pdgpu_ctx *ctx, int64_t *n_on, int64_t *n_total, int64_t *steps_on,
+                          int64_t *steps_total) {
+  if (!ctx || !n_on || !n_total || !steps_on || !steps_total) return PDGPU_ERR_ARG;
+  *n_on = *n_total = *steps_on = *steps_total = 0;
+  if (ctx->sur.empty()) return PDGPU_OK;
+  const size_t np = ctx->hp.size();
+  std::vector<uint8_t> on(np), near(np);
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(on.data(), ctx->d.sur_on, np, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(near.data(), ctx->d.sur_near, np, cudaMemcpyDeviceToHost));
+  for (size_t p = 0; p < np; p++) *n_on += on[p] && !near[p];
+  for (auto &S : ctx->sur) *n_total += S.P;
+  unsigned long long cnt[2];
+  CK(cudaMemcpy(cnt, ctx->sur_count, 16, cudaMemcpyDeviceToHost));
+  *steps_on = (int64_t)cnt[0];
+  *steps_total = (int64_t)cnt[1];
+  int32_t flag = 0;
+  CK(cudaMemcpy(&flag, ctx->sur_errflag, 4, cudaMemcpyDeviceToHost));
+  if (flag) return fail(ctx, PDGPU_ERR_CUDA, "a tensor-core wait of the surrogate timed out");
+  return PDGPU_OK;
+}
+
+int pdgpu_surrogate_errors(pdgpu_ctx *ctx, double *err2, int64_t n) {
+  if (!ctx || !err2 || n != 2 * (int64_t)ctx->hp.size()) return PDGPU_ERR_ARG;
+  if (ctx->sur.empty()) return fail(ctx, PDGPU_ERR_STATE, "no surrogate set");
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(err2, ctx->sur_err2, (size_t)n * 8, cudaMemcpyDeviceToHost));
   return PDGPU_OK;
 }
 

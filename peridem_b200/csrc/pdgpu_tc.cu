@@ -102,12 +102,12 @@ __device__ __forceinline__ uint32_t tile_off(int r, int k8, int R) {
   return (uint32_t)((k8 * (R / 8) + (r >> 3)) * 128 + (r & 7) * 16);
 }
 
+// one 128 x N tile of C at (row0, col0); called by every thread of the CTA
 template <int N>
-__global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *__restrict__ A, int lda,
-                                                   const __nv_bfloat16 *__restrict__ B, int ldb, int M,
-                                                   int Ntot, int K, const float *__restrict__ bias, int act,
-                                                   float *__restrict__ Cf, __nv_bfloat16 *__restrict__ Cb,
-                                                   int ldc, int *err) {
+__device__ __forceinline__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, int lda,
+                                          const __nv_bfloat16 *__restrict__ B, int ldb, int M, int Ntot, int K,
+                                          const float *__restrict__ bias, int act, float *__restrict__ Cf,
+                                          __nv_bfloat16 *__restrict__ Cb, int ldc, int *err, int row0, int col0) {
   constexpr uint32_t kCols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
   constexpr int kKc = N >= 256 ? 32 : 64;
   __shared__ __align__(128) unsigned char sA[kRows * kKc * 2];
@@ -115,8 +115,6 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *__restri
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_base;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row0 = blockIdx.x * kRows;
-  const int col0 = blockIdx.y * N;  // this CTA's columns of C (rows of B)
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa(&tmem_base)),
                  "r"(kCols));
@@ -203,6 +201,26 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *__restri
   }
 }
 
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *__restrict__ A, int lda,
+                                                   const __nv_bfloat16 *__restrict__ B, int ldb, int M,
+                                                   int Ntot, int K, const float *__restrict__ bias, int act,
+                                                   float *__restrict__ Cf, __nv_bfloat16 *__restrict__ Cb,
+                                                   int ldc, int *err) {
+  gemm_tile<N>(A, lda, B, ldb, M, Ntot, K, bias, act, Cf, Cb, ldc, err, blockIdx.x * kRows, blockIdx.y * N);
+}
+
+// several independent problems in one launch: blockIdx.z picks the problem,
+// CTAs outside its M x N extent return before touching tensor memory
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_gemm_grouped(const GemmProblem *__restrict__ probs, int *err) {
+  const GemmProblem p = probs[blockIdx.z];
+  const int row0 = blockIdx.x * kRows, col0 = blockIdx.y * N;
+  if (row0 >= p.M || col0 >= p.N) return;  // uniform over the CTA
+  gemm_tile<N>(static_cast<const __nv_bfloat16 *>(p.A), p.lda, static_cast<const __nv_bfloat16 *>(p.B), p.ldb,
+               p.M, p.N, p.K, p.bias, p.act, p.Cf, static_cast<__nv_bfloat16 *>(p.Cb), p.ldc, err, row0, col0);
+}
+
 }  // namespace tc
 
 // C = act(A B^T + bias) on `stream`; returns a CUDA error code of the launch
@@ -218,6 +236,24 @@ int launch_tc_gemm(const void *A, int lda, const void *B, int ldb, int M, int N,
   else if (N <= 64) k_gemm<64><<<dim3(gx, 1), kThreads, 0, s>>>(a, lda, b, ldb, M, N, K, bias, act, Cf, cb, ldc, err);
   else if (N <= 128) k_gemm<128><<<dim3(gx, 1), kThreads, 0, s>>>(a, lda, b, ldb, M, N, K, bias, act, Cf, cb, ldc, err);
   else k_gemm<256><<<dim3(gx, (unsigned)((N + 255) / 256)), kThreads, 0, s>>>(a, lda, b, ldb, M, N, K, bias, act, Cf, cb, ldc, err);
+  return (int)cudaGetLastError();
+}
+
+// n_probs problems (device array) in one launch with tiles of ncol (32,
+// 64, 128 or 256) columns; max_m / max_n bound every problem's M / N.  The
+// problems' K, N, lda, ldb obey the limits above (checked by the caller).
+int launch_tc_gemm_grouped(const GemmProblem *probs, int n_probs, int max_m, int max_n, int ncol, int *err,
+                           cudaStream_t s) {
+  using namespace tc;
+  if (n_probs <= 0 || max_m <= 0 || max_n <= 0) return (int)cudaErrorInvalidValue;
+  const dim3 grid((unsigned)((max_m + kRows - 1) / kRows), (unsigned)((max_n + ncol - 1) / ncol), (unsigned)n_probs);
+  switch (ncol) {
+    case 32: k_gemm_grouped<32><<<grid, kThreads, 0, s>>>(probs, err); break;
+    case 64: k_gemm_grouped<64><<<grid, kThreads, 0, s>>>(probs, err); break;
+    case 128: k_gemm_grouped<128><<<grid, kThreads, 0, s>>>(probs, err); break;
+    case 256: k_gemm_grouped<256><<<grid, kThreads, 0, s>>>(probs, err); break;
+    default: return (int)cudaErrorInvalidValue;
+  }
   return (int)cudaGetLastError();
 }
 

@@ -98,6 +98,10 @@ class Scene:
     ic_velocity: Optional[np.ndarray] = None
     ic_particles: Optional[np.ndarray] = None
     name: str = "scene"
+    # per particle: size relative to its zone's reference mesh and rotation
+    # about z (set by the scene builder; used by the learned surrogate)
+    p_scale: Optional[np.ndarray] = None
+    p_orient: Optional[np.ndarray] = None
 
     @property
     def n_nodes(self) -> int:
@@ -347,6 +351,20 @@ class GpuDEMModel:
             a = np.ascontiguousarray(values, dtype=np.float64).reshape(self.scene.n_nodes, 3)
             ptr = a.ctypes.data_as(ctypes.c_void_p)
         self._check(self.lib.pdgpu_upload_field(self.ctx, FIELD[name], ptr))
+
+    def surrogate_stats(self):
+        """(particles on the learned surrogate now, particles it covers,
+        particle-steps on the surrogate so far, particle-steps covered)."""
+        v = [ctypes.c_int64() for _ in range(4)]
+        self._check(self.lib.pdgpu_surrogate_stats(self.ctx, *(ctypes.byref(x) for x in v)))
+        return tuple(x.value for x in v)
+
+    def surrogate_errors(self) -> np.ndarray:
+        """The last check step per particle: (sum |f_s - f|^2, sum |f|^2),
+        an (n_particles, 2) array."""
+        out = np.zeros((self.scene.n_particles, 2), dtype=np.float64)
+        self._check(self.lib.pdgpu_surrogate_errors(self.ctx, _ptr(out, ctypes.c_double), out.size))
+        return out
 
     def compute_pd_forces(self) -> None:
         """DEMModel::computePeridynamicForces alone on the current state

@@ -832,6 +832,7 @@ def build_scene(spec: SceneSpec):
             sites = zs.sites
         rep_r = zs.geom_params[0]
         for (c, r, o) in sites:
+            scale, oo = 1.0, 0.0
             if zs.is_wall:
                 xg = local.copy()
                 vg = lvol.copy()
@@ -857,7 +858,7 @@ def build_scene(spec: SceneSpec):
                               all_fixed=1 if zs.all_dofs_constrained else 0,
                               compute_force=0 if zs.all_dofs_constrained else 1,
                               material=code, horizon=horizon, h=h,
-                              density=zs.material.density, rc=0.95 * h,
+                              density=zs.material.density, rc=0.95 * h, scale=scale, orient=oo,
                               kn=(18. / (math.pi * math.pow(horizon, 5))) * Kp,
                               bound_r=bound, mat=mat))
     if spec.test_name == "two_particle":
@@ -932,6 +933,7 @@ def build_scene(spec: SceneSpec):
         p_zone=P["zone"], p_compute_force=P["compute_force"], p_all_fixed=P["all_fixed"],
         p_material=P["material"], p_horizon=P["horizon"], p_h=P["h"], p_density=P["density"],
         p_rc=P["rc"], p_kn=P["kn"], p_bound_r=P["bound_r"], p_mat=pmat,
+        p_scale=P["scale"].astype(float), p_orient=P["orient"].astype(float),
         inf_type=inf_type, inf_params=inf, gravity=np.array(spec.gravity, dtype=float),
         time_scheme=1 if spec.time_scheme == "velocity_verlet" else 0,
         multi_particle=True, n_zones=nz, c_rc=crc.ravel(), c_kn=ckn.ravel(),

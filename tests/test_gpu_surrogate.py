@@ -1,0 +1,187 @@
+"""The learned surrogate.
+
+* gradients: one forward/backward pass of the trainer (tensor-core GEMMs and
+  the pdgpu_sur_* kernels) against a NumPy FP64 oracle that applies the same
+  BF16 roundings to the GEMM operands; max |g - g_oracle| <= 1e-2 max |g|.
+* training: on held-out bond-loop samples, the network's force error is
+  below that of the same reduced model without it (the bond loop's tangent
+  on the modes alone): what the network gains.
+* in the step, on deformed particles: the device chain (gather, tensor-core
+  GEMMs, lift) judged against the bond loop on the first check step, with
+  and without the network.
+* in the step, over a run: with the gates the wall reaction of a dense
+  compression stays within 1e-3 of the FP64 form, and on a loose packing the
+  surrogate carries most particle-steps without changing the result.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16(x):
+    import torch
+    return torch.as_tensor(np.asarray(x, dtype=np.float64)).to(torch.bfloat16).to(torch.float64).numpy()
+
+
+def test_trainer_gradients_match_cpu_oracle():
+    import torch
+    from peridem_b200.surrogate import Trainer, RANK
+    B = 64
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((B, RANK)).astype(np.float32)
+    T = rng.standard_normal((B, RANK)).astype(np.float32)
+    tr = Trainer(seed=5)
+    Xd = torch.as_tensor(X, device="cuda").to(torch.bfloat16)
+    Td = torch.as_tensor(T, device="cuda")
+    Y, cache = tr.forward(Xd)
+    loss, grads = tr.backward(Y, Td, cache)
+    torch.cuda.synchronize()
+    g = [x.cpu().numpy().astype(np.float64) for x in grads]
+    W = [w.cpu().numpy().astype(np.float64) for w in tr.W]
+    b = [x.cpu().numpy().astype(np.float64) for x in tr.b]
+    # oracle
+    Xb = _bf16(X)
+    Wb = [_bf16(w) for w in W]
+    H1 = np.tanh(Xb @ Wb[0].T + b[0]); H1b = _bf16(H1)
+    H2 = np.tanh(H1b @ Wb[1].T + b[1]); H2b = _bf16(H2)
+    Yo = H2b @ Wb[2].T + b[2]
+    n = Yo.size
+    dY = 2.0 / n * (Yo - T); dYb = _bf16(dY)
+    dW3 = dYb.T @ H2b; db3 = dY.sum(0)
+    dH2 = dYb @ Wb[2]; dZ2 = dH2 * (1 - H2 ** 2); dZ2b = _bf16(dZ2)
+    dW2 = dZ2b.T @ H1b; db2 = dZ2.sum(0)
+    dH1 = dZ2b @ Wb[1]; dZ1 = dH1 * (1 - H1 ** 2); dZ1b = _bf16(dZ1)
+    dW1 = dZ1b.T @ Xb; db1 = dZ1.sum(0)
+    ref = [dW1, dW2, dW3, db1, db2, db3]
+    assert abs(float(loss.item()) - float(((Yo - T) ** 2).sum())) <= 1e-3 * float(((Yo - T) ** 2).sum())
+    for name, a, r in zip(["dW1", "dW2", "dW3", "db1", "db2", "db3"], g, ref):
+        e = np.max(np.abs(a - r)) / max(np.max(np.abs(r)), 1e-30)
+        print(f"{name}: rel err {e:.2e}")
+        assert a.shape == r.shape
+        assert e <= 1e-2, name
+
+
+def _scene(seed, n, gapf, sf=5.0, wall=-2.0):
+    from peridem_b200 import scene as scn
+    h = 1e-3 / 8
+    return scn.build_scene(scn.compressive_2d(n_particles=n, r_range=(1e-3, 1.3e-3), h_div=8, width=10e-3,
+                                              seed=seed, gap=gapf * h, wall_speed=wall, nt=40000,
+                                              search_factor=sf))
+
+
+_MODEL = {}
+
+
+def _trained():
+    """Trained on snapshots of a 16-particle compression (wall at 1 m/s)."""
+    from peridem_b200 import surrogate as sg
+    if "s" not in _MODEL:
+        _MODEL["s"] = sg.build(_scene(4, 16, 1.02, wall=-1.0), steps=12000, every=40, iters=6000,
+                               samples_per_particle=1200)
+    return _MODEL["s"]
+
+
+def test_training_beats_linear_reduced_model():
+    s = _trained()
+    for S in s.shapes:
+        r = S.report
+        print(S.zone, {k: round(v, 5) for k, v in r.items()})
+        assert r["n_test_loaded"] > 0
+        assert r["force_err_mlp"] < 0.05
+        assert r["force_err_mlp"] < r["force_err_linear"]
+
+
+def _run(sc, prec, steps, sur=None, near=True, chk=50):
+    from peridem_b200.model import GpuDEMModel
+    m = GpuDEMModel(sc, precision=prec, build_neighbors=True, compute_mx=True)
+    try:
+        if sur is not None:
+            sur.attach(m, check_interval=chk, near_gate=near)
+        m.integrate_begin()
+        m.integrate_step(steps, graph_steps=1)
+        m.sync()
+        return m.history(), m.field("u"), (m.surrogate_stats() if sur is not None else None)
+    finally:
+        m.close()
+
+
+def test_surrogate_chain_on_deformed_particles():
+    """Every particle of a held-out packing gets a deformation in its
+    shape's modes with an RMS nodal displacement of 2e-7 of the reference
+    mesh (peak bond stretch a few tenths of the critical stretch, inside the
+    gate, where the material law is already nonlinear); on the first step
+    the bond loop runs for all particles and the scatter compares the
+    surrogate's force with it, per particle."""
+    import copy
+    from peridem_b200 import surrogate as sg
+    from peridem_b200.model import GpuDEMModel, PREC_MIXED
+    s = _trained()
+    sc = _scene(9, 12, 1.02)
+    rng = np.random.default_rng(11)
+    u = np.zeros((sc.n_nodes, 3))
+    for S in s.shapes:
+        for p in sg._zone_particles(sc, S.zone):
+            c = rng.standard_normal(sg.RANK)
+            c *= 2e-7 / np.linalg.norm(c)
+            sg._place(sc, u, p, (S.phi @ c) * np.sqrt(S.n_nodes))
+    linear = copy.deepcopy(s)
+    for S in linear.shapes:   # the network's output is zero: the tangent part alone
+        S.W[2] = np.zeros_like(S.W[2])
+        S.b[2] = np.zeros_like(S.b[2])
+
+    def errors(model):
+        m = GpuDEMModel(sc, precision=PREC_MIXED, build_neighbors=True, compute_mx=True)
+        try:
+            model.attach(m, check_interval=50, near_gate=False)
+            # after integrate_begin (forces of the undeformed state): the
+            # first step moves u by gravity alone, a rigid translation
+            m.integrate_begin()
+            m.set_field("u", u)
+            m.integrate_step(1)
+            m.sync()
+            e = m.surrogate_errors()
+            zmax = float(np.max(m.field("Z")))
+        finally:
+            m.close()
+        assert zmax < 0.5, zmax   # inside the stretch gate
+        sel = e[:, 1] > 0
+        return np.sqrt(e[sel, 0] / e[sel, 1])
+
+    e_mlp, e_lin = errors(s), errors(linear)
+    print(f"in-step relative force error per particle: network median {np.median(e_mlp):.4f} max "
+          f"{e_mlp.max():.4f}; tangent alone median {np.median(e_lin):.4f} max {e_lin.max():.4f}")
+    assert len(e_mlp) == len(e_lin) > 0
+    assert e_mlp.max() < 0.05
+    assert np.median(e_mlp) < np.median(e_lin)
+
+
+def test_gated_surrogate_keeps_the_wall_reaction():
+    """Dense compression (lattice gaps 1.02 h, wall at 2 m/s, 3000 steps):
+    every particle has contact candidates, so the proximity gate keeps the
+    bond loop everywhere and the contact reaction matches the FP64 form."""
+    from peridem_b200.model import PREC_FP64, PREC_MIXED
+    sc = _scene(7, 12, 1.02)
+    h64, u64, _ = _run(sc, PREC_FP64, 3000)
+    hs, us, st = _run(sc, PREC_MIXED, 3000, sur=_trained())
+    den = float(np.max(np.abs(h64[:, 3])))
+    err = float(np.max(np.abs(hs[:, 3] - h64[:, 3]))) / den
+    print(f"contact reaction max {den:.3e}, rel err {err:.2e}; particle-steps on the surrogate {st[2]}/{st[3]}")
+    assert den > 0, "the wall never touched the packing"
+    assert err <= 1e-3
+    assert st[3] == 3000 * st[1]
+
+
+def test_surrogate_carries_a_loose_packing():
+    """Loose packing (gaps 3 h, search radius 1.9 h, 8000 steps): most
+    particle-steps run on the surrogate and the displacements stay within
+    1e-3 of the mixed form without it."""
+    from peridem_b200.model import PREC_MIXED
+    sc = _scene(7, 12, 3.0, sf=2.0)
+    _, ua, _ = _run(sc, PREC_MIXED, 8000)
+    _, ub, st = _run(sc, PREC_MIXED, 8000, sur=_trained())
+    frac = st[2] / st[3]
+    du = float(np.max(np.abs(ua - ub))) / max(float(np.max(np.abs(ua))), 1e-300)
+    print(f"particle-steps on the surrogate {st[2]}/{st[3]} ({frac:.3f}); displacement rel err {du:.2e}")
+    assert frac > 0.9
+    assert du <= 1e-3
