@@ -315,6 +315,26 @@ PDGPU_API int pdgpu_enable_timing(pdgpu_ctx *ctx, int32_t on);
 PDGPU_API int pdgpu_kernel_times(pdgpu_ctx *ctx, int32_t max_kernels, const char **names, double *ms,
                        int64_t *launches, int32_t *count);
 
+/* A batched ensemble (no counterpart in the reference, which runs one scene
+ * per process): the uploaded nodes and particles hold n_scenes independent
+ * scenes, each a contiguous run of particles (particle_offsets, n_scenes + 1
+ * entries from 0 to the particle count; nodes follow their particles), far
+ * enough apart that no contact candidate joins two scenes, with zone ids
+ * distinct per scene and a block-diagonal contact table.  All scenes share
+ * dt and advance together: one bond-loop launch over every scene's tiles,
+ * one contact pass, one graph per step.  Particle damping pairs stay within
+ * a scene.  test_walls[s] is the particle of scene s whose compressive-test
+ * output (ppCompressiveTest: time, wall displacement, reaction sum f vol,
+ * contact reaction) is recorded every test_interval steps (-1: none), in
+ * test_dir; up to 4096 records per scene.  Call before the first step. */
+PDGPU_API int pdgpu_set_scenes(pdgpu_ctx *ctx, int32_t n_scenes, const int64_t *particle_offsets,
+                               const int64_t *test_walls);
+
+/* The compressive-test records of one scene of an ensemble (like
+ * pdgpu_get_history); *count = records so far (at most 4096). */
+PDGPU_API int pdgpu_get_scene_history(pdgpu_ctx *ctx, int32_t scene, double *t, double *delta, double *force,
+                                      double *cforce, int64_t cap, int64_t *count);
+
 /* Building block of the learned surrogate (no counterpart in the
  * reference): C = act(A B^T + bias) on the tensor cores (tcgen05, BF16
  * operands, FP32 accumulation).  A is M x K and B is N x K, both row-major

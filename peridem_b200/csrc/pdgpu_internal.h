@@ -46,6 +46,7 @@ struct ContactPair {
 struct DampParticle {
   double bound_r, density;
   int32_t zone, type;
+  int32_t q0, q1;  // the particles of its scene (all particles outside an ensemble)
 };
 
 struct Influence {
@@ -206,7 +207,7 @@ struct DevData {
   double *fc;
   // short dependency chains for the contact and damping passes
   int2 *c_span;          // [c_row[i], c_row[i + 1]) of compacted node t = c_nodes[t]
-  uint8_t *nzone;        // zone of each node's particle
+  uint16_t *nzone;        // zone of each node's particle
   DampParticle *dpart;   // per particle: bounding radius, density, zone, type
   double *pcen;          // per particle: centre position and velocity (8 doubles), this step
 
@@ -245,6 +246,18 @@ struct DevData {
   float4 *xv_mixed;  // per node {x, y, z, vol}: reference coordinates minus the centre's, FP32
   int32_t use16;
   float inf_p0, inf_p1;
+
+  // batched ensemble (pdgpu_set_scenes): independent scenes side by side in
+  // one model.  Per scene its node range and test wall; per particle whether
+  // it is a scene's test wall; per compacted contact node its term of the
+  // wall reaction; per scene the compressive-test history [cap][4].
+  int32_t n_scenes;
+  int64_t *scene_node;
+  int32_t *scene_wall;
+  uint8_t *pwall_test;
+  double *cr_t;
+  double *scene_hist;
+  int64_t scene_hist_cap;
 
   // learned surrogate (pdgpu_set_surrogate): per particle the gate's verdict
   // at the last check, and whether the last contact-list rebuild found
@@ -306,6 +319,7 @@ int rebuild_grid_blocks(const DevData &d, int lanes);
 cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, int lanes, int init,
                                    cudaStream_t s);
 void launch_damping(const DevData &d, cudaStream_t s);
+void launch_scene_post(const DevData &d, cudaStream_t s);  // per-scene test output of an ensemble
 void launch_external(const DevData &d, cudaStream_t s);
 void launch_postprocess(const DevData &d, cudaStream_t s);
 void launch_build_pd(const DevData &d, double cell, int64_t *row_tmp, int32_t *cnt, void *scan_tmp,

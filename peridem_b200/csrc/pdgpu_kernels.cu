@@ -922,8 +922,8 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
     for (int a = threadIdx.x; a < nz * nz; a += kBlock) cps[a] = d.contact[a];
   {
     // particle centres (position, velocity) of this step for the damping pass
-    const int64_t p = (int64_t)blockIdx.x * kBlock + threadIdx.x;
-    if (p < d.n_particles) {
+    for (int64_t p = (int64_t)blockIdx.x * kBlock + threadIdx.x; p < d.n_particles;
+         p += (int64_t)gridDim.x * kBlock) {
       const int64_t c = d.particles[p].center;
       double xc[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
       ldv<DIM>(d.x, c, xc);
@@ -999,7 +999,7 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
           if (slot < d.wp_cap) d.wp[(int64_t)pi * d.wp_cap + slot] = j;
           else set_error(d.ctrl, DEV_ERR_WALLPAIR_OVERFLOW, pi);
         }
-        if (pj == d.test_wall) {
+        if (d.pwall_test ? d.pwall_test[pj] != 0 : pj == d.test_wall) {
           const int td = d.test_dir;
           crd += td == 0 ? cx + mf * et[0] : (td == 1 ? cy + mf * et[1] : cz + mf * et[2]);
         }
@@ -1013,6 +1013,7 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
       const double f[3] = {fx, fy, fz};
       stv<DIM>(d.fc, i, f);
       crd_acc += crd * d.vol[i];
+      if (d.cr_t) d.cr_t[t] = crd * d.vol[i];
     }
   }
   // deterministic per-block partial of the test wall's contact reaction
@@ -1058,8 +1059,8 @@ __global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
     vc[q] = d.pcen[8 * p + 3 + q];
   }
   double acc[3] = {0.0, 0.0, 0.0};
-  // particle-particle
-  for (int q = threadIdx.x; q < d.n_particles; q += blockDim.x) {
+  // particle-particle, over the particles of this particle's scene
+  for (int q = P.q0 + threadIdx.x; q < P.q1; q += blockDim.x) {
     if (q == p) continue;
     const DampParticle Q = d.dpart[q];
     if (Q.type != 0) continue;
@@ -1312,6 +1313,63 @@ __device__ __noinline__ void postprocess_block(const DevData &d) {
       c->contact_area_radius = car;
       c->max_y = is_less(0.0, my) ? my : 0.0;
     }
+  }
+}
+
+// Compressive-test output of every scene of a batched ensemble, one CTA per
+// scene (the single-scene form is postprocess_block): the test wall's
+// reaction sum f vol over its nodes, the contact reaction summed over the
+// scene's run of the compacted contact nodes (ascending node ids, so each
+// scene's nodes form one run), and the wall's displacement.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_scene_post(const __grid_constant__ DevData d) {
+  __shared__ double red[2][8];
+  __shared__ int64_t range[2];
+  const CtrlState *c = d.ctrl;
+  if (c->error) return;
+  const int64_t n = c->n;
+  if (!(n % d.test_interval == 0 && n >= d.test_interval)) return;
+  const int64_t h = n / d.test_interval - 1;
+  const int s = blockIdx.x;
+  if (h >= d.scene_hist_cap || s >= d.n_scenes || d.scene_wall[s] < 0) return;
+  const int st = DIM == 2 ? 2 : 4;
+  const DevParticle W = d.particles[d.scene_wall[s]];
+  const int dir = d.test_dir;
+  const int64_t nn = c->c_nnodes;
+  if (threadIdx.x < 2) {
+    const int64_t key = d.scene_node[s + threadIdx.x];
+    int64_t lo = 0, hi = nn;  // first compacted index whose node is >= key
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (d.c_nodes[mid] < key) lo = mid + 1;
+      else hi = mid;
+    }
+    range[threadIdx.x] = lo;
+  }
+  __syncthreads();
+  double rs = 0.0, rc = 0.0;
+  for (int64_t i = W.start + threadIdx.x; i < W.end; i += blockDim.x) rs += d.f[st * i + dir] * d.vol[i];
+  for (int64_t t = range[0] + threadIdx.x; t < range[1]; t += blockDim.x) rc += d.cr_t[t];
+  for (int o = 16; o > 0; o >>= 1) {
+    rs += __shfl_xor_sync(0xffffffffu, rs, o);
+    rc += __shfl_xor_sync(0xffffffffu, rc, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = rs;
+    red[1][threadIdx.x >> 5] = rc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < 8; w++) {
+      a += red[0][w];
+      b += red[1][w];
+    }
+    double *o = d.scene_hist + 4 * ((int64_t)s * d.scene_hist_cap + h);
+    o[0] = c->time;
+    o[1] = d.x[st * W.start + dir] - d.xref[st * W.start + dir];
+    o[2] = a;
+    o[3] = -b;
   }
 }
 
@@ -1583,6 +1641,12 @@ void launch_contact_force(const DevData &d, int lanes, cudaStream_t s) {
     else if (lanes == 8) k_contact<3, 8><<<g, kBlock, 0, s>>>(d);
     else k_contact<3, 32><<<g, kBlock, 0, s>>>(d);
   }
+}
+
+void launch_scene_post(const DevData &d, cudaStream_t s) {
+  if (d.n_scenes <= 1) return;
+  if (d.dim == 2) k_scene_post<2><<<d.n_scenes, 256, 0, s>>>(d);
+  else k_scene_post<3><<<d.n_scenes, 256, 0, s>>>(d);
 }
 
 void launch_damping(const DevData &d, cudaStream_t s) {

@@ -21,6 +21,7 @@ namespace {
 
 constexpr int kMaxTimed = 64;
 constexpr int64_t kHistoryCap = 1 << 16;
+constexpr int64_t kSceneHistCap = 1 << 12;  // test records per scene of an ensemble
 // tail padding of the bond arrays: the bond loop copies whole 16-byte
 // blocks of neighbour columns and bitmap words around each tile's range
 constexpr int64_t kBondPad = 16;
@@ -81,6 +82,9 @@ struct pdgpu_ctx {
   // contact and damping run on `branch` beside the bond loop on `stream`
   cudaStream_t branch = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+
+  // batched ensemble (pdgpu_set_scenes): particle offsets (CSR) and test walls
+  std::vector<int64_t> scene_poff, scene_walls;
 
   // learned surrogate (pdgpu_set_surrogate): per shape its particles, BF16
   // weights and the activations of the chain (P + 1 rows: row P is a zero
@@ -731,16 +735,47 @@ int prepare(pdgpu_ctx *ctx) {
   CK(cudaMemset(d.c_span, 0, (size_t)N * sizeof(int2)));
   {
     // per-node zone and compact per-particle damping constants
-    if (d.n_zones > 255) return fail(ctx, PDGPU_ERR_ARG, "at most 255 contact zones");
-    std::vector<uint8_t> nz((size_t)N, 0);
+    if (d.n_zones > 65535) return fail(ctx, PDGPU_ERR_ARG, "at most 65535 contact zones");
+    std::vector<uint16_t> nz((size_t)N, 0);
     std::vector<DampParticle> dp(ctx->hp.size());
-    for (size_t p = 0; p < ctx->hp.size(); p++) {
-      const DevParticle &P = ctx->hp[p];
-      for (int64_t i = P.start; i < P.end; i++) nz[i] = (uint8_t)P.zone;
-      dp[p] = DampParticle{P.bound_r, P.density, P.zone, P.type};
+    const int ns = ctx->scene_poff.empty() ? 1 : (int)ctx->scene_poff.size() - 1;
+    for (int sc = 0; sc < ns; sc++) {
+      const int32_t q0 = ctx->scene_poff.empty() ? 0 : (int32_t)ctx->scene_poff[sc];
+      const int32_t q1 = ctx->scene_poff.empty() ? (int32_t)ctx->hp.size() : (int32_t)ctx->scene_poff[sc + 1];
+      for (int32_t p = q0; p < q1; p++) {
+        const DevParticle &P = ctx->hp[p];
+        for (int64_t i = P.start; i < P.end; i++) nz[i] = (uint16_t)P.zone;
+        dp[p] = DampParticle{P.bound_r, P.density, P.zone, P.type, q0, q1};
+      }
     }
     TRY(dalloc(ctx, &d.nzone, (size_t)N));
-    CK(cudaMemcpy(d.nzone, nz.data(), (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.nzone, nz.data(), (size_t)N * 2, cudaMemcpyHostToDevice));
+    if (ns > 1) {
+      // batched ensemble: scene node ranges, test walls and histories
+      std::vector<int64_t> sn(ns + 1);
+      std::vector<int32_t> sw(ns);
+      std::vector<uint8_t> pw(ctx->hp.size(), 0);
+      for (int sc = 0; sc < ns; sc++) {
+        sn[sc] = ctx->hp[ctx->scene_poff[sc]].start;
+        sw[sc] = (int32_t)ctx->scene_walls[sc];
+        if (sw[sc] >= 0) pw[sw[sc]] = 1;
+      }
+      sn[ns] = N;
+      d.n_scenes = ns;
+      TRY(dalloc(ctx, &d.scene_node, sn.size()));
+      CK(cudaMemcpy(d.scene_node, sn.data(), sn.size() * 8, cudaMemcpyHostToDevice));
+      TRY(dalloc(ctx, &d.scene_wall, sw.size()));
+      CK(cudaMemcpy(d.scene_wall, sw.data(), sw.size() * 4, cudaMemcpyHostToDevice));
+      TRY(dalloc(ctx, &d.pwall_test, pw.size()));
+      CK(cudaMemcpy(d.pwall_test, pw.data(), pw.size(), cudaMemcpyHostToDevice));
+      TRY(dalloc(ctx, &d.cr_t, (size_t)N));
+      CK(cudaMemset(d.cr_t, 0, (size_t)N * 8));
+      d.scene_hist_cap = kSceneHistCap;
+      TRY(dalloc(ctx, &d.scene_hist, (size_t)ns * kSceneHistCap * 4));
+      CK(cudaMemset(d.scene_hist, 0, (size_t)ns * kSceneHistCap * 4 * 8));
+      d.test_dir = ctx->desc.test_dir;
+      d.test_interval = ctx->desc.test_interval > 0 ? ctx->desc.test_interval : 1;
+    }
     TRY(dalloc(ctx, &d.dpart, dp.size()));
     CK(cudaMemcpy(d.dpart, dp.data(), dp.size() * sizeof(DampParticle), cudaMemcpyHostToDevice));
     TRY(dalloc(ctx, &d.pcen, 8 * dp.size()));
@@ -873,6 +908,7 @@ void compute_forces(pdgpu_ctx *ctx, bool step) {
   // the post-processing
   const bool verlet = ctx->desc.time_scheme == 1;
   run(ctx, "step_end", [&] { launch_step_end(d, step && verlet, step ? 1 : 0, s); });
+  if (step && d.n_scenes > 1) run(ctx, "scene_post", [&] { launch_scene_post(d, s); });
 }
 
 // DEMModel::integrateStep (demModel.cpp:342-460) + post-processing
@@ -944,6 +980,7 @@ cudaError_t graph_step(pdgpu_ctx *ctx, const char **where) {
   }
   *where = "kernels after the join";
   launch_step_end(d, verlet ? 1 : 0, 1, s);
+  launch_scene_post(d, s);
   return cudaGetLastError();
 }
 
@@ -1577,6 +1614,48 @@ int pdgpu_surrogate_stats(pdgpu_ctx *ctx, int64_t *n_on, int64_t *n_total, int64
   int32_t flag = 0;
   CK(cudaMemcpy(&flag, ctx->sur_errflag, 4, cudaMemcpyDeviceToHost));
   if (flag) return fail(ctx, PDGPU_ERR_CUDA, "a tensor-core wait of the surrogate timed out");
+  return PDGPU_OK;
+}
+
+int pdgpu_set_scenes(pdgpu_ctx *ctx, int32_t n_scenes, const int64_t *particle_offsets, const int64_t *test_walls) {
+  if (!ctx || n_scenes <= 0 || !particle_offsets || !test_walls) return PDGPU_ERR_ARG;
+  if (ctx->prepared || ctx->begun) return fail(ctx, PDGPU_ERR_STATE, "set the scenes before the first step");
+  if (!ctx->particles) return fail(ctx, PDGPU_ERR_STATE, "upload particles first");
+  const int64_t np = (int64_t)ctx->hp.size();
+  if (particle_offsets[0] != 0 || particle_offsets[n_scenes] != np)
+    return fail(ctx, PDGPU_ERR_ARG, "scene offsets must run from 0 to the number of particles");
+  for (int s = 0; s < n_scenes; s++) {
+    if (particle_offsets[s + 1] <= particle_offsets[s]) return fail(ctx, PDGPU_ERR_ARG, "scene %d is empty", s);
+    const int64_t w = test_walls[s];
+    if (w >= 0 && (w < particle_offsets[s] || w >= particle_offsets[s + 1]))
+      return fail(ctx, PDGPU_ERR_ARG, "test wall of scene %d lies outside it", s);
+  }
+  ctx->scene_poff.assign(particle_offsets, particle_offsets + n_scenes + 1);
+  ctx->scene_walls.assign(test_walls, test_walls + n_scenes);
+  return PDGPU_OK;
+}
+
+int pdgpu_get_scene_history(pdgpu_ctx *ctx, int32_t scene, double *t, double *delta, double *force,
+                            double *cforce, int64_t cap, int64_t *count) {
+  if (!ctx || !count) return PDGPU_ERR_ARG;
+  const DevData &d = ctx->d;
+  if (d.n_scenes <= 1 || scene < 0 || scene >= d.n_scenes) return fail(ctx, PDGPU_ERR_ARG, "no scene %d", scene);
+  CK(cudaStreamSynchronize(ctx->stream));
+  CtrlState c;
+  CK(cudaMemcpy(&c, d.ctrl, sizeof(c), cudaMemcpyDeviceToHost));
+  const int64_t recorded = c.n >= d.test_interval ? c.n / d.test_interval : 0;
+  *count = std::min<int64_t>(recorded, d.scene_hist_cap);
+  const int64_t n = std::min<int64_t>(cap, *count);
+  if (n <= 0 || !t || !delta || !force || !cforce) return PDGPU_OK;
+  std::vector<double> h((size_t)n * 4);
+  CK(cudaMemcpy(h.data(), d.scene_hist + 4 * (int64_t)scene * d.scene_hist_cap, h.size() * 8,
+                cudaMemcpyDeviceToHost));
+  for (int64_t k = 0; k < n; k++) {
+    t[k] = h[4 * k];
+    delta[k] = h[4 * k + 1];
+    force[k] = h[4 * k + 2];
+    cforce[k] = h[4 * k + 3];
+  }
   return PDGPU_OK;
 }
 

@@ -36,9 +36,10 @@ class BCSet:
     zero: bool
     time_params: np.ndarray        # 4
     spatial_params: np.ndarray     # 2
-    particle_sel: np.ndarray       # uint8 [Np]
-    node_sel: np.ndarray           # uint8 [N]
+    particle_sel: np.ndarray       # uint8 [Np] (sparse: selected particle ids)
+    node_sel: np.ndarray           # uint8 [N] (sparse: selected node ids)
     particle_box: np.ndarray       # float64 [Np, 6]
+    sparse: bool = False           # selections given as index lists (merged scenes)
 
 
 @dataclass
@@ -102,6 +103,14 @@ class Scene:
     # about z (set by the scene builder; used by the learned surrogate)
     p_scale: Optional[np.ndarray] = None
     p_orient: Optional[np.ndarray] = None
+    # batched ensemble (scene.merge_scenes): particle offsets of the scenes
+    # (CSR, n_scenes + 1) and each scene's test wall (-1: none)
+    scene_poff: Optional[np.ndarray] = None
+    scene_walls: Optional[np.ndarray] = None
+
+    @property
+    def n_scenes(self) -> int:
+        return 1 if self.scene_poff is None else len(self.scene_poff) - 1
 
     @property
     def n_nodes(self) -> int:
@@ -209,6 +218,10 @@ class GpuDEMModel:
             for q in range(6):
                 P.mat[q] = float(s.p_mat[k, q])
         self._check(L.pdgpu_upload_particles(c, Np, parts))
+        if s.scene_poff is not None:
+            po = np.ascontiguousarray(s.scene_poff, dtype=np.int64)
+            tw = np.ascontiguousarray(s.scene_walls, dtype=np.int64)
+            self._check(L.pdgpu_set_scenes(c, len(po) - 1, _ptr(po, ctypes.c_int64), _ptr(tw, ctypes.c_int64)))
         ip = (ctypes.c_double * 2)(*[float(a) for a in s.inf_params[:2]])
         self._check(L.pdgpu_set_influence(c, int(s.inf_type), ip))
         if s.multi_particle:
@@ -243,8 +256,14 @@ class GpuDEMModel:
                 for q in range(2):
                     bc.spatial_params[q] = (float(b.spatial_params[q])
                                             if q < len(b.spatial_params) else 0.0)
-                ps = np.ascontiguousarray(b.particle_sel, dtype=np.uint8)
-                ns = np.ascontiguousarray(b.node_sel, dtype=np.uint8)
+                if b.sparse:
+                    ps = np.zeros(Np, dtype=np.uint8)
+                    ps[np.asarray(b.particle_sel, dtype=np.int64)] = 1
+                    ns = np.zeros(N, dtype=np.uint8)
+                    ns[np.asarray(b.node_sel, dtype=np.int64)] = 1
+                else:
+                    ps = np.ascontiguousarray(b.particle_sel, dtype=np.uint8)
+                    ns = np.ascontiguousarray(b.node_sel, dtype=np.uint8)
                 bx = _f64(b.particle_box).reshape(-1)
                 self._check(fn(c, ctypes.byref(bc), _ptr(ps, ctypes.c_uint8),
                                _ptr(ns, ctypes.c_uint8), _ptr(bx, ctypes.c_double)))
@@ -351,6 +370,18 @@ class GpuDEMModel:
             a = np.ascontiguousarray(values, dtype=np.float64).reshape(self.scene.n_nodes, 3)
             ptr = a.ctypes.data_as(ctypes.c_void_p)
         self._check(self.lib.pdgpu_upload_field(self.ctx, FIELD[name], ptr))
+
+    def scene_history(self, scene: int) -> np.ndarray:
+        """Compressive-test records of one scene of an ensemble: rows of
+        (time, wall displacement, reaction, contact reaction)."""
+        cnt = ctypes.c_int64()
+        self._check(self.lib.pdgpu_get_scene_history(self.ctx, scene, None, None, None, None, 0,
+                                                     ctypes.byref(cnt)))
+        n = cnt.value
+        cols = [np.empty(n) for _ in range(4)]
+        self._check(self.lib.pdgpu_get_scene_history(self.ctx, scene, *[_ptr(c, ctypes.c_double) for c in cols],
+                                                     n, ctypes.byref(cnt)))
+        return np.stack(cols, axis=1)
 
     def surrogate_stats(self):
         """(particles on the learned surrogate now, particles it covers,

@@ -632,7 +632,45 @@ def _is_greater(a: float, b: float) -> bool:
 
 def mesh_size(x: np.ndarray) -> float:
     """util::computeMeshSize (src/util/geom.cpp:578-603): scan i, j in
-    order, keep the first distance that is isLess than the running guess."""
+    order, keep the first distance that is isLess than the running guess.
+
+    The guess starts at |x0 - x1| and only ever moves to a smaller distance,
+    so only pairs closer than |x0 - x1| can change it: those are found with a
+    k-d tree, their distances recomputed with the scan's own arithmetic, and
+    the scan's sequence of replacements replayed over them in (i, j) order.
+    Same result as the full scan (mesh_size_scan), in O(n log n)."""
+    n = len(x)
+    if n < 2:
+        return 0.0
+    try:
+        from scipy.spatial import cKDTree
+    except ImportError:  # pragma: no cover
+        return mesh_size_scan(x)
+    x = np.asarray(x, dtype=np.float64)
+    guess = float(np.sqrt(((x[0] - x[1]) ** 2).sum(axis=-1)))
+    pairs = cKDTree(x).query_pairs(guess * (1.0 + 1e-9) + 1e-300, output_type="ndarray")
+    if len(pairs) == 0:
+        return guess
+    i = np.concatenate([pairs[:, 0], pairs[:, 1]])
+    j = np.concatenate([pairs[:, 1], pairs[:, 0]])
+    order = np.lexsort((j, i))
+    i, j = i[order], j[order]
+    d = x[i] - x[j]
+    dist = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+    start = 0
+    while True:
+        thr = dist[start:]
+        cand = (guess - thr) > (np.maximum(np.abs(thr), abs(guess)) * 1.0e-5)
+        if not cand.any():
+            break
+        k = int(np.argmax(cand)) + start
+        guess = float(dist[k])
+        start = k + 1
+    return guess
+
+
+def mesh_size_scan(x: np.ndarray) -> float:
+    """The full O(n^2) scan of util::computeMeshSize."""
     n = len(x)
     if n < 2:
         return 0.0
@@ -946,3 +984,134 @@ def build_scene(spec: SceneSpec):
         ubc=ubc, fbc=fbc,
         ic_velocity=np.array(spec.ic_velocity) if spec.ic_velocity is not None else None,
         ic_particles=np.array(spec.ic_particles, dtype=np.uint64), name=spec.name)
+
+
+# ---------------------------------------------------------------------------
+# batched ensembles
+# ---------------------------------------------------------------------------
+def ensemble_specs(n_scenes: int = 256, seed: int = 0, n_range: Tuple[int, int] = (20, 200),
+                   r_range: Tuple[float, float] = (0.8e-3, 1.6e-3), h_div_range: Tuple[int, int] = (8, 16),
+                   speed_range: Tuple[float, float] = (0.05, 0.2), material: str = "RNPBond",
+                   nt: int = 20000, search_factor: float = 5.0) -> List[SceneSpec]:
+    """Independent 2-D compression scenes of uneven size: per scene a
+    particle count U[n_range], a mesh h = R / U{h_div_range}, a top-wall
+    speed U[speed_range] and its own packing seed; discs and hexagons with
+    radii U[r_range].  Every scene takes the smallest stable step of the set,
+    so that they can advance together."""
+    rng = np.random.default_rng(seed)
+    picks = []
+    for s in range(n_scenes):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        hd = int(rng.integers(h_div_range[0], h_div_range[1] + 1))
+        v = float(rng.uniform(*speed_range))
+        picks.append((n, hd, v))
+    dt = min(stable_dt(2.0e9, 1200.0, r_range[0] / hd) for _, hd, _ in picks)
+    spacing = 2.0 * r_range[1] + 1.05 * r_range[0] / h_div_range[0]
+    specs = []
+    for s, (n, hd, v) in enumerate(picks):
+        width = math.ceil(math.sqrt(n)) * spacing
+        specs.append(compressive_2d(n_particles=n, r_range=r_range, h_div=hd, width=width,
+                                    seed=seed * 100003 + s, material=material, wall_speed=-v, dt=dt, nt=nt,
+                                    search_factor=search_factor))
+    return specs
+
+
+def merge_scenes(scenes, pad: Optional[float] = None):
+    """One model of independent scenes laid out on a grid, each shifted so
+    that no contact candidate can join two scenes (``pad`` between their
+    bounding boxes; default 4 search radii plus 2 mm).  Zones are renumbered
+    per scene and the contact table is block-diagonal (no contact between
+    scenes); the scenes' displacement BCs become sparse sets; particle
+    offsets and test walls go to the ensemble tables (pdgpu_set_scenes).
+    All scenes must share dt, influence function, time scheme, gravity and
+    search parameters.  Zero-displacement sets are left out: the reference
+    applies them through particle 0 only, which in these scenes is never a
+    wall."""
+    from .model import Scene, BCSet
+    s0 = scenes[0]
+    for sc in scenes:
+        if (sc.dt != s0.dt or sc.inf_type != s0.inf_type or np.any(sc.inf_params != s0.inf_params)
+                or sc.time_scheme != s0.time_scheme or np.any(sc.gravity != s0.gravity)
+                or sc.search_factor != s0.search_factor or sc.search_interval != s0.search_interval
+                or sc.dim != s0.dim or sc.test_dir != s0.test_dir or sc.test_interval != s0.test_interval):
+            raise ValueError("scenes of an ensemble must share dt, influence, scheme, gravity, search and test")
+        if sc.ic_velocity is not None and len(sc.ic_particles):
+            raise ValueError("initial-velocity sets are not merged")
+    dim = s0.dim
+    max_rc = max(sc.max_contact_r for sc in scenes)
+    if pad is None:
+        pad = 4.0 * s0.search_factor * max_rc + 2e-3
+    ext = [(sc.xref.min(axis=0), sc.xref.max(axis=0)) for sc in scenes]
+    cw = max(hi[0] - lo[0] for lo, hi in ext) + pad
+    ch = max(hi[1] - lo[1] for lo, hi in ext) + pad
+    cols = int(math.ceil(math.sqrt(len(scenes))))
+    xs, xr, vol, fix, ptid = [], [], [], [], []
+    P = {k: [] for k in ("p_start", "p_end", "p_center", "p_type", "p_zone", "p_compute_force",
+                         "p_all_fixed", "p_material", "p_horizon", "p_h", "p_density", "p_rc", "p_kn",
+                         "p_bound_r", "p_mat", "p_scale", "p_orient")}
+    nz_tot = sum(sc.n_zones for sc in scenes)
+    tabs = {k: np.zeros((nz_tot, nz_tot)) for k in ("c_rc", "c_kn", "c_mu", "c_betan", "c_kappa")}
+    ubc, poff, walls = [], [0], []
+    n_off = p_off = z_off = 0
+    for k, sc in enumerate(scenes):
+        lo, _ = ext[k]
+        shift = np.zeros(3)
+        shift[0] = (k % cols) * cw - lo[0]
+        shift[1] = (k // cols) * ch - lo[1]
+        xr.append(sc.xref + shift)
+        xs.append((sc.x if sc.x is not None else sc.xref) + shift)
+        vol.append(sc.vol)
+        fix.append(sc.fix)
+        ptid.append(np.asarray(sc.ptid, dtype=np.uint64) + np.uint64(p_off))
+        for key in P:
+            a = getattr(sc, key)
+            if key in ("p_start", "p_end", "p_center"):
+                a = np.asarray(a) + n_off
+            elif key == "p_zone":
+                a = np.asarray(a) + z_off
+            P[key].append(np.asarray(a))
+        nz = sc.n_zones
+        for key in tabs:
+            tabs[key][z_off:z_off + nz, z_off:z_off + nz] = np.asarray(getattr(sc, key)).reshape(nz, nz)
+        for b in sc.ubc:
+            if b.zero:
+                continue
+            sel = np.nonzero(b.particle_sel)[0]
+            nodes = np.nonzero(b.node_sel)[0]
+            ubc.append(BCSet(time_fn=b.time_fn, spatial_fn=b.spatial_fn, dir_mask=b.dir_mask, zero=False,
+                             time_params=b.time_params, spatial_params=b.spatial_params,
+                             particle_sel=sel + p_off, node_sel=nodes + n_off,
+                             particle_box=np.zeros((0, 6)), sparse=True))
+        walls.append(int(sc.test_wall) + p_off if sc.test == 2 else -1)
+        n_off += sc.n_nodes
+        p_off += sc.n_particles
+        z_off += nz
+        poff.append(p_off)
+    Np = p_off
+    for b in ubc:
+        b.particle_box = np.zeros((Np, 6))
+    cat = lambda key: np.concatenate(P[key]) if key != "p_mat" else np.concatenate(P[key], axis=0)
+    xref = np.concatenate(xr)
+    return Scene(
+        dim=dim, dt=s0.dt, nt=s0.nt, xref=xref, vol=np.concatenate(vol), fix=np.concatenate(fix),
+        ptid=np.concatenate(ptid),
+        **{key: cat(key) for key in P},
+        inf_type=s0.inf_type, inf_params=s0.inf_params, gravity=s0.gravity, time_scheme=s0.time_scheme,
+        multi_particle=True, n_zones=nz_tot, **{key: tabs[key].ravel() for key in tabs},
+        max_contact_r=max_rc, search_factor=s0.search_factor, search_interval=s0.search_interval,
+        test=0, test_wall=0, test_dir=s0.test_dir, test_interval=s0.test_interval,
+        x=np.concatenate(xs), u=np.zeros_like(xref), v=np.zeros_like(xref), ubc=ubc, fbc=[],
+        ic_velocity=None, ic_particles=np.zeros(0, dtype=np.uint64), name=f"ensemble_{len(scenes)}",
+        scene_poff=np.array(poff, dtype=np.int64), scene_walls=np.array(walls, dtype=np.int64))
+
+
+def build_scenes(specs: Sequence[SceneSpec], workers: int = 0) -> list:
+    """build_scene over many specs, in a pool of spawned processes (the
+    set-up is per-particle host work: transforms, mesh sizes, constants)."""
+    if workers == 1 or len(specs) < 4:
+        return [build_scene(s) for s in specs]
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    n = workers or min(len(specs), os.cpu_count() or 1, 64)
+    with cf.ProcessPoolExecutor(max_workers=n, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(build_scene, specs, chunksize=max(1, len(specs) // (4 * n))))
