@@ -31,7 +31,11 @@ using bonds_mixed::gmask;
 using bonds_mixed::gsum;
 using bonds_mixed::gmax;
 
-constexpr int kThreads = 256;
+// threads per CTA: 256 in 2-D; in 3-D, where a tile's neighbour window is
+// large and few CTAs fit an SM, enough lane groups for a 256-node tile in
+// one pass (up to 1024 threads)
+template <int DIM, int LPN>
+constexpr int kThreadsFor = DIM == 3 ? (256 * LPN < 1024 ? 256 * LPN : 1024) : 256;
 constexpr unsigned kWaitTries = 1u << 22;  // bounded mbarrier wait
 
 // ---- bulk copy + mbarrier (PTX) ----
@@ -240,7 +244,7 @@ __device__ __forceinline__ void tile_nodes(const DevData &d, const BondTile &T, 
   const int shift = sizeof(CT) == 2 ? (int)(M.start - T.win_begin) : (int)(-T.win_begin);
   const bool gauss = d.inf.type == PDGPU_INF_GAUSSIAN;
   // every node of a tile computes forces (tiles cover force-computing particles only)
-  for (int64_t i = T.node_begin + threadIdx.x / LPN; i < T.node_end; i += kThreads / LPN) {
+  for (int64_t i = T.node_begin + threadIdx.x / LPN; i < T.node_end; i += kThreadsFor<DIM, LPN> / LPN) {
     const int k0 = (int)(s_row[i - p.row0] - kb), k1 = (int)(s_row[i + 1 - p.row0] - kb);
     const int li = (int)(i - T.win_begin);
     float xi[3], ui[3], vi;
@@ -276,18 +280,86 @@ __device__ __forceinline__ void tile_nodes(const DevData &d, const BondTile &T, 
   }
 }
 
+// PD state pre-pass, one bond (demModel.cpp:610-679): the extension
+// e = |y| - r (cancellation-free) and, for a bond that is not broken, its
+// term r e J(r) vol_j of the dilatation sum; a bond whose stretch exceeds
+// the critical stretch breaks here (the main loop then sees it broken).
+template <int DIM, bool BROKEN_KNOWN_CLEAR>
+__device__ __forceinline__ void pre_bond(const DevData &d, const MixParticle &M, const View<DIM> &V,
+                                         const float (&xi)[3], const float (&ui)[3], int lj, bool broken,
+                                         bool gauss, int64_t kglob, float &th) {
+  float xj[3], uj[3], volj;
+  V.node(lj, xj, uj, volj);
+  float dx[3], eta[3], y[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    dx[q] = xj[q] - xi[q];
+    eta[q] = uj[q] - ui[q];
+    y[q] = dx[q] + eta[q];
+  }
+  const float r2 = dot<DIM>(dx, dx);
+  const float inv_r = rsqrtf(r2);
+  const float rji = r2 * inv_r;
+  const float y2 = dot<DIM>(y, y);
+  const float l = y2 * rsqrtf(y2);
+  const float cl = __fdividef(2.f * dot<DIM>(dx, eta) + dot<DIM>(eta, eta), l + rji);
+  if (BROKEN_KNOWN_CLEAR || !broken) {
+    if (fabsf(cl * inv_r) > M.s0_thr) {
+      atomicOr(d.bond_bits + (kglob >> 5), 1u << (kglob & 31));
+    } else {
+      const float vol = volj * (rji > M.low_thr ? fmaf(-rji, M.inv_h, M.cu_h) : 1.f);
+      const float J = gauss ? M.j0 * ex2(r2 * M.j1) : fmaf(M.j1, rji, M.j0);
+      th = fmaf(rji * cl, J * vol, th);
+    }
+  }
+}
+
+// the pre-pass over one staged tile: theta_i = 3 sum / m_x,i
+template <int DIM, int LPN, typename CT>
+__device__ __forceinline__ void tile_theta(const DevData &d, const BondTile &T, const MixParticle &M,
+                                           const View<DIM> &V, const CT *s_col, const uint32_t *s_bits,
+                                           const int64_t *s_row, const Plan &p) {
+  const int lane = threadIdx.x % LPN;
+  const unsigned gm = gmask<LPN>();
+  const int64_t kb = T.bond_begin;
+  const int col_off = (int)(kb - p.col0);
+  const int bit_off = (int)(kb - 32 * p.word0);
+  const int shift = sizeof(CT) == 2 ? (int)(M.start - T.win_begin) : (int)(-T.win_begin);
+  const bool gauss = d.inf.type == PDGPU_INF_GAUSSIAN;
+  for (int64_t i = T.node_begin + threadIdx.x / LPN; i < T.node_end; i += kThreadsFor<DIM, LPN> / LPN) {
+    const int k0 = (int)(s_row[i - p.row0] - kb), k1 = (int)(s_row[i + 1 - p.row0] - kb);
+    const int li = (int)(i - T.win_begin);
+    float xi[3], ui[3], vi;
+    V.node(li, xi, ui, vi);
+    float th = 0.f;
+    if (!any_broken<LPN>(s_bits, k0 + bit_off, k1 + bit_off, gm)) {
+#pragma unroll 2
+      for (int k = k0 + lane; k < k1; k += LPN)
+        pre_bond<DIM, true>(d, M, V, xi, ui, (int)s_col[k + col_off] + shift, false, gauss, kb + k, th);
+    } else {
+      for (int k = k0 + lane; k < k1; k += LPN) {
+        const int b = k + bit_off;
+        const bool broken = (s_bits[b >> 5] >> (b & 31)) & 1u;
+        pre_bond<DIM, false>(d, M, V, xi, ui, (int)s_col[k + col_off] + shift, broken, gauss, kb + k, th);
+      }
+    }
+    const double t = gsum<LPN>((double)th, gm);
+    if (lane == 0) d.theta[i] = 3.0 * t / d.mx[i];
+  }
+}
+
 // Persistent: a fixed grid (below full occupancy, so that the contact and
 // damping passes running beside it find room) claims tiles from a counter in
 // the step-control state; the claim for the next tile is made while the
 // current one is staged.  The last CTA out resets the counter.
-template <int DIM, int LPN, int LAW, typename CT>
-__global__ void __launch_bounds__(kThreads) k_bonds_mixed(DevData d, const BondTile *tiles, int n_tiles,
+template <int DIM, int LPN, int LAW, typename CT, bool PRE = false>
+__global__ void __launch_bounds__(kThreadsFor<DIM, LPN>) k_bonds_mixed(DevData d, const BondTile *tiles, int n_tiles,
                                                          const CT *col) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_tile[2];
   if (d.ctrl->error) return;
-  constexpr bool state = LAW == LAW_STATE;
+  constexpr bool state = LAW == LAW_STATE && !PRE;  // the pre-pass needs no m, theta stage
   if (threadIdx.x == 0) {
     bar_init(&bar);
     s_tile[0] = (int)atomicAdd(&d.ctrl->tile_next, 1u);
@@ -336,7 +408,7 @@ __global__ void __launch_bounds__(kThreads) k_bonds_mixed(DevData d, const BondT
       double uc[DIM];
 #pragma unroll
       for (int q = 0; q < DIM; q++) uc[q] = d.u[st * T.center + q];
-      for (int a = threadIdx.x; a < w; a += kThreads) {
+      for (int a = threadIdx.x; a < w; a += kThreadsFor<DIM, LPN>) {
         const int64_t j = T.win_begin + a;
         if constexpr (DIM == 2) {
           const double2 uj = *reinterpret_cast<const double2 *>(d.u + 2 * j);
@@ -365,7 +437,8 @@ __global__ void __launch_bounds__(kThreads) k_bonds_mixed(DevData d, const BondT
     }
 
     View<DIM> V{s_xv, s_u2, s_u4, s_m};
-    tile_nodes<DIM, LPN, LAW, CT>(d, T, M, V, s_col, s_bits, s_row, p);
+    if constexpr (PRE) tile_theta<DIM, LPN, CT>(d, T, M, V, s_col, s_bits, s_row, p);
+    else tile_nodes<DIM, LPN, LAW, CT>(d, T, M, V, s_col, s_bits, s_row, p);
     const int t_next = s_tile[(k + 1) & 1];
     __syncthreads();  // the stage is free for the next tile's copies
     t = t_next;
@@ -382,7 +455,7 @@ __global__ void __launch_bounds__(kThreads) k_bonds_mixed(DevData d, const BondT
 
 // CTAs per SM for the persistent bond loop: one below the occupancy limit
 template <class K>
-int bond_grid(K kernel, size_t smem, int n_tiles) {
+int bond_grid(K kernel, int threads, size_t smem, int n_tiles) {
   static int sms = 0;
   if (!sms) {
     int dev = 0;
@@ -391,27 +464,28 @@ int bond_grid(K kernel, size_t smem, int n_tiles) {
     if (sms <= 0) sms = 148;
   }
   int per = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
   const int g = sms * (per > 1 ? per - 1 : 1);
   return g < n_tiles ? g : n_tiles;
 }
 
-template <int DIM, int LPN, int LAW, typename CT>
+template <int DIM, int LPN, int LAW, typename CT, bool PRE = false>
 void launch_one(const DevData &d, const CT *col, const BondTile *t, int n, size_t smem, cudaStream_t s) {
-  auto *k = k_bonds_mixed<DIM, LPN, LAW, CT>;
-  k<<<bond_grid(k, smem, n), kThreads, smem, s>>>(d, t, n, col);
+  auto *k = k_bonds_mixed<DIM, LPN, LAW, CT, PRE>;
+  constexpr int kT = kThreadsFor<DIM, LPN>;
+  k<<<bond_grid(k, kT, smem, n), kT, smem, s>>>(d, t, n, col);
 }
 
-template <int DIM, int LAW, typename CT>
+template <int DIM, int LAW, typename CT, bool PRE = false>
 void launch_law(const DevData &d, const CT *col, const BondTile *t, int n, int lanes, size_t smem,
                 cudaStream_t s) {
   switch (lanes) {
-    case 1: launch_one<DIM, 1, LAW, CT>(d, col, t, n, smem, s); break;
-    case 2: launch_one<DIM, 2, LAW, CT>(d, col, t, n, smem, s); break;
-    case 4: launch_one<DIM, 4, LAW, CT>(d, col, t, n, smem, s); break;
-    case 8: launch_one<DIM, 8, LAW, CT>(d, col, t, n, smem, s); break;
-    case 16: launch_one<DIM, 16, LAW, CT>(d, col, t, n, smem, s); break;
-    default: launch_one<DIM, 32, LAW, CT>(d, col, t, n, smem, s); break;
+    case 1: launch_one<DIM, 1, LAW, CT, PRE>(d, col, t, n, smem, s); break;
+    case 2: launch_one<DIM, 2, LAW, CT, PRE>(d, col, t, n, smem, s); break;
+    case 4: launch_one<DIM, 4, LAW, CT, PRE>(d, col, t, n, smem, s); break;
+    case 8: launch_one<DIM, 8, LAW, CT, PRE>(d, col, t, n, smem, s); break;
+    case 16: launch_one<DIM, 16, LAW, CT, PRE>(d, col, t, n, smem, s); break;
+    default: launch_one<DIM, 32, LAW, CT, PRE>(d, col, t, n, smem, s); break;
   }
 }
 
@@ -445,11 +519,11 @@ void launch_pre(const DevData &d, const BondTile *t, int n, int lanes, size_t sm
   }
 }
 
-template <int DIM, int LAW, typename CT>
+template <int DIM, int LAW, typename CT, bool PRE = false>
 bool set_law_limit(size_t bytes) {
-  const void *fs[] = {(const void *)k_bonds_mixed<DIM, 1, LAW, CT>, (const void *)k_bonds_mixed<DIM, 2, LAW, CT>,
-                      (const void *)k_bonds_mixed<DIM, 4, LAW, CT>, (const void *)k_bonds_mixed<DIM, 8, LAW, CT>,
-                      (const void *)k_bonds_mixed<DIM, 16, LAW, CT>, (const void *)k_bonds_mixed<DIM, 32, LAW, CT>};
+  const void *fs[] = {(const void *)k_bonds_mixed<DIM, 1, LAW, CT, PRE>, (const void *)k_bonds_mixed<DIM, 2, LAW, CT, PRE>,
+                      (const void *)k_bonds_mixed<DIM, 4, LAW, CT, PRE>, (const void *)k_bonds_mixed<DIM, 8, LAW, CT, PRE>,
+                      (const void *)k_bonds_mixed<DIM, 16, LAW, CT, PRE>, (const void *)k_bonds_mixed<DIM, 32, LAW, CT, PRE>};
   for (auto f : fs)
     if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
       return false;
@@ -468,7 +542,9 @@ int set_limit(size_t bytes) {
   const bool ok = set_law_limit<DIM, LAW_RNP, uint16_t>(bytes) && set_law_limit<DIM, LAW_PMB, uint16_t>(bytes) &&
                   set_law_limit<DIM, LAW_ELASTIC, uint16_t>(bytes) && set_law_limit<DIM, LAW_STATE, uint16_t>(bytes) &&
                   set_law_limit<DIM, LAW_RNP, int32_t>(bytes) && set_law_limit<DIM, LAW_PMB, int32_t>(bytes) &&
-                  set_law_limit<DIM, LAW_ELASTIC, int32_t>(bytes) && set_law_limit<DIM, LAW_STATE, int32_t>(bytes);
+                  set_law_limit<DIM, LAW_ELASTIC, int32_t>(bytes) && set_law_limit<DIM, LAW_STATE, int32_t>(bytes) &&
+                  set_law_limit<DIM, LAW_STATE, uint16_t, true>(bytes) &&
+                  set_law_limit<DIM, LAW_STATE, int32_t, true>(bytes);
   return ok ? 0 : -1;
 }
 
@@ -483,6 +559,23 @@ void launch_pd_tiled_mixed(const DevData &d, const BondTile *t, const int *law_b
   } else {
     if (d.dim == 2) launch_dim<2>(d, (const int32_t *)d.pd_col, t, law_begin, lanes, smem, s);
     else launch_dim<3>(d, (const int32_t *)d.pd_col, t, law_begin, lanes, smem, s);
+  }
+}
+
+// PD state pre-pass over the tiles of state-based particles, persistent like
+// the bond loop
+void launch_prepass_mixed(const DevData &d, const BondTile *t, const int *law_begin, int lanes, size_t smem,
+                          cudaStream_t s) {
+  using namespace mixed_loop;
+  const int b = law_begin[PDGPU_MAT_PDSTATE], n = law_begin[PDGPU_MAT_PDSTATE + 1] - b;
+  if (n <= 0) return;
+  if (d.use16) {
+    if (d.dim == 2) launch_law<2, LAW_STATE, uint16_t, true>(d, d.pd_col16, t + b, n, lanes, smem, s);
+    else launch_law<3, LAW_STATE, uint16_t, true>(d, d.pd_col16, t + b, n, lanes, smem, s);
+  } else {
+    const int32_t *col = (const int32_t *)d.pd_col;
+    if (d.dim == 2) launch_law<2, LAW_STATE, int32_t, true>(d, col, t + b, n, lanes, smem, s);
+    else launch_law<3, LAW_STATE, int32_t, true>(d, col, t + b, n, lanes, smem, s);
   }
 }
 

@@ -308,6 +308,9 @@ void launch_pd_tiled_mixed(const DevData &d, const BondTile *tiles, const int *l
                            size_t smem, cudaStream_t s);
 void launch_prepass_tiled_mixed(const DevData &d, const BondTile *tiles, int n_tiles, int lanes,
                                 size_t smem, cudaStream_t s);
+// persistent PD state pre-pass of the mixed form over the state-based tiles
+void launch_prepass_mixed(const DevData &d, const BondTile *tiles, const int *law_begin, int lanes,
+                          size_t smem, cudaStream_t s);
 size_t tile_smem_fp64(int dim, bool state, int64_t window);
 size_t tile_smem_mixed(int dim, bool state, int64_t window);       // state pre-pass
 size_t tile_smem_mixed_main(int dim, bool state, bool col16, const BondTile &t);

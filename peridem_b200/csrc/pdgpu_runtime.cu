@@ -513,6 +513,7 @@ int prepare_mixed(pdgpu_ctx *ctx) {
         M.G = (float)P.mat[1];
         M.s0 = (float)P.mat[2];
         M.inv_s0 = (float)(1.0 / P.mat[2]);
+        M.s0_thr = (float)((P.mat[2] + 1.0e-10) / rel);  // the pre-pass breaks bonds beyond it
         M.tf_coef = (float)(3.0 * P.mat[0] - 5.0 * P.mat[1]);
         M.am_coef = (float)(15.0 * P.mat[1]);
         break;
@@ -826,7 +827,7 @@ void pd_forces(pdgpu_ctx *ctx) {
   if (ctx->state_prepass) {
     if (mixed)
       run(ctx, "pd_prepass_mixed", [&] {
-        launch_prepass_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
+        launch_prepass_mixed(d, ctx->tiles, ctx->tile_law, ctx->pd_lanes, ctx->tile_smem_pd, s);
       });
     else
       run(ctx, "pd_prepass", [&] {
@@ -961,7 +962,7 @@ cudaError_t graph_step(pdgpu_ctx *ctx, const char **where) {
   }
   // main: bond loop
   if (ctx->state_prepass) {
-    if (mixed) launch_prepass_tiled_mixed(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
+    if (mixed) launch_prepass_mixed(d, ctx->tiles, ctx->tile_law, ctx->pd_lanes, ctx->tile_smem_pd, s);
     else launch_prepass_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
   }
   const size_t smem = ctx->tile_smem_pd;

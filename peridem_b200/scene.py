@@ -516,9 +516,14 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
 def column_3d(n_spheres: int = 4096, median_r: float = 1e-3, sigma: float = 0.2,
               h_div: int = 10, box: Tuple[float, float, float] = (20e-3, 20e-3, 60e-3),
               seed: int = 0, material: str = "PDState", piston_speed: float = -0.05,
-              dt: Optional[float] = None, nt: int = 5000) -> SceneSpec:
+              dt: Optional[float] = None, nt: int = 5000, footprint: Optional[Tuple[int, int]] = None,
+              wall_h: Optional[float] = None, wall_layers: float = 3.0) -> SceneSpec:
     """3-D granular column: spheres with lognormal radii on a jittered cubic
-    lattice inside a fixed box, a piston on top moving at ``piston_speed``."""
+    lattice inside a fixed box, a piston on top moving at ``piston_speed``.
+    The lattice is as wide as ``box`` allows (or ``footprint`` = (nx, ny)
+    sites per layer) and as tall as the spheres need; the box and piston are
+    meshed at ``wall_h`` (default: the smallest sphere's h) with walls
+    ``wall_layers`` mesh sizes thick."""
     rng = np.random.default_rng(seed)
     r_ref = median_r
     h_ref = r_ref / h_div
@@ -530,6 +535,8 @@ def column_3d(n_spheres: int = 4096, median_r: float = 1e-3, sigma: float = 0.2,
     spacing = 2.0 * float(radii.max()) + 2.0 * h_min
     nx = max(1, int(math.floor(box[0] / spacing)))
     ny = max(1, int(math.floor(box[1] / spacing)))
+    if footprint is not None:
+        nx, ny = footprint
     sites = []
     for p in range(n_spheres):
         layer, rem = divmod(p, nx * ny)
@@ -540,15 +547,16 @@ def column_3d(n_spheres: int = 4096, median_r: float = 1e-3, sigma: float = 0.2,
         sites.append(((c[0] + j[0], c[1] + j[1], c[2] + j[2]), float(radii[p]), 0.0))
     height = (int(math.ceil(n_spheres / (nx * ny)))) * spacing
     mat = elastic_material(material, 5.0e9)
-    t = 3.0 * h_min
+    hw = h_min if wall_h is None else wall_h
+    t = wall_layers * hw
     W = (nx * spacing, ny * spacing)
     lo = [-t - h_min, -t - h_min, -t - h_min]
     hi = [W[0] + t + h_min, W[1] + t + h_min, height + 2 * t]
-    box_n, box_v = box_mesh(lo, hi, h_min, 3, hole_lo=[-0.5 * h_min, -0.5 * h_min, -0.5 * h_min],
+    box_n, box_v = box_mesh(lo, hi, hw, 3, hole_lo=[-0.5 * h_min, -0.5 * h_min, -0.5 * h_min],
                             hole_hi=[W[0] + 0.5 * h_min, W[1] + 0.5 * h_min, hi[2] + 1.0])
     pis_n, pis_v = box_mesh([0.5 * h_min, 0.5 * h_min, height], [W[0] - 0.5 * h_min,
                                                                  W[1] - 0.5 * h_min, height + t],
-                            h_min, 3)
+                            hw, 3)
     zones = [ZoneSpec("sphere", False, "sphere", [r_ref, 0.0, 0.0, 0.0], s_n, s_v, mat, sites=sites),
              ZoneSpec("box", True, "cuboid", lo + hi, box_n, box_v, mat, all_dofs_constrained=True),
              ZoneSpec("piston", True, "cuboid",
@@ -618,6 +626,14 @@ def csv_float(text: str) -> float:
     return -x if neg else x
 
 
+def _csv_array(a: np.ndarray) -> np.ndarray:
+    """csv_float(_f(v)) elementwise, evaluated once per distinct value (mesh
+    coordinates repeat along every lattice line)."""
+    a = np.asarray(a, dtype=np.float64)
+    uniq, inv = np.unique(a, return_inverse=True)
+    return np.array([csv_float(_f(v)) for v in uniq])[inv].reshape(a.shape)
+
+
 def _csvv(v: float) -> float:
     return csv_float(_f(v))
 
@@ -628,6 +644,25 @@ def _is_less(a: float, b: float) -> bool:
 
 def _is_greater(a: float, b: float) -> bool:
     return (a - b) > (max(abs(a), abs(b)) * 1.0e-5)
+
+
+def _record_chain(values: np.ndarray, guess: float):
+    """Scan non-negative ``values`` in order, replacing the running guess by
+    every value that is util::isLess than it; returns (index of the last
+    replacement or -1, final guess).  A replacement lies below the guess by
+    more than the relative tolerance, hence below every value skipped since
+    the previous one: it is a strict new running minimum.  So only the
+    positions where the running minimum falls are tested, in order."""
+    values = np.asarray(values, dtype=np.float64)
+    if len(values) == 0:
+        return -1, guess
+    prev = np.concatenate(([np.inf], np.minimum.accumulate(values)[:-1]))
+    idx = -1
+    for k in np.nonzero(values < prev)[0]:
+        v = float(values[k])
+        if (guess - v) > max(abs(v), abs(guess)) * 1.0e-5:
+            guess, idx = v, int(k)
+    return idx, guess
 
 
 def mesh_size(x: np.ndarray) -> float:
@@ -648,24 +683,24 @@ def mesh_size(x: np.ndarray) -> float:
         return mesh_size_scan(x)
     x = np.asarray(x, dtype=np.float64)
     guess = float(np.sqrt(((x[0] - x[1]) ** 2).sum(axis=-1)))
+    # row 0 in full: afterwards the guess is within the tolerance of node 0's
+    # nearest-neighbour distance, which bounds every later replacement
+    d = x[0] - x
+    row0 = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+    row0[0] = np.inf
+    _, guess = _record_chain(row0, guess)
     pairs = cKDTree(x).query_pairs(guess * (1.0 + 1e-9) + 1e-300, output_type="ndarray")
     if len(pairs) == 0:
         return guess
     i = np.concatenate([pairs[:, 0], pairs[:, 1]])
     j = np.concatenate([pairs[:, 1], pairs[:, 0]])
+    keep = i > 0
+    i, j = i[keep], j[keep]
     order = np.lexsort((j, i))
     i, j = i[order], j[order]
     d = x[i] - x[j]
     dist = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
-    start = 0
-    while True:
-        thr = dist[start:]
-        cand = (guess - thr) > (np.maximum(np.abs(thr), abs(guess)) * 1.0e-5)
-        if not cand.any():
-            break
-        k = int(np.argmax(cand)) + start
-        guess = float(dist[k])
-        start = k + 1
+    _, guess = _record_chain(dist, guess)
     return guess
 
 
@@ -849,21 +884,16 @@ def build_scene(spec: SceneSpec):
     # (material.h:273-288); particles are created zone by zone
     for z, zs in enumerate(spec.zones):
         zone_K.append(zs.material.K)
-        node_txt = np.vectorize(lambda v: csv_float(_f(v)))
-        local = node_txt(zs.mesh_nodes) if len(zs.mesh_nodes) else zs.mesh_nodes
+        local = _csv_array(zs.mesh_nodes) if len(zs.mesh_nodes) else zs.mesh_nodes
         local[:, 2] = local[:, 2] if dim == 3 else 0.0
-        lvol = np.array([csv_float(_f(v)) for v in zs.mesh_vol])
+        lvol = _csv_array(zs.mesh_vol)
         # RefParticle centre node: closest to the geometry centre
         # (refParticle.cpp:27-36)
         gc = np.zeros(3) if not zs.is_wall else (
             0.5 * (np.array(zs.geom_params[:3]) + np.array(zs.geom_params[3:6])))
-        best = _bounding_radius(zs.geom_type, zs.geom_params)
-        center = 0
         dd = np.sqrt(((gc - local) ** 2).sum(axis=1))
-        for i in range(len(local)):
-            if _is_less(float(dd[i]), best):
-                best = float(dd[i])
-                center = i
+        center, best = _record_chain(dd, _bounding_radius(zs.geom_type, zs.geom_params))
+        center = max(center, 0)
         if zs.is_wall:
             sites = [(None, None, None)]
         else:
