@@ -267,6 +267,27 @@ PDGPU_API int pdgpu_download(pdgpu_ctx *ctx, int32_t field, void *dst);
  * host-buffer step below and by restarts. */
 PDGPU_API int pdgpu_upload_field(pdgpu_ctx *ctx, int32_t field, const void *src);
 
+/* DEMModel::output (demModel.cpp:1962-2024) with
+ * rw::writer::VtkParticleWriter::appendNodes (vtkParticleWriter.cpp:39-270):
+ * writes the current state to an XML UnstructuredGrid file `path` (.vtu):
+ * the current positions as points (no cells), the model time as the field
+ * array TIME, and one point array per tag named in the comma-separated
+ * `tags` among Displacement, Velocity, Force_Density, Force (f vol), Fixity,
+ * Particle_ID, Zone_ID, Nodal_Volume, Damage_Z, Theta (other tags are
+ * ignored, as in the reference).  Data are appended raw (Float64, UInt64
+ * block headers).  Blocking. */
+PDGPU_API int pdgpu_write_vtu(pdgpu_ctx *ctx, const char *path, const char *tags);
+
+/* DEMModel::restart (demModel.cpp:84-102) with
+ * rw::reader::VtkParticleReader::readNodes (vtkParticleReader.cpp:41-120):
+ * reads the points (current positions), Displacement (else x - x_ref) and
+ * Velocity of a file written by pdgpu_write_vtu, and makes
+ * pdgpu_integrate_begin resume at `step` (time step * dt; no initial
+ * condition; the contact-search counter of the restart step as in
+ * demModel.cpp:1833-1837).  Like the reference, the bond states are not
+ * restored.  Call before pdgpu_integrate_begin. */
+PDGPU_API int pdgpu_restart(pdgpu_ctx *ctx, const char *path, int64_t step);
+
 /* DEMModel::computePeridynamicForces (demModel.cpp:602-789) alone on the
  * current state: the state-based pre-pass and the bond loop write the
  * peridynamic force density f and damage Z and may break bonds; contact,

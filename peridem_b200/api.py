@@ -95,6 +95,8 @@ SIGNATURES = {
                       c_vp, c_vp],
     "pdgpu_build_neighbors_noalloc": [c_vp, c_vp, c_vp, c_i64, c_i32, c_vp, c_vp, c_i64, P(c_i64),
                                       c_vp, ctypes.c_char_p, ctypes.c_size_t],
+    "pdgpu_write_vtu": [c_vp, ctypes.c_char_p, ctypes.c_char_p],
+    "pdgpu_restart": [c_vp, ctypes.c_char_p, c_i64],
     "pdgpu_set_scenes": [c_vp, c_i32, P(c_i64), P(c_i64)],
     "pdgpu_get_scene_history": [c_vp, c_i32, P(c_d), P(c_d), P(c_d), P(c_d), c_i64, P(c_i64)],
     "pdgpu_set_surrogate": [c_vp, c_i32, c_vp, P(c_d), P(c_d), P(c_d), P(c_d), c_i32, c_d, c_d, c_i32],

@@ -247,6 +247,9 @@ struct DevData {
   int32_t use16;
   float inf_p0, inf_p1;
 
+  // the step a restart resumes from (pdgpu_restart), -1 without one
+  int64_t restart_step;
+
   // batched ensemble (pdgpu_set_scenes): independent scenes side by side in
   // one model.  Per scene its node range and test wall; per particle whether
   // it is a scene's test wall; per compacted contact node its term of the

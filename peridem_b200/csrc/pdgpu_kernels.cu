@@ -309,6 +309,8 @@ __device__ __noinline__ void ctrl_step(const DevData &d, int mode) {
       return;
     }
   }
+  // restart: the counter of the restart step (demModel.cpp:1833-1837)
+  if (d.restart_step >= 0 && n == d.restart_step) c.counter = n % c.interval;
   if (c.interval == 1) {
     c.radius = d.max_contact_r;
     c.counter += 1;

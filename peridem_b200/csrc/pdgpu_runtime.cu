@@ -1060,6 +1060,7 @@ int pdgpu_create(const pdgpu_desc *desc, pdgpu_ctx **out) {
   d.dim = desc->dim;
   d.precision = desc->precision;
   d.dt = desc->dt;
+  d.restart_step = -1;
   for (int q = 0; q < 3; q++) d.gravity[q] = desc->gravity[q];
   const double gl = std::sqrt(desc->gravity[0] * desc->gravity[0] + desc->gravity[1] * desc->gravity[1] +
                               desc->gravity[2] * desc->gravity[2]);
@@ -1378,7 +1379,16 @@ int pdgpu_integrate_begin(pdgpu_ctx *ctx) {
   if (ctx->begun) return fail(ctx, PDGPU_ERR_STATE, "integrate_begin called twice");
   DevData &d = ctx->d;
   cudaStream_t s = ctx->stream;
-  if (d.ic_active) run(ctx, "initial_condition", [&] { launch_apply_ic(d, s); });
+  if (d.restart_step > 0) {
+    // DEMModel::restart (demModel.cpp:84-102): step and time of the restart
+    CtrlState c;
+    CK(cudaMemcpy(&c, d.ctrl, sizeof c, cudaMemcpyDeviceToHost));
+    c.n = d.restart_step;
+    c.time = (double)d.restart_step * d.dt;
+    CK(cudaMemcpy(d.ctrl, &c, sizeof c, cudaMemcpyHostToDevice));
+  }
+  // DEMModel::integrate (demModel.cpp:277-283): the initial condition only at step 0
+  if (d.ic_active && d.restart_step <= 0) run(ctx, "initial_condition", [&] { launch_apply_ic(d, s); });
   run(ctx, "displacement_bc", [&] { launch_bc(d, s); });
   run(ctx, "ctrl", [&] { launch_ctrl(d, 1, s); });
   compute_forces(ctx, false);
@@ -1480,6 +1490,219 @@ int pdgpu_download(pdgpu_ctx *ctx, int32_t field, void *dst) {
     CK(cudaMemcpyAsync(dst, ctx->stage, (size_t)3 * N * 8, cudaMemcpyDeviceToHost, s));
   }
   CK(cudaStreamSynchronize(s));
+  return PDGPU_OK;
+}
+
+// ---- VTU output and restart ----
+}  // extern "C"
+
+namespace {
+
+// one appended block: UInt64 byte count, then the bytes
+struct VtuArray {
+  std::string name, type;
+  int comps;
+  std::vector<unsigned char> bytes;
+};
+
+template <typename T>
+VtuArray vtu_array(const std::string &name, const char *type, int comps, const std::vector<T> &v) {
+  VtuArray a{name, type, comps, {}};
+  a.bytes.resize(v.size() * sizeof(T));
+  if (!v.empty()) std::memcpy(a.bytes.data(), v.data(), a.bytes.size());
+  return a;
+}
+
+bool has_tag(const std::string &tags, const char *tag) {
+  size_t b = 0;
+  while (b <= tags.size()) {
+    size_t e = tags.find(',', b);
+    if (e == std::string::npos) e = tags.size();
+    std::string t = tags.substr(b, e - b);
+    while (!t.empty() && t.front() == ' ') t.erase(t.begin());
+    while (!t.empty() && t.back() == ' ') t.pop_back();
+    if (t == tag) return true;
+    b = e + 1;
+  }
+  return false;
+}
+
+std::string xml_attr(const std::string &tag, const char *key) {
+  const std::string k = std::string(key) + "=\"";
+  const size_t p = tag.find(k);
+  if (p == std::string::npos) return "";
+  const size_t q = tag.find('"', p + k.size());
+  return q == std::string::npos ? "" : tag.substr(p + k.size(), q - p - k.size());
+}
+
+}  // namespace
+
+extern "C" {
+
+int pdgpu_write_vtu(pdgpu_ctx *ctx, const char *path, const char *tags) {
+  if (!ctx || !path) return PDGPU_ERR_ARG;
+  if (!ctx->nodes || !ctx->particles) return fail(ctx, PDGPU_ERR_STATE, "write_vtu: no nodes");
+  const std::string T = tags ? tags : "";
+  const int64_t N = ctx->d.n_nodes;
+  std::vector<double> x(3 * N);
+  TRY(pdgpu_download(ctx, PDGPU_FIELD_X, x.data()));
+  std::vector<VtuArray> pdata;
+  auto vec3 = [&](int field, const char *name, bool times_vol) -> int {
+    std::vector<double> v(3 * N);
+    TRY(pdgpu_download(ctx, field, v.data()));
+    if (times_vol) {
+      std::vector<double> vol(N);
+      CK(cudaMemcpy(vol.data(), ctx->d.vol, N * 8, cudaMemcpyDeviceToHost));
+      for (int64_t i = 0; i < N; i++)
+        for (int q = 0; q < 3; q++) v[3 * i + q] *= vol[i];
+    }
+    pdata.push_back(vtu_array(name, "Float64", 3, v));
+    return PDGPU_OK;
+  };
+  // the arrays of VtkParticleWriter::appendNodes (vtkParticleWriter.cpp:39-270), in its order
+  if (has_tag(T, "Displacement")) TRY(vec3(PDGPU_FIELD_U, "Displacement", false));
+  if (has_tag(T, "Velocity")) TRY(vec3(PDGPU_FIELD_V, "Velocity", false));
+  if (has_tag(T, "Force_Density")) TRY(vec3(PDGPU_FIELD_F, "Force_Density", false));
+  if (has_tag(T, "Force")) TRY(vec3(PDGPU_FIELD_F, "Force", true));
+  if (has_tag(T, "Fixity")) {
+    std::vector<double> v(N);
+    for (int64_t i = 0; i < N; i++) v[i] = (double)ctx->fix[i];
+    pdata.push_back(vtu_array("Fixity", "Float64", 1, v));
+  }
+  if (has_tag(T, "Particle_ID")) {
+    std::vector<double> v(N);
+    for (int64_t i = 0; i < N; i++) v[i] = (double)ctx->ptid[i];
+    pdata.push_back(vtu_array("Particle_ID", "Float64", 1, v));
+  }
+  if (has_tag(T, "Zone_ID")) {
+    std::vector<double> v(N);
+    for (int64_t i = 0; i < N; i++) v[i] = (double)ctx->hp[ctx->ptid[i]].zone;
+    pdata.push_back(vtu_array("Zone_ID", "Float64", 1, v));
+  }
+  if (has_tag(T, "Nodal_Volume")) {
+    std::vector<double> v(N);
+    CK(cudaMemcpy(v.data(), ctx->d.vol, N * 8, cudaMemcpyDeviceToHost));
+    pdata.push_back(vtu_array("Nodal_Volume", "Float64", 1, v));
+  }
+  if (has_tag(T, "Damage_Z")) {
+    std::vector<float> z(N);
+    TRY(pdgpu_download(ctx, PDGPU_FIELD_Z, z.data()));
+    pdata.push_back(vtu_array("Damage_Z", "Float64", 1, std::vector<double>(z.begin(), z.end())));
+  }
+  if (has_tag(T, "Theta") && ctx->d.theta) {
+    std::vector<double> v(N);
+    TRY(pdgpu_download(ctx, PDGPU_FIELD_THETA, v.data()));
+    pdata.push_back(vtu_array("Theta", "Float64", 1, v));
+  }
+  pdgpu_scalars sc{};
+  TRY(pdgpu_get_scalars(ctx, &sc));
+  const VtuArray time = vtu_array("TIME", "Float64", 1, std::vector<double>{sc.time});
+  const VtuArray pts = vtu_array("Points", "Float64", 3, x);
+  const VtuArray conn = vtu_array("connectivity", "Int64", 1, std::vector<int64_t>{});
+  const VtuArray offs = vtu_array("offsets", "Int64", 1, std::vector<int64_t>{});
+  const VtuArray types = vtu_array("types", "UInt8", 1, std::vector<uint8_t>{});
+  std::vector<const VtuArray *> order{&time};
+  for (auto &a : pdata) order.push_back(&a);
+  order.push_back(&pts);
+  order.push_back(&conn);
+  order.push_back(&offs);
+  order.push_back(&types);
+  std::vector<uint64_t> off(order.size());
+  uint64_t o = 0;
+  for (size_t k = 0; k < order.size(); k++) {
+    off[k] = o;
+    o += 8 + order[k]->bytes.size();
+  }
+  auto decl = [&](size_t k, int64_t tuples) {
+    const VtuArray &a = *order[k];
+    std::string s = "<DataArray type=\"" + a.type + "\" Name=\"" + a.name + "\"";
+    if (a.comps > 1) {
+      s += " NumberOfComponents=\"" + std::to_string(a.comps) + "\"";
+      if (a.comps == 3) s += " ComponentName0=\"x\" ComponentName1=\"y\" ComponentName2=\"z\"";
+    }
+    if (tuples >= 0) s += " NumberOfTuples=\"" + std::to_string(tuples) + "\"";
+    s += " format=\"appended\" offset=\"" + std::to_string(off[k]) + "\"/>\n";
+    return s;
+  };
+  std::string head = "<?xml version=\"1.0\"?>\n"
+                     "<VTKFile type=\"UnstructuredGrid\" version=\"1.0\" byte_order=\"LittleEndian\" "
+                     "header_type=\"UInt64\">\n<UnstructuredGrid>\n<FieldData>\n";
+  head += decl(0, 1);
+  head += "</FieldData>\n<Piece NumberOfPoints=\"" + std::to_string(N) + "\" NumberOfCells=\"0\">\n<PointData>\n";
+  for (size_t k = 1; k <= pdata.size(); k++) head += decl(k, -1);
+  head += "</PointData>\n<Points>\n" + decl(pdata.size() + 1, -1) + "</Points>\n<Cells>\n";
+  for (size_t k = pdata.size() + 2; k < order.size(); k++) head += decl(k, -1);
+  head += "</Cells>\n</Piece>\n</UnstructuredGrid>\n<AppendedData encoding=\"raw\">\n_";
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return fail(ctx, PDGPU_ERR_ARG, "write_vtu: cannot open %s", path);
+  bool ok = std::fwrite(head.data(), 1, head.size(), f) == head.size();
+  for (auto *a : order) {
+    const uint64_t nb = a->bytes.size();
+    ok = ok && std::fwrite(&nb, 8, 1, f) == 1;
+    if (nb) ok = ok && std::fwrite(a->bytes.data(), 1, nb, f) == nb;
+  }
+  const char *tail = "\n</AppendedData>\n</VTKFile>\n";
+  ok = ok && std::fwrite(tail, 1, std::strlen(tail), f) == std::strlen(tail);
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? PDGPU_OK : fail(ctx, PDGPU_ERR_ARG, "write_vtu: write to %s failed", path);
+}
+
+int pdgpu_restart(pdgpu_ctx *ctx, const char *path, int64_t step) {
+  if (!ctx || !path || step < 0) return PDGPU_ERR_ARG;
+  if (ctx->begun) return fail(ctx, PDGPU_ERR_STATE, "restart before pdgpu_integrate_begin");
+  if (!ctx->nodes) return fail(ctx, PDGPU_ERR_STATE, "restart: upload nodes first");
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(ctx, PDGPU_ERR_ARG, "restart: cannot open %s", path);
+  std::string buf;
+  {
+    std::vector<char> chunk(1 << 20);
+    size_t n;
+    while ((n = std::fread(chunk.data(), 1, chunk.size(), f)) > 0) buf.append(chunk.data(), n);
+    std::fclose(f);
+  }
+  const size_t app = buf.find("<AppendedData encoding=\"raw\">");
+  const size_t base = app == std::string::npos ? std::string::npos : buf.find('_', app);
+  if (base == std::string::npos)
+    return fail(ctx, PDGPU_ERR_ARG, "restart: %s has no raw appended data (files of pdgpu_write_vtu)", path);
+  const int64_t N = ctx->d.n_nodes;
+  const std::string np = xml_attr(buf.substr(0, app), "NumberOfPoints");
+  if (np.empty() || std::stoll(np) != N)
+    return fail(ctx, PDGPU_ERR_ARG, "restart: %s has %s points, the model %lld", path, np.c_str(), (long long)N);
+  // DataArray name -> its block of N x 3 doubles
+  auto block = [&](const char *name, std::vector<double> *out) -> bool {
+    const std::string key = std::string("Name=\"") + name + "\"";
+    size_t p = buf.find(key);
+    if (p == std::string::npos || p > app) return false;
+    const size_t b = buf.rfind('<', p), e = buf.find('>', p);
+    const std::string tag = buf.substr(b, e - b);
+    if (xml_attr(tag, "type") != "Float64" || xml_attr(tag, "NumberOfComponents") != "3") return false;
+    const uint64_t off = std::stoull(xml_attr(tag, "offset"));
+    const size_t at = base + 1 + off;
+    uint64_t nb = 0;
+    if (at + 8 > buf.size()) return false;
+    std::memcpy(&nb, buf.data() + at, 8);
+    if (nb != (uint64_t)N * 24 || at + 8 + nb > buf.size()) return false;
+    out->resize(3 * N);
+    std::memcpy(out->data(), buf.data() + at + 8, nb);
+    return true;
+  };
+  // VtkParticleReader::readNodes (vtkParticleReader.cpp:41-120): current
+  // positions, displacement (else x - x_ref) and velocity (required)
+  std::vector<double> x, u, v;
+  if (!block("Points", &x)) return fail(ctx, PDGPU_ERR_ARG, "restart: no Float64 points in %s", path);
+  if (!block("Velocity", &v)) return fail(ctx, PDGPU_ERR_ARG, "restart: no Velocity array in %s", path);
+  if (!block("Displacement", &u)) {
+    u.resize(3 * N);
+    for (int64_t k = 0; k < 3 * N; k++) u[k] = x[k] - ctx->xref[k];
+  }
+  TRY(pdgpu_upload_field(ctx, PDGPU_FIELD_X, x.data()));
+  TRY(pdgpu_upload_field(ctx, PDGPU_FIELD_U, u.data()));
+  TRY(pdgpu_upload_field(ctx, PDGPU_FIELD_V, v.data()));
+  ctx->d.restart_step = step;
+  if (ctx->gexec) {
+    cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+  }
   return PDGPU_OK;
 }
 

@@ -371,6 +371,15 @@ class GpuDEMModel:
             ptr = a.ctypes.data_as(ctypes.c_void_p)
         self._check(self.lib.pdgpu_upload_field(self.ctx, FIELD[name], ptr))
 
+    def write_vtu(self, path: str, tags=("Displacement", "Velocity", "Force", "Force_Density", "Damage_Z",
+                                         "Particle_ID", "Zone_ID", "Fixity", "Nodal_Volume")) -> None:
+        """DEMModel::output: the current state as a .vtu file (pdgpu_write_vtu)."""
+        self._check(self.lib.pdgpu_write_vtu(self.ctx, path.encode(), ",".join(tags).encode()))
+
+    def restart(self, path: str, step: int) -> None:
+        """DEMModel::restart from a file of write_vtu; before integrate_begin."""
+        self._check(self.lib.pdgpu_restart(self.ctx, path.encode(), int(step)))
+
     def scene_history(self, scene: int) -> np.ndarray:
         """Compressive-test records of one scene of an ensemble: rows of
         (time, wall displacement, reaction, contact reaction)."""
