@@ -32,10 +32,11 @@ using bonds_mixed::gsum;
 using bonds_mixed::gmax;
 
 // threads per CTA: 256 in 2-D; in 3-D, where a tile's neighbour window is
-// large and few CTAs fit an SM, enough lane groups for a 256-node tile in
-// one pass (up to 1024 threads)
+// large (~100 KB of stage) and only two CTAs fit an SM, up to 512, so that
+// two CTAs per SM (one computing while the other waits at a tile barrier)
+// fit the register file
 template <int DIM, int LPN>
-constexpr int kThreadsFor = DIM == 3 ? (256 * LPN < 1024 ? 256 * LPN : 1024) : 256;
+constexpr int kThreadsFor = DIM == 3 ? (256 * LPN < 512 ? 256 * LPN : 512) : 256;
 constexpr unsigned kWaitTries = 1u << 22;  // bounded mbarrier wait
 
 // ---- bulk copy + mbarrier (PTX) ----
@@ -454,6 +455,7 @@ __global__ void __launch_bounds__(kThreadsFor<DIM, LPN>) k_bonds_mixed(DevData d
 }
 
 // CTAs per SM for the persistent bond loop: one below the occupancy limit
+// (the occupancy limit itself when it is two or less)
 template <class K>
 int bond_grid(K kernel, int threads, size_t smem, int n_tiles) {
   static int sms = 0;
@@ -465,7 +467,9 @@ int bond_grid(K kernel, int threads, size_t smem, int n_tiles) {
   }
   int per = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
-  const int g = sms * (per > 1 ? per - 1 : 1);
+  // one slot per SM stays free for the contact and damping passes when at
+  // least three fit; with two, both go to the bond loop
+  const int g = sms * (per > 2 ? per - 1 : (per > 0 ? per : 1));
   return g < n_tiles ? g : n_tiles;
 }
 
