@@ -274,9 +274,11 @@ __device__ __forceinline__ void ctrl_commit(CtrlState *dst, const CtrlState &c) 
   dst->sur_check = c.sur_check;
 }
 
-__device__ __noinline__ void ctrl_step(const DevData &d, int mode) {
+// pre: a copy of the state taken earlier in the same kernel (its fields are
+// written only here), or null to read it now
+__device__ __noinline__ void ctrl_step(const DevData &d, int mode, const CtrlState *pre = nullptr) {
   CtrlState *cp = d.ctrl;
-  CtrlState c = *cp;  // one pass over the state instead of a chain of loads
+  CtrlState c = pre ? *pre : *cp;  // one pass over the state instead of a chain of loads
   if (c.error) return;
   if (mode == 0) {
     c.n += 1;
@@ -433,22 +435,29 @@ template <int DIM, bool VERLET>
 __global__ void __launch_bounds__(kBlock) k_step_begin(const __grid_constant__ DevData d) {
   __shared__ double smax[kBlock / 32];
   __shared__ int last;
+  __shared__ __align__(8) CtrlState s_ctrl;
+  static_assert(sizeof(CtrlState) % 8 == 0 && sizeof(CtrlState) / 8 <= kBlock, "CtrlState copy");
+  // every block copies the step-control state now, while its nodes load: the
+  // last block's step control then starts without a chain of cold loads
+  if (threadIdx.x < sizeof(CtrlState) / 8)
+    reinterpret_cast<uint64_t *>(&s_ctrl)[threadIdx.x] = reinterpret_cast<const uint64_t *>(d.ctrl)[threadIdx.x];
   // CTAs run in reverse node order: the boundary-condition nodes (walls, at
   // the end of the node array) then start in the first wave
   const int64_t i = (int64_t)(gridDim.x - 1 - blockIdx.x) * blockDim.x + threadIdx.x;
   double vm = 0.0;
   if (i < d.n_nodes && !d.ctrl->error) {
+    // every load first (independent of the node's flags), then the update
     const uint8_t fl = d.flags[i];
+    const uint8_t fix = d.fix[i];
+    const int32_t pid = d.ptid[i];
+    double v[3], u[3], x[3], f[3];
+    ldv<DIM>(d.v, i, v);
+    ldv<DIM>(d.u, i, u);
+    ldv<DIM>(d.x, i, x);
+    ldv<DIM>(d.f, i, f);
     if (fl & (NODE_ACTIVE | NODE_UBC)) {
-      double v[3], u[3], x[3];
-      ldv<DIM>(d.v, i, v);
-      ldv<DIM>(d.u, i, u);
-      ldv<DIM>(d.x, i, x);
       if (fl & NODE_ACTIVE) {
-        const double rho = d.particles[d.ptid[i]].density;
-        const uint8_t fix = d.fix[i];
-        double f[3];
-        ldv<DIM>(d.f, i, f);
+        const double rho = d.particles[pid].density;
         const double dt = d.dt;
         const double k = VERLET ? 0.5 * (dt / rho) : dt / rho;
 #pragma unroll
@@ -486,7 +495,7 @@ __global__ void __launch_bounds__(kBlock) k_step_begin(const __grid_constant__ D
   if (last && threadIdx.x == 0) {
     __threadfence();
     d.ctrl->begin_done = 0u;
-    ctrl_step(d, 0);
+    ctrl_step(d, 0, &s_ctrl);
   }
 }
 
@@ -1391,11 +1400,18 @@ template <int DIM, bool VERLET>
 __global__ void __launch_bounds__(kBlock) k_step_end(const __grid_constant__ DevData d, int post) {
   __shared__ int last;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n_step = d.ctrl->n;
   if (i < d.n_nodes && !d.ctrl->error) {
-    double f[3] = {0.0, 0.0, 0.0};
+    // the node's own loads first (independent of its flags), then the sums;
+    // the contact force only where the node searches (elsewhere it is never
+    // written and its lines are cold)
     const uint8_t fl = d.flags[i];
+    const int32_t p = d.ptid[i];
+    double f[3] = {0.0, 0.0, 0.0}, fa[3];
+    ldv<DIM>(d.f, i, fa);
     if (fl & NODE_ACTIVE) {
-      ldv<DIM>(d.f, i, f);
+#pragma unroll
+      for (int q = 0; q < DIM; q++) f[q] = fa[q];
       if (d.fc && (fl & (NODE_SEARCH | NODE_SEARCH0))) {
         double c[3];
         ldv<DIM>(d.fc, i, c);
@@ -1407,7 +1423,6 @@ __global__ void __launch_bounds__(kBlock) k_step_end(const __grid_constant__ Dev
         }
       }
     }
-    const int32_t p = d.ptid[i];
     if (fl & NODE_PARTICLE) {
 #pragma unroll
       for (int q = 0; q < DIM; q++) f[q] += d.fdamp[4 * p + q];
@@ -1432,7 +1447,9 @@ __global__ void __launch_bounds__(kBlock) k_step_end(const __grid_constant__ Dev
       d.vmag[i] = len3<DIM>(v);
     }
   }
+  // the post-processing tail only on the steps that record test output
   if (!post || d.test == PDGPU_TEST_NONE) return;
+  if (!(n_step % d.test_interval == 0 && n_step >= d.test_interval)) return;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
