@@ -14,8 +14,8 @@
 // mbarrier; the accumulator is read back with tcgen05.ld (warp w owns TMEM
 // lanes 32w..32w+31 = rows 32w..32w+31 of the tile).
 //
-// Limits: K a multiple of 16, N a multiple of 16, lda/ldb multiples of 8
-// elements (16-byte rows).  Waits are bounded: on timeout the kernel sets
+// Limits: K a multiple of 16, N a multiple of 16, lda/ldb/ldc multiples of 8
+// elements, A, B, bias and C 16-byte aligned.  Waits are bounded: on timeout the kernel sets
 // *err and returns after a further bounded wait for its own MMAs.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -67,11 +67,13 @@ __device__ __forceinline__ void commit(uint64_t *bar) {
                : "memory");
 }
 
+// non-blocking test of the phase (test_wait, not try_wait: no suspension
+// window between polls)
 __device__ __forceinline__ bool bar_try(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
       : "r"(sa(bar)), "r"(parity)
@@ -83,6 +85,18 @@ __device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t parity) {
   for (unsigned t = 0; t < kTries; t++)
     if (bar_try(bar, parity)) return true;
   return false;
+}
+
+// 8 columns of this warp's 32 TMEM lanes into registers; the caller waits
+// (tcgen05.wait::ld) before reading them
+__device__ __forceinline__ void ld8_nowait(uint32_t taddr, float *v) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(taddr));
+#pragma unroll
+  for (int q = 0; q < 8; q++) v[q] = __uint_as_float(r[q]);
 }
 
 __device__ __forceinline__ void ld8(uint32_t taddr, float (&v)[8]) {
@@ -131,22 +145,45 @@ __device__ __forceinline__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, i
   const uint32_t id = idesc(N);
   bool ok = true;
   uint32_t parity = 0;
+  // stage tiles: every thread issues all its global loads first (fixed trip
+  // counts, so they are in flight together), then writes shared memory; rows
+  // past M / Ntot and columns past K are zero.  The loads of stage s + 1 are
+  // issued right after the MMAs of stage s, so they overlap them.
+  constexpr int k8f = kKc / 8;                // 16-byte vectors per row in a full stage
+  constexpr int kA = kRows * k8f / kThreads;  // per thread
+  constexpr int kB = (N * k8f + kThreads - 1) / kThreads;
+  uint4 ra[kA], rb[kB];
+  auto load_stage = [&](int k0) {
+    const int kc = min(kKc, K - k0);
+#pragma unroll
+    for (int t = 0; t < kA; t++) {
+      const int v = threadIdx.x + t * kThreads;
+      const int r = v / k8f, k8 = v % k8f;
+      ra[t] = make_uint4(0, 0, 0, 0);
+      if (row0 + r < M && 8 * k8 < kc)
+        ra[t] = *reinterpret_cast<const uint4 *>(A + (size_t)(row0 + r) * lda + k0 + 8 * k8);
+    }
+#pragma unroll
+    for (int t = 0; t < kB; t++) {
+      const int v = threadIdx.x + t * kThreads;
+      const int r = v / k8f, k8 = v % k8f;
+      rb[t] = make_uint4(0, 0, 0, 0);
+      if (v < N * k8f && col0 + r < Ntot && 8 * k8 < kc)
+        rb[t] = *reinterpret_cast<const uint4 *>(B + (size_t)(col0 + r) * ldb + k0 + 8 * k8);
+    }
+  };
+  load_stage(0);
   for (int k0 = 0; k0 < K; k0 += kKc) {
     const int kc = min(kKc, K - k0);  // a multiple of 16
-    const int k8n = kc >> 3;          // 16-byte vectors per row in this stage
-    // A tile: 128 rows x kc (rows past M are zero)
-    for (int v = threadIdx.x; v < kRows * k8n; v += kThreads) {
-      const int r = v / k8n, k8 = v % k8n;
-      uint4 val = make_uint4(0, 0, 0, 0);
-      if (row0 + r < M) val = *reinterpret_cast<const uint4 *>(A + (size_t)(row0 + r) * lda + k0 + 8 * k8);
-      *reinterpret_cast<uint4 *>(sA + tile_off(r, k8, kRows)) = val;
+#pragma unroll
+    for (int t = 0; t < kA; t++) {
+      const int v = threadIdx.x + t * kThreads;
+      *reinterpret_cast<uint4 *>(sA + tile_off(v / k8f, v % k8f, kRows)) = ra[t];
     }
-    // B tile: N rows x kc (rows past Ntot are zero)
-    for (int v = threadIdx.x; v < N * k8n; v += kThreads) {
-      const int r = v / k8n, k8 = v % k8n;
-      uint4 val = make_uint4(0, 0, 0, 0);
-      if (col0 + r < Ntot) val = *reinterpret_cast<const uint4 *>(B + (size_t)(col0 + r) * ldb + k0 + 8 * k8);
-      *reinterpret_cast<uint4 *>(sB + tile_off(r, k8, N)) = val;
+#pragma unroll
+    for (int t = 0; t < kB; t++) {
+      const int v = threadIdx.x + t * kThreads;
+      if (v < N * k8f) *reinterpret_cast<uint4 *>(sB + tile_off(v / k8f, v % k8f, N)) = rb[t];
     }
     // generic-proxy writes become visible to the tensor core
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -162,6 +199,7 @@ __device__ __forceinline__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, i
       }
       commit(&bar);
     }
+    if (k0 + kKc < K) load_stage(k0 + kKc);  // in flight during the MMAs
     // the stage is reused only after the MMAs that read it completed
     const bool landed = bar_wait(&bar, parity);
     parity ^= 1u;
@@ -172,20 +210,46 @@ __device__ __forceinline__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, i
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
   if (ok) {
-    // epilogue: warp w reads rows 32w + lane, 8 columns at a time
+    // epilogue: warp w owns rows 32w + lane; 32 columns per TMEM wait; each
+    // thread writes its 8 consecutive columns as one 32-byte sector (FP32)
+    // or 16 bytes (BF16)
     const int r = row0 + warp * 32 + lane;
-    for (int c = 0; c < N; c += 8) {
-      float v[8];
-      ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-      if (r < M) {
+#pragma unroll 1
+    for (int c = 0; c < N; c += 32) {
+      float v[32];
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-          const int col = col0 + c + q;
-          if (col >= Ntot) continue;
-          float x = v[q] + (bias ? bias[col] : 0.f);
-          if (act == 1) x = tanhf(x);
-          if (Cf) Cf[(size_t)r * ldc + col] = x;
-          if (Cb) Cb[(size_t)r * ldc + col] = __float2bfloat16(x);
+      for (int j = 0; j < 4; j++)
+        if (c + 8 * j < N) ld8_nowait(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c + 8 * j), v + 8 * j);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int col = col0 + c + 8 * j;
+        if (c + 8 * j >= N || col >= Ntot || r >= M) continue;
+        float x[8];
+        if (bias) {
+          const float4 b0 = *reinterpret_cast<const float4 *>(bias + col);
+          const float4 b1 = *reinterpret_cast<const float4 *>(bias + col + 4);
+          const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+          for (int q = 0; q < 8; q++) x[q] = v[8 * j + q] + bb[q];
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; q++) x[q] = v[8 * j + q];
+        }
+        if (act == 1) {
+#pragma unroll
+          for (int q = 0; q < 8; q++) x[q] = tanhf(x[q]);
+        }
+        if (Cf) {
+          float4 *o = reinterpret_cast<float4 *>(Cf + (size_t)r * ldc + col);
+          o[0] = make_float4(x[0], x[1], x[2], x[3]);
+          o[1] = make_float4(x[4], x[5], x[6], x[7]);
+        }
+        if (Cb) {
+          __nv_bfloat162 h[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) h[q] = __floats2bfloat162_rn(x[2 * q], x[2 * q + 1]);
+          *reinterpret_cast<uint4 *>(Cb + (size_t)r * ldc + col) = *reinterpret_cast<const uint4 *>(h);
         }
       }
     }
@@ -227,7 +291,9 @@ __global__ void __launch_bounds__(kThreads) k_gemm_grouped(const GemmProblem *__
 int launch_tc_gemm(const void *A, int lda, const void *B, int ldb, int M, int N, int K, const float *bias,
                    int act, float *Cf, void *Cb, int ldc, int *err, cudaStream_t s) {
   using namespace tc;
-  if (M <= 0 || N <= 0 || K <= 0 || K % 16 || N % 16 || lda % 8 || ldb % 8) return (int)cudaErrorInvalidValue;
+  if (M <= 0 || N <= 0 || K <= 0 || K % 16 || N % 16 || lda % 8 || ldb % 8 || ldc % 8) return (int)cudaErrorInvalidValue;
+  auto a16 = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
+  if (!a16(A) || !a16(B) || !a16(bias) || !a16(Cf) || !a16(Cb)) return (int)cudaErrorInvalidValue;
   const auto *a = static_cast<const __nv_bfloat16 *>(A);
   const auto *b = static_cast<const __nv_bfloat16 *>(B);
   auto *cb = static_cast<__nv_bfloat16 *>(Cb);
