@@ -431,6 +431,8 @@ __global__ void k_bc(const __grid_constant__ DevData d) {
 // after k_ctrl: zero-displacement sets are not re-applied), then — in the
 // last CTA to finish — the step control (as k_ctrl, mode 0).
 // ---------------------------------------------------------------------------
+constexpr int kBeginNodes = 2;  // nodes per thread of the step-begin kernel
+
 template <int DIM, bool VERLET>
 __global__ void __launch_bounds__(kBlock) k_step_begin(const __grid_constant__ DevData d) {
   __shared__ double smax[kBlock / 32];
@@ -442,40 +444,63 @@ __global__ void __launch_bounds__(kBlock) k_step_begin(const __grid_constant__ D
   if (threadIdx.x < sizeof(CtrlState) / 8)
     reinterpret_cast<uint64_t *>(&s_ctrl)[threadIdx.x] = reinterpret_cast<const uint64_t *>(d.ctrl)[threadIdx.x];
   // CTAs run in reverse node order: the boundary-condition nodes (walls, at
-  // the end of the node array) then start in the first wave
-  const int64_t i = (int64_t)(gridDim.x - 1 - blockIdx.x) * blockDim.x + threadIdx.x;
+  // the end of the node array) then start in the first wave.  Each thread
+  // takes kBeginNodes nodes, kBlock apart, and issues every load of all of
+  // them before the first update.
+  const int64_t base = (int64_t)(gridDim.x - 1 - blockIdx.x) * (kBlock * kBeginNodes) + threadIdx.x;
   double vm = 0.0;
-  if (i < d.n_nodes && !d.ctrl->error) {
-    // every load first (independent of the node's flags), then the update
-    const uint8_t fl = d.flags[i];
-    const uint8_t fix = d.fix[i];
-    const int32_t pid = d.ptid[i];
-    double v[3], u[3], x[3], f[3];
-    ldv<DIM>(d.v, i, v);
-    ldv<DIM>(d.u, i, u);
-    ldv<DIM>(d.x, i, x);
-    ldv<DIM>(d.f, i, f);
-    if (fl & (NODE_ACTIVE | NODE_UBC)) {
-      if (fl & NODE_ACTIVE) {
-        const double rho = d.particles[pid].density;
+  if (!d.ctrl->error) {
+    uint8_t fl[kBeginNodes], fix[kBeginNodes];
+    int32_t pid[kBeginNodes];
+    double v[kBeginNodes][3], u[kBeginNodes][3], x[kBeginNodes][3], f[kBeginNodes][3];
+#pragma unroll
+    for (int k = 0; k < kBeginNodes; k++) {
+      const int64_t i = base + (int64_t)k * kBlock;
+      fl[k] = 0;
+      if (i < d.n_nodes) {
+        fl[k] = d.flags[i];
+        fix[k] = d.fix[i];
+        pid[k] = d.ptid[i];
+        ldv<DIM>(d.v, i, v[k]);
+        ldv<DIM>(d.u, i, u[k]);
+        ldv<DIM>(d.x, i, x[k]);
+        ldv<DIM>(d.f, i, f[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kBeginNodes; k++) {
+      const int64_t i = base + (int64_t)k * kBlock;
+      if (!(fl[k] & (NODE_ACTIVE | NODE_UBC))) continue;
+      if (fl[k] & NODE_ACTIVE) {
+        const double rho = d.particles[pid[k]].density;
         const double dt = d.dt;
-        const double k = VERLET ? 0.5 * (dt / rho) : dt / rho;
+        const double kk = VERLET ? 0.5 * (dt / rho) : dt / rho;
 #pragma unroll
         for (int dof = 0; dof < DIM; dof++) {
-          if (!((fix >> dof) & 1u)) {
-            v[dof] += k * f[dof];
-            u[dof] += dt * v[dof];
-            x[dof] += dt * v[dof];
+          if (!((fix[k] >> dof) & 1u)) {
+            v[k][dof] += kk * f[k][dof];
+            u[k][dof] += dt * v[k][dof];
+            x[k][dof] += dt * v[k][dof];
           }
         }
-        vm = len3<DIM>(v);
-        d.vmag[i] = vm;
+        const double m = len3<DIM>(v[k]);
+        vm = fmax(vm, m);
+        d.vmag[i] = m;
       }
-      // the step control advances time by dt before the BC pass
-      if (fl & NODE_UBC) apply_ubc<DIM>(d, d.ubc_of[i], i, d.ctrl->time + d.dt, 0, u, v, x);
-      stv<DIM>(d.v, i, v);
-      stv<DIM>(d.u, i, u);
-      stv<DIM>(d.x, i, x);
+      // the step control advances time by dt before the BC pass (through
+      // copies: only they have their address taken, so the per-node arrays
+      // stay in registers)
+      if (fl[k] & NODE_UBC) {
+        double ub[3], vb[3], xb[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) ub[q] = u[k][q], vb[q] = v[k][q], xb[q] = x[k][q];
+        apply_ubc<DIM>(d, d.ubc_of[i], i, d.ctrl->time + d.dt, 0, ub, vb, xb);
+#pragma unroll
+        for (int q = 0; q < 3; q++) u[k][q] = ub[q], v[k][q] = vb[q], x[k][q] = xb[q];
+      }
+      stv<DIM>(d.v, i, v[k]);
+      stv<DIM>(d.u, i, u[k]);
+      stv<DIM>(d.x, i, x[k]);
     }
   }
   // block max of |v| -> one atomic per block
@@ -1433,7 +1458,12 @@ __global__ void __launch_bounds__(kBlock) k_step_end(const __grid_constant__ Dev
 #pragma unroll
       for (int q = 0; q < DIM; q++) f[q] += rho * d.gravity[q];
     }
-    if (fl & NODE_FBC) apply_fbc<DIM>(d, d.fbc_of[i], d.ctrl->time, f);
+    if (fl & NODE_FBC) {  // through a copy, so that f stays in registers
+      double fb[3] = {f[0], f[1], f[2]};
+      apply_fbc<DIM>(d, d.fbc_of[i], d.ctrl->time, fb);
+#pragma unroll
+      for (int q = 0; q < 3; q++) f[q] = fb[q];
+    }
     stv<DIM>(d.f, i, f);
     if (VERLET && (fl & NODE_ACTIVE)) {
       const uint8_t fix = d.fix[i];
@@ -1680,7 +1710,7 @@ void launch_external(const DevData &d, cudaStream_t s) {
 }
 
 void launch_step_begin(const DevData &d, int verlet, cudaStream_t s) {
-  const unsigned g = blocks_for(d.n_nodes, kBlock);
+  const unsigned g = blocks_for(d.n_nodes, kBlock * kBeginNodes);
   if (d.dim == 2) {
     if (verlet) k_step_begin<2, true><<<g, kBlock, 0, s>>>(d);
     else k_step_begin<2, false><<<g, kBlock, 0, s>>>(d);
