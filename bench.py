@@ -451,8 +451,14 @@ def main():
         try:
             r = cpu_reference(args, args.cpu_steps, 1)
             if r is not None:
-                what = ("the ensemble's first scene (%d nodes; the reference runs one scene per process)"
-                        % int(r["nodes"]) if args.workload == "ensemble" else "the same scene")
+                if args.workload == "ensemble":
+                    what = ("the ensemble's first scene (%d nodes; the reference runs one scene per process)"
+                            % int(r["nodes"]))
+                elif args.workload == "column3d":
+                    what = ("an 8-sphere column of the same sphere mesh and material (%d nodes, most of "
+                            "them box walls)" % int(r["nodes"]))
+                else:
+                    what = "the same scene"
                 cpu = {"value": r["node_steps_per_s"], "unit": UNIT, "cores": r["threads"],
                        "kind": "reference",
                        "sample": f"{r['steps']} steps of {what} after one warm-up step "
