@@ -255,8 +255,10 @@ __device__ __forceinline__ void tile_nodes(const DevData &d, const BondTile &T, 
     float F[3] = {0.f, 0.f, 0.f};
     float zmax = 0.f;
     if (!any_broken<LPN>(s_bits, k0 + bit_off, k1 + bit_off, gm)) {
-      // no bond of this node starts broken: no per-bond state test
-#pragma unroll 2
+      // no bond of this node starts broken: no per-bond state test; four
+      // bonds in flight per thread (measured: 17 % faster than two on a
+      // bond loop beyond L2, 9 % on config 1)
+#pragma unroll 4
       for (int k = k0 + lane; k < k1; k += LPN)
         bond<DIM, LAW, true>(d, M, V, xi, ui, mi, (int)s_col[k + col_off] + shift, false, gauss,
                              kb + k, F, zmax);
