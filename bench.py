@@ -44,6 +44,9 @@ def workload_spec(args):
     if args.workload == "column3d":
         # bounded CPU sample: 8 spheres of the same size distribution and mesh
         return scn.column_3d(n_spheres=8, median_r=2e-3, h_div=10, seed=args.seed)
+    if args.workload == "surrogate":
+        return scn.compressive_2d(n_particles=2000, r_range=(1e-3, 1.5e-3), h_div=15, width=80e-3,
+                                  seed=args.seed, material="RNPBond", wall_speed=-0.1, nt=100000)
     return scn.compressive_2d(n_particles=args.particles, r_range=(1e-3, 1.5e-3), h_div=15,
                               width=40e-3, seed=args.seed, material="RNPBond", wall_speed=-0.1,
                               nt=50000)
@@ -53,6 +56,8 @@ def build_workload(args):
     from peridem_b200 import scene as scn
     if args.workload == "ensemble":
         return scn.merge_scenes(scn.build_scenes(scn.ensemble_specs(n_scenes=args.scenes, seed=args.seed)))
+    if args.workload == "surrogate":
+        return scn.build_scene(workload_spec(args))
     if args.workload == "column3d":
         # median radius 2 mm: at 1 mm and h = R/10 the smaller spheres' weighted
         # volume m_x falls under the reference's absolute 1e-18 guard
@@ -70,6 +75,18 @@ def workload_config(args, sc):
                             "RNPBond, top-wall speed U[0.05,0.2] m/s per scene, shared dt" % args.scenes,
                 "scenes": args.scenes,
                 "particles": int(sc.n_particles) if sc is not None else None}
+    elif args.workload == "surrogate":
+        head = {"workload": "surrogate form of the 2-D compressive test scaled to 2000 particles: discs/hexagons "
+                            "R~U[1,1.5] mm, h=R/15, horizon 3h, RNPBond, top wall 0.1 m/s; per shape rank-32 "
+                            "modes, MLP 32-256-256-32 (BF16, FP32 accumulate), full bond-loop check every 50 "
+                            "steps, stretch, error and contact-proximity gates",
+                "particles": 2000}
+    elif args.workload == "surrogate":
+        head = {"workload": "surrogate form of the 2-D compressive test scaled to 2000 particles: discs/hexagons "
+                            "R~U[1,1.5] mm, h=R/15, horizon 3h, RNPBond, top wall 0.1 m/s; per shape rank-32 "
+                            "modes, MLP 32-256-256-32 (BF16, FP32 accumulate), full bond-loop check every 50 "
+                            "steps, stretch, error and contact-proximity gates",
+                "particles": 2000}
     elif args.workload == "column3d":
         force = (int(sum(int(sc.p_end[p] - sc.p_start[p]) for p in range(sc.n_particles) if sc.p_compute_force[p]))
                  if sc is not None else None)
@@ -256,6 +273,21 @@ def run_ours(args, rank, world):
                         pd_lanes=args.pd_lanes, tile_nodes=args.tile_nodes)
     rp, col = model.pd_neighbors()
     sc.pd_rowptr, sc.pd_col = rp, col
+    sur = None
+    if args.workload == "surrogate":
+        # trained beforehand (not timed) on a 64-particle packing of the same
+        # meshes, driven harder so that its trajectory deforms the particles
+        from peridem_b200 import surrogate as sg
+        t0 = time.perf_counter()
+        train = scn.build_scene(scn.compressive_2d(n_particles=64, r_range=(1e-3, 1.5e-3), h_div=15,
+                                                   width=22e-3, seed=args.seed + 1, wall_speed=-1.0,
+                                                   nt=20000))
+        model_s = sg.build(train, steps=12000, every=40, iters=6000, samples_per_particle=400)
+        t_train = time.perf_counter() - t0
+        model_s.attach(model, check_interval=50)
+        sur = {"train_seconds": round(t_train, 1),
+               "shapes": [{"zone": S.zone, "nodes": S.n_nodes,
+                           **{k: round(v, 5) for k, v in S.report.items()}} for S in model_s.shapes]}
     model.integrate_begin()
     stream = torch.cuda.ExternalStream(model.stream_handle(), device=dev)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -310,6 +342,10 @@ def run_ours(args, rank, world):
         model.sync()
     ktimes = model.kernel_times()
     model.enable_timing(False)
+    if sur is not None:
+        on, tot, steps_on, steps_all = model.surrogate_stats()
+        sur.update({"particles_on_now": on, "particles_covered": tot, "particle_steps_on": steps_on,
+                    "particle_steps": steps_all, "fraction_on": round(steps_on / max(steps_all, 1), 4)})
     sc_vals = model.scalars()
 
     # end to end through the host-buffer call: H2D of u, v, x and D2H of
@@ -363,6 +399,7 @@ def run_ours(args, rank, world):
     model.close()
     return {"value": value, "ms_per_step": total_ms / args.steps, "e2e": e2e, "roofline": roof,
             "kernels": kt, "clocks": clk.summary(), "gpu_launches": gpu_launches, "autotune": tuned,
+            "surrogate": sur,
             "scalars": {k: sc_vals[k] for k in ("n", "contact_updates", "contact_entries",
                                                  "contact_update_interval", "broken_bonds",
                                                  "reaction", "contact_reaction")},
@@ -405,9 +442,10 @@ def main():
     ap.add_argument("--pd-lanes", type=int, default=0, help="lanes per node in the bond loop (0 = auto)")
     ap.add_argument("--tile-nodes", type=int, default=0, help="nodes per bond-loop tile (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="compressive", choices=["compressive", "ensemble", "column3d"],
+    ap.add_argument("--workload", default="compressive", choices=["compressive", "ensemble", "column3d", "surrogate"],
                     help="compressive: one 502-particle scene; ensemble: --scenes independent scenes in "
-                         "one model; column3d: --spheres spheres in a 3-D column")
+                         "one model; column3d: --spheres spheres in a 3-D column; surrogate: the learned "
+                         "surrogate on 2000 particles (its training, untimed, took ~40 min at h = R/15)")
     ap.add_argument("--scenes", type=int, default=256)
     ap.add_argument("--spheres", type=int, default=4096)
     ap.add_argument("--autotune", action="store_true",
@@ -478,6 +516,8 @@ def main():
                 "kernels": res["kernels"], "scalars": res["scalars"]}
         if res.get("autotune"):
             line["autotune"] = res["autotune"]
+        if res.get("surrogate"):
+            line["surrogate"] = res["surrogate"]
         print(json.dumps(line))
     if world > 1:
         import torch
