@@ -78,7 +78,6 @@ struct pdgpu_ctx {
   // graph replay
   cudaGraphExec_t gexec = nullptr;
   int graph_steps = 0;
-  cudaStream_t side = nullptr;  // captures the body of the rebuild's conditional node
   // contact and damping run on `branch` beside the bond loop on `stream`
   cudaStream_t branch = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -1087,7 +1086,6 @@ void pdgpu_destroy(pdgpu_ctx *ctx) {
   cudaSetDevice(ctx->desc.device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
-  if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->branch) cudaStreamDestroy(ctx->branch);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
