@@ -1,0 +1,121 @@
+"""Host-side logic without a GPU: the surrogate's body-frame transforms and
+basis completion, the scene builder's sequential record chain, the
+autotuner's search order, and the bench's workload descriptions."""
+import numpy as np
+import pytest
+
+from peridem_b200 import scene as scn
+
+
+def _scene():
+    return scn.build_scene(scn.compressive_2d(n_particles=6, r_range=(1e-3, 1.3e-3), h_div=6, width=8e-3,
+                                              seed=3))
+
+
+def test_body_frame_inverts_placement():
+    from peridem_b200 import surrogate as sg
+    sc = _scene()
+    rng = np.random.default_rng(0)
+    u = np.zeros((sc.n_nodes, 3))
+    rows = {}
+    for p in range(sc.n_particles):
+        if sc.p_type[p] != 0:
+            continue
+        n = int(sc.p_end[p] - sc.p_start[p])
+        rows[p] = rng.standard_normal(2 * n) * 1e-6
+        sg._place(sc, u, p, rows[p])
+    for p, ub in rows.items():
+        # forces: a pure rotation back
+        assert np.allclose(sg.body_frame(sc, u, p, relative=False), ub * sc.p_scale[p], rtol=0, atol=1e-18)
+        # displacements: relative to the centre node, over the scale
+        c = int(sc.p_center[p] - sc.p_start[p])
+        rel = (ub.reshape(-1, 2) - ub.reshape(-1, 2)[c]).reshape(-1)
+        assert np.allclose(sg.body_frame(sc, u, p, relative=True), rel, rtol=0, atol=1e-18)
+
+
+def test_reference_coords_are_the_unrotated_mesh():
+    from peridem_b200 import surrogate as sg
+    sc = _scene()
+    zs = sg.surrogate_zones(sc)
+    assert zs  # discs and hexagons share one mesh each
+    for z in zs:
+        ps = sg._zone_particles(sc, z)
+        X0 = sg.reference_coords(sc, ps[0])
+        for p in ps[1:]:
+            assert np.allclose(sg.reference_coords(sc, p), X0, rtol=0, atol=1e-12)
+
+
+def test_complete_basis_is_orthonormal():
+    from peridem_b200 import surrogate as sg
+    sc = _scene()
+    X = sg.reference_coords(sc, sg._zone_particles(sc, sg.surrogate_zones(sc)[0])[0])
+    rng = np.random.default_rng(1)
+    traj = np.linalg.qr(rng.standard_normal((2 * len(X), 5)))[0]
+    B = sg.complete_basis(traj, X)
+    assert B.shape == (2 * len(X), sg.RANK)
+    assert np.allclose(B.T @ B, np.eye(sg.RANK), atol=1e-10)
+    # the trajectory modes come first and span the same space
+    assert np.allclose(np.abs(np.diag(traj.T @ B[:, :5])), 1.0, atol=1e-10)
+    # constant translations are in the span (lowest-degree polynomials)
+    t = np.tile([1.0, 0.0], len(X))
+    t /= np.linalg.norm(t)
+    assert np.linalg.norm(B @ (B.T @ t) - t) < 1e-10
+
+
+def test_record_chain_matches_a_literal_scan():
+    rng = np.random.default_rng(2)
+
+    def literal(vals, g):
+        idx = -1
+        for k, v in enumerate(vals):
+            if (g - v) > max(abs(v), abs(g)) * 1e-5:
+                g, idx = float(v), k
+        return idx, g
+
+    for t in range(300):
+        n = int(rng.integers(0, 200))
+        if t % 3 == 0:   # near-ties within the tolerance
+            vals = 1.0 + 1e-6 * rng.standard_normal(n)
+        elif t % 3 == 1:  # repeated lattice distances
+            vals = np.repeat(rng.uniform(0, 1, size=n // 4 + 1), 4)[:n]
+        else:
+            vals = np.abs(rng.standard_normal(n))
+        g = float(rng.uniform(0, 2))
+        assert scn._record_chain(vals, g) == literal(vals, g)
+
+
+def test_autotune_descends_then_tries_skins(monkeypatch):
+    from peridem_b200 import autotune as at
+    from peridem_b200.model import PREC_MIXED
+    sc = _scene()
+    sc.search_factor = 5.0
+    cost = {(1, 256, 5.0): 1.0, (4, 128, 5.0): 0.9, (1, 128, 5.0): 1.2, (4, 256, 5.0): 1.1,
+            (4, 128, 2.0): 0.8, (4, 128, 3.0): 0.95}
+    seen = []
+
+    def fake(scene, precision, pd_lanes, tile_nodes, steps, warmup, device=0):
+        key = (pd_lanes, tile_nodes, float(scene.search_factor))
+        seen.append(key)
+        return cost.get(key, 2.0)
+
+    monkeypatch.setattr(at, "time_candidate", fake)
+    ch = at.autotune(sc, PREC_MIXED, lanes=(1, 4), tiles=(128, 256), skins=(2.0, 3.0, 5.0))
+    assert (ch.pd_lanes, ch.tile_nodes, ch.search_factor) == (4, 128, 2.0)
+    assert ch.ms_per_step == pytest.approx(0.8)
+    # lanes x tiles on the scene's own skin first, then the other skins with the best pair
+    assert seen[:4] == [(1, 128, 5.0), (1, 256, 5.0), (4, 128, 5.0), (4, 256, 5.0)]
+    assert seen[4:] == [(4, 128, 2.0), (4, 128, 3.0)]
+    assert sc.search_factor == 5.0  # the caller's scene is not modified
+    assert len(ch.table) == 6
+
+
+@pytest.mark.parametrize("workload", ["compressive", "ensemble", "column3d", "surrogate"])
+def test_bench_describes_every_workload(workload):
+    import argparse
+    import bench
+    args = argparse.Namespace(workload=workload, particles=502, scenes=256, spheres=4096, precision="mixed",
+                              graph_steps=1, pd_lanes=0, tile_nodes=0, seed=0)
+    cfg = bench.workload_config(args, None)
+    assert cfg["workload"] and cfg["precision"] == "mixed" and "l2" in cfg
+    spec = bench.workload_spec(args)
+    assert spec.dim in (2, 3)
