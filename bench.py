@@ -252,6 +252,24 @@ def algorithmic_bytes(kernel, sc, precision):
 
 
 # ---------------------------------------------------------------------------
+def max_over_ranks(x: float, world: int, device: str) -> float:
+    """The largest x over the ranks of the process group (x itself on one
+    rank): a multi-GPU time is the slowest rank's."""
+    if world <= 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(nodes: int, steps: int, world: int, max_ms: float) -> float:
+    """Whole-job node-steps/s of N independent replicas: every rank advances
+    its own scene of `nodes` nodes by `steps` steps; the job takes as long
+    as its slowest rank."""
+    return nodes * steps * world / (max_ms * 1e-3)
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
@@ -325,13 +343,9 @@ def run_ours(args, rank, world):
             model.sync()
             torch.cuda.synchronize()
         step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(sum(step_ms)), world, f"cuda:{dev}")
     nodes = sc.n_nodes
-    value = nodes * args.steps * world / (total_ms * 1e-3)
+    value = job_throughput(nodes, args.steps, world, total_ms)
 
     # per-kernel device times over a second timed pass (same flush)
     model.enable_timing(True)
@@ -362,11 +376,7 @@ def run_ours(args, rank, world):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         model.step_host(u_h, v_h, x_h, f_h, 1)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, f"cuda:{dev}")
     e2e = {"value": nodes * e2e_steps * world / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": 3 * N * 3 * 8, "d2h_bytes_per_step": 4 * N * 3 * 8,
            "call": "pdgpu_step_host (host u,v,x in; u,v,x,f out; 1 step per call)"}
@@ -455,15 +465,15 @@ def main():
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    if world > 1:
+    if args.impl == "reference" and rank != 0:
+        return  # the reference arm runs on rank 0 alone and needs no collective
+    if world > 1 and args.impl != "reference":
         import torch
         import datetime
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     if args.impl == "reference":
-        if rank != 0:
-            return
         t0 = time.perf_counter()
         res = cpu_reference(args, args.steps, args.warmup)
         if res is None:
