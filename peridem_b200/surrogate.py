@@ -185,7 +185,11 @@ def collect_snapshots(sc, steps: int, every: int, fscale: np.ndarray, zones: Lis
     """Run the mixed-precision solver on ``sc`` for ``steps`` steps and, every
     ``every`` steps, record (u_b, f_b) of every particle whose damage is
     below z_max; f is the bond loop's force for that displacement and bond
-    state, evaluated on a probe context."""
+    state, evaluated on a probe context.  The run stops early once a
+    snapshot finds no particle below z_max: nothing later can be recorded,
+    and a packing that far gone (broken bonds pressed together) is usually
+    one whose step has become unstable, with a contact-list rebuild every
+    step."""
     from .model import GpuDEMModel, PREC_MIXED
     run = GpuDEMModel(sc, precision=PREC_MIXED, build_neighbors=True, compute_mx=True)
     probe = _probe(sc)
@@ -203,6 +207,7 @@ def collect_snapshots(sc, steps: int, every: int, fscale: np.ndarray, zones: Lis
             probe.compute_pd_forces()
             f = probe.field("f")
             Z = probe.field("Z")
+            kept = 0
             for z in zones:
                 for p in _zone_particles(sc, z):
                     a, b = int(sc.p_start[p]), int(sc.p_end[p])
@@ -210,6 +215,9 @@ def collect_snapshots(sc, steps: int, every: int, fscale: np.ndarray, zones: Lis
                         continue
                     snap.u[z].append(body_frame(sc, u, p, relative=True))
                     snap.f[z].append(body_frame(sc, f, p, relative=False) / fscale[p])
+                    kept += 1
+            if kept == 0:
+                break
     finally:
         run.close()
         probe.close()

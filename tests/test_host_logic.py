@@ -1,6 +1,7 @@
 """Host-side logic without a GPU: the surrogate's body-frame transforms and
 basis completion, the scene builder's sequential record chain, the
-autotuner's search order, and the bench's workload descriptions."""
+autotuner's search order, the bench's workload descriptions, and the early
+stop of the surrogate's snapshot collection (solver faked)."""
 import numpy as np
 import pytest
 
@@ -119,3 +120,45 @@ def test_bench_describes_every_workload(workload):
     assert cfg["workload"] and cfg["precision"] == "mixed" and "l2" in cfg
     spec = bench.workload_spec(args)
     assert spec.dim in (2, 3)
+
+
+def test_snapshot_collection_stops_when_no_particle_is_below_the_gate(monkeypatch):
+    from peridem_b200 import model as mdl
+    from peridem_b200 import surrogate as sg
+    sc = _scene()
+    zones = sg.surrogate_zones(sc)
+    state = {"n": 0, "steps": []}
+
+    class Fake:
+        def __init__(self, scene, **kw):
+            self.n = scene.n_nodes
+
+        def integrate_begin(self):
+            pass
+
+        def integrate_step(self, k, graph_steps=0):
+            state["n"] += k
+            state["steps"].append(k)
+
+        def field(self, name):
+            if name == "Z":  # every particle past the gate from step 120 on
+                return np.full(self.n, 0.9 if state["n"] >= 120 else 0.1, dtype=np.float32)
+            if name == "bonds":
+                return np.zeros(8, dtype=np.uint8)
+            return np.zeros((self.n, 3))
+
+        def set_field(self, name, values):
+            pass
+
+        def compute_pd_forces(self):
+            pass
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(mdl, "GpuDEMModel", Fake)
+    monkeypatch.setattr(sg, "_probe", lambda s: Fake(s))
+    snap = sg.collect_snapshots(sc, steps=400, every=40, fscale=np.ones(sc.n_particles), zones=zones)
+    assert state["steps"] == [40, 40, 40]  # stopped at the first snapshot with nothing to record
+    for z in zones:
+        assert len(snap.u[z]) == 2 * len(sg._zone_particles(sc, z))
