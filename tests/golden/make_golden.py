@@ -3,7 +3,8 @@ itself: each scene deck is run by oracle/_ref/peridem_ref (the reference's
 own DEMModel compiled from its sources) and the init state plus the states
 after selected steps are stored as compressed npz.
 
-    python tests/golden/make_golden.py        (needs oracle/_ref/peridem_ref)
+    python tests/golden/make_golden.py [name ...]   (needs oracle/_ref/peridem_ref;
+                                                     all cases when no name is given)
 
 ORACLE TEST INFRASTRUCTURE: fixtures pin the oracle restatement; they are
 never inputs of the product path.
@@ -44,13 +45,20 @@ def cases():
     out["cmp6_rnp"] = (scene.compressive_2d(n_particles=6, r_range=(R, 1.2 * R), h_div=4,
                                             width=8e-3, seed=5, gap=1.02 * h, wall_speed=-3.0,
                                             nt=200, search_interval=10), 200, [1, 50, 200])
+    # 3-D: two PD-state spheres in a box under a piston (walls meshed coarser
+    # than the spheres to keep the fixture small)
+    out["col3_state"] = (scene.column_3d(n_spheres=2, median_r=R, sigma=0.0, h_div=4,
+                                         box=(3e-3, 3e-3, 6e-3), seed=1, material="PDState",
+                                         piston_speed=-2.0, nt=150, wall_h=5e-4), 150, [1, 150])
     return out
 
 
-def main():
+def main(only=()):
     if not refrun.have_reference():
         sys.exit("oracle/_ref/peridem_ref is not built (make -C oracle ref)")
     for name, (spec, steps, dsteps) in cases().items():
+        if only and name not in only:
+            continue
         with tempfile.TemporaryDirectory() as d:
             scene.write_deck(spec, d)
             init, dumps = refrun.run_reference(d, steps, dsteps)
@@ -65,4 +73,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -64,7 +64,8 @@ def test_oracle_matches_golden(name):
 
 
 @pytest.mark.skipif(not refrun.have_reference(), reason="reference binary not built")
-@pytest.mark.parametrize("case", ["two_particle_rnp", "two_particle_state", "compressive_small"])
+@pytest.mark.parametrize("case", ["two_particle_rnp", "two_particle_state", "two_particle_verlet",
+                                  "compressive_small", "column_3d_small"])
 def test_oracle_matches_reference_live(case, tmp_path):
     factory, steps, dsteps = scenarios.CASES[case]
     scn.write_deck(factory(), str(tmp_path))
