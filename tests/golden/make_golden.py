@@ -50,6 +50,9 @@ def cases():
     out["col3_state"] = (scene.column_3d(n_spheres=2, median_r=R, sigma=0.0, h_div=4,
                                          box=(3e-3, 3e-3, 6e-3), seed=1, material="PDState",
                                          piston_speed=-2.0, nt=150, wall_h=5e-4), 150, [1, 150])
+    out["col3_rnp"] = (scene.column_3d(n_spheres=2, median_r=R, sigma=0.0, h_div=4,
+                                       box=(3e-3, 3e-3, 6e-3), seed=2, material="RNPBond",
+                                       piston_speed=-2.0, nt=150, wall_h=5e-4), 150, [1, 150])
     return out
 
 
