@@ -50,3 +50,44 @@ def test_struct_layouts_match_header():
     # sizes of the ABI structs as the C compiler lays them out
     assert ctypes.sizeof(api.Particle) == 3 * 8 + 6 * 4 + 6 * 8 + 6 * 8
     assert ctypes.sizeof(api.BcSet) == 4 * 4 + 6 * 8
+
+
+def _null_args(argtypes):
+    out = []
+    for t in argtypes:
+        if t in (ctypes.c_float, ctypes.c_double):
+            out.append(t(0.0))
+        elif t in (ctypes.c_int32, ctypes.c_int64, ctypes.c_uint8, ctypes.c_size_t, ctypes.c_int,
+                   ctypes.c_uint32, ctypes.c_uint64):
+            out.append(t(0))
+        else:  # every pointer: NULL
+            out.append(None)
+    return out
+
+
+@pytest.mark.skipif(not os.path.exists(api.LIB_PATH), reason="libpdgpu.so not built")
+def test_every_entry_point_rejects_null_arguments_before_device_work():
+    """The error behaviour of the interface: a NULL context or NULL buffer is
+    PDGPU_ERR_ARG, returned before any CUDA call (so this runs without a
+    GPU); pdgpu_destroy(NULL) is a no-op."""
+    L = api.lib()
+    skip = {"pdgpu_device_check"}  # reports on the device, takes no pointer it needs
+    for name, argtypes in sorted(api.SIGNATURES.items()):
+        if name in skip:
+            continue
+        rc = getattr(L, name)(*_null_args(argtypes))
+        if name == "pdgpu_destroy":
+            assert rc is None
+        else:
+            assert rc == -1, (name, rc)  # PDGPU_ERR_ARG
+
+
+@pytest.mark.skipif(not os.path.exists(api.LIB_PATH), reason="libpdgpu.so not built")
+def test_device_check_reports_no_device_without_a_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    L = api.lib()
+    buf = ctypes.create_string_buffer(128)
+    assert L.pdgpu_device_check(0, buf, 128) == -7  # PDGPU_ERR_NODEVICE
+    assert buf.value
