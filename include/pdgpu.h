@@ -113,8 +113,11 @@ typedef struct pdgpu_desc {
   double search_factor;    /* PNeighborDeck::d_sFactor */
   int64_t search_interval; /* PNeighborDeck::d_neighUpdateInterval */
   double max_contact_r;    /* ModelData::d_maxContactR (after setupContact) */
-  /* Capacity hints (0 = library default); lists that outgrow them are
-   * regrown by the library between steps. */
+  /* Capacities (0 = library default: 64 candidates per searching node, at
+   * least 2^20 entries; 2048 wall pairs per particle, at most 4096).  A list
+   * that outgrows its capacity is not written past it: the step stops with
+   * PDGPU_ERR_OVERFLOW, and pdgpu_last_error names the size needed; create
+   * the context again with a larger capacity. */
   int64_t contact_capacity;   /* total contact candidate entries */
   int64_t wall_pair_capacity; /* particle-wall node pairs per particle */
 } pdgpu_desc;
