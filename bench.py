@@ -222,9 +222,13 @@ def traffic_from_profiles(kernel):
 
 
 def algorithmic_bytes(kernel, sc, precision):
-    """Bytes one launch must move at minimum (per bond: neighbour index and
-    broken bit; per active node: its own coordinates, displacement, volume,
-    row offset, force and damage; neighbour data are re-read from cache)."""
+    """Bytes one launch must move at minimum, counted independently of the
+    storage layout: per bond a 32-bit neighbour index and the broken bit; per
+    active node its reference coordinates and displacement (FP64, or FP32 in
+    the mixed form), volume, row offset and force (FP64) and damage (FP32);
+    neighbour data are re-read from cache.  The mixed form's own layout moves
+    less (16-bit neighbour columns where a tile's window allows them, FP32
+    node records, FP64 displacement)."""
     import numpy as np
     dim = sc.dim
     active = np.zeros(sc.n_nodes, dtype=bool)
@@ -238,7 +242,7 @@ def algorithmic_bytes(kernel, sc, precision):
     if kernel == "pd_force":
         per_bond, per_node = 4 + 1 / 8, 8 * dim * 3 + 8 + 8 + 4 + (16 if state else 0)
     elif kernel == "pd_force_mixed":
-        per_bond, per_node = 2 + 1 / 8, 4 * dim + 8 * dim + 4 + 8 + 8 * dim + 4 + (16 if state else 0)
+        per_bond, per_node = 4 + 1 / 8, 4 * dim + 4 * dim + 8 + 8 + 8 * dim + 4 + (16 if state else 0)
     else:
         return None, None
     return bonds * per_bond + nodes * per_node, {"bonds": bonds, "nodes": nodes,

@@ -1,7 +1,8 @@
 """Host-side logic without a GPU: the surrogate's body-frame transforms and
 basis completion, the scene builder's sequential record chain, the
-autotuner's search order, the bench's workload descriptions, and the early
-stop of the surrogate's snapshot collection (solver faked)."""
+autotuner's search order, the bench's workload descriptions and its
+layout-independent algorithmic byte count, and the early stop of the
+surrogate's snapshot collection (solver faked)."""
 import numpy as np
 import pytest
 
@@ -162,3 +163,27 @@ def test_snapshot_collection_stops_when_no_particle_is_below_the_gate(monkeypatc
     assert state["steps"] == [40, 40, 40]  # stopped at the first snapshot with nothing to record
     for z in zones:
         assert len(snap.u[z]) == 2 * len(sg._zone_particles(sc, z))
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_bench_algorithmic_bytes_are_layout_independent(dim):
+    """Per bond a 32-bit index and the broken bit; per active node FP64 (or,
+    in the mixed form, FP32) coordinates and displacement, FP64 volume, row
+    offset and force, FP32 damage."""
+    import bench
+
+    class S:
+        pass
+
+    sc = S()
+    sc.dim, sc.n_nodes, sc.n_particles = dim, 5, 2
+    sc.p_compute_force, sc.p_start, sc.p_end = [1, 0], [0, 3], [3, 5]
+    sc.pd_rowptr = np.array([0, 2, 5, 6, 8, 9])
+    sc.p_material = [0, 0]
+    b64, u64 = bench.algorithmic_bytes("pd_force", sc, "fp64")
+    b32, u32 = bench.algorithmic_bytes("pd_force_mixed", sc, "mixed")
+    assert u64["bonds"] == u32["bonds"] == 6 and u64["nodes"] == u32["nodes"] == 3
+    assert u64["bytes_per_bond"] == u32["bytes_per_bond"] == 4.125
+    assert u64["bytes_per_node"] == 8 * dim * 3 + 8 + 8 + 4
+    assert u32["bytes_per_node"] == 4 * dim * 2 + 8 + 8 + 8 * dim + 4
+    assert b32 == 6 * 4.125 + 3 * u32["bytes_per_node"]
