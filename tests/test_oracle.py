@@ -3,7 +3,8 @@
 * golden fixtures produced by the reference itself (tests/golden): the
   oracle starting from the reference's init state must reproduce forces,
   velocities, positions, bond states, damage and the contact-search control
-  BIT FOR BIT (same arithmetic order, same neighbour-list order);
+  BIT FOR BIT (same arithmetic order, same neighbour-list order), and the
+  same contact candidate set per node;
 * when the reference binary is built here, the same check on the parity
   scenarios, run live.
 """
@@ -17,7 +18,17 @@ import scenarios
 from peridem_b200 import scene as scn
 
 
-def _check(tag, o, ref, N, exact=True):
+def _searching_nodes(init):
+    """Nodes whose candidate lists the contact pass reads: those of non-wall,
+    force-computing particles that are not fully constrained."""
+    out = []
+    for p in range(int(init["Np"][0])):
+        if init["p_type"][p] == 0 and init["p_computeForce"][p] and not init["p_allDofsConstrained"][p]:
+            out.extend(range(int(init["p_globStart"][p]), int(init["p_globEnd"][p])))
+    return out
+
+
+def _check(tag, o, ref, N, exact=True, searching=None):
     for k, ok in (("f", "f"), ("v", "v"), ("u", "u"), ("x", "x")):
         a, b = o.field(k), ref[ok].reshape(N, 3)
         if exact:
@@ -26,6 +37,10 @@ def _check(tag, o, ref, N, exact=True):
             assert refrun.rel_err(a, b, 1e-30) < 1e-12, tag
     assert np.array_equal(o.field("bonds"), ref["bond_state"]), f"{tag}: bond states differ"
     assert np.array_equal(o.field("Z"), ref["Z"]), f"{tag}: damage differs"
+    if searching is not None and "c_rowptr" in ref:  # candidate sets the contact pass reads
+        rp, col = o.contact_lists()
+        assert refrun.csr_sets(rp, col, searching) == \
+            refrun.csr_sets(ref["c_rowptr"], ref["c_col"], searching), f"{tag}: contact candidates differ"
     cs = o.contact_state()
     assert cs["interval"] == int(ref["contNeighUpdateInterval"][0]), tag
     assert cs["counter"] == int(ref["contNeighTimestepCounter"][0]), tag
@@ -41,7 +56,8 @@ def test_oracle_matches_golden(name):
     o.integrate_begin()
     # the chaotic fracture case keeps exactness only until contact ordering matters
     exact = True
-    _check(f"{name} n=0", o, init, N, exact)
+    srch = _searching_nodes(init)
+    _check(f"{name} n=0", o, init, N, exact, srch)
     n = 0
     for k in sorted(steps):
         o.step(k - n)
@@ -51,7 +67,7 @@ def test_oracle_matches_golden(name):
             assert np.array_equal(o.field("bonds"), ref["bond_state"]) or \
                 abs(int(o.field("bonds").sum()) - int(ref["bond_state"].sum())) <= 2, name
             continue
-        _check(f"{name} n={k}", o, ref, N, exact)
+        _check(f"{name} n={k}", o, ref, N, exact, srch)
         if int(init["test"][0]) == 2 and k % int(init["dtTestOut"][0]) == 0:
             tv = o.test_values()
             assert tv["reaction"] == float(ref["reaction"][0])
@@ -77,7 +93,7 @@ def test_oracle_matches_reference_live(case, tmp_path):
     for k in sorted(dumps):
         o.step(k - n)
         n = k
-        _check(f"{case} n={k}", o, dumps[k], sc.n_nodes)
+        _check(f"{case} n={k}", o, dumps[k], sc.n_nodes, True, _searching_nodes(init))
     o.close()
 
 
