@@ -288,7 +288,10 @@ PDGPU_API int pdgpu_write_vtu(pdgpu_ctx *ctx, const char *path, const char *tags
  * pdgpu_integrate_begin resume at `step` (time step * dt; no initial
  * condition; the contact-search counter of the restart step as in
  * demModel.cpp:1833-1837).  Like the reference, the bond states are not
- * restored.  Call before pdgpu_integrate_begin. */
+ * restored from the file; a host that keeps them saves them with
+ * pdgpu_download(PDGPU_FIELD_BONDS) and writes them back with
+ * pdgpu_upload_field (or passes them to pdgpu_upload_pd_neighbors) before
+ * pdgpu_integrate_begin.  Call before pdgpu_integrate_begin. */
 PDGPU_API int pdgpu_restart(pdgpu_ctx *ctx, const char *path, int64_t step);
 
 /* DEMModel::computePeridynamicForces (demModel.cpp:602-789) alone on the
