@@ -438,23 +438,34 @@ PDGPU_API int pdgpu_sur_adam(float *p, float *m, float *v, const float *g, int64
 /* Peridynamic neighbour lists built WITHOUT ANY DEVICE ALLOCATION, for
  * callers that cannot call cudaMalloc: a host whose device memory is held by
  * another allocator (a framework's caching allocator that owns the GPU), or
- * code that must not allocate or synchronise the device at that point (a
- * latency-bound loop, or work that another component is capturing).  No
- * counterpart in the reference (its kd-tree search is host code).
+ * a code path where allocation is not allowed.  No counterpart in the
+ * reference (its kd-tree search is host code).
  *
  * Inputs and outputs are caller-owned DEVICE buffers: x (n_nodes*3 doubles,
  * util::Point layout), particle (n_nodes particle ids), horizon (one per
  * particle id); rowptr receives n_nodes+1 offsets and col up to col_capacity
  * neighbour indices.  The sets equal pdgpu_build_pd_neighbors' (same
  * particle, j != i, strict |x_i - x_j|^2 < horizon^2), rows ascending.
- * Pass col = NULL to learn the size in *n_bonds.  Work runs on `stream`
- * (a cudaStream_t, NULL = default stream); the call returns when done.
+ * Pass col = NULL to learn the size in *n_bonds.
  *
- * Limits: n_nodes <= 262144.  Scratch is a 16 MiB static device array
- * that every GPU loading this library keeps until the process exits; the
- * first call on a device looks its address up (make that first call before
- * any stream capture).  All calls share that array, so calls that overlap on
- * the GPU race.  Errors come back as a code and a message in err. */
+ * The call BLOCKS THE HOST: work runs on `stream` (a cudaStream_t, NULL =
+ * the default stream), and the call waits for that stream three times and
+ * returns when the lists are written.  It cannot be captured into a CUDA
+ * graph: it returns PDGPU_ERR_STATE when `stream` is capturing (or, for the
+ * default stream, when another stream captures in global mode); a host with
+ * a capture in progress passes a non-default stream that is not capturing.
+ *
+ * Limits: n_nodes <= 262144; at most 1024 neighbours per node (the size
+ * query already returns PDGPU_ERR_OVERFLOW beyond that); at most 8192 nodes
+ * in one grid cell of the search (cells are about one horizon wide, and
+ * grow coarser when the domain spans more than 2^20 of them; a sparse
+ * domain that crowds more nodes into one cell is refused with
+ * PDGPU_ERR_ARG).  Scratch is a 16 MiB static device array that every GPU
+ * loading this library keeps until the process exits; the first call on a
+ * device looks its address up, and the call must not be used on a device
+ * after cudaDeviceReset in the same process.  All calls share that array,
+ * so calls that overlap on the GPU race.  Errors come back as a code and a
+ * message in err. */
 PDGPU_API int pdgpu_build_neighbors_noalloc(const double *x, const uint32_t *particle,
                                             const double *horizon, int64_t n_nodes, int32_t dim,
                                             uint64_t *rowptr, uint32_t *col, int64_t col_capacity,

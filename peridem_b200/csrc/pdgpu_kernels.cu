@@ -1569,7 +1569,10 @@ __global__ void k_pd_sort_rows(DevData d, int32_t *tmp) {
   }
 }
 
-// material::computeStateMxI (materialUtil.cpp:21-73)
+// material::computeStateMxI (materialUtil.cpp:21-73).  One thread per node
+// sums its row in list order, as the reference does, so that with the
+// reference's own neighbour order the result is the reference's to the bit
+// (FP64, no FMA contraction in this unit).
 template <int DIM, int LPN>
 __global__ void k_mx(DevData d) {
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPN;
@@ -1761,10 +1764,9 @@ void launch_build_pd(const DevData &d, double cell, int64_t *row, int32_t *tmp, 
 }
 
 void launch_compute_mx(const DevData &d, cudaStream_t s) {
-  const int lanes = d.dim == 2 ? 8 : 32;
-  const unsigned g = blocks_for(d.n_nodes * lanes, kBlock);
-  if (d.dim == 2) k_mx<2, 8><<<g, kBlock, 0, s>>>(d);
-  else k_mx<3, 32><<<g, kBlock, 0, s>>>(d);
+  const unsigned g = blocks_for(d.n_nodes, kBlock);
+  if (d.dim == 2) k_mx<2, 1><<<g, kBlock, 0, s>>>(d);
+  else k_mx<3, 1><<<g, kBlock, 0, s>>>(d);
 }
 
 }  // namespace pdgpu

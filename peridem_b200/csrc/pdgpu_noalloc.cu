@@ -5,16 +5,24 @@
 // sorted by node index), for callers that cannot allocate device memory:
 // hosts whose device memory is owned by another allocator (for example a
 // framework's caching allocator that has reserved the GPU), or code paths in
-// which cudaMalloc is not allowed or would stall the device (inside a
-// latency-bound loop, or while another component is capturing work).
+// which cudaMalloc is not allowed.
+//
+// The call blocks the host: it waits for its stream three times (bounding
+// box, grid-cell occupancy, neighbour count) and copies small results to
+// host memory.  It therefore cannot run inside a stream capture; it checks
+// for one on entry and returns PDGPU_ERR_STATE.  A host with a capture in
+// progress on another stream must pass a non-default stream of its own
+// (work on the legacy default stream would break that capture).
 //
 // All scratch lives in one file-scope device array (kScratchBytes, 16 MiB),
 // which every GPU that loads this library keeps until the process exits.
 // Its host-side name is only a stand-in: the device address is fetched once
 // per device with cudaGetSymbolAddress (first call on that device, with it
-// current) and passed to the kernels.  Every call shares the array and
-// overwrites what the last call left there; calls that overlap on the GPU
-// (two streams, or two host threads on one device) race on it.
+// current) and passed to the kernels.  A cudaDeviceReset of that device can
+// move the array, so the call must not be used on a device after it was
+// reset in the same process.  Every call shares the array and overwrites
+// what the last call left there; calls that overlap on the GPU (two streams,
+// or two host threads on one device) race on it.
 //
 // This file is compiled with --fmad=false (the distance test must round like
 // the reference's).
@@ -33,6 +41,7 @@ namespace {
 constexpr int64_t kMaxNodes = int64_t(1) << 18;   // 262 144 nodes
 constexpr int64_t kMaxCells = int64_t(1) << 20;   // 1 048 576 grid cells
 constexpr int kMaxRow = 1024;                     // neighbours of one node
+constexpr int kMaxCellNodes = 8192;               // nodes of one grid cell
 constexpr int kScanBlock = 1024;
 constexpr int64_t kMaxScanBlocks = (kMaxCells + 1 + kScanBlock - 1) / kScanBlock + 1;
 
@@ -45,7 +54,7 @@ constexpr size_t kOffCellStart = kOffCellCnt + 4 * (kMaxCells + 1);
 constexpr size_t kOffCellFill = kOffCellStart + 4 * (kMaxCells + 1);
 constexpr size_t kOffBlock = ((kOffCellFill + 4 * kMaxCells + 255) / 256) * 256;
 constexpr size_t kOffBox = kOffBlock + 8 * kMaxScanBlocks;
-constexpr size_t kOffFlag = kOffBox + 8 * 8;
+constexpr size_t kOffFlag = kOffBox + 8 * 8;     // int32: row overflow, largest cell, largest row
 constexpr size_t kScratchUsed = kOffFlag + 64;
 constexpr size_t kScratchBytes = size_t(16) << 20;
 static_assert(kScratchUsed <= kScratchBytes, "scratch layout exceeds the static array");
@@ -56,7 +65,7 @@ struct Scratch {
   int32_t *cell_of, *cell_tmp, *cell_nodes, *cell_cnt, *cell_start, *cell_fill;
   long long *block_sums;
   unsigned long long *box;  // 3 mins, 3 maxes (order-preserving encodings), horizon max
-  int32_t *flag;            // row-overflow flag
+  int32_t *flag;            // [0] row-overflow flag, [1] largest cell count, [2] largest row
 };
 
 Scratch carve(unsigned char *base) {
@@ -116,7 +125,8 @@ __global__ void k_count_cells(const double *x, int64_t n, int dim, Grid3 g, Scra
   int c = coord(x[3 * i], g, 0) + g.dims[0] * coord(x[3 * i + 1], g, 1);
   if (dim == 3) c += g.dims[0] * g.dims[1] * coord(x[3 * i + 2], g, 2);
   s.cell_of[i] = c;
-  atomicAdd(s.cell_cnt + c, 1);
+  const int had = atomicAdd(s.cell_cnt + c, 1);
+  atomicMax(s.flag + 1, had + 1);
 }
 
 // exclusive scan in three launches; block sums live in the scratch array
@@ -242,7 +252,10 @@ __global__ void k_cand(const double *x, const uint32_t *pt, const double *hz, in
           }
         }
       }
-  if (!FILL && lane == 0) rowptr[i] = (uint64_t)count;
+  if (!FILL && lane == 0) {
+    rowptr[i] = (uint64_t)count;
+    atomicMax(s.flag + 2, (int)(count < 0x7fffffff ? count : 0x7fffffff));
+  }
 }
 
 // order each row by node index inside a per-warp shared-memory slice
@@ -294,6 +307,19 @@ extern "C" PDGPU_API int pdgpu_build_neighbors_noalloc(const double *x, const ui
     return say(err, err_len, PDGPU_ERR_ARG, msg);
   }
   cudaStream_t s = (cudaStream_t)stream;
+  {
+    // the call synchronises its stream, which no capture allows; on the
+    // legacy default stream the query itself fails while another stream
+    // captures in global mode
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const cudaError_t e = cudaStreamIsCapturing(s, &cs);
+    if (e != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      if (e != cudaSuccess) cudaGetLastError();
+      return say(err, err_len, PDGPU_ERR_STATE,
+                 "a stream capture is in progress: this call blocks the host and cannot be captured "
+                 "(pass a non-default stream that is not capturing)");
+    }
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return say(err, err_len, PDGPU_ERR_CUDA, "cudaGetDevice failed");
@@ -355,9 +381,24 @@ extern "C" PDGPU_API int pdgpu_build_neighbors_noalloc(const double *x, const ui
   // cell list
   if ((rc = ck(cudaMemsetAsync(sc.cell_cnt, 0, 4 * (ncells + 1), s), "memset"))) return rc;
   if ((rc = ck(cudaMemsetAsync(sc.cell_fill, 0, 4 * ncells, s), "memset"))) return rc;
-  if ((rc = ck(cudaMemsetAsync(sc.flag, 0, 4, s), "memset"))) return rc;
+  if ((rc = ck(cudaMemsetAsync(sc.flag, 0, 16, s), "memset"))) return rc;
   const unsigned gn = (unsigned)((n_nodes + 255) / 256);
   k_count_cells<<<gn, 256, 0, s>>>(x, n_nodes, dim, g, sc);
+  {
+    // a grid made coarse to fit the scratch array can put most nodes in one
+    // cell; the per-cell sort and the candidate scan are quadratic in a
+    // cell's count, so such inputs are refused before those passes run
+    int32_t big = 0;
+    if ((rc = ck(cudaMemcpyAsync(&big, sc.flag + 1, 4, cudaMemcpyDeviceToHost, s), "cell read")))
+      return rc;
+    if ((rc = ck(cudaStreamSynchronize(s), "cells"))) return rc;
+    if (big > kMaxCellNodes) {
+      snprintf(msg, sizeof msg,
+               "domain too large for the allocation-free grid: one cell holds %d nodes (at most %d)",
+               big, kMaxCellNodes);
+      return say(err, err_len, PDGPU_ERR_ARG, msg);
+    }
+  }
   // cell_start[c] = sum of counts below c; cell_start[ncells] = n_nodes
   const int64_t nb_c = (ncells + kScanBlock - 1) / kScanBlock;
   k_scan_blocks<int32_t><<<(unsigned)nb_c, 256, 0, s>>>(sc.cell_cnt, ncells, sc.block_sums);
@@ -376,10 +417,20 @@ extern "C" PDGPU_API int pdgpu_build_neighbors_noalloc(const double *x, const ui
   k_scan_apply<uint64_t, uint64_t><<<(unsigned)nb_r, kScanBlock, 0, s>>>(rowptr, rowptr, n_nodes,
                                                                         sc.block_sums);
   uint64_t total = 0;
+  int32_t longest = 0;
   if ((rc = ck(cudaMemcpyAsync(&total, rowptr + n_nodes, 8, cudaMemcpyDeviceToHost, s), "count read")))
+    return rc;
+  if ((rc = ck(cudaMemcpyAsync(&longest, sc.flag + 2, 4, cudaMemcpyDeviceToHost, s), "row read")))
     return rc;
   if ((rc = ck(cudaStreamSynchronize(s), "count"))) return rc;
   *n_bonds = (int64_t)total;
+  if (longest > kMaxRow) {
+    // rows are sorted in a per-warp shared-memory slice of kMaxRow entries;
+    // the size query already refuses what the build could not sort
+    snprintf(msg, sizeof msg, "a node has %d neighbours, more than the %d the allocation-free build sorts",
+             longest, kMaxRow);
+    return say(err, err_len, PDGPU_ERR_OVERFLOW, msg);
+  }
   if (!col) return say(err, err_len, PDGPU_OK, "");  // size query
   if ((int64_t)total > col_capacity) {
     snprintf(msg, sizeof msg, "need room for %llu neighbours, col holds %lld",

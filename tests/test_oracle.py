@@ -114,3 +114,17 @@ def test_oracle_weighted_volume_matches_reference(name):
     init, _ = golden_io.load(name)
     sc = refrun.scene_from_dump(init)
     assert np.array_equal(pdoracle.compute_mx(sc), init["mX"])
+
+
+def test_golden_fixtures_hold_what_the_gpu_parity_tests_read():
+    import parity
+    for name in golden_io.names():
+        init, steps = golden_io.load(name)
+        for k in ("pd_rowptr", "pd_col", "mX", "p_boundR", "test", "dtTestOut", "is_multi"):
+            assert k in init, (name, k)
+        for n, st in steps.items():
+            for k in ("f", "u", "v", "x", "Z", "bond_state", "reaction", "pen_dist", "max_y",
+                      "contNeighUpdateInterval", "contNeighTimestepCounter", "contNeighSearchRadius",
+                      "c_rowptr", "c_col"):
+                assert k in st, (name, n, k)
+    assert parity.F_TOL_STEP == 1e-12

@@ -1,7 +1,12 @@
 """pdgpu_build_neighbors_noalloc: the peridynamic neighbour lists built with
-no device allocation, against the allocating build of the same library
-(pdgpu_build_pd_neighbors, whose sets the parity tests tie to the reference's
-kd-tree search).  Both sort each row by node index, so rows must be equal.
+no device allocation, for hosts whose device memory belongs to another
+allocator, against the allocating build of the same library
+(pdgpu_build_pd_neighbors, whose sets tests/test_gpu_setup_parity.py ties to
+the reference's kd-tree search).  Both sort each row by node index, so rows
+must be equal.  Inputs outside the entry point's limits (a sparse domain
+that forces the coarse search grid, a node with more than 1024 neighbours,
+a stream that is capturing) are checked against a brute-force search or
+against the documented error codes.
 
 Device buffers are allocated here by torch; the entry point itself only uses
 the caller's buffers and its static scratch array.  Named so that pytest
@@ -17,7 +22,7 @@ from peridem_b200 import scene as scn
 
 R = 1e-3
 MAX_NODES = 1 << 18
-PDGPU_ERR_ARG, PDGPU_ERR_OVERFLOW = -1, -4   # codes of include/pdgpu.h
+PDGPU_ERR_ARG, PDGPU_ERR_OVERFLOW, PDGPU_ERR_STATE = -1, -4, -6   # codes of include/pdgpu.h
 
 
 def _call(x, pt, hz, n, dim, rowptr, col, cap, stream=None):
@@ -58,6 +63,32 @@ def _noalloc(sc, calls=2):
         out.append((rowptr.cpu().numpy().view(np.uint64).copy(),
                      col.cpu().numpy().view(np.uint32).astype(np.uint64)))
     return out
+
+
+def _device_inputs(x, pt, hz):
+    import torch
+    dev = torch.device("cuda:0")
+    return (torch.as_tensor(np.ascontiguousarray(x, dtype=np.float64), device=dev),
+            torch.as_tensor(np.asarray(pt, dtype=np.int32), device=dev),
+            torch.as_tensor(np.asarray(hz, dtype=np.float64), device=dev))
+
+
+def _brute(x, pt, hz):
+    """Rows of the strict squared-distance search, summed in the kd-tree's
+    order (dims 0, 1, 2 of query minus point), ascending."""
+    n = len(x)
+    rows = []
+    for i in range(n):
+        d = (x[i, 0] - x[:, 0]) * (x[i, 0] - x[:, 0])
+        d = d + (x[i, 1] - x[:, 1]) * (x[i, 1] - x[:, 1])
+        d = d + (x[i, 2] - x[:, 2]) * (x[i, 2] - x[:, 2])
+        r = hz[pt[i]]
+        hit = (d < r * r) & (pt == pt[i])
+        hit[i] = False
+        rows.append(np.nonzero(hit)[0])
+    rp = np.zeros(n + 1, dtype=np.uint64)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    return rp, np.concatenate(rows).astype(np.uint64)
 
 
 def _allocating(sc):
@@ -105,6 +136,76 @@ def test_noalloc_reports_short_column_buffer():
     rc, nb, msg = _call(x.data_ptr(), pt.data_ptr(), hz.data_ptr(), N, sc.dim, rowptr.data_ptr(),
                         col.data_ptr(), 16, None)
     assert rc == PDGPU_ERR_OVERFLOW and nb > 16 and "neighbours" in msg
+
+
+@pytest.mark.gpu
+def test_noalloc_coarse_grid_of_a_sparse_domain_matches_brute_force():
+    """Two clusters 2e4 horizons apart: the horizon-sized grid would need
+    ~4e8 cells, so the build coarsens its cells until they fit the scratch
+    array; the sets must not change."""
+    import torch
+    rng = np.random.default_rng(7)
+    h = 1e-4
+    a = np.stack([rng.uniform(0, 20 * h, 300), rng.uniform(0, 20 * h, 300), np.zeros(300)], 1)
+    b = a + np.array([2e4 * 3 * h, 1e4 * 3 * h, 0.0])
+    x = np.concatenate([a, b])
+    pt = np.repeat(np.arange(2), 300)
+    hz = np.array([3 * h, 3 * h])
+    rp_ref, col_ref = _brute(x, pt, hz)
+    xd, ptd, hzd = _device_inputs(x, pt, hz)
+    N = len(x)
+    rowptr = torch.empty(N + 1, dtype=torch.int64, device=xd.device)
+    rc, nb, msg = _call(xd.data_ptr(), ptd.data_ptr(), hzd.data_ptr(), N, 2, rowptr.data_ptr(), None, 0)
+    assert rc == 0, msg
+    col = torch.full((nb,), -1, dtype=torch.int32, device=xd.device)
+    for k in range(2):
+        rc, nb2, msg = _call(xd.data_ptr(), ptd.data_ptr(), hzd.data_ptr(), N, 2, rowptr.data_ptr(),
+                             col.data_ptr(), nb)
+        assert rc == 0, msg
+        torch.cuda.synchronize()
+        assert np.array_equal(rowptr.cpu().numpy().view(np.uint64), rp_ref), f"rows differ on call {k + 1}"
+        assert np.array_equal(col.cpu().numpy().view(np.uint32).astype(np.uint64), col_ref), \
+            f"columns differ on call {k + 1}"
+
+
+@pytest.mark.gpu
+def test_noalloc_size_query_refuses_rows_longer_than_it_sorts():
+    """A 40 x 40 grid with a horizon of 30 spacings: inner nodes have ~2800
+    neighbours; the size query already reports PDGPU_ERR_OVERFLOW."""
+    import torch
+    h = 1e-4
+    g = np.arange(40) * h
+    X, Y = np.meshgrid(g, g, indexing="ij")
+    x = np.stack([X.ravel(), Y.ravel(), np.zeros(X.size)], 1)
+    pt = np.zeros(len(x), dtype=np.int64)
+    hz = np.array([30 * h])
+    xd, ptd, hzd = _device_inputs(x, pt, hz)
+    rowptr = torch.empty(len(x) + 1, dtype=torch.int64, device=xd.device)
+    rc, nb, msg = _call(xd.data_ptr(), ptd.data_ptr(), hzd.data_ptr(), len(x), 2, rowptr.data_ptr(),
+                        None, 0)
+    assert rc == PDGPU_ERR_OVERFLOW, (rc, msg)
+    assert "1024" in msg
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_a_capturing_stream():
+    """The call blocks the host, so it must refuse to run inside a capture
+    instead of breaking it."""
+    import torch
+    _, sc = next(_scenes())
+    xd, ptd, hzd = _device_inputs(sc.xref, sc.ptid.astype(np.int64), sc.p_horizon)
+    N = sc.n_nodes
+    rowptr = torch.empty(N + 1, dtype=torch.int64, device=xd.device)
+    side = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    scratch = torch.zeros(4, device=xd.device)
+    with torch.cuda.graph(g, stream=side):
+        scratch.add_(1.0)
+        rc, _, msg = _call(xd.data_ptr(), ptd.data_ptr(), hzd.data_ptr(), N, sc.dim, rowptr.data_ptr(),
+                           None, 0, side.cuda_stream)
+    del g
+    assert rc == PDGPU_ERR_STATE, (rc, msg)
+    assert "capture" in msg
 
 
 def test_noalloc_rejects_too_many_nodes_before_touching_the_device():
