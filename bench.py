@@ -50,7 +50,7 @@ def workload_spec(args):
                                   seed=args.seed, material="RNPBond", wall_speed=-0.1, nt=100000)
     return scn.compressive_2d(n_particles=args.particles, r_range=(1e-3, 1.5e-3), h_div=15,
                               width=40e-3, seed=args.seed, material="RNPBond", wall_speed=-0.1,
-                              nt=50000)
+                              nt=50000, packing="deposit")
 
 
 def build_workload(args):
@@ -91,8 +91,10 @@ def workload_config(args, sc):
                 "spheres": args.spheres, "sphere_nodes": force}
     else:
         head = {"workload": "2-D compressive test, %d discs/hexagons R~U[1,1.5] mm, h=R/15, "
-                            "horizon 3h, RNPBond, top wall 0.1 m/s" % args.particles,
-                "particles": args.particles}
+                            "horizon 3h, RNPBond, top wall 0.1 m/s, seeded ballistic-deposition packing; "
+                            "timed from the state after an untimed %d-step pre-run of the compression"
+                            % (args.particles, args.prerun),
+                "particles": args.particles, "prerun_steps": args.prerun}
     return head | {"nodes": int(sc.n_nodes) if sc is not None else None,
                    "dt": sc.dt if sc is not None else None,
                    "precision": args.precision, "l2": "flushed between timed steps (512 MiB write, then read back)",
@@ -269,6 +271,41 @@ def job_throughput(nodes: int, steps: int, world: int, max_ms: float) -> float:
     return nodes * steps * world / (max_ms * 1e-3)
 
 
+def mixed_error(a, b, steps, every):
+    """Error of run a (FP32 bond loop) against run b (plain FP64) over the
+    timed window: relative max-norm error of the compressive-test wall
+    reaction (the reference's Σ_wall f·vol) and of the contact reaction on
+    the wall, over the records of the window's test steps; the broken-bond
+    fraction and the fraction of nodes with damage Z >= 1 at the window's
+    end (absolute differences); relative max-norm error of u at the end."""
+    import numpy as np
+    ha, hb = a["hist"], b["hist"]
+    rows = []
+    for k in range(min(len(ha), len(hb))):
+        if abs(ha[k, 0] - hb[k, 0]) > 1e-12 * max(abs(hb[k, 0]), 1e-30):
+            raise RuntimeError("compressive-test records of the two runs are not aligned")
+        rows.append(k)
+    n0, n1 = steps
+    dt_rows = [k for k in rows if hb[k, 0] > 0]
+    # records are written every `every` steps; the window's are the last ones
+    nwin = max(1, (n1 - n0 + 1) // max(every, 1))
+    win = dt_rows[-nwin:]
+    out = {"records": len(win)}
+    for col, key in ((2, "wall_reaction"), (3, "contact_reaction")):
+        ref = hb[win, col]
+        den = float(np.max(np.abs(ref))) if len(win) else 0.0
+        diff = float(np.max(np.abs(ha[win, col] - ref))) if len(win) else 0.0
+        out[key + "_max_abs"] = den
+        out[key + "_rel_err"] = diff / den if den > 0 else None
+    B = max(len(b["bonds"]), 1)
+    out["broken_fraction"] = float(b["bonds"].sum()) / B
+    out["broken_fraction_abs_err"] = abs(float(a["bonds"].sum()) - float(b["bonds"].sum())) / B
+    out["z_ge_1_fraction_abs_err"] = abs(float(np.mean(a["Z"] >= 1.0)) - float(np.mean(b["Z"] >= 1.0)))
+    ub = np.abs(b["u"]).max()
+    out["u_rel_err"] = float(np.abs(a["u"] - b["u"]).max() / ub) if ub > 0 else None
+    return out
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
@@ -321,35 +358,81 @@ def run_ours(args, rank, world):
         buf.fill_(float(k))
         buf.sum()
 
-    def step():
-        # one step per launch (the L2 flush sits between steps); graph replay
-        # by default, the plain stream path with --graph-steps 0
-        if args.graph_steps:
-            model.integrate_step(args.graph_steps, graph_steps=args.graph_steps)
-        else:
-            model.integrate_step(1)
-
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            step()
-        model.sync()
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
-        with ClockSampler(dev) as clk:
+    def timed_window(m, s):
+        """W untimed steps, then K steps each timed with CUDA events on the
+        model's stream, the L2 flushed before each; per-step ms."""
+        def step():
+            # one step per launch (the L2 flush sits between steps); graph
+            # replay by default, the plain stream path with --graph-steps 0
+            if args.graph_steps:
+                m.integrate_step(args.graph_steps, graph_steps=args.graph_steps)
+            else:
+                m.integrate_step(1)
+        with torch.cuda.stream(s):
+            for _ in range(args.warmup):
+                step()
+            m.sync()
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(args.steps)]
             for k in range(args.steps):
                 flush_l2(flush, k)
-                ev[k][0].record(stream)
+                ev[k][0].record(s)
                 step()
-                ev[k][1].record(stream)
-            model.sync()
+                ev[k][1].record(s)
+            m.sync()
             torch.cuda.synchronize()
-        step_ms = [a.elapsed_time(b) for a, b in ev]
+        return [a.elapsed_time(b) for a, b in ev]
+
+    # untimed pre-run: the wall presses the packing before the timed window
+    snap = None
+    t_pre = time.perf_counter()
+    if args.prerun > 0:
+        with torch.cuda.stream(stream):
+            model.integrate_step(args.prerun, graph_steps=min(args.prerun, 500))
+            model.sync()
+    pre_s = time.perf_counter() - t_pre
+    if args.prerun > 0 and args.workload == "compressive":
+        snap = os.path.join(tempfile.mkdtemp(prefix="pdgpu_bench_"), "prerun.pdsnap")
+        model.save_state(snap)
+    before = model.scalars()
+    with ClockSampler(dev) as clk:
+        step_ms = timed_window(model, stream)
+    after = model.scalars()
+    window = {"steps": [int(before["n"]) + args.warmup + 1, int(after["n"])],
+              "contact_rebuilds": int(after["contact_updates"] - before["contact_updates"]),
+              "contact_entries": int(after["contact_entries"]),
+              "contact_reaction": after["contact_reaction"], "reaction": after["reaction"],
+              "max_velocity": after["max_velocity"], "prerun_seconds": round(pre_s, 2)}
+    mixed_end = None
+    if prec == PREC_MIXED and args.fp64_arm:
+        mixed_end = {"hist": model.history(), "bonds": model.field("bonds"), "Z": model.field("Z"),
+                     "u": model.field("u")}
     total_ms = max_over_ranks(float(sum(step_ms)), world, f"cuda:{dev}")
     nodes = sc.n_nodes
     value = job_throughput(nodes, args.steps, world, total_ms)
+
+    # the plain FP64 form (the drop-in) on the same state and steps: its
+    # throughput, and the FP32 form's error against it over the window
+    fp64 = None
+    if mixed_end is not None:
+        m64 = GpuDEMModel(sc, precision=PREC_FP64, device=dev, build_neighbors=True, compute_mx=True)
+        try:
+            if snap:
+                m64.load_state(snap)
+            else:
+                m64.integrate_begin()
+            s64 = torch.cuda.ExternalStream(m64.stream_handle(), device=dev)
+            ms64 = max_over_ranks(float(sum(timed_window(m64, s64))), world, f"cuda:{dev}")
+            fp64 = {"value": job_throughput(nodes, args.steps, world, ms64), "ms_per_step": ms64 / args.steps}
+            fp64["speedup_of_mixed"] = value / fp64["value"]
+            fp64["error_of_mixed"] = mixed_error(mixed_end, {"hist": m64.history(), "bonds": m64.field("bonds"),
+                                                             "Z": m64.field("Z"), "u": m64.field("u")},
+                                                 window["steps"], sc.test_interval)
+        finally:
+            m64.close()
 
     # per-kernel device times over a second timed pass (same flush)
     model.enable_timing(True)
@@ -413,16 +496,18 @@ def run_ours(args, rank, world):
     model.close()
     return {"value": value, "ms_per_step": total_ms / args.steps, "e2e": e2e, "roofline": roof,
             "kernels": kt, "clocks": clk.summary(), "gpu_launches": gpu_launches, "autotune": tuned,
-            "surrogate": sur,
+            "surrogate": sur, "fp64": fp64, "window": window, "snapshot": snap,
             "scalars": {k: sc_vals[k] for k in ("n", "contact_updates", "contact_entries",
                                                  "contact_update_interval", "broken_bonds",
                                                  "reaction", "contact_reaction")},
             "sc": sc}
 
 
-def cpu_reference(args, steps, warmup):
+def cpu_reference(args, steps, warmup, load=None):
     """The reference's own CPU step (oracle/_ref/peridem_ref, Taskflow on all
-    host threads) on the same workload deck; returns the parsed JSON line."""
+    host threads) on the same workload deck, from the state snapshot `load`
+    when given (the portable part: x, u, v, broken bonds, step, contact
+    control); returns the parsed JSON line."""
     from peridem_b200 import scene as scn
     ref = os.path.join(ROOT, "oracle", "_ref", "peridem_ref")
     if not os.path.exists(ref):
@@ -431,14 +516,45 @@ def cpu_reference(args, steps, warmup):
     threads = os.cpu_count() or 1
     with tempfile.TemporaryDirectory(prefix="peridem_deck_") as d:
         scn.write_deck(spec, d)
-        r = subprocess.run([ref, "-i", "deck.yaml", "-nThreads", str(threads), "-time", str(steps)],
-                           cwd=d, capture_output=True, text=True, timeout=1800)
+        cmd = [ref, "-i", "deck.yaml", "-nThreads", str(threads), "-time", str(steps)]
+        if load:
+            cmd += ["-load", load]
+        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=1800)
     for line in r.stdout.splitlines()[::-1]:
         if line.startswith("{"):
             out = json.loads(line)
             out["threads"] = threads
             return out
     raise RuntimeError("reference timing failed: " + r.stdout[-500:] + r.stderr[-500:])
+
+
+def prerun_snapshot(args):
+    """The state the timed window starts from, for the reference arm: the
+    same untimed pre-run on the GPU (state preparation only; the reference's
+    own code is what is timed), saved as a state snapshot.  Without a GPU,
+    or without a pre-run, the reference starts from the deck's initial
+    state; returns (path or None, description)."""
+    if args.prerun <= 0:
+        return None, "from the deck's initial state"
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None, "from the deck's initial state (no GPU to run the pre-run)"
+        from peridem_b200.model import GpuDEMModel, PREC_MIXED
+        sc = build_workload(args)
+        m = GpuDEMModel(sc, precision=PREC_MIXED, build_neighbors=True, compute_mx=True)
+        try:
+            m.integrate_begin()
+            m.integrate_step(args.prerun, graph_steps=min(args.prerun, 500))
+            m.sync()
+            path = os.path.join(tempfile.mkdtemp(prefix="pdgpu_bench_"), "prerun.pdsnap")
+            m.save_state(path)
+        finally:
+            m.close()
+        return path, ("from the state after the %d-step pre-run of the compression (made on the GPU, "
+                      "loaded by peridem_ref -load)" % args.prerun)
+    except Exception as e:  # report, do not hide
+        return None, f"from the deck's initial state (pre-run failed: {e})"
 
 
 def main():
@@ -464,7 +580,14 @@ def main():
     ap.add_argument("--autotune", action="store_true",
                     help="choose lanes, tile size and search skin by timing the scene first")
     ap.add_argument("--tune-steps", type=int, default=100)
+    ap.add_argument("--prerun", type=int, default=20000,
+                    help="untimed steps of the compression before the timed window (compressive "
+                         "workload); the state they reach is what every arm times")
+    ap.add_argument("--no-fp64", dest="fp64_arm", action="store_false",
+                    help="skip the plain FP64 form on the same state (and the mixed form's error)")
     args = ap.parse_args()
+    if args.workload != "compressive":
+        args.prerun = 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -478,10 +601,14 @@ def main():
 
     if args.impl == "reference":
         t0 = time.perf_counter()
-        res = cpu_reference(args, args.steps, args.warmup)
+        snap, how = prerun_snapshot(args)
+        res = cpu_reference(args, args.steps, args.warmup, load=snap)
         if res is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference binary oracle/_ref/peridem_ref not built"}))
             return
+        if snap:
+            import shutil
+            shutil.rmtree(os.path.dirname(snap), ignore_errors=True)
         v = res["node_steps_per_s"]
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup,
@@ -490,7 +617,7 @@ def main():
                 "config": workload_config(args, None) | {"nodes": int(res["nodes"])},
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": res["threads"], "kind": "reference",
                                  "sample": f"{res['steps']} steps of the full scene after one warm-up step "
-                                           f"(init {res['init_seconds']:.1f} s excluded)"},
+                                           f"(init {res['init_seconds']:.1f} s excluded), {how}"},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "wall_s": time.perf_counter() - t0}
         print(json.dumps(line))
@@ -500,7 +627,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            r = cpu_reference(args, args.cpu_steps, 1)
+            r = cpu_reference(args, args.cpu_steps, 1, load=res.get("snapshot"))
             if r is not None:
                 if args.workload == "ensemble":
                     what = ("the ensemble's first scene (%d nodes; the reference runs one scene per process)"
@@ -508,6 +635,9 @@ def main():
                 elif args.workload == "column3d":
                     what = ("an 8-sphere column of the same sphere mesh and material (%d nodes, most of "
                             "them box walls)" % int(r["nodes"]))
+                elif res.get("snapshot"):
+                    what = ("the same scene from the GPU's state after the %d-step pre-run (x, u, v, broken "
+                            "bonds, step and contact control loaded by peridem_ref -load)" % args.prerun)
                 else:
                     what = "the same scene"
                 cpu = {"value": r["node_steps_per_s"], "unit": UNIT, "cores": r["threads"],
@@ -517,6 +647,9 @@ def main():
         except Exception as e:  # report, do not hide
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {e}"}
+    if res.get("snapshot"):
+        import shutil
+        shutil.rmtree(os.path.dirname(res["snapshot"]), ignore_errors=True)
     if rank == 0:
         sc = res.pop("sc")
         line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
@@ -526,7 +659,13 @@ def main():
                 "data": "synthetic", "config": workload_config(args, sc),
                 "e2e": res["e2e"], "roofline": res["roofline"], "cpu_baseline": cpu,
                 "clocks": res["clocks"], "gpu_launches": res["gpu_launches"],
-                "kernels": res["kernels"], "scalars": res["scalars"]}
+                "kernels": res["kernels"], "scalars": res["scalars"], "window": res["window"]}
+        if res.get("fp64"):
+            f64 = res["fp64"]
+            line["fp64_value"] = f64["value"]
+            line["fp64_ms_per_step"] = f64["ms_per_step"]
+            line["speedup_vs_fp64"] = f64["speedup_of_mixed"]
+            line["error_vs_fp64"] = f64["error_of_mixed"]
         if res.get("autotune"):
             line["autotune"] = res["autotune"]
         if res.get("surrogate"):

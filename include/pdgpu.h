@@ -294,6 +294,28 @@ PDGPU_API int pdgpu_write_vtu(pdgpu_ctx *ctx, const char *path, const char *tags
  * pdgpu_integrate_begin.  Call before pdgpu_integrate_begin. */
 PDGPU_API int pdgpu_restart(pdgpu_ctx *ctx, const char *path, int64_t step);
 
+/* State snapshot: a restart that keeps everything (no counterpart in the
+ * reference, whose DEMModel::restart, demModel.cpp:84-102, restores positions
+ * and velocities only and resets every bond to intact).
+ *
+ * pdgpu_save_state writes, between steps (after pdgpu_integrate_begin),
+ * everything a step reads that earlier steps wrote: x, u, v, f, Z, |v|,
+ * dilatation, the bond-broken bits, the step and time, the contact-search
+ * control, the contact candidate lists and particle-wall damping pairs of
+ * the last rebuild, the compressive-test history and the learned
+ * surrogate's per-particle flags.  Blocking.  The file starts with a
+ * portable part that any host can read without this library: a fixed
+ * header (step, time, contact-search interval, counter, radius, max
+ * velocity), x, u, v as util::Point arrays, and the broken bonds as (i, j)
+ * node pairs, independent of neighbour-list order.
+ *
+ * pdgpu_load_state takes the place of pdgpu_integrate_begin on a context
+ * with the same scene uploaded (same nodes, bonds, particles, contact
+ * capacities; either precision): the context continues exactly as the saved
+ * one would have.  A file of another scene is refused with PDGPU_ERR_ARG. */
+PDGPU_API int pdgpu_save_state(pdgpu_ctx *ctx, const char *path);
+PDGPU_API int pdgpu_load_state(pdgpu_ctx *ctx, const char *path);
+
 /* DEMModel::computePeridynamicForces (demModel.cpp:602-789) alone on the
  * current state: the state-based pre-pass and the bond loop write the
  * peridynamic force density f and damage Z and may break bonds; contact,

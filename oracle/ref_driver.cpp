@@ -15,6 +15,12 @@
 //   -steps K       number of integrateStep() calls (default: the deck's Nt).
 //   -time K        time K steady-state steps (after one warm-up step) and print
 //                  one JSON line with node-steps/s.
+//   -load FILE     before the first step, put the model into the state of a
+//                  pdgpu state snapshot (its portable part: step, time,
+//                  contact-search interval and radius, x, u, v and the broken
+//                  bonds as node pairs); the contact lists are rebuilt at the
+//                  first contact update.  Used to time the reference from the
+//                  same loaded state as the GPU.
 //
 // The step loop below follows model::DEMModel::integrate
 // (src/model/dem/demModel.cpp:268-340): applyInitialCondition,
@@ -383,6 +389,60 @@ public:
     d.s("max_y", d_dbgData.count("max_y") ? getKeyData("max_y") : 0.);
   }
 
+  // the portable part of a pdgpu state snapshot (SnapHeader of the
+  // library's pdgpu_runtime.cu, then x, u, v and broken (i, j) pairs)
+  void loadState(const std::string &path) {
+    struct Head {
+      char magic[8];
+      int64_t dim, n_nodes, n_bonds, n_particles, stride, n_broken, n_words, entries, wp_cap, history,
+          n_scenes, scene_hist_cap, surrogate, multi_particle, step;
+      double time;
+      int64_t contact_interval, contact_counter;
+      double contact_radius, max_velocity;
+      int64_t ctrl_bytes;
+    } h{};
+    std::ifstream f(path, std::ios::binary);
+    if (!f.read((char *)&h, sizeof h) || std::memcmp(h.magic, "PDSNAP01", 8) != 0) {
+      std::cerr << "peridem_ref: " << path << " is not a state snapshot\n";
+      std::exit(2);
+    }
+    const size_t N = d_x.size();
+    if ((size_t)h.n_nodes != N) {
+      std::cerr << "peridem_ref: snapshot has " << h.n_nodes << " nodes, the deck " << N << "\n";
+      std::exit(2);
+    }
+    std::vector<double> a(3 * N);
+    for (auto *dst : {&d_x, &d_u, &d_v}) {
+      f.read((char *)a.data(), (std::streamsize)(a.size() * 8));
+      for (size_t i = 0; i < N; i++) (*dst)[i] = util::Point(a[3 * i], a[3 * i + 1], a[3 * i + 2]);
+    }
+    std::vector<uint64_t> pr(2 * (size_t)h.n_broken);
+    f.read((char *)pr.data(), (std::streamsize)(pr.size() * 8));
+    if (!f) {
+      std::cerr << "peridem_ref: " << path << " is truncated\n";
+      std::exit(2);
+    }
+    for (size_t k = 0; k < (size_t)h.n_broken; k++) {
+      const size_t i = pr[2 * k], j = pr[2 * k + 1];
+      const auto &nb = d_neighPd[i];
+      auto it = std::find(nb.begin(), nb.end(), j);
+      if (it == nb.end()) {
+        std::cerr << "peridem_ref: snapshot bond (" << i << ", " << j << ") is not a bond of the deck\n";
+        std::exit(2);
+      }
+      d_fracture_p->setBondState(i, (size_t)(it - nb.begin()), true);
+    }
+    for (size_t i = 0; i < N; i++) d_vMag[i] = d_v[i].length();
+    d_n = (size_t)h.step;
+    d_time = h.time;
+    d_contNeighUpdateInterval = (size_t)h.contact_interval;
+    d_contNeighSearchRadius = h.contact_radius;
+    d_maxVelocity = h.max_velocity;
+    // counter 0: the next contact update step rebuilds the lists from the
+    // loaded positions (demModel.cpp:1808-1955)
+    d_contNeighTimestepCounter = 0;
+  }
+
   // post-processing exactly as the reference's integrate() loop does it
   void postStep() {
     if (d_pDeck_p->d_testName == "two_particle")
@@ -404,7 +464,7 @@ std::vector<long> parseList(const std::string &s) {
 }  // namespace
 
 int main(int argc, char **argv) {
-  std::string deck_file, dump_dir, dump_steps;
+  std::string deck_file, dump_dir, dump_steps, load_file;
   long steps = -1, time_steps = 0;
   unsigned threads = 1;
   for (int a = 1; a < argc; a++) {
@@ -422,6 +482,7 @@ int main(int argc, char **argv) {
     else if (k == "-steps") steps = std::stol(next());
     else if (k == "-dumpSteps") dump_steps = next();
     else if (k == "-time") time_steps = std::stol(next());
+    else if (k == "-load") load_file = next();
     else {
       std::cerr << "peridem_ref: unknown option " << k << "\n";
       return 2;
@@ -429,7 +490,7 @@ int main(int argc, char **argv) {
   }
   if (deck_file.empty()) {
     std::cerr << "usage: peridem_ref -i deck.yaml [-nThreads T] [-dump DIR] [-steps K] "
-                 "[-dumpSteps a,b] [-time K]\n";
+                 "[-dumpSteps a,b] [-time K] [-load FILE]\n";
     return 2;
   }
 
@@ -440,6 +501,7 @@ int main(int argc, char **argv) {
   auto t0 = std::chrono::steady_clock::now();
   dem->init();
   auto t1 = std::chrono::steady_clock::now();
+  if (!load_file.empty()) dem->loadState(load_file);
 
   // the first part of DEMModel::integrate()
   if (dem->d_n == 0) dem->applyInitialCondition();

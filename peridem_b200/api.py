@@ -65,6 +65,8 @@ SIGNATURES = {
     "pdgpu_set_influence": [c_vp, c_i32, P(c_d)],
     "pdgpu_upload_contact": [c_vp, c_i32, P(c_d), P(c_d), P(c_d), P(c_d), P(c_d)],
     "pdgpu_upload_pd_neighbors": [c_vp, P(c_u64), P(c_u64), P(c_u8)],
+    "pdgpu_save_state": [c_vp, ctypes.c_char_p],
+    "pdgpu_load_state": [c_vp, ctypes.c_char_p],
     "pdgpu_build_pd_neighbors": [c_vp],
     "pdgpu_upload_mx": [c_vp, P(c_d)],
     "pdgpu_compute_mx": [c_vp],

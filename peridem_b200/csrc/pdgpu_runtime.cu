@@ -2088,3 +2088,278 @@ int pdgpu_kernel_times(pdgpu_ctx *ctx, int32_t maxk, const char **names, double 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// State snapshot (no counterpart in the reference, whose restart
+// demModel.cpp:84-102 reads positions and velocities back and resets every
+// bond to intact).  A snapshot taken between steps holds everything a step
+// reads that earlier steps wrote, so a context loaded from it continues
+// exactly as the saved one would have: x, u, v, f, damage, |v|, dilatation,
+// the bond-broken bits, the step-control state (step, time, contact-search
+// counters, post-processing results), the contact candidate lists and the
+// particle-wall damping pairs of the last rebuild, the compressive-test
+// history, and the learned surrogate's per-particle flags.
+//
+// File layout (little-endian):
+//   SnapHeader
+//   portable part, for any loader (util::Point layout):
+//     x, u, v      [N][3] double each
+//     broken bonds [n_broken][2] uint64 (i, j): pairs, so the bond order of
+//                  the loader's own neighbour lists does not matter
+//   device part (this library's layout; same scene and capacities):
+//     x, u, v, f   [N][stride] double; Z [N] float; vmag, theta [N] double
+//     bond bits    [n_words] uint32
+//     CtrlState
+//     contact: row [N+1] int64, count [N] int64, nodes [N] int32,
+//              spans [N] int2, columns [entries] int32,
+//              wall pairs [Np][wp_cap] int32, wall pair counts [Np] int32
+//     history [hist][4] double; scene history [n_scenes][cap][4] double
+//     surrogate flags: on [Np] uint8, near [Np] uint8 (when set)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct SnapHeader {
+  char magic[8];        // "PDSNAP01"
+  int64_t dim, n_nodes, n_bonds, n_particles;
+  int64_t stride;       // doubles per node vector on the device (2 or 4)
+  int64_t n_broken;     // pairs in the portable part
+  int64_t n_words;      // bond-bit words in the device part
+  int64_t entries;      // contact candidate entries
+  int64_t wp_cap;       // particle-wall pair capacity per particle
+  int64_t history;      // compressive-test records
+  int64_t n_scenes, scene_hist_cap;
+  int64_t surrogate;    // 1: surrogate flags follow
+  int64_t multi_particle;
+  // the step, and the contact-search state a loader of the portable part
+  // needs (ModelData::d_n, d_time, d_contNeighUpdateInterval,
+  // d_contNeighTimestepCounter, d_contNeighSearchRadius, d_maxVelocity)
+  int64_t step;
+  double time;
+  int64_t contact_interval, contact_counter;
+  double contact_radius, max_velocity;
+  int64_t ctrl_bytes;   // sizeof(CtrlState) of the writer
+};
+
+template <typename T>
+int dl(pdgpu_ctx *ctx, std::vector<T> *h, const T *d, size_t n) {
+  h->resize(n);
+  if (n) CK(cudaMemcpyAsync(h->data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  return PDGPU_OK;
+}
+
+template <typename T>
+int ul(pdgpu_ctx *ctx, T *d, const std::vector<T> &h) {
+  if (!h.empty()) CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  return PDGPU_OK;
+}
+
+template <typename T>
+bool wr(FILE *f, const std::vector<T> &v) {
+  return v.empty() || std::fwrite(v.data(), sizeof(T), v.size(), f) == v.size();
+}
+
+template <typename T>
+bool rd(FILE *f, std::vector<T> *v, size_t n) {
+  v->resize(n);
+  return n == 0 || std::fread(v->data(), sizeof(T), n, f) == n;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pdgpu_save_state(pdgpu_ctx *ctx, const char *path) {
+  if (!ctx || !path) return PDGPU_ERR_ARG;
+  if (!ctx->begun) return fail(ctx, PDGPU_ERR_STATE, "save_state: call pdgpu_integrate_begin first");
+  TRY(device_error(ctx));
+  DevData &d = ctx->d;
+  const int64_t N = d.n_nodes, B = d.n_bonds, st = d.dim == 2 ? 2 : 4;
+  const int64_t Np = (int64_t)ctx->hp.size(), nw = (B + 31) / 32;
+  const bool multi = ctx->desc.multi_particle != 0;
+  CtrlState c;
+  TRY(read_ctrl(ctx, &c));
+  // portable part
+  std::vector<double> xa(3 * N), ua(3 * N), va(3 * N);
+  TRY(pdgpu_download(ctx, PDGPU_FIELD_X, xa.data()));
+  TRY(pdgpu_download(ctx, PDGPU_FIELD_U, ua.data()));
+  TRY(pdgpu_download(ctx, PDGPU_FIELD_V, va.data()));
+  std::vector<uint32_t> bits;
+  std::vector<int64_t> prow;
+  std::vector<int32_t> pcol;
+  TRY(dl(ctx, &bits, d.bond_bits, (size_t)nw));
+  TRY(dl(ctx, &prow, d.pd_row, (size_t)N + 1));
+  TRY(dl(ctx, &pcol, d.pd_col, (size_t)B));
+  // device part
+  std::vector<double> x, u, v, f, vmag, theta;
+  std::vector<float> Z;
+  TRY(dl(ctx, &x, d.x, (size_t)(st * N)));
+  TRY(dl(ctx, &u, d.u, (size_t)(st * N)));
+  TRY(dl(ctx, &v, d.v, (size_t)(st * N)));
+  TRY(dl(ctx, &f, d.f, (size_t)(st * N)));
+  TRY(dl(ctx, &Z, d.Z, (size_t)N));
+  TRY(dl(ctx, &vmag, d.vmag, (size_t)N));
+  TRY(dl(ctx, &theta, d.theta, (size_t)N));
+  std::vector<int64_t> crow, ccnt;
+  std::vector<int32_t> cnodes, cspan, ccol, wp, wpc;
+  if (multi) {
+    TRY(dl(ctx, &crow, d.c_row, (size_t)N + 1));
+    TRY(dl(ctx, &ccnt, d.c_cnt, (size_t)N));
+    TRY(dl(ctx, &cnodes, d.c_nodes, (size_t)N));
+    TRY(dl(ctx, &cspan, reinterpret_cast<const int32_t *>(d.c_span), (size_t)(2 * N)));
+    TRY(dl(ctx, &wp, d.wp, (size_t)(Np * d.wp_cap)));
+    TRY(dl(ctx, &wpc, d.wp_cnt, (size_t)Np));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (multi) TRY(dl(ctx, &ccol, d.c_col, (size_t)crow[N]));
+  const int64_t nh = std::min<int64_t>(c.history_count, d.history_cap);
+  std::vector<double> hist, shist;
+  TRY(dl(ctx, &hist, d.history, (size_t)(4 * std::max<int64_t>(nh, 0))));
+  if (d.n_scenes > 1) TRY(dl(ctx, &shist, d.scene_hist, (size_t)(d.n_scenes * d.scene_hist_cap * 4)));
+  std::vector<uint8_t> son, snear;
+  if (d.sur_on) {
+    TRY(dl(ctx, &son, d.sur_on, (size_t)Np));
+    TRY(dl(ctx, &snear, d.sur_near, (size_t)Np));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<uint64_t> pairs;
+  for (int64_t i = 0; i < N; i++)
+    for (int64_t k = prow[i]; k < prow[i + 1]; k++)
+      if ((bits[k >> 5] >> (k & 31)) & 1u) {
+        pairs.push_back((uint64_t)i);
+        pairs.push_back((uint64_t)pcol[k]);
+      }
+  SnapHeader h{};
+  std::memcpy(h.magic, "PDSNAP01", 8);
+  h.dim = d.dim;
+  h.n_nodes = N;
+  h.n_bonds = B;
+  h.n_particles = Np;
+  h.stride = st;
+  h.n_broken = (int64_t)pairs.size() / 2;
+  h.n_words = nw;
+  h.entries = multi ? crow[N] : 0;
+  h.wp_cap = multi ? d.wp_cap : 0;
+  h.history = std::max<int64_t>(nh, 0);
+  h.n_scenes = d.n_scenes;
+  h.scene_hist_cap = d.n_scenes > 1 ? d.scene_hist_cap : 0;
+  h.surrogate = d.sur_on ? 1 : 0;
+  h.multi_particle = multi ? 1 : 0;
+  h.step = c.n;
+  h.time = c.time;
+  h.contact_interval = c.interval;
+  h.contact_counter = c.counter;
+  h.contact_radius = c.radius;
+  h.max_velocity = c.max_velocity;
+  h.ctrl_bytes = (int64_t)sizeof(CtrlState);
+  FILE *fo = std::fopen(path, "wb");
+  if (!fo) return fail(ctx, PDGPU_ERR_ARG, "save_state: cannot write %s", path);
+  bool ok = std::fwrite(&h, sizeof h, 1, fo) == 1 && wr(fo, xa) && wr(fo, ua) && wr(fo, va) && wr(fo, pairs) &&
+            wr(fo, x) && wr(fo, u) && wr(fo, v) && wr(fo, f) && wr(fo, Z) && wr(fo, vmag) && wr(fo, theta) &&
+            wr(fo, bits) && std::fwrite(&c, sizeof c, 1, fo) == 1;
+  if (ok && multi) ok = wr(fo, crow) && wr(fo, ccnt) && wr(fo, cnodes) && wr(fo, cspan) && wr(fo, ccol) &&
+                        wr(fo, wp) && wr(fo, wpc);
+  if (ok) ok = wr(fo, hist) && wr(fo, shist) && wr(fo, son) && wr(fo, snear);
+  ok = (std::fclose(fo) == 0) && ok;
+  if (!ok) return fail(ctx, PDGPU_ERR_ARG, "save_state: writing %s failed", path);
+  return PDGPU_OK;
+}
+
+int pdgpu_load_state(pdgpu_ctx *ctx, const char *path) {
+  if (!ctx || !path) return PDGPU_ERR_ARG;
+  if (ctx->begun)
+    return fail(ctx, PDGPU_ERR_STATE, "load_state takes the place of pdgpu_integrate_begin: the model has started");
+  TRY(prepare(ctx));
+  const bool multi = ctx->desc.multi_particle != 0;
+  if (multi && !ctx->contact_init) TRY(pdgpu_init_contact(ctx));
+  DevData &d = ctx->d;
+  const int64_t N = d.n_nodes, B = d.n_bonds, st = d.dim == 2 ? 2 : 4;
+  const int64_t Np = (int64_t)ctx->hp.size(), nw = (B + 31) / 32;
+  FILE *fi = std::fopen(path, "rb");
+  if (!fi) return fail(ctx, PDGPU_ERR_ARG, "load_state: cannot open %s", path);
+  SnapHeader h{};
+  bool ok = std::fread(&h, sizeof h, 1, fi) == 1 && std::memcmp(h.magic, "PDSNAP01", 8) == 0;
+  if (!ok) {
+    std::fclose(fi);
+    return fail(ctx, PDGPU_ERR_ARG, "load_state: %s is not a pdgpu state snapshot", path);
+  }
+  const char *why = nullptr;
+  if (h.dim != d.dim || h.n_nodes != N || h.n_bonds != B || h.n_particles != Np || h.stride != st)
+    why = "it holds another scene (dimension, nodes, bonds or particles differ)";
+  else if (h.n_words != nw || h.ctrl_bytes != (int64_t)sizeof(CtrlState))
+    why = "it was written by an incompatible library";
+  else if (h.multi_particle != (multi ? 1 : 0))
+    why = "contact is on in one model and off in the other";
+  else if (multi && (h.entries > d.contact_cap || h.wp_cap != d.wp_cap))
+    why = "its contact lists do not fit this model's capacities";
+  else if (h.n_scenes != d.n_scenes || (d.n_scenes > 1 && h.scene_hist_cap != d.scene_hist_cap))
+    why = "its scene layout differs";
+  if (why) {
+    std::fclose(fi);
+    return fail(ctx, PDGPU_ERR_ARG, "load_state: %s: %s", path, why);
+  }
+  std::vector<double> skip, x, u, v, f, vmag, theta, hist, shist;
+  std::vector<uint64_t> pairs;
+  std::vector<float> Z;
+  std::vector<uint32_t> bits;
+  std::vector<int64_t> crow, ccnt;
+  std::vector<int32_t> cnodes, cspan, ccol, wp, wpc;
+  std::vector<uint8_t> son, snear;
+  CtrlState c;
+  ok = rd(fi, &skip, (size_t)(9 * N)) && rd(fi, &pairs, (size_t)(2 * h.n_broken)) &&
+       rd(fi, &x, (size_t)(st * N)) && rd(fi, &u, (size_t)(st * N)) && rd(fi, &v, (size_t)(st * N)) &&
+       rd(fi, &f, (size_t)(st * N)) && rd(fi, &Z, (size_t)N) && rd(fi, &vmag, (size_t)N) &&
+       rd(fi, &theta, (size_t)N) && rd(fi, &bits, (size_t)nw) && std::fread(&c, sizeof c, 1, fi) == 1;
+  if (ok && multi)
+    ok = rd(fi, &crow, (size_t)N + 1) && rd(fi, &ccnt, (size_t)N) && rd(fi, &cnodes, (size_t)N) &&
+         rd(fi, &cspan, (size_t)(2 * N)) && rd(fi, &ccol, (size_t)h.entries) &&
+         rd(fi, &wp, (size_t)(Np * d.wp_cap)) && rd(fi, &wpc, (size_t)Np);
+  if (ok)
+    ok = rd(fi, &hist, (size_t)(4 * h.history)) &&
+         rd(fi, &shist, (size_t)(h.n_scenes > 1 ? h.n_scenes * h.scene_hist_cap * 4 : 0));
+  if (ok && h.surrogate) ok = rd(fi, &son, (size_t)Np) && rd(fi, &snear, (size_t)Np);
+  std::fclose(fi);
+  if (!ok) return fail(ctx, PDGPU_ERR_ARG, "load_state: %s is truncated", path);
+  if (multi && (crow[0] != 0 || crow[N] != h.entries))
+    return fail(ctx, PDGPU_ERR_ARG, "load_state: %s: contact row offsets are inconsistent", path);
+  if (h.history > d.history_cap) return fail(ctx, PDGPU_ERR_ARG, "load_state: %s: history too long", path);
+  // the step resumes from the saved state: no restart rule, nothing in flight
+  c.error = 0;
+  c.error_info = 0;
+  c.begin_done = c.end_done = 0;
+  c.tile_next = c.tile_done = 0;
+  d.restart_step = -1;
+  TRY(ul(ctx, d.x, x));
+  TRY(ul(ctx, d.u, u));
+  TRY(ul(ctx, d.v, v));
+  TRY(ul(ctx, d.f, f));
+  TRY(ul(ctx, d.Z, Z));
+  TRY(ul(ctx, d.vmag, vmag));
+  TRY(ul(ctx, d.theta, theta));
+  TRY(ul(ctx, d.bond_bits, bits));
+  CK(cudaMemcpyAsync(d.ctrl, &c, sizeof c, cudaMemcpyHostToDevice, ctx->stream));
+  if (multi) {
+    TRY(ul(ctx, d.c_row, crow));
+    TRY(ul(ctx, d.c_cnt, ccnt));
+    TRY(ul(ctx, d.c_nodes, cnodes));
+    TRY(ul(ctx, reinterpret_cast<int32_t *>(d.c_span), cspan));
+    TRY(ul(ctx, d.c_col, ccol));
+    TRY(ul(ctx, d.wp, wp));
+    TRY(ul(ctx, d.wp_cnt, wpc));
+    CK(cudaMemsetAsync(d.fc, 0, (size_t)(st * N) * 8, ctx->stream));
+  }
+  TRY(ul(ctx, d.history, hist));
+  if (d.n_scenes > 1) TRY(ul(ctx, d.scene_hist, shist));
+  if (d.sur_on && h.surrogate) {
+    TRY(ul(ctx, d.sur_on, son));
+    TRY(ul(ctx, d.sur_near, snear));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->gexec) {
+    cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+  }
+  ctx->begun = true;
+  return PDGPU_OK;
+}
+
+}  // extern "C"

@@ -376,6 +376,15 @@ class GpuDEMModel:
         """DEMModel::output: the current state as a .vtu file (pdgpu_write_vtu)."""
         self._check(self.lib.pdgpu_write_vtu(self.ctx, path.encode(), ",".join(tags).encode()))
 
+    def save_state(self, path: str) -> None:
+        """Snapshot of the whole step state, bond bits included (pdgpu_save_state)."""
+        self._check(self.lib.pdgpu_save_state(self.ctx, path.encode()))
+
+    def load_state(self, path: str) -> None:
+        """Continue from a snapshot of the same scene; in place of
+        integrate_begin (pdgpu_load_state)."""
+        self._check(self.lib.pdgpu_load_state(self.ctx, path.encode()))
+
     def restart(self, path: str, step: int) -> None:
         """DEMModel::restart from a file of write_vtu; before integrate_begin."""
         self._check(self.lib.pdgpu_restart(self.ctx, path.encode(), int(step)))

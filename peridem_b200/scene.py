@@ -420,21 +420,66 @@ def two_particle(h_div: int = 10, radius: float = 1e-3, material: str = "RNPBond
                      ic_velocity=(0.0, v0, 0.0), ic_particles=[1])
 
 
+def deposit_2d(radii: np.ndarray, width: float, gap: float, rng: np.random.Generator,
+               trials: int = 8) -> np.ndarray:
+    """Seeded ballistic deposition of circles (radii) into a box of the given
+    width with a floor at y = 0: circle k falls straight down at a random x
+    (of `trials` draws, the one where it comes to rest lowest) until it
+    rests, at clearance `gap`, on the floor or on the first circle placed
+    before it that it meets.  Side walls at x = 0 and x = width keep the same
+    clearance.  Every circle thus rests on a support below it (a connected
+    chain down to the floor), and no two circles come closer than `gap`.
+    Returns the centres [n, 2]."""
+    n = len(radii)
+    r = np.asarray(radii, dtype=np.float64)
+    cen = np.zeros((n, 2))
+    for k in range(n):
+        best_y, best_x = math.inf, 0.0
+        for x in rng.uniform(gap + r[k], width - gap - r[k], size=trials):
+            y = gap + r[k]
+            if k:
+                dx = x - cen[:k, 0]
+                reach = r[k] + r[:k] + gap
+                near = np.abs(dx) < reach
+                if np.any(near):
+                    # falling from above it stops at the first circle it
+                    # meets: the highest of its resting heights on the
+                    # circles within reach (at or above it, it clears all)
+                    lift = cen[:k, 1][near] + np.sqrt(reach[near] ** 2 - dx[near] ** 2)
+                    y = max(y, float(lift.max()))
+            if y < best_y:
+                best_y, best_x = y, x
+        cen[k] = (best_x, best_y)
+    return cen
+
+
 def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3, 1.5e-3),
                    h_div: int = 15, width: float = 40e-3, seed: int = 0,
                    material: str = "RNPBond", wall_speed: float = -0.1,
                    dt: Optional[float] = None, nt: int = 50000, gravity: float = -10.0,
                    search_factor: float = 5.0, search_interval: int = 40,
                    friction: bool = True, gap: Optional[float] = None,
-                   jitter: float = 0.5) -> SceneSpec:
-    """2-D compression: discs and hexagons (50/50) on a jittered triangular
-    lattice inside a fixed frame, pressed by a top wall moving at
-    ``wall_speed``.  One reference mesh per shape at h = R_ref/h_div, scaled
-    per particle, so every particle has the same node count.  ``gap`` is the
+                   jitter: float = 0.5, packing: str = "lattice") -> SceneSpec:
+    """2-D compression: discs and hexagons (50/50) inside a fixed frame,
+    pressed by a top wall moving at ``wall_speed``.  One reference mesh per
+    shape at h = R_ref/h_div, scaled per particle, so every particle has the
+    same node count.
+
+    packing "lattice": a jittered triangular lattice; ``gap`` is the
     clearance between lattice neighbours of maximal radius and between the
     packing and the walls (default 1.05 h_min, just beyond the contact
-    radius 0.95 h_min, so nothing starts in contact); the top wall starts
-    ``gap`` above the highest particle."""
+    radius 0.95 h_min, so nothing starts in contact).
+
+    packing "deposit": ballistic deposition (``deposit_2d``) of the
+    particles' bounding circles at clearance ``gap`` (default 0.96 h_min,
+    just beyond the contact radius 0.95 h_min): every particle rests on the
+    floor or on a particle below it, so the wall's load reaches the floor
+    through chains of supports, and no node pair of two bodies starts inside
+    the contact radius (contacts open as the wall presses instead of as
+    preloaded penalty springs).  The top wall starts ``gap`` above the
+    highest node.
+
+    With the lattice the top wall starts ``gap`` above the highest particle."""
     rng = np.random.default_rng(seed)
     r_ref = r_range[0]
     h_ref = r_ref / h_div
@@ -445,7 +490,9 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
     shapes = np.arange(n_particles) % 2          # 0 disc, 1 hexagon
     rng.shuffle(shapes)
     h_min = r_range[0] / h_div
-    gap = 1.05 * h_min if gap is None else gap
+    if packing not in ("lattice", "deposit"):
+        raise ValueError(f"unknown packing {packing!r}")
+    gap = (1.05 if packing == "lattice" else 0.96) * h_min if gap is None else gap
     dt = stable_dt(2.0e9, 1200.0, h_min) if dt is None else dt
     spacing = 2.0 * r_range[1] + gap
     # triangular-lattice slots; odd rows shift by half a spacing and drop the
@@ -466,14 +513,26 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
             raise ValueError("box too narrow for one particle")
     sites_by_shape = {0: [], 1: []}
     top = 0.0
+    if packing == "deposit":
+        cen = deposit_2d(radii, width, gap, rng)
     for p in range(n_particles):
-        cx, cy = slots[p]
-        room = max(0.0, spacing - 2.0 * radii[p] - gap)
-        jx, jy = rng.uniform(-0.5, 0.5, size=2) * room * jitter
-        jy = max(jy, -(cy - radii[p] - gap))
-        sites_by_shape[int(shapes[p])].append(((cx + jx, cy + jy, 0.0), float(radii[p]),
-                                               float(orients[p])))
-        top = max(top, cy + jy + radii[p])
+        if packing == "deposit":
+            cx, cy = float(cen[p, 0]), float(cen[p, 1])
+        else:
+            cx, cy = slots[p]
+            room = max(0.0, spacing - 2.0 * radii[p] - gap)
+            jx, jy = rng.uniform(-0.5, 0.5, size=2) * room * jitter
+            jy = max(jy, -(cy - radii[p] - gap))
+            cx, cy = cx + jx, cy + jy
+        sites_by_shape[int(shapes[p])].append(((cx, cy, 0.0), float(radii[p]), float(orients[p])))
+        if packing == "deposit":
+            # the highest node of the placed particle (scaled, rotated mesh)
+            mesh = disc_n if shapes[p] == 0 else hex_n
+            o = float(orients[p])
+            ys = cy + (radii[p] / r_ref) * (math.sin(o) * mesh[:, 0] + math.cos(o) * mesh[:, 1])
+            top = max(top, float(ys.max()))
+        else:
+            top = max(top, cy + radii[p])
     height = top + gap
     mat = elastic_material(material, 2.0e9)
     zones = [

@@ -116,7 +116,7 @@ def test_bench_describes_every_workload(workload):
     import argparse
     import bench
     args = argparse.Namespace(workload=workload, particles=502, scenes=256, spheres=4096, precision="mixed",
-                              graph_steps=1, pd_lanes=0, tile_nodes=0, seed=0)
+                              graph_steps=1, pd_lanes=0, tile_nodes=0, seed=0, prerun=20000)
     cfg = bench.workload_config(args, None)
     assert cfg["workload"] and cfg["precision"] == "mixed" and "l2" in cfg
     spec = bench.workload_spec(args)

@@ -59,3 +59,38 @@ def test_compressive_packing_has_no_overlap():
     d = np.sqrt(((c[:, None, :] - c[None, :, :]) ** 2).sum(-1)) - r[:, None] - r[None, :]
     np.fill_diagonal(d, np.inf)
     assert d.min() > 0.95 * 1e-3 / 15
+
+
+def test_deposit_packing_is_settled_and_clear():
+    """Ballistic deposition: no two bounding circles closer than the
+    clearance, each circle resting on the floor or on a circle placed before
+    it (clearance within 1e-9 relative), the top wall just above the highest
+    node, and no node pair of two bodies inside the contact radius."""
+    import math
+    import numpy as np
+    from scipy.spatial import cKDTree
+    from peridem_b200 import scene as scn
+    rng = np.random.default_rng(3)
+    r = rng.uniform(1e-3, 1.5e-3, 60)
+    gap = 1e-5
+    c = scn.deposit_2d(r, 12e-3, gap, rng)
+    d = np.sqrt(((c[:, None, :] - c[None, :, :]) ** 2).sum(-1)) - r[:, None] - r[None, :]
+    np.fill_diagonal(d, np.inf)
+    assert d.min() >= gap * (1 - 1e-9)
+    for k in range(len(r)):
+        on_floor = abs(c[k, 1] - (r[k] + gap)) <= 1e-9 * r[k]
+        on_lower = np.any(np.abs(d[k, :k] - gap) <= 1e-9 * r[k])
+        assert on_floor or on_lower, k
+    assert np.all(c[:, 0] - r >= gap * (1 - 1e-9)) and np.all(c[:, 0] + r <= 12e-3 - gap * (1 - 1e-9))
+    spec = scn.compressive_2d(n_particles=40, width=12e-3, seed=1, packing="deposit", nt=10)
+    sc = scn.build_scene(spec)
+    walls = [p for p in range(sc.n_particles) if sc.p_type[p] == 1]
+    top = walls[-1]
+    parts = [p for p in range(sc.n_particles) if sc.p_type[p] == 0]
+    ymax = max(float(sc.xref[sc.p_start[p]:sc.p_end[p], 1].max()) for p in parts)
+    wall_low = float(sc.xref[sc.p_start[top]:sc.p_end[top], 1].min())
+    h = 1e-3 / 15
+    assert math.isclose(wall_low - ymax, 0.96 * h, rel_tol=1e-6)
+    pt = np.asarray(sc.ptid, dtype=np.int64)
+    pairs = cKDTree(sc.xref[:, :2]).query_pairs(float(np.max(sc.c_rc)), output_type="ndarray")
+    assert not np.any(pt[pairs[:, 0]] != pt[pairs[:, 1]])
