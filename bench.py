@@ -48,9 +48,12 @@ def workload_spec(args):
     if args.workload == "surrogate":
         return scn.compressive_2d(n_particles=2000, r_range=(1e-3, 1.5e-3), h_div=15, width=80e-3,
                                   seed=args.seed, material="RNPBond", wall_speed=-0.1, nt=100000)
+    # dt = 5e-8 s as configured; the contact spring softened to omega dt = 0.3
+    # (scene.stable_kn), since the configured 10x-bulk stiffness blows up at
+    # this step in the reference itself (tests/test_reference_stability.py)
     return scn.compressive_2d(n_particles=args.particles, r_range=(1e-3, 1.5e-3), h_div=15,
                               width=40e-3, seed=args.seed, material="RNPBond", wall_speed=-0.1,
-                              nt=50000, packing="deposit")
+                              dt=5e-8, nt=50000, packing="deposit")
 
 
 def build_workload(args):

@@ -176,11 +176,52 @@ typedef struct pdgpu_scalars {
   double contact_area_radius;
 } pdgpu_scalars;
 
+/* A zone's material deck (inp::MaterialDeck, src/inp/decks/materialDeck.h),
+ * the values pdgpu_material_constants derives the bond-law constants from.
+ * Values not given are negative, as in the deck. */
+typedef struct pdgpu_material_deck {
+  int32_t law;          /* PDGPU_MAT_* (d_materialType) */
+  int32_t irreversible; /* d_irreversibleBondBreak */
+  double E, K, G, nu;   /* d_matData.d_E, d_K, d_G, d_nu */
+  double Gc;            /* d_matData.d_Gc */
+  double check_sc_factor; /* d_checkScFactor */
+} pdgpu_material_deck;
+
 typedef struct pdgpu_ctx pdgpu_ctx;
 
 /* Library / device check.  Returns PDGPU_OK when a device of compute
  * capability 10.0 is visible. */
 PDGPU_API int pdgpu_device_check(int device, char *msg, size_t msg_len);
+
+/* Deck-level constants for a host that holds only the input decks (no
+ * device work; no counterpart call in the reference, whose material
+ * constructors compute these into private members):
+ *   pdgpu_influence_params: the influence function's two parameters from the
+ *     deck's type and parameter list (influenceFn.cpp:13-85 defaults), as
+ *     pdgpu_set_influence takes them;
+ *   pdgpu_material_constants: pdgpu_particle.mat for a particle of the given
+ *     horizon (RnpMaterial material.h:541-620, PmbMaterial :919-997,
+ *     PdElastic :1257-1305, PdState :1579-1700, same evaluation order) and
+ *     the bulk modulus BaseParticle uses for the internal contact stiffness
+ *     of broken bonds (baseParticle.cpp:156-179). */
+PDGPU_API int pdgpu_influence_params(int32_t type, int32_t n_params, const double *params, int32_t dim,
+                                     double out[2]);
+PDGPU_API int pdgpu_material_constants(const pdgpu_material_deck *deck, int32_t dim, double horizon,
+                                       int32_t inf_type, const double inf_params[2], double mat[6],
+                                       double *bulk_modulus);
+
+/* Mesh size of every particle on the device (no context needed):
+ * util::computeMeshSize (src/util/geom.cpp:578-604), the d_h that
+ * BaseParticle sets (baseParticle.cpp:146) and from which the horizon and the
+ * contact radii follow.  Same result as the reference's O(n^2) scan, record
+ * for record: starting from |x_start - x_start+1|, the pairs of the
+ * particle's nodes in (i, j) scan order replace the guess when
+ * util::isLess(distance, guess).  x is a host array of n_nodes util::Points;
+ * particle p owns nodes [particle_start[p], particle_end[p]); h receives
+ * n_particles values (0 for a particle of fewer than two nodes).  Blocking;
+ * allocates its scratch on `device` and frees it before returning. */
+PDGPU_API int pdgpu_mesh_size(int32_t device, const double *x, int64_t n_nodes, const int64_t *particle_start,
+                              const int64_t *particle_end, int64_t n_particles, double *h);
 
 /* Context lifetime: the DEMModel constructor / destructor. */
 PDGPU_API int pdgpu_create(const pdgpu_desc *desc, pdgpu_ctx **out);
@@ -346,14 +387,24 @@ PDGPU_API int pdgpu_num_bonds(pdgpu_ctx *ctx, int64_t *n_bonds);
 PDGPU_API int pdgpu_download_pd_neighbors(pdgpu_ctx *ctx, uint64_t *rowptr, uint64_t *col);
 
 /* Launch shape of the bond loop and the contact kernel: lanes per node
- * (4, 8, 16 or 32 for the bond loop, also 1 or 2 in the mixed form; 4, 8 or
- * 32 for contact); 0 keeps the current choice.  Set before the first step. */
+ * (4, 8, 16 or 32 for the bond loop, also 1 or 2 in the mixed form; 1, 2,
+ * 4, 8 or 32 for the contact pass, default 4); 0 keeps the current choice.
+ * Set before the first step. */
 PDGPU_API int pdgpu_set_tuning(pdgpu_ctx *ctx, int32_t pd_lanes, int32_t contact_lanes);
 
 /* Nodes per bond-loop tile (one CTA each); 0 = automatic.  Set before the
  * first step; tiles shrink by themselves when a window outgrows shared
  * memory. */
 PDGPU_API int pdgpu_set_tile_nodes(pdgpu_ctx *ctx, int32_t nodes);
+
+/* How the mixed-precision 2-D bond loop visits bonds (no counterpart in the
+ * reference): 0 (default) evaluates a bond whose two nodes share a tile once
+ * and hands the far node its share through shared memory (where rows and
+ * tiles fit its 16-bit layout); 1 evaluates every bond from both ends.  Set
+ * before the first step.  pdgpu_bond_scheme reports the one in use (it
+ * prepares the context). */
+PDGPU_API int pdgpu_set_bond_scheme(pdgpu_ctx *ctx, int32_t scheme);
+PDGPU_API int pdgpu_bond_scheme(pdgpu_ctx *ctx, int32_t *scheme);
 
 /* The context's CUDA stream (a cudaStream_t) for callers that time work. */
 PDGPU_API int pdgpu_get_stream(pdgpu_ctx *ctx, void **stream);

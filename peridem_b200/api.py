@@ -41,6 +41,12 @@ class Particle(ctypes.Structure):
                 ("bound_r", c_d), ("mat", c_d * 6)]
 
 
+class MaterialDeck(ctypes.Structure):
+    _fields_ = [("law", ctypes.c_int32), ("irreversible", ctypes.c_int32), ("E", ctypes.c_double),
+                ("K", ctypes.c_double), ("G", ctypes.c_double), ("nu", ctypes.c_double),
+                ("Gc", ctypes.c_double), ("check_sc_factor", ctypes.c_double)]
+
+
 class BcSet(ctypes.Structure):
     _fields_ = [("time_fn", c_i32), ("spatial_fn", c_i32), ("dir_mask", c_i32), ("zero", c_i32),
                 ("time_params", c_d * 4), ("spatial_params", c_d * 2)]
@@ -66,6 +72,11 @@ SIGNATURES = {
     "pdgpu_upload_contact": [c_vp, c_i32, P(c_d), P(c_d), P(c_d), P(c_d), P(c_d)],
     "pdgpu_upload_pd_neighbors": [c_vp, P(c_u64), P(c_u64), P(c_u8)],
     "pdgpu_save_state": [c_vp, ctypes.c_char_p],
+    "pdgpu_mesh_size": [c_i32, P(c_d), c_i64, P(c_i64), P(c_i64), c_i64, P(c_d)],
+    "pdgpu_influence_params": [c_i32, c_i32, P(c_d), c_i32, P(c_d)],
+    "pdgpu_material_constants": [P(MaterialDeck), c_i32, c_d, c_i32, P(c_d), P(c_d), P(c_d)],
+    "pdgpu_set_bond_scheme": [c_vp, c_i32],
+    "pdgpu_bond_scheme": [c_vp, P(c_i32)],
     "pdgpu_load_state": [c_vp, ctypes.c_char_p],
     "pdgpu_build_pd_neighbors": [c_vp],
     "pdgpu_upload_mx": [c_vp, P(c_d)],

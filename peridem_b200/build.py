@@ -27,6 +27,8 @@ UNITS = [
     ("pdgpu_tc.cu", []),
     ("pdgpu_surrogate.cu", []),
     ("pdgpu_runtime.cu", []),
+    ("pdgpu_decks.cu", ["--fmad=false"]),
+    ("pdgpu_meshsize.cu", ["--fmad=false"]),
 ]
 
 

@@ -351,11 +351,206 @@ __device__ __forceinline__ void tile_theta(const DevData &d, const BondTile &T, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Symmetric form (2-D): a bond (i, j) whose nodes both lie in the tile is
+// evaluated once, by node i's thread when i < j.  Stretch, influence, volume
+// correction and law factor are symmetric in (i, j); only the neighbour's
+// volume differs, so the thread adds c vol_j dir to node i and leaves
+// -c vol_i dir and the bond's damage measure in a tile-local slot for node j.
+// After a barrier, node j's thread adds the slots of its bonds to earlier
+// nodes.  Bonds that leave the tile are evaluated from both ends, as before.
+// A row is ordered [to later tile nodes | leaving the tile | to earlier tile
+// nodes] (sym_col; sym_pos maps an entry back to its place in pd_col), so the
+// evaluated entries come first and the slot reads last.  Deterministic: every
+// sum has a fixed order.
+// ---------------------------------------------------------------------------
+struct SymPlan {
+  int64_t meta0;        // first node metadata entry copied
+  uint32_t meta_bytes;  // bulk-copied node metadata
+  uint32_t off_meta, off_part_f, off_part_z, off_fj, off_zq, total;
+};
+
+__host__ __device__ inline SymPlan sym_plan(const Plan &p, int64_t nb, int64_t ne, int slots) {
+  SymPlan q;
+  q.meta0 = nb / 2 * 2;
+  const int64_t meta1 = (ne + 1) / 2 * 2;
+  q.meta_bytes = (uint32_t)((meta1 - q.meta0) * 8);
+  const uint32_t nodes = (uint32_t)(ne - nb);
+  q.off_meta = p.total;                                          // 16-byte aligned
+  q.off_part_f = q.off_meta + (q.meta_bytes + 15u) / 16u * 16u;  // double2 per tile node
+  q.off_part_z = q.off_part_f + 16u * nodes;                     // float per tile node
+  q.off_fj = (q.off_part_z + 4u * nodes + 15u) / 16u * 16u;      // float2 per slot
+  q.off_zq = q.off_fj + 8u * (uint32_t)slots;                    // float per slot
+  q.total = (q.off_zq + 4u * (uint32_t)slots + 15u) / 16u * 16u;
+  return q;
+}
+
+// one bond of phase A: force on i added to F; with slot >= 0 (j a later node
+// of the tile) j's share and the damage measure go to the slot.  e is the
+// bond's index in the symmetric order; row_i node i's first entry in pd_col.
+template <int LAW, bool BROKEN_KNOWN_CLEAR>
+__device__ __forceinline__ void bond_sym(const DevData &d, const MixParticle &M, const View<2> &V,
+                                         const float (&xi)[3], const float (&ui)[3], float vi, float2 mi,
+                                         int lj, bool broken, bool gauss, int64_t e, int64_t row_i,
+                                         int64_t i, int64_t win_begin, int slot, float2 *s_fj, float *s_zq,
+                                         float (&F)[3], float &zmax) {
+  float xj[3], uj[3], volj;
+  V.node(lj, xj, uj, volj);
+  float dx[2], du[2], y[2];
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    dx[q] = xj[q] - xi[q];
+    du[q] = uj[q] - ui[q];
+    y[q] = dx[q] + du[q];
+  }
+  const float r2 = dx[0] * dx[0] + dx[1] * dx[1];
+  const float inv_r = rsqrtf(r2);
+  const float rji = r2 * inv_r;
+  const float dxdu = dx[0] * du[0] + dx[1] * du[1];
+  float S, zq, inv_ly = 0.f;
+  if constexpr (LAW == LAW_RNP) {
+    S = dxdu * (inv_r * inv_r);
+    zq = S * S * rji;
+  } else {
+    const float y2 = y[0] * y[0] + y[1] * y[1];
+    inv_ly = rsqrtf(y2);
+    const float ly = y2 * inv_ly;
+    S = __fdividef(2.f * dxdu + (du[0] * du[0] + du[1] * du[1]), rji * (ly + rji));
+    zq = fabsf(S);
+  }
+  zmax = fmaxf(zmax, zq);
+  float c = 0.f;  // force per unit neighbour volume, along dir
+  bool along_ref = LAW == LAW_RNP;
+  if (BROKEN_KNOWN_CLEAR || !broken) {
+    const float corr = rji > M.low_thr ? fmaf(-rji, M.inv_h, M.cu_h) : 1.f;
+    const float kJ = gauss ? M.kj0 * ex2(rji * rji * M.j1) : fmaf(M.kj1, rji, M.kj0);
+    bool breaks = false;
+    if constexpr (LAW == LAW_RNP) {
+      breaks = M.irreversible && zq > M.fsc_q;
+      if (!breaks) c = kJ * S * ex2(M.nbeta_l2e * zq) * corr * inv_r;
+    } else if constexpr (LAW == LAW_PMB) {
+      breaks = zq > M.s0_thr;
+      if (!breaks) c = kJ * S * corr * inv_ly;
+    } else if constexpr (LAW == LAW_ELASTIC) {
+      c = kJ * S * corr * inv_ly;
+    } else {
+      const float2 mj = V.m[lj];
+      c = kJ * rji * ((mi.x + mj.x) + S * (mi.y + mj.y)) * corr * inv_ly;
+    }
+    if (breaks) {
+      // both directed bonds break together (the same stretch from either end)
+      const int64_t g = row_i + d.sym_pos[e];
+      atomicOr(d.bond_bits + (g >> 5), 1u << (g & 31));
+      if (slot >= 0) {
+        const int64_t j = win_begin + lj;
+        for (int64_t m = d.pd_row[j]; m < d.pd_row[j + 1]; m++)
+          if (d.pd_col[m] == (int32_t)i) {
+            atomicOr(d.bond_bits + (m >> 5), 1u << (m & 31));
+            break;
+          }
+      }
+    }
+  } else {
+    // broken bond: short-range repulsion between the two nodes
+    const float inv_R = rsqrtf(y[0] * y[0] + y[1] * y[1]);
+    c = fminf(M.kn * (1.f - M.rc * inv_R), 0.f);
+    along_ref = false;
+  }
+  const float d0 = along_ref ? dx[0] : y[0], d1 = along_ref ? dx[1] : y[1];
+  const float ci = c * volj;
+  F[0] = fmaf(ci, d0, F[0]);
+  F[1] = fmaf(ci, d1, F[1]);
+  if (slot >= 0) {
+    const float cj = -c * vi;
+    s_fj[slot] = make_float2(cj * d0, cj * d1);
+    s_zq[slot] = zq;
+  }
+}
+
+template <int LPN, int LAW, typename CT>
+__device__ __forceinline__ void tile_sym(const DevData &d, const BondTile &T, const MixParticle &M,
+                                         const View<2> &V, const CT *s_col, const uint32_t *s_bits,
+                                         const int64_t *s_row, const Plan &p, const SymPlan &q,
+                                         unsigned char *smem) {
+  constexpr int kT = kThreadsFor<2, LPN>;
+  const int lane = threadIdx.x % LPN;
+  const unsigned gm = gmask<LPN>();
+  const int64_t kb = T.bond_begin;
+  const int col_off = (int)(kb - p.col0);
+  const int bit_off = (int)(kb - 32 * p.word0);
+  const int shift = (int)(M.start - T.win_begin);
+  const bool gauss = d.inf.type == PDGPU_INF_GAUSSIAN;
+  const uint2 *s_meta = reinterpret_cast<const uint2 *>(smem + q.off_meta);
+  double2 *s_pf = reinterpret_cast<double2 *>(smem + q.off_part_f);
+  float *s_pz = reinterpret_cast<float *>(smem + q.off_part_z);
+  float2 *s_fj = reinterpret_cast<float2 *>(smem + q.off_fj);
+  float *s_zq = reinterpret_cast<float *>(smem + q.off_zq);
+  // phase A: bonds to later tile nodes and bonds leaving the tile
+  for (int64_t i = T.node_begin + threadIdx.x / LPN; i < T.node_end; i += kT / LPN) {
+    const int64_t row_i = s_row[i - p.row0];
+    const int k0 = (int)(row_i - kb), k1 = (int)(s_row[i + 1 - p.row0] - kb);
+    const uint2 meta = s_meta[i - q.meta0];
+    const int base = (int)meta.x, n_up = (int)(meta.y & 0xffffu), n_uo = (int)(meta.y >> 16);
+    const int li = (int)(i - T.win_begin);
+    float xi[3], ui[3], vi;
+    V.node(li, xi, ui, vi);
+    float2 mi = make_float2(0.f, 0.f);
+    if constexpr (LAW == LAW_STATE) mi = V.m[li];
+    float F[3] = {0.f, 0.f, 0.f};
+    float zmax = 0.f;
+    if (!any_broken<LPN>(s_bits, k0 + bit_off, k1 + bit_off, gm)) {
+#pragma unroll 4
+      for (int k = k0 + lane; k < k0 + n_uo; k += LPN)
+        bond_sym<LAW, true>(d, M, V, xi, ui, vi, mi, (int)s_col[k + col_off] + shift, false, gauss, kb + k,
+                            row_i, i, T.win_begin, k - k0 < n_up ? base + k - k0 : -1, s_fj, s_zq, F, zmax);
+    } else {
+      for (int k = k0 + lane; k < k0 + n_uo; k += LPN) {
+        const int b = (int)(row_i - 32 * p.word0) + (int)d.sym_pos[kb + k];
+        const bool broken = (s_bits[b >> 5] >> (b & 31)) & 1u;
+        bond_sym<LAW, false>(d, M, V, xi, ui, vi, mi, (int)s_col[k + col_off] + shift, broken, gauss, kb + k,
+                             row_i, i, T.win_begin, k - k0 < n_up ? base + k - k0 : -1, s_fj, s_zq, F, zmax);
+      }
+    }
+    const double Fx = gsum<LPN>((double)F[0], gm);
+    const double Fy = gsum<LPN>((double)F[1], gm);
+    const float zq = gmax<LPN>(zmax, gm);
+    if (lane == 0) {
+      s_pf[i - T.node_begin] = make_double2(Fx, Fy);
+      s_pz[i - T.node_begin] = zq;
+    }
+  }
+  __syncthreads();
+  // phase B: the shares earlier tile nodes left for this node
+  for (int64_t i = T.node_begin + threadIdx.x / LPN; i < T.node_end; i += kT / LPN) {
+    const int k0 = (int)(s_row[i - p.row0] - kb), k1 = (int)(s_row[i + 1 - p.row0] - kb);
+    const int n_uo = (int)(s_meta[i - q.meta0].y >> 16);
+    float fx = 0.f, fy = 0.f, zmax = 0.f;
+#pragma unroll 4
+    for (int k = k0 + n_uo + lane; k < k1; k += LPN) {
+      const int slot = (int)s_col[k + col_off];
+      const float2 f = s_fj[slot];
+      fx += f.x;
+      fy += f.y;
+      zmax = fmaxf(zmax, s_zq[slot]);
+    }
+    const double Bx = gsum<LPN>((double)fx, gm);
+    const double By = gsum<LPN>((double)fy, gm);
+    const float zb = gmax<LPN>(zmax, gm);
+    if (lane == 0) {
+      const double2 a = s_pf[i - T.node_begin];
+      d.f[2 * i] = a.x + Bx;
+      d.f[2 * i + 1] = a.y + By;
+      const float zq = fmaxf(s_pz[i - T.node_begin], zb);
+      d.Z[i] = LAW == LAW_RNP ? sqrtf(zq) * M.inv_rbar : zq * M.inv_s0;
+    }
+  }
+}
+
 // Persistent: a fixed grid (below full occupancy, so that the contact and
 // damping passes running beside it find room) claims tiles from a counter in
 // the step-control state; the claim for the next tile is made while the
 // current one is staged.  The last CTA out resets the counter.
-template <int DIM, int LPN, int LAW, typename CT, bool PRE = false>
+template <int DIM, int LPN, int LAW, typename CT, bool PRE = false, bool SYM = false>
 __global__ void __launch_bounds__(kThreadsFor<DIM, LPN>) k_bonds_mixed(DevData d, const BondTile *tiles, int n_tiles,
                                                          const CT *col) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -384,6 +579,8 @@ __global__ void __launch_bounds__(kThreadsFor<DIM, LPN>) k_bonds_mixed(DevData d
     }
     const int w = (int)(T.win_end - T.win_begin);
     const Plan p = plan(DIM, state, (int)sizeof(CT), T.bond_begin, T.bond_end, T.node_begin, T.node_end, w);
+    SymPlan q{};
+    if constexpr (SYM) q = sym_plan(p, T.node_begin, T.node_end, T.slots);
     CT *s_col = reinterpret_cast<CT *>(smem);
     uint32_t *s_bits = reinterpret_cast<uint32_t *>(smem + p.col_bytes);
     int64_t *s_row = reinterpret_cast<int64_t *>(smem + p.off_row);
@@ -396,7 +593,8 @@ __global__ void __launch_bounds__(kThreadsFor<DIM, LPN>) k_bonds_mixed(DevData d
     // tile: bulk copies; then the claim of the next tile
     if (threadIdx.x == 0) {
       fence_async_smem();
-      bar_arrive_tx(&bar, p.col_bytes + p.bit_bytes + p.row_bytes + 16u * (uint32_t)w);
+      bar_arrive_tx(&bar, p.col_bytes + p.bit_bytes + p.row_bytes + 16u * (uint32_t)w + (SYM ? q.meta_bytes : 0u));
+      if constexpr (SYM) bulk_load(smem + q.off_meta, d.sym_meta + q.meta0, q.meta_bytes, &bar);
       if (p.col_bytes) bulk_load(s_col, col + p.col0, p.col_bytes, &bar);
       if (p.bit_bytes) bulk_load(s_bits, d.bond_bits + p.word0, p.bit_bytes, &bar);
       bulk_load(s_row, d.pd_row + p.row0, p.row_bytes, &bar);
@@ -441,6 +639,7 @@ __global__ void __launch_bounds__(kThreadsFor<DIM, LPN>) k_bonds_mixed(DevData d
 
     View<DIM> V{s_xv, s_u2, s_u4, s_m};
     if constexpr (PRE) tile_theta<DIM, LPN, CT>(d, T, M, V, s_col, s_bits, s_row, p);
+    else if constexpr (SYM && DIM == 2) tile_sym<LPN, LAW, CT>(d, T, M, V, s_col, s_bits, s_row, p, q, smem);
     else tile_nodes<DIM, LPN, LAW, CT>(d, T, M, V, s_col, s_bits, s_row, p);
     const int t_next = s_tile[(k + 1) & 1];
     __syncthreads();  // the stage is free for the next tile's copies
@@ -475,23 +674,40 @@ int bond_grid(K kernel, int threads, size_t smem, int n_tiles) {
   return g < n_tiles ? g : n_tiles;
 }
 
-template <int DIM, int LPN, int LAW, typename CT, bool PRE = false>
+template <int DIM, int LPN, int LAW, typename CT, bool PRE = false, bool SYM = false>
 void launch_one(const DevData &d, const CT *col, const BondTile *t, int n, size_t smem, cudaStream_t s) {
-  auto *k = k_bonds_mixed<DIM, LPN, LAW, CT, PRE>;
+  auto *k = k_bonds_mixed<DIM, LPN, LAW, CT, PRE, SYM>;
   constexpr int kT = kThreadsFor<DIM, LPN>;
   k<<<bond_grid(k, kT, smem, n), kT, smem, s>>>(d, t, n, col);
 }
 
-template <int DIM, int LAW, typename CT, bool PRE = false>
+template <int DIM, int LAW, typename CT, bool PRE = false, bool SYM = false>
 void launch_law(const DevData &d, const CT *col, const BondTile *t, int n, int lanes, size_t smem,
                 cudaStream_t s) {
   switch (lanes) {
-    case 1: launch_one<DIM, 1, LAW, CT, PRE>(d, col, t, n, smem, s); break;
-    case 2: launch_one<DIM, 2, LAW, CT, PRE>(d, col, t, n, smem, s); break;
-    case 4: launch_one<DIM, 4, LAW, CT, PRE>(d, col, t, n, smem, s); break;
-    case 8: launch_one<DIM, 8, LAW, CT, PRE>(d, col, t, n, smem, s); break;
-    case 16: launch_one<DIM, 16, LAW, CT, PRE>(d, col, t, n, smem, s); break;
-    default: launch_one<DIM, 32, LAW, CT, PRE>(d, col, t, n, smem, s); break;
+    case 1: launch_one<DIM, 1, LAW, CT, PRE, SYM>(d, col, t, n, smem, s); break;
+    case 2: launch_one<DIM, 2, LAW, CT, PRE, SYM>(d, col, t, n, smem, s); break;
+    case 4: launch_one<DIM, 4, LAW, CT, PRE, SYM>(d, col, t, n, smem, s); break;
+    case 8: launch_one<DIM, 8, LAW, CT, PRE, SYM>(d, col, t, n, smem, s); break;
+    case 16: launch_one<DIM, 16, LAW, CT, PRE, SYM>(d, col, t, n, smem, s); break;
+    default: launch_one<DIM, 32, LAW, CT, PRE, SYM>(d, col, t, n, smem, s); break;
+  }
+}
+
+// the symmetric form: 2-D, 16-bit columns
+void launch_sym(const DevData &d, const BondTile *t, const int *law_begin, int lanes, size_t smem,
+                cudaStream_t s) {
+  for (int law = 0; law < 4; law++) {
+    const int b = law_begin[law], n = law_begin[law + 1] - b;
+    if (n <= 0) continue;
+    switch (law) {
+      case PDGPU_MAT_RNP: launch_law<2, LAW_RNP, uint16_t, false, true>(d, d.sym_col, t + b, n, lanes, smem, s); break;
+      case PDGPU_MAT_PMB: launch_law<2, LAW_PMB, uint16_t, false, true>(d, d.sym_col, t + b, n, lanes, smem, s); break;
+      case PDGPU_MAT_PDELASTIC:
+        launch_law<2, LAW_ELASTIC, uint16_t, false, true>(d, d.sym_col, t + b, n, lanes, smem, s);
+        break;
+      default: launch_law<2, LAW_STATE, uint16_t, false, true>(d, d.sym_col, t + b, n, lanes, smem, s); break;
+    }
   }
 }
 
@@ -525,11 +741,14 @@ void launch_pre(const DevData &d, const BondTile *t, int n, int lanes, size_t sm
   }
 }
 
-template <int DIM, int LAW, typename CT, bool PRE = false>
+template <int DIM, int LAW, typename CT, bool PRE = false, bool SYM = false>
 bool set_law_limit(size_t bytes) {
-  const void *fs[] = {(const void *)k_bonds_mixed<DIM, 1, LAW, CT, PRE>, (const void *)k_bonds_mixed<DIM, 2, LAW, CT, PRE>,
-                      (const void *)k_bonds_mixed<DIM, 4, LAW, CT, PRE>, (const void *)k_bonds_mixed<DIM, 8, LAW, CT, PRE>,
-                      (const void *)k_bonds_mixed<DIM, 16, LAW, CT, PRE>, (const void *)k_bonds_mixed<DIM, 32, LAW, CT, PRE>};
+  const void *fs[] = {(const void *)k_bonds_mixed<DIM, 1, LAW, CT, PRE, SYM>,
+                      (const void *)k_bonds_mixed<DIM, 2, LAW, CT, PRE, SYM>,
+                      (const void *)k_bonds_mixed<DIM, 4, LAW, CT, PRE, SYM>,
+                      (const void *)k_bonds_mixed<DIM, 8, LAW, CT, PRE, SYM>,
+                      (const void *)k_bonds_mixed<DIM, 16, LAW, CT, PRE, SYM>,
+                      (const void *)k_bonds_mixed<DIM, 32, LAW, CT, PRE, SYM>};
   for (auto f : fs)
     if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
       return false;
@@ -551,7 +770,15 @@ int set_limit(size_t bytes) {
                   set_law_limit<DIM, LAW_ELASTIC, int32_t>(bytes) && set_law_limit<DIM, LAW_STATE, int32_t>(bytes) &&
                   set_law_limit<DIM, LAW_STATE, uint16_t, true>(bytes) &&
                   set_law_limit<DIM, LAW_STATE, int32_t, true>(bytes);
-  return ok ? 0 : -1;
+  if (!ok) return -1;
+  if constexpr (DIM == 2) {
+    const bool sym = set_law_limit<2, LAW_RNP, uint16_t, false, true>(bytes) &&
+                     set_law_limit<2, LAW_PMB, uint16_t, false, true>(bytes) &&
+                     set_law_limit<2, LAW_ELASTIC, uint16_t, false, true>(bytes) &&
+                     set_law_limit<2, LAW_STATE, uint16_t, false, true>(bytes);
+    if (!sym) return -1;
+  }
+  return 0;
 }
 
 }  // namespace mixed_loop
@@ -559,6 +786,10 @@ int set_limit(size_t bytes) {
 void launch_pd_tiled_mixed(const DevData &d, const BondTile *t, const int *law_begin, int lanes,
                            size_t smem, cudaStream_t s) {
   using namespace mixed_loop;
+  if (d.use_sym && d.dim == 2 && d.use16) {
+    launch_sym(d, t, law_begin, lanes, smem, s);
+    return;
+  }
   if (d.use16) {
     if (d.dim == 2) launch_dim<2>(d, d.pd_col16, t, law_begin, lanes, smem, s);
     else launch_dim<3>(d, d.pd_col16, t, law_begin, lanes, smem, s);
@@ -596,10 +827,10 @@ size_t tile_smem_mixed(int dim, bool state, int64_t window) {
   return bonds_mixed::tile_smem_bytes(dim, state, (int)window);
 }
 
-size_t tile_smem_mixed_main(int dim, bool state, bool col16, const BondTile &t) {
-  return mixed_loop::plan(dim, state, col16 ? 2 : 4, t.bond_begin, t.bond_end, t.node_begin,
-                          t.node_end, t.win_end - t.win_begin)
-      .total;
+size_t tile_smem_mixed_main(int dim, bool state, bool col16, const BondTile &t, bool sym) {
+  const mixed_loop::Plan p = mixed_loop::plan(dim, state, col16 ? 2 : 4, t.bond_begin, t.bond_end, t.node_begin,
+                                              t.node_end, t.win_end - t.win_begin);
+  return sym ? mixed_loop::sym_plan(p, t.node_begin, t.node_end, t.slots).total : p.total;
 }
 
 int set_tile_smem_limit_mixed(int dim, size_t bytes) {

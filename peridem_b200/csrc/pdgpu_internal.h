@@ -130,7 +130,7 @@ struct MixParticle {
 // particle, whose bonds reach node indices inside [win_begin, win_end).
 struct BondTile {
   int32_t particle;
-  int32_t pad;
+  int32_t slots;  // symmetric mixed bond loop: bonds (i, j) with both nodes in the tile, i < j
   int64_t node_begin, node_end, win_begin, win_end;
   int64_t bond_begin, bond_end;  // pd_row[node_begin], pd_row[node_end]
   int64_t center;                // the particle's centre node
@@ -242,6 +242,17 @@ struct DevData {
   // mixed-precision bond loop: particle-local FP32 reference coordinates,
   // FP32 volumes, particle-local 16-bit neighbour offsets when they fit
   uint16_t *pd_col16;
+  // symmetric mixed bond loop (2-D): per bond, each node's row reordered as
+  // [bonds to later nodes of its tile | bonds leaving the tile | bonds to
+  // earlier nodes of its tile]; sym_col holds the particle-local neighbour
+  // of the first two kinds and, for the third, the tile-local slot in which
+  // the earlier node's thread leaves this node's share of their bond;
+  // sym_pos the entry's offset in the node's row of pd_col.  sym_meta per
+  // node: {first slot of its bonds to later nodes, count of those | count
+  // of the first two kinds << 16}.
+  uint16_t *sym_col, *sym_pos;
+  uint2 *sym_meta;
+  int32_t use_sym;
   MixParticle *mixp;
   float4 *xv_mixed;  // per node {x, y, z, vol}: reference coordinates minus the centre's, FP32
   int32_t use16;
@@ -300,6 +311,15 @@ void launch_step_begin(const DevData &d, int verlet, cudaStream_t s);
 void launch_step_end(const DevData &d, int verlet, int post, cudaStream_t s);
 void launch_bc(const DevData &d, cudaStream_t s);
 void launch_mixed_setup(const DevData &d, cudaStream_t s);
+// symmetric layout: per node its tile (node_tile) -> counts (n_up, n_uo into
+// sym_meta.y) -> slot bases from an exclusive scan of n_up (scan, N + 1) ->
+// reordered rows; tiles get their slot counts
+void launch_sym_count(const DevData &d, const BondTile *tiles, const int32_t *node_tile, int64_t *n_up,
+                      cudaStream_t s);
+void launch_sym_fill(const DevData &d, BondTile *tiles, int n_tiles, const int32_t *node_tile,
+                     const int64_t *scan, cudaStream_t s);
+void launch_node_tiles(const BondTile *tiles, int n_tiles, int32_t *node_tile, cudaStream_t s);
+void launch_sym_bits(const DevData &d, const BondTile *tiles, const int32_t *node_tile, cudaStream_t s);
 void launch_tile_windows(const DevData &d, BondTile *tiles, int n_tiles, cudaStream_t s);
 // tiled bond loop (pdgpu_bonds_fp64.cu / pdgpu_bonds_mixed.cu)
 void launch_pd_tiled_fp64(const DevData &d, const BondTile *tiles, int n_tiles, int lanes,
@@ -316,7 +336,7 @@ void launch_prepass_mixed(const DevData &d, const BondTile *tiles, const int *la
                           size_t smem, cudaStream_t s);
 size_t tile_smem_fp64(int dim, bool state, int64_t window);
 size_t tile_smem_mixed(int dim, bool state, int64_t window);       // state pre-pass
-size_t tile_smem_mixed_main(int dim, bool state, bool col16, const BondTile &t);
+size_t tile_smem_mixed_main(int dim, bool state, bool col16, const BondTile &t, bool sym = false);
 int set_tile_smem_limit_fp64(int dim, size_t bytes);
 int set_tile_smem_limit_mixed(int dim, size_t bytes);
 

@@ -1685,11 +1685,15 @@ cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, in
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s) {
   const unsigned g = (unsigned)d.contact_grid;
   if (d.dim == 2) {
-    if (lanes == 4) k_contact<2, 4><<<g, kBlock, 0, s>>>(d);
+    if (lanes == 1) k_contact<2, 1><<<g, kBlock, 0, s>>>(d);
+    else if (lanes == 2) k_contact<2, 2><<<g, kBlock, 0, s>>>(d);
+    else if (lanes == 4) k_contact<2, 4><<<g, kBlock, 0, s>>>(d);
     else if (lanes == 8) k_contact<2, 8><<<g, kBlock, 0, s>>>(d);
     else k_contact<2, 32><<<g, kBlock, 0, s>>>(d);
   } else {
-    if (lanes == 4) k_contact<3, 4><<<g, kBlock, 0, s>>>(d);
+    if (lanes == 1) k_contact<3, 1><<<g, kBlock, 0, s>>>(d);
+    else if (lanes == 2) k_contact<3, 2><<<g, kBlock, 0, s>>>(d);
+    else if (lanes == 4) k_contact<3, 4><<<g, kBlock, 0, s>>>(d);
     else if (lanes == 8) k_contact<3, 8><<<g, kBlock, 0, s>>>(d);
     else k_contact<3, 32><<<g, kBlock, 0, s>>>(d);
   }

@@ -56,7 +56,123 @@ __global__ void k_mixed_setup(DevData d) {
     d.pd_col16[k] = (uint16_t)(d.pd_col[k] - P.start);
 }
 
+// Symmetric layout, pass 1: per node of a tile, how many of its bonds go to
+// later nodes of the same tile (n_up) and how many leave the tile.
+__global__ void k_sym_count(DevData d, const BondTile *tiles, const int32_t *node_tile, int64_t *n_up) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_nodes) return;
+  const int32_t t = node_tile[i];
+  if (t < 0) {
+    n_up[i] = 0;
+    d.sym_meta[i] = make_uint2(0u, 0u);
+    return;
+  }
+  const int64_t nb = tiles[t].node_begin, ne = tiles[t].node_end;
+  uint32_t up = 0, out = 0;
+  for (int64_t k = d.pd_row[i]; k < d.pd_row[i + 1]; k++) {
+    const int64_t j = d.pd_col[k];
+    if (j >= nb && j < ne) up += j > i;
+    else out++;
+  }
+  n_up[i] = up;
+  d.sym_meta[i] = make_uint2(0u, up | ((up + out) << 16));
+}
+
+// Pass 2: slot bases (exclusive scan of n_up, relative to the tile's first
+// node) and the reordered rows.  The slots of node i's bonds to later nodes
+// follow its row order; the bond (j, i) of a later node j finds its slot as
+// slot_base[i] + the rank of j among i's bonds to later nodes.
+__global__ void k_sym_fill(DevData d, BondTile *tiles, const int32_t *node_tile, const int64_t *scan) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_nodes) return;
+  const int32_t t = node_tile[i];
+  if (t < 0) return;
+  BondTile &T = tiles[t];
+  const int64_t nb = T.node_begin, ne = T.node_end;
+  const int64_t start = d.particles[T.particle].start;
+  const uint2 m = d.sym_meta[i];
+  const uint32_t n_up = m.y & 0xffffu, n_uo = m.y >> 16;
+  const int64_t r0 = d.pd_row[i], r1 = d.pd_row[i + 1];
+  int64_t e_up = r0, e_out = r0 + n_up, e_low = r0 + n_uo;
+  for (int64_t k = r0; k < r1; k++) {
+    const int64_t j = d.pd_col[k];
+    const uint16_t pos = (uint16_t)(k - r0);
+    if (j >= nb && j < ne && j > i) {
+      d.sym_col[e_up] = (uint16_t)(j - start);
+      d.sym_pos[e_up++] = pos;
+    } else if (j < nb || j >= ne) {
+      d.sym_col[e_out] = (uint16_t)(j - start);
+      d.sym_pos[e_out++] = pos;
+    } else {
+      // rank of i among j's bonds to later nodes of the tile, in row order
+      uint32_t rank = 0;
+      for (int64_t q = d.pd_row[j]; q < d.pd_row[j + 1]; q++) {
+        const int64_t c = d.pd_col[q];
+        if (c == i) break;
+        rank += (c > j && c < ne);
+      }
+      d.sym_col[e_low] = (uint16_t)(scan[j] - scan[nb] + rank);
+      d.sym_pos[e_low++] = pos;
+    }
+  }
+  d.sym_meta[i].x = (uint32_t)(scan[i] - scan[nb]);
+  if (i == nb) {
+    // the tile's slot count (written once per tile, by its first node)
+    T.slots = (int32_t)(scan[ne] - scan[nb]);
+  }
+}
+
+// The symmetric loop reads one broken bit per pair of tile nodes (node i's,
+// for i < j); both directions must agree, as in every state the reference
+// produces (a bond breaks from both ends at the same step).  Where a host
+// uploaded only one direction as broken, the pair is made broken both ways.
+__global__ void k_sym_bits(DevData d, const BondTile *tiles, const int32_t *node_tile) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_nodes) return;
+  const int32_t t = node_tile[i];
+  if (t < 0) return;
+  const int64_t ne = tiles[t].node_end;
+  for (int64_t k = d.pd_row[i]; k < d.pd_row[i + 1]; k++) {
+    const int64_t j = d.pd_col[k];
+    if (j <= i || j >= ne) continue;
+    for (int64_t m = d.pd_row[j]; m < d.pd_row[j + 1]; m++)
+      if (d.pd_col[m] == (int32_t)i) {
+        const bool a = (d.bond_bits[k >> 5] >> (k & 31)) & 1u, b = (d.bond_bits[m >> 5] >> (m & 31)) & 1u;
+        if (a != b) {
+          atomicOr(d.bond_bits + (k >> 5), 1u << (k & 31));
+          atomicOr(d.bond_bits + (m >> 5), 1u << (m & 31));
+        }
+        break;
+      }
+  }
+}
+
+__global__ void k_node_tiles(const BondTile *tiles, int n_tiles, int32_t *node_tile) {
+  const int t = blockIdx.x;
+  if (t >= n_tiles) return;
+  for (int64_t i = tiles[t].node_begin + threadIdx.x; i < tiles[t].node_end; i += blockDim.x) node_tile[i] = t;
+}
+
 }  // namespace
+
+void launch_sym_count(const DevData &d, const BondTile *tiles, const int32_t *node_tile, int64_t *n_up,
+                      cudaStream_t s) {
+  k_sym_count<<<(unsigned)((d.n_nodes + 255) / 256), 256, 0, s>>>(d, tiles, node_tile, n_up);
+}
+
+void launch_sym_fill(const DevData &d, BondTile *tiles, int n_tiles, const int32_t *node_tile,
+                     const int64_t *scan, cudaStream_t s) {
+  (void)n_tiles;
+  k_sym_fill<<<(unsigned)((d.n_nodes + 255) / 256), 256, 0, s>>>(d, tiles, node_tile, scan);
+}
+
+void launch_sym_bits(const DevData &d, const BondTile *tiles, const int32_t *node_tile, cudaStream_t s) {
+  k_sym_bits<<<(unsigned)((d.n_nodes + 255) / 256), 256, 0, s>>>(d, tiles, node_tile);
+}
+
+void launch_node_tiles(const BondTile *tiles, int n_tiles, int32_t *node_tile, cudaStream_t s) {
+  if (n_tiles > 0) k_node_tiles<<<n_tiles, 256, 0, s>>>(tiles, n_tiles, node_tile);
+}
 
 void launch_tile_windows(const DevData &d, BondTile *tiles, int n_tiles, cudaStream_t s) {
   if (n_tiles > 0) k_tile_windows<<<n_tiles, 256, 0, s>>>(d, tiles);

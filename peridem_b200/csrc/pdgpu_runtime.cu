@@ -63,7 +63,7 @@ struct pdgpu_ctx {
   double *stage = nullptr;  // N*3 AoS staging
   void *scan_tmp = nullptr;
   size_t scan_bytes = 0;
-  int pd_lanes = 0, contact_lanes = 8;
+  int pd_lanes = 0, contact_lanes = 4;
   int64_t *rebuild_bsum = nullptr;
   int rebuild_grid = 0;
   // tiled bond loop
@@ -71,6 +71,9 @@ struct pdgpu_ctx {
   int n_tiles = 0;
   size_t tile_smem = 0, tile_smem_state = 0;  // pre-pass stage; FP64 bond loop with m_x, theta
   size_t tile_smem_pd = 0;                     // the bond-loop launch
+  size_t tile_smem_sym = 0;                    // the symmetric bond-loop launch (mixed, 2-D)
+  int bond_scheme = 0;                         // 0: symmetric where it applies, 1: per node
+  int32_t *node_tile = nullptr;                // per node its bond tile (-1: none), symmetric form
   int tile_law[5] = {0, 0, 0, 0, 0};           // tiles of law m: [tile_law[m], tile_law[m + 1])
   int64_t tile_nodes = 0;  // nodes per tile (0 = chosen at set-up)
   bool state_prepass = false;
@@ -637,6 +640,73 @@ int prepare_tiles(pdgpu_ctx *ctx) {
               "order each particle's nodes spatially");
 }
 
+// both directions of a bond between two nodes of one tile share their broken
+// state in the symmetric form (see k_sym_bits)
+int sym_bits(pdgpu_ctx *ctx) {
+  if (!ctx->d.use_sym) return PDGPU_OK;
+  launch_sym_bits(ctx->d, ctx->tiles, ctx->node_tile, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PDGPU_OK;
+}
+
+// The symmetric layout of the mixed 2-D bond loop (see pdgpu_bonds_mixed.cu):
+// built on the device from the tiles and neighbour lists; used when every
+// row and every tile's slot count fits 16 bits and the stage with the slots
+// fits shared memory, else the per-node form stays.
+int prepare_sym(pdgpu_ctx *ctx) {
+  DevData &d = ctx->d;
+  d.use_sym = 0;
+  if (d.precision != PDGPU_PREC_MIXED || d.dim != 2 || !d.use16 || ctx->bond_scheme != 0 || ctx->n_tiles == 0)
+    return PDGPU_OK;
+  const int64_t N = d.n_nodes;
+  std::vector<int64_t> row((size_t)N + 1);
+  CK(cudaMemcpy(row.data(), d.pd_row, ((size_t)N + 1) * 8, cudaMemcpyDeviceToHost));
+  for (int64_t i = 0; i < N; i++)
+    if (row[i + 1] - row[i] >= 65536) return PDGPU_OK;
+  if (!d.sym_col) {
+    TRY(dalloc(ctx, &d.sym_col, d.n_bonds + kBondPad));
+    TRY(dalloc(ctx, &d.sym_pos, d.n_bonds + kBondPad));
+    TRY(dalloc(ctx, &d.sym_meta, (size_t)N + 2));
+    CK(cudaMemset(d.sym_col, 0, (d.n_bonds + kBondPad) * 2));
+    CK(cudaMemset(d.sym_pos, 0, (d.n_bonds + kBondPad) * 2));
+    CK(cudaMemset(d.sym_meta, 0, ((size_t)N + 2) * sizeof(uint2)));
+  }
+  int64_t *n_up = nullptr, *scan_d = nullptr;
+  if (!ctx->node_tile) TRY(dalloc(ctx, &ctx->node_tile, (size_t)N));
+  int32_t *node_tile = ctx->node_tile;
+  TRY(dalloc(ctx, &n_up, (size_t)N));
+  TRY(dalloc(ctx, &scan_d, (size_t)N + 1));
+  CK(cudaMemsetAsync(node_tile, 0xff, (size_t)N * 4, ctx->stream));
+  launch_node_tiles(ctx->tiles, ctx->n_tiles, node_tile, ctx->stream);
+  launch_sym_count(d, ctx->tiles, node_tile, n_up, ctx->stream);
+  CK(cudaGetLastError());
+  std::vector<int64_t> up((size_t)N), scan((size_t)N + 1, 0);
+  CK(cudaMemcpyAsync(up.data(), n_up, (size_t)N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int64_t i = 0; i < N; i++) scan[i + 1] = scan[i] + up[i];
+  CK(cudaMemcpyAsync(scan_d, scan.data(), ((size_t)N + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+  launch_sym_fill(d, ctx->tiles, ctx->n_tiles, node_tile, scan_d, ctx->stream);
+  CK(cudaGetLastError());
+  std::vector<BondTile> t((size_t)ctx->n_tiles);
+  CK(cudaMemcpyAsync(t.data(), ctx->tiles, t.size() * sizeof(BondTile), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, n_up);
+  dfree(ctx, scan_d);
+  size_t need = 0;
+  for (auto &b : t) {
+    if (b.slots < 0 || b.slots > 65535) return PDGPU_OK;
+    need = std::max(need, tile_smem_mixed_main(2, ctx->hp[b.particle].material == PDGPU_MAT_PDSTATE, true, b, true));
+  }
+  const size_t limit = 227 * 1024 - 1024;
+  if (need > limit) return PDGPU_OK;
+  if (set_tile_smem_limit_mixed(2, std::max(need, ctx->tile_smem_pd)) != 0)
+    return fail(ctx, PDGPU_ERR_CUDA, "cannot raise the shared-memory limit to %zu bytes", need);
+  ctx->tile_smem_sym = need;
+  d.use_sym = 1;
+  return sym_bits(ctx);
+}
+
 // flags, BC tables, grid and contact buffers: done once before stepping
 int prepare(pdgpu_ctx *ctx) {
   if (ctx->prepared) return PDGPU_OK;
@@ -701,8 +771,10 @@ int prepare(pdgpu_ctx *ctx) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // one CTA per SM: the pass is latency-bound and runs beside the bond loop
-    d.contact_grid = sms > 0 ? sms : 148;
+    // four CTAs per SM: the pass is bound by the latency of its gathers (a
+    // cold L2 after every step), so it wants many candidates in flight; the
+    // CTAs that find no free slot beside the bond loop start as it drains
+    d.contact_grid = 4 * (sms > 0 ? sms : 148);
   }
   d.cr_blocks = d.contact_grid;
   TRY(dalloc(ctx, &d.cr_partial, (size_t)d.cr_blocks + 1));
@@ -812,6 +884,7 @@ int prepare(pdgpu_ctx *ctx) {
   ctx->state_prepass = !ctx->hp.empty() && ctx->hp[0].material == PDGPU_MAT_PDSTATE;
   if (d.precision == PDGPU_PREC_MIXED) TRY(prepare_mixed(ctx));
   TRY(prepare_tiles(ctx));
+  TRY(prepare_sym(ctx));
   ctx->prepared = true;
   return PDGPU_OK;
 }
@@ -833,7 +906,7 @@ void pd_forces(pdgpu_ctx *ctx) {
         launch_prepass_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
       });
   }
-  const size_t smem = ctx->tile_smem_pd;
+  const size_t smem = d.use_sym ? ctx->tile_smem_sym : ctx->tile_smem_pd;
   if (mixed)
     run(ctx, "pd_force_mixed", [&] {
       launch_pd_tiled_mixed(d, ctx->tiles, ctx->tile_law, ctx->pd_lanes, smem, s);
@@ -964,7 +1037,7 @@ cudaError_t graph_step(pdgpu_ctx *ctx, const char **where) {
     if (mixed) launch_prepass_mixed(d, ctx->tiles, ctx->tile_law, ctx->pd_lanes, ctx->tile_smem_pd, s);
     else launch_prepass_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, ctx->tile_smem, s);
   }
-  const size_t smem = ctx->tile_smem_pd;
+  const size_t smem = d.use_sym ? ctx->tile_smem_sym : ctx->tile_smem_pd;
   if (mixed) launch_pd_tiled_mixed(d, ctx->tiles, ctx->tile_law, ctx->pd_lanes, smem, s);
   else launch_pd_tiled_fp64(d, ctx->tiles, ctx->n_tiles, ctx->pd_lanes, smem, s);
   if (sur) {
@@ -1909,7 +1982,7 @@ int pdgpu_upload_field(pdgpu_ctx *ctx, int32_t field, const void *src) {
       if (b[k]) bits[k >> 5] |= 1u << (k & 31);
     CK(cudaMemcpyAsync(d.bond_bits, bits.data(), bits.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    return PDGPU_OK;
+    return sym_bits(ctx);
   }
   double *vec = field == PDGPU_FIELD_X ? d.x : field == PDGPU_FIELD_U ? d.u : field == PDGPU_FIELD_V ? d.v : nullptr;
   if (!vec) return fail(ctx, PDGPU_ERR_ARG, "upload_field: only x, u, v and bonds can be written");
@@ -2038,8 +2111,9 @@ int pdgpu_set_tuning(pdgpu_ctx *ctx, int32_t pd_lanes, int32_t contact_lanes) {
                     pd_lanes == 16 || pd_lanes == 32))
     return fail(ctx, PDGPU_ERR_ARG, "set_tuning: pd_lanes must be 4, 8, 16 or 32 (also 1 or 2 in the mixed form)");
   if (ctx->prepared && pd_lanes) return fail(ctx, PDGPU_ERR_STATE, "set_tuning: lanes are fixed once stepping starts");
-  if (contact_lanes && contact_lanes != 4 && contact_lanes != 8 && contact_lanes != 32)
-    return fail(ctx, PDGPU_ERR_ARG, "set_tuning: contact_lanes must be 4, 8 or 32");
+  if (contact_lanes && contact_lanes != 1 && contact_lanes != 2 && contact_lanes != 4 && contact_lanes != 8 &&
+      contact_lanes != 32)
+    return fail(ctx, PDGPU_ERR_ARG, "set_tuning: contact_lanes must be 1, 2, 4, 8 or 32");
   if (pd_lanes) ctx->pd_lanes = pd_lanes;
   if (contact_lanes) ctx->contact_lanes = contact_lanes;
   if (ctx->gexec) {
@@ -2053,6 +2127,20 @@ int pdgpu_set_tile_nodes(pdgpu_ctx *ctx, int32_t nodes) {
   if (!ctx || nodes < 0 || nodes > 4096) return PDGPU_ERR_ARG;
   if (ctx->prepared) return fail(ctx, PDGPU_ERR_STATE, "set_tile_nodes: tiles are fixed once stepping starts");
   ctx->tile_nodes = nodes;
+  return PDGPU_OK;
+}
+
+int pdgpu_set_bond_scheme(pdgpu_ctx *ctx, int32_t scheme) {
+  if (!ctx || (scheme != 0 && scheme != 1)) return PDGPU_ERR_ARG;
+  if (ctx->prepared) return fail(ctx, PDGPU_ERR_STATE, "set_bond_scheme: set it before the first step");
+  ctx->bond_scheme = scheme;
+  return PDGPU_OK;
+}
+
+int pdgpu_bond_scheme(pdgpu_ctx *ctx, int32_t *scheme) {
+  if (!ctx || !scheme) return PDGPU_ERR_ARG;
+  TRY(prepare(ctx));
+  *scheme = ctx->d.use_sym ? 0 : 1;
   return PDGPU_OK;
 }
 
@@ -2358,6 +2446,7 @@ int pdgpu_load_state(pdgpu_ctx *ctx, const char *path) {
     cudaGraphExecDestroy(ctx->gexec);
     ctx->gexec = nullptr;
   }
+  TRY(sym_bits(ctx));
   ctx->begun = true;
   return PDGPU_OK;
 }

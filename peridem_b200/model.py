@@ -145,7 +145,7 @@ class GpuDEMModel:
     def __init__(self, scene: Scene, precision: int = PREC_FP64, device: int = 0,
                  build_neighbors: bool = False, compute_mx: bool = False,
                  contact_capacity: int = 0, wall_pair_capacity: int = 0,
-                 pd_lanes: int = 0, tile_nodes: int = 0):
+                 pd_lanes: int = 0, tile_nodes: int = 0, bond_scheme: int = 0):
         self.lib = api.lib()
         self.scene = scene
         desc = api.Desc()
@@ -179,6 +179,8 @@ class GpuDEMModel:
             api.set_lanes(self, pd_lanes)
         if tile_nodes:
             self._check(self.lib.pdgpu_set_tile_nodes(self.ctx, tile_nodes))
+        if bond_scheme:
+            self._check(self.lib.pdgpu_set_bond_scheme(self.ctx, bond_scheme))
         self._upload(build_neighbors, compute_mx)
 
     # ---- DEMModel::init: upload ModelData -----------------------------------
@@ -375,6 +377,12 @@ class GpuDEMModel:
                                          "Particle_ID", "Zone_ID", "Fixity", "Nodal_Volume")) -> None:
         """DEMModel::output: the current state as a .vtu file (pdgpu_write_vtu)."""
         self._check(self.lib.pdgpu_write_vtu(self.ctx, path.encode(), ",".join(tags).encode()))
+
+    def bond_scheme(self) -> int:
+        """0: symmetric bond visits in the mixed 2-D loop, 1: every bond from both ends."""
+        v = ctypes.c_int32()
+        self._check(self.lib.pdgpu_bond_scheme(self.ctx, ctypes.byref(v)))
+        return v.value
 
     def save_state(self, path: str) -> None:
         """Snapshot of the whole step state, bond bits included (pdgpu_save_state)."""

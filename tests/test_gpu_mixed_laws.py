@@ -114,12 +114,56 @@ def test_mixed_force_on_smooth_deformation(law, dim, strain):
                              seed=1, material=law, piston_speed=-2.0, nt=10)
     sc = scn.build_scene(spec)
     u = _smooth_u(sc, strain)
+    bonds = _prebroken(sc)
+    _compare(f"{law} {dim}-D strain {strain:g}", sc, u, bonds)
+
+
+def _prebroken(sc, every=50):
+    """Every `every`-th bond broken, in both directions (as the reference's
+    bonds break), to exercise the broken-bond branch."""
     from peridem_b200.model import PREC_FP64
     m = _model(sc, PREC_FP64)
     try:
-        bonds = np.zeros(len(m.pd_neighbors()[1]), dtype=np.uint8)
+        rp, col = m.pd_neighbors()
     finally:
         m.close()
-    # pre-break every 50th bond to exercise the broken-bond branch
-    bonds[::50] = 1
-    _compare(f"{law} {dim}-D strain {strain:g}", sc, u, bonds)
+    rp = rp.astype(np.int64)
+    col = col.astype(np.int64)
+    bonds = np.zeros(len(col), dtype=np.uint8)
+    owner = np.repeat(np.arange(sc.n_nodes), np.diff(rp))
+    for k in range(0, len(col), every):
+        i, j = owner[k], col[k]
+        bonds[k] = 1
+        row = col[rp[j]:rp[j + 1]]
+        bonds[rp[j] + int(np.nonzero(row == i)[0][0])] = 1
+    return bonds
+
+
+@pytest.mark.parametrize("law", LAW_NAMES)
+def test_symmetric_bond_visits_match_per_node_visits(law):
+    """The mixed 2-D loop's two schemes on the same state: bond states and
+    damage identical (the same FP32 stretch from either end), forces equal
+    up to FP32 rounding of the sums (1e-5 of the largest)."""
+    from peridem_b200.model import GpuDEMModel, PREC_MIXED
+    sc = scn.build_scene(scn.compressive_2d(n_particles=12, r_range=(R, 1.3 * R), h_div=10, width=10e-3,
+                                            seed=4, material=law, nt=10))
+    u = _smooth_u(sc, 2e-2, seed=3)
+    bonds = _prebroken(sc, 37)
+    out = []
+    for scheme in (0, 1):
+        m = GpuDEMModel(sc, precision=PREC_MIXED, build_neighbors=True, compute_mx=True, bond_scheme=scheme)
+        try:
+            m.set_field("u", u)
+            m.set_field("bonds", bonds)
+            m.compute_pd_forces()
+            out.append((m.bond_scheme(), m.field("f"), m.field("Z"), m.field("bonds")))
+        finally:
+            m.close()
+    (s0, f0, z0, b0), (s1, f1, z1, b1) = out
+    assert (s0, s1) == (0, 1), "the symmetric scheme should apply to this 2-D scene"
+    assert np.array_equal(b0, b1), int(np.sum(b0 != b1))
+    assert np.array_equal(z0, z1), float(np.max(np.abs(z0 - z1)))
+    fmax = float(np.max(np.abs(f1)))
+    df = float(np.max(np.abs(f0 - f1))) / fmax
+    print(f"{law}: broken {int(b0.sum())} (pre-broken {int(bonds.sum())}), f {df:.2e}")
+    assert df <= 1e-5, df

@@ -3,7 +3,7 @@
 sets a scene up and steps it; the FP64 CUDA path starts from the same
 ModelData (same neighbour-list order) and must reproduce its state at every
 dump step within the tolerances of tests/parity.py (forces to 1e-12 after
-the prelude and the first step, 1e-11 later; bond flags and contact sets
+the prelude and the first step, 1e-10 later; bond flags and contact sets
 exactly).  The scenes cover the four bond laws, the three influence
 functions, both time schemes, every displacement and force boundary
 condition time function with the spatial factors, 2-D and 3-D.

@@ -187,3 +187,63 @@ def test_bench_algorithmic_bytes_are_layout_independent(dim):
     assert u64["bytes_per_node"] == 8 * dim * 3 + 8 + 8 + 4
     assert u32["bytes_per_node"] == 4 * dim * 2 + 8 + 8 + 8 * dim + 4
     assert b32 == 6 * 4.125 + 3 * u32["bytes_per_node"]
+
+
+@pytest.mark.parametrize("kind", ["RNPBond", "PMBBond", "PDElasticBond", "PDState"])
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("inf_type", [0, 1, 2])
+def test_library_deck_constants_equal_the_scene_builder_and_reference(kind, dim, inf_type):
+    """pdgpu_material_constants / pdgpu_influence_params (host functions of
+    the library, for bindings that hold only the decks) give the same bits as
+    the scene builder's restatement, which tests/test_scene.py pins to the
+    reference's own init."""
+    import ctypes
+    from peridem_b200 import api
+    from peridem_b200.model import MATERIAL_CODES
+    L = api.lib()
+    m = scn.elastic_material(kind, 2.0e9)
+    m.influence_type = inf_type
+    t, inf = scn.influence_params(m, dim)
+    out = (ctypes.c_double * 2)()
+    assert L.pdgpu_influence_params(inf_type, 0, None, dim, out) == 0
+    assert (t, float(inf[0]), float(inf[1])) == (inf_type, out[0], out[1])
+    for horizon in (3e-4, 1.234567e-4):
+        code, mat, Kp = scn.material_constants(m, dim, horizon, t, inf)
+        deck = api.MaterialDeck(law=MATERIAL_CODES[kind], irreversible=1 if m.irreversible else 0, E=m.E, K=m.K,
+                                G=m.G, nu=m.nu, Gc=m.Gc, check_sc_factor=m.check_sc_factor)
+        got = (ctypes.c_double * 6)()
+        kb = ctypes.c_double()
+        ip = (ctypes.c_double * 2)(*inf)
+        assert L.pdgpu_material_constants(ctypes.byref(deck), dim, horizon, t, ip, got, ctypes.byref(kb)) == 0
+        assert list(got) == [float(v) for v in mat], (kind, dim, inf_type)
+        assert kb.value == Kp
+
+
+def test_library_deck_constants_equal_the_reference_dump():
+    """The reference's own constants (dumped from its materials) for the
+    golden scenes: RNP, PMB, PD elastic and PD state, 2-D and 3-D."""
+    import ctypes
+    import golden_io
+    from peridem_b200 import api
+    L = api.lib()
+    kinds = {"tp6_rnp": "RNPBond", "tp6_pmb_impact": "PMBBond", "tp6_state": "PDState",
+             "tp6_pdelastic_verlet": "PDElasticBond", "col3_state": "PDState", "col3_rnp": "RNPBond"}
+    for name, kind in kinds.items():
+        init, _ = golden_io.load(name)
+        dim = int(init["dim"][0])
+        Np = int(init["Np"][0])
+        mp = init["p_mat_params"].reshape(Np, 8)
+        ip = (ctypes.c_double * 2)(*[float(v) for v in init["inf_params"][:2]])
+        for p in range(Np):
+            if int(init["p_type"][p]) != 0:
+                continue
+            deck = api.MaterialDeck(law=int(init["p_mat_type"][p]), irreversible=1, E=-1.0, K=-1.0, G=-1.0,
+                                    nu=-1.0, Gc=500.0, check_sc_factor=1.0)
+            E = 2.0e9 if name.startswith("tp6") else 5.0e9
+            deck.E, deck.K = E, E / (3.0 * (1.0 - 2.0 * 0.25))
+            got = (ctypes.c_double * 6)()
+            rc = L.pdgpu_material_constants(ctypes.byref(deck), dim, float(init["p_horizon"][p]),
+                                            int(init["inf_type"][0]), ip, got, None)
+            assert rc == 0
+            n = {0: 6, 1: 2, 2: 1, 3: 3}[int(init["p_mat_type"][p])]
+            assert list(got)[:n] == [float(v) for v in mp[p, :n]], (name, kind, p)

@@ -1,14 +1,10 @@
-"""The reference-side binding shown in INTEGRATION.md (a model::DEMModel
-subclass that drives libpdgpu) compiles against the reference's own headers
-and include/pdgpu.h: every C++ block of the document is extracted and
-syntax-checked with the include paths and shims the oracle build of the
-reference uses.  The binding asks the maintainer to make it a friend of the
-four bond-law classes (their constants are private); the test applies that
-same one-line change to a temporary copy of the material header, which it
-puts first on the include path.  Skipped where the reference sources are
-absent."""
+"""The C++ drop-in (peridem_b200/host/gpu_dem_model.h: model::GpuDEMModel,
+a subclass of the reference's model::DEMModel) compiles against the
+reference's unmodified headers and links with the reference's own objects
+and libpdgpu.so into pdgpu_peridem (peridem_b200/host/Makefile).  No GPU is
+needed to build it; tests/test_gpu_dropin.py runs it.  Skipped where the
+reference sources or its compiled objects are absent."""
 import os
-import re
 import shutil
 import subprocess
 import sys
@@ -19,42 +15,29 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 from __graft_entry__ import REF  # noqa: E402
 
-
-def _friend_material_header(dst):
-    """A copy of the reference's material header with `friend class
-    model::GpuDEMModel;` in each bond-law class, as INTEGRATION.md asks."""
-    src = os.path.join(REF, "src", "material", "mparticle", "material.h")
-    text = open(src).read()
-    text = text.replace('#include "influenceFn.h"', '#include "material/mparticle/influenceFn.h"', 1)
-    text = text.replace("namespace material {", "namespace model {\nclass GpuDEMModel;\n}\n\nnamespace material {", 1)
-    for cls in ("RnpMaterial", "PmbMaterial", "PdElastic", "PdState"):
-        head = f"class {cls} : public Material {{"
-        assert head in text, head
-        text = text.replace(head, head + "\n  friend class model::GpuDEMModel;", 1)
-    out = dst / "material" / "mparticle"
-    out.mkdir(parents=True)
-    (out / "material.h").write_text(text)
-    return str(dst)
-
-
-def _blocks():
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    return re.findall(r"```cpp\n(.*?)```", text, flags=re.S)
+OBJ = os.path.join(ROOT, "oracle", "_ref", "obj")
+LIB = os.path.join(ROOT, "peridem_b200", "_lib", "libpdgpu.so")
 
 
 @pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "src")), reason="reference sources absent")
+@pytest.mark.skipif(not os.path.isdir(OBJ), reason="reference objects absent (make -C oracle ref)")
+@pytest.mark.skipif(not os.path.exists(LIB), reason="libpdgpu.so not built")
 @pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
-def test_integration_binding_compiles(tmp_path):
-    blocks = _blocks()
-    assert blocks, "INTEGRATION.md holds no C++ block"
+def test_dropin_program_builds_against_the_unmodified_reference(tmp_path):
+    out = tmp_path / "pdgpu_peridem"
+    host = os.path.join(ROOT, "peridem_b200", "host")
+    objs = sorted(os.path.join(d, f) for d, _, fs in os.walk(OBJ) for f in fs
+                  if f.endswith(".o") and f != "ref_driver.o")
     shim = os.path.join(ROOT, "oracle", "shim")
-    friend = _friend_material_header(tmp_path / "friend")
-    for k, code in enumerate(blocks):
-        src = tmp_path / f"block{k}.cpp"
-        src.write_text(code)
-        cmd = ["g++", "-std=c++23", "-fsyntax-only", "-DFMT_HEADER_ONLY", "-w", "-I", friend,
-               "-I", shim, "-I", os.path.join(shim, "vtk"), "-I", os.path.join(REF, "src"),
-               "-I", os.path.join(REF, "external"), "-I", os.path.join(REF, "external", "fmt", "include"),
-               "-I", os.path.join(ROOT, "include"), "-x", "c++", str(src)]
-        r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
-        assert r.returncode == 0, r.stderr[-3000:]
+    cmd = ["g++", "-std=c++23", "-O1", "-DFMT_HEADER_ONLY", "-w", "-I", host, "-I", os.path.join(ROOT, "include"),
+           "-I", shim, "-I", os.path.join(shim, "vtk"), "-I", os.path.join(REF, "src"),
+           "-I", os.path.join(REF, "external"), "-I", os.path.join(REF, "external", "fmt", "include"),
+           "-o", str(out), os.path.join(host, "pdgpu_peridem.cpp"), *objs,
+           "-L", os.path.dirname(LIB), "-lpdgpu", "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert out.exists()
+    # the header asks nothing private of the reference: no friend declaration
+    # and no access-specifier override
+    text = open(os.path.join(host, "gpu_dem_model.h")).read()
+    assert "friend" not in text and "#define private" not in text
