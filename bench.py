@@ -103,6 +103,7 @@ def workload_config(args, sc):
                    "precision": args.precision, "l2": "flushed between timed steps (512 MiB write, then read back)",
                    "graph_steps_per_launch": args.graph_steps,
                    "pd_lanes": args.pd_lanes or "auto", "tile_nodes": args.tile_nodes or "auto",
+                   "contact_lanes": getattr(args, "contact_lanes", 0) or "auto",
                    "search_factor": sc.search_factor if sc is not None else None}
 
 
@@ -319,15 +320,25 @@ def run_ours(args, rank, world):
     torch.cuda.set_device(dev)
     sc = build_workload(args)
     prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
+    # untimed pre-run: the wall presses the packing; every arm starts from
+    # the state it reaches (a state snapshot)
+    snap, pre_s = None, 0.0
+    if args.prerun > 0:
+        snap, pre_s = prerun_state(sc, args, dev)
     tuned = None
     if args.autotune:
-        from peridem_b200.autotune import autotune
+        from peridem_b200.autotune import autotune, CONTACT_LANES
         t0 = time.perf_counter()
-        ch = autotune(sc, prec, steps=args.tune_steps, warmup=5, device=dev)
+        ch = autotune(sc, prec, steps=args.tune_steps, warmup=5, device=dev, contact_lanes=CONTACT_LANES,
+                      state=snap)
         args.pd_lanes, args.tile_nodes, sc.search_factor = ch.pd_lanes, ch.tile_nodes, ch.search_factor
+        args.contact_lanes = ch.contact_lanes
         tuned = {"seconds": round(time.perf_counter() - t0, 1), "candidates": ch.table}
     model = GpuDEMModel(sc, precision=prec, device=dev, build_neighbors=True, compute_mx=True,
                         pd_lanes=args.pd_lanes, tile_nodes=args.tile_nodes)
+    if args.contact_lanes:
+        from peridem_b200 import api
+        api.set_lanes(model, 0, args.contact_lanes)
     rp, col = model.pd_neighbors()
     sc.pd_rowptr, sc.pd_col = rp, col
     sur = None
@@ -350,7 +361,10 @@ def run_ours(args, rank, world):
         sur = {"train_seconds": round(t_train, 1),
                "shapes": [{"zone": S.zone, "nodes": S.n_nodes,
                            **{k: round(v, 5) for k, v in S.report.items()}} for S in model_s.shapes]}
-    model.integrate_begin()
+    if snap:
+        model.load_state(snap)
+    else:
+        model.integrate_begin()
     stream = torch.cuda.ExternalStream(model.stream_handle(), device=dev)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
@@ -389,20 +403,13 @@ def run_ours(args, rank, world):
             torch.cuda.synchronize()
         return [a.elapsed_time(b) for a, b in ev]
 
-    # untimed pre-run: the wall presses the packing before the timed window
-    snap = None
-    t_pre = time.perf_counter()
-    if args.prerun > 0:
-        with torch.cuda.stream(stream):
-            model.integrate_step(args.prerun, graph_steps=min(args.prerun, 500))
-            model.sync()
-    pre_s = time.perf_counter() - t_pre
-    if args.prerun > 0 and args.workload == "compressive":
-        snap = os.path.join(tempfile.mkdtemp(prefix="pdgpu_bench_"), "prerun.pdsnap")
-        model.save_state(snap)
     before = model.scalars()
+    if args.profile_window:
+        torch.cuda.profiler.start()  # cudaProfilerStart: a profiler started with it off sees the window only
     with ClockSampler(dev) as clk:
         step_ms = timed_window(model, stream)
+    if args.profile_window:
+        torch.cuda.profiler.stop()
     after = model.scalars()
     window = {"steps": [int(before["n"]) + args.warmup + 1, int(after["n"])],
               "contact_rebuilds": int(after["contact_updates"] - before["contact_updates"]),
@@ -423,6 +430,9 @@ def run_ours(args, rank, world):
     if mixed_end is not None:
         m64 = GpuDEMModel(sc, precision=PREC_FP64, device=dev, build_neighbors=True, compute_mx=True)
         try:
+            if args.contact_lanes:
+                from peridem_b200 import api
+                api.set_lanes(m64, 0, args.contact_lanes)
             if snap:
                 m64.load_state(snap)
             else:
@@ -436,6 +446,19 @@ def run_ours(args, rank, world):
                                                  window["steps"], sc.test_interval)
         finally:
             m64.close()
+    # the surrogate form against the same scene without it (mixed form):
+    # what the learned part gains or costs, and its error against FP64
+    if sur is not None:
+        m2 = GpuDEMModel(sc, precision=PREC_MIXED, device=dev, build_neighbors=True, compute_mx=True,
+                         pd_lanes=args.pd_lanes, tile_nodes=args.tile_nodes)
+        try:
+            m2.integrate_begin()
+            s2 = torch.cuda.ExternalStream(m2.stream_handle(), device=dev)
+            ms2 = max_over_ranks(float(sum(timed_window(m2, s2))), world, f"cuda:{dev}")
+            sur["without_surrogate_value"] = job_throughput(nodes, args.steps, world, ms2)
+            sur["speedup_of_surrogate"] = value / sur["without_surrogate_value"]
+        finally:
+            m2.close()
 
     # per-kernel device times over a second timed pass (same flush)
     model.enable_timing(True)
@@ -531,6 +554,23 @@ def cpu_reference(args, steps, warmup, load=None):
     raise RuntimeError("reference timing failed: " + r.stdout[-500:] + r.stderr[-500:])
 
 
+def prerun_state(sc, args, device=0):
+    """The untimed pre-run of the compression (mixed form, graph replay),
+    saved as a state snapshot; returns (path, seconds)."""
+    from peridem_b200.model import GpuDEMModel, PREC_MIXED
+    t0 = time.perf_counter()
+    m = GpuDEMModel(sc, precision=PREC_MIXED, device=device, build_neighbors=True, compute_mx=True)
+    try:
+        m.integrate_begin()
+        m.integrate_step(args.prerun, graph_steps=min(args.prerun, 500))
+        m.sync()
+        path = os.path.join(tempfile.mkdtemp(prefix="pdgpu_bench_"), "prerun.pdsnap")
+        m.save_state(path)
+    finally:
+        m.close()
+    return path, time.perf_counter() - t0
+
+
 def prerun_snapshot(args):
     """The state the timed window starts from, for the reference arm: the
     same untimed pre-run on the GPU (state preparation only; the reference's
@@ -543,17 +583,7 @@ def prerun_snapshot(args):
         import torch
         if not torch.cuda.is_available():
             return None, "from the deck's initial state (no GPU to run the pre-run)"
-        from peridem_b200.model import GpuDEMModel, PREC_MIXED
-        sc = build_workload(args)
-        m = GpuDEMModel(sc, precision=PREC_MIXED, build_neighbors=True, compute_mx=True)
-        try:
-            m.integrate_begin()
-            m.integrate_step(args.prerun, graph_steps=min(args.prerun, 500))
-            m.sync()
-            path = os.path.join(tempfile.mkdtemp(prefix="pdgpu_bench_"), "prerun.pdsnap")
-            m.save_state(path)
-        finally:
-            m.close()
+        path, _ = prerun_state(build_workload(args), args)
         return path, ("from the state after the %d-step pre-run of the compression (made on the GPU, "
                       "loaded by peridem_ref -load)" % args.prerun)
     except Exception as e:  # report, do not hide
@@ -586,6 +616,9 @@ def main():
     ap.add_argument("--prerun", type=int, default=20000,
                     help="untimed steps of the compression before the timed window (compressive "
                          "workload); the state they reach is what every arm times")
+    ap.add_argument("--contact-lanes", type=int, default=0, help="lanes per node in the contact pass (0 = auto)")
+    ap.add_argument("--profile-window", action="store_true",
+                    help="bracket the timed window with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--no-fp64", dest="fp64_arm", action="store_false",
                     help="skip the plain FP64 form on the same state (and the mixed form's error)")
     args = ap.parse_args()

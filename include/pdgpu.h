@@ -322,6 +322,16 @@ PDGPU_API int pdgpu_upload_field(pdgpu_ctx *ctx, int32_t field, const void *src)
  * block headers).  Blocking. */
 PDGPU_API int pdgpu_write_vtu(pdgpu_ctx *ctx, const char *path, const char *tags);
 
+/* DEMModel::output without stopping the step loop (no counterpart in the
+ * reference, whose output blocks): the state as of this call (in stream
+ * order) is copied on the device, downloaded on a stream of its own and
+ * written by a host thread to `path`, exactly as pdgpu_write_vtu would; the
+ * call returns at once and steps issued after it run meanwhile.  One file is
+ * in flight at a time (a second call waits for the first);
+ * pdgpu_output_wait waits for it and reports its status. */
+PDGPU_API int pdgpu_write_vtu_async(pdgpu_ctx *ctx, const char *path, const char *tags);
+PDGPU_API int pdgpu_output_wait(pdgpu_ctx *ctx);
+
 /* DEMModel::restart (demModel.cpp:84-102) with
  * rw::reader::VtkParticleReader::readNodes (vtkParticleReader.cpp:41-120):
  * reads the points (current positions), Displacement (else x - x_ref) and

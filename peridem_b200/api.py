@@ -72,6 +72,8 @@ SIGNATURES = {
     "pdgpu_upload_contact": [c_vp, c_i32, P(c_d), P(c_d), P(c_d), P(c_d), P(c_d)],
     "pdgpu_upload_pd_neighbors": [c_vp, P(c_u64), P(c_u64), P(c_u8)],
     "pdgpu_save_state": [c_vp, ctypes.c_char_p],
+    "pdgpu_write_vtu_async": [c_vp, ctypes.c_char_p, ctypes.c_char_p],
+    "pdgpu_output_wait": [c_vp],
     "pdgpu_mesh_size": [c_i32, P(c_d), c_i64, P(c_i64), P(c_i64), c_i64, P(c_d)],
     "pdgpu_influence_params": [c_i32, c_i32, P(c_d), c_i32, P(c_d)],
     "pdgpu_material_constants": [P(MaterialDeck), c_i32, c_d, c_i32, P(c_d), P(c_d), P(c_d)],

@@ -29,6 +29,7 @@ enum : int {
   DEV_ERR_CELL_OVERFLOW = 3,
   DEV_ERR_NONFINITE = 4,
   DEV_ERR_STAGE_TIMEOUT = 5,  // a bond tile's bulk copies did not complete
+  DEV_ERR_BARRIER_TIMEOUT = 6,  // a grid-wide barrier of the contact rebuild gave up
 };
 
 struct DevParticle {
@@ -87,6 +88,9 @@ struct CtrlState {
   // the surrogate is judged against it (every sur_interval-th step)
   int32_t sur_check;
   int32_t pad2;
+  // grid-wide barrier of the cooperative contact rebuild: arrivals of the
+  // current barrier and the barriers passed so far
+  uint32_t bar_count, bar_gen;
 };
 
 // Cell grid fixed at set-up; nodes outside are clamped to the border cells,

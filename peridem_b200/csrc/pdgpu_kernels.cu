@@ -588,10 +588,50 @@ __global__ void k_zero_cells(DevData d) {
 namespace cg = cooperative_groups;
 constexpr int kCoopBlock = 256;
 
+// Grid-wide barrier with a bounded wait: thread 0 of each block arrives on
+// a counter in the step-control state; the last to arrive resets it and
+// advances the generation the others poll.  All blocks of the cooperative
+// launch are resident, so the wait ends unless a block faulted; after
+// kBarTries polls the block records DEV_ERR_BARRIER_TIMEOUT and every block
+// leaves the rebuild at its next barrier (the step's later kernels see the
+// error word and do nothing).  Returns false when the rebuild must stop.
+constexpr unsigned kBarTries = 1u << 22;
+
+__device__ bool grid_bar(CtrlState *c) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = &c->bar_gen;
+    const unsigned g0 = *gen;
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(&c->bar_count, 1u) == gridDim.x - 1) {
+      atomicExch(&c->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&c->bar_gen, 1u);
+    } else {
+      unsigned t = 0;
+      while (*gen == g0) {
+        if (++t > kBarTries) {
+          ok = 0;
+          atomicCAS(&c->error, 0, DEV_ERR_BARRIER_TIMEOUT);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok && !((volatile int *)&c->error)[0];
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 // exclusive scan over the whole grid: out[i] = sum_{k<i} in(k) for
-// i = 0..n, each block scanning one contiguous chunk
+// i = 0..n, each block scanning one contiguous chunk; false when a barrier
+// gave up
 template <class Tout, class F>
-__device__ void grid_scan(cg::grid_group &g, F in, Tout *out, int64_t n, int64_t *bsum) {
+__device__ bool grid_scan(CtrlState *gc, F in, Tout *out, int64_t n, int64_t *bsum) {
   __shared__ int64_t wsum[kCoopBlock / 32];
   __shared__ int64_t carry;
   const int64_t nb = gridDim.x;
@@ -609,7 +649,7 @@ __device__ void grid_scan(cg::grid_group &g, F in, Tout *out, int64_t n, int64_t
     for (int w = 0; w < kCoopBlock / 32; w++) s += wsum[w];
     bsum[blockIdx.x] = s;
   }
-  g.sync();
+  if (!grid_bar(gc)) return false;
   if (threadIdx.x == 0) {
     int64_t s = 0;
     for (int64_t b = 0; b < blockIdx.x; b++) s += bsum[b];
@@ -638,7 +678,7 @@ __device__ void grid_scan(cg::grid_group &g, F in, Tout *out, int64_t n, int64_t
     __syncthreads();
   }
   if (blockIdx.x == nb - 1 && threadIdx.x == 0) out[n] = (Tout)carry;
-  g.sync();
+  return grid_bar(gc);
 }
 
 
@@ -865,7 +905,7 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
   extern __shared__ __align__(16) unsigned char cand_smem[];
   CandWarp<DIM> *stage = reinterpret_cast<CandWarp<DIM> *>(cand_smem);
   if (d.ctrl->error || !d.ctrl->update) return;
-  cg::grid_group g = cg::this_grid();
+  CtrlState *gc = d.ctrl;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nth = (int64_t)gridDim.x * blockDim.x;
   const int64_t N = d.n_nodes;
@@ -876,7 +916,7 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
   }
   if (d.sur_near_gate)
     for (int64_t p = tid; p < d.n_particles; p += nth) d.sur_near[p] = 0;
-  g.sync();
+  if (!grid_bar(gc)) return;
   for (int64_t i = tid; i < N; i += nth) {
     double p[3];
     ldv<DIM>(d.x, i, p);
@@ -884,14 +924,14 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
     d.cell_of[i] = c;
     atomicAdd(d.cell_cnt + c, 1);
   }
-  g.sync();
+  if (!grid_bar(gc)) return;
   const int32_t *cc = d.cell_cnt;
-  grid_scan<int32_t>(g, [cc](int64_t k) { return cc[k]; }, d.cell_start, G.ncells, bsum);
+  if (!grid_scan<int32_t>(gc, [cc](int64_t k) { return cc[k]; }, d.cell_start, G.ncells, bsum)) return;
   for (int64_t i = tid; i < N; i += nth) {
     const int c = d.cell_of[i];
     d.cell_tmp[d.cell_start[c] + atomicAdd(d.cell_fill + c, 1)] = (int32_t)i;
   }
-  g.sync();
+  if (!grid_bar(gc)) return;
   {
     const int lane = threadIdx.x & 31;
     for (int64_t c = tid >> 5; c < G.ncells; c += nth >> 5) {
@@ -904,12 +944,12 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
       }
     }
   }
-  g.sync();
+  if (!grid_bar(gc)) return;
   cand_cells<DIM, LPN, false>(d, search_bit, stage);
-  g.sync();
+  if (!grid_bar(gc)) return;
   const int64_t *cn = d.c_cnt;
-  grid_scan<int64_t>(g, [cn](int64_t k) { return cn[k]; }, d.c_row, N, bsum);
-  grid_scan<int64_t>(g, [cn](int64_t k) { return (int64_t)(cn[k] > 0); }, d.c_tmp, N, bsum);
+  if (!grid_scan<int64_t>(gc, [cn](int64_t k) { return cn[k]; }, d.c_row, N, bsum)) return;
+  if (!grid_scan<int64_t>(gc, [cn](int64_t k) { return (int64_t)(cn[k] > 0); }, d.c_tmp, N, bsum)) return;
   for (int64_t i = tid; i < N; i += nth)
     if (cn[i] > 0) {
       d.c_nodes[d.c_tmp[i]] = (int32_t)i;
@@ -917,7 +957,7 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
       if (d.sur_near_gate) d.sur_near[d.ptid[i]] = 1;  // every writer stores the same value
     }
   if (tid == 0) d.ctrl->c_nnodes = d.c_tmp[N];
-  g.sync();  // the compacted list is complete
+  if (!grid_bar(gc)) return;  // the compacted list is complete
   cand_fill_nodes<DIM>(d, d.c_tmp[N]);
   if (tid == 0) {
     const int64_t total = d.c_row[N];

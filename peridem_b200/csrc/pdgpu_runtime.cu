@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pdgpu_internal.h"
@@ -48,6 +49,7 @@ struct pdgpu_ctx {
   std::vector<double> xref;      // N*3
   std::vector<int32_t> ptid;     // N
   std::vector<uint8_t> fix;      // N
+  std::vector<double> vol_host;  // N, copied for output on first use
   std::vector<DevParticle> hp;   // particles
   std::vector<double> vmag0;     // initial |v|
   std::vector<uint8_t> ic_sel;   // per particle
@@ -109,6 +111,17 @@ struct pdgpu_ctx {
   double sur_err_gate = 0.05;
   cudaStream_t sur_stream = nullptr;
   cudaEvent_t ev_sur0 = nullptr, ev_sur1 = nullptr;
+
+  // asynchronous VTU output (pdgpu_write_vtu_async): a device copy of the
+  // state taken on the context stream, its download on out_stream into
+  // pinned buffers, the file written by out_thread
+  cudaStream_t out_stream = nullptr;
+  cudaEvent_t ev_out0 = nullptr, ev_out1 = nullptr;
+  double *out_dev = nullptr, *out_host = nullptr;  // [4 * stride * N + 2 * N + 1] doubles
+  size_t out_doubles = 0;
+  std::thread out_thread;
+  int out_rc = 0;
+  std::string out_err;
 
   // timing
   bool timing = false;
@@ -465,6 +478,9 @@ int device_error(pdgpu_ctx *ctx) {
     case DEV_ERR_STAGE_TIMEOUT:
       return fail(ctx, PDGPU_ERR_CUDA, "bond tile %lld: shared-memory bulk copies did not complete",
                   (long long)c.error_info);
+    case DEV_ERR_BARRIER_TIMEOUT:
+      return fail(ctx, PDGPU_ERR_CUDA, "contact-list rebuild: a grid-wide barrier gave up waiting (step %lld)",
+                  (long long)c.n);
     case DEV_ERR_NONFINITE:
       return fail(ctx, PDGPU_ERR_NAN, "weighted volume of node %lld is too close to zero",
                   (long long)c.error_info);
@@ -1157,6 +1173,11 @@ int pdgpu_create(const pdgpu_desc *desc, pdgpu_ctx **out) {
 void pdgpu_destroy(pdgpu_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->desc.device);
+  if (ctx->out_thread.joinable()) ctx->out_thread.join();
+  if (ctx->out_stream) cudaStreamDestroy(ctx->out_stream);
+  if (ctx->ev_out0) cudaEventDestroy(ctx->ev_out0);
+  if (ctx->ev_out1) cudaEventDestroy(ctx->ev_out1);
+  if (ctx->out_host) cudaFreeHost(ctx->out_host);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   if (ctx->branch) cudaStreamDestroy(ctx->branch);
@@ -1598,43 +1619,32 @@ bool has_tag(const std::string &tags, const char *tag) {
   return false;
 }
 
-std::string xml_attr(const std::string &tag, const char *key) {
-  const std::string k = std::string(key) + "=\"";
-  const size_t p = tag.find(k);
-  if (p == std::string::npos) return "";
-  const size_t q = tag.find('"', p + k.size());
-  return q == std::string::npos ? "" : tag.substr(p + k.size(), q - p - k.size());
-}
+// host copy of what one .vtu file holds (AoS util::Point arrays)
+struct VtuFrame {
+  int64_t n = 0;
+  double time = 0.;
+  std::vector<double> x, u, v, f, theta;
+  std::vector<float> Z;
+};
 
-}  // namespace
-
-extern "C" {
-
-int pdgpu_write_vtu(pdgpu_ctx *ctx, const char *path, const char *tags) {
-  if (!ctx || !path) return PDGPU_ERR_ARG;
-  if (!ctx->nodes || !ctx->particles) return fail(ctx, PDGPU_ERR_STATE, "write_vtu: no nodes");
-  const std::string T = tags ? tags : "";
-  const int64_t N = ctx->d.n_nodes;
-  std::vector<double> x(3 * N);
-  TRY(pdgpu_download(ctx, PDGPU_FIELD_X, x.data()));
+// The arrays of VtkParticleWriter::appendNodes (vtkParticleWriter.cpp:39-270),
+// in its order, as raw appended VTK XML.  Host work only (safe on another
+// thread: reads the frame and the context's constant host arrays).
+bool write_frame(const pdgpu_ctx *ctx, const VtuFrame &fr, const std::string &T, const char *path,
+                 std::string *err) {
+  const int64_t N = fr.n;
   std::vector<VtuArray> pdata;
-  auto vec3 = [&](int field, const char *name, bool times_vol) -> int {
-    std::vector<double> v(3 * N);
-    TRY(pdgpu_download(ctx, field, v.data()));
-    if (times_vol) {
-      std::vector<double> vol(N);
-      CK(cudaMemcpy(vol.data(), ctx->d.vol, N * 8, cudaMemcpyDeviceToHost));
+  auto vec3 = [&](const std::vector<double> &src, const char *name, bool times_vol) {
+    std::vector<double> v(src);
+    if (times_vol)
       for (int64_t i = 0; i < N; i++)
-        for (int q = 0; q < 3; q++) v[3 * i + q] *= vol[i];
-    }
+        for (int q = 0; q < 3; q++) v[3 * i + q] *= ctx->vol_host[i];
     pdata.push_back(vtu_array(name, "Float64", 3, v));
-    return PDGPU_OK;
   };
-  // the arrays of VtkParticleWriter::appendNodes (vtkParticleWriter.cpp:39-270), in its order
-  if (has_tag(T, "Displacement")) TRY(vec3(PDGPU_FIELD_U, "Displacement", false));
-  if (has_tag(T, "Velocity")) TRY(vec3(PDGPU_FIELD_V, "Velocity", false));
-  if (has_tag(T, "Force_Density")) TRY(vec3(PDGPU_FIELD_F, "Force_Density", false));
-  if (has_tag(T, "Force")) TRY(vec3(PDGPU_FIELD_F, "Force", true));
+  if (has_tag(T, "Displacement")) vec3(fr.u, "Displacement", false);
+  if (has_tag(T, "Velocity")) vec3(fr.v, "Velocity", false);
+  if (has_tag(T, "Force_Density")) vec3(fr.f, "Force_Density", false);
+  if (has_tag(T, "Force")) vec3(fr.f, "Force", true);
   if (has_tag(T, "Fixity")) {
     std::vector<double> v(N);
     for (int64_t i = 0; i < N; i++) v[i] = (double)ctx->fix[i];
@@ -1650,25 +1660,12 @@ int pdgpu_write_vtu(pdgpu_ctx *ctx, const char *path, const char *tags) {
     for (int64_t i = 0; i < N; i++) v[i] = (double)ctx->hp[ctx->ptid[i]].zone;
     pdata.push_back(vtu_array("Zone_ID", "Float64", 1, v));
   }
-  if (has_tag(T, "Nodal_Volume")) {
-    std::vector<double> v(N);
-    CK(cudaMemcpy(v.data(), ctx->d.vol, N * 8, cudaMemcpyDeviceToHost));
-    pdata.push_back(vtu_array("Nodal_Volume", "Float64", 1, v));
-  }
-  if (has_tag(T, "Damage_Z")) {
-    std::vector<float> z(N);
-    TRY(pdgpu_download(ctx, PDGPU_FIELD_Z, z.data()));
-    pdata.push_back(vtu_array("Damage_Z", "Float64", 1, std::vector<double>(z.begin(), z.end())));
-  }
-  if (has_tag(T, "Theta") && ctx->d.theta) {
-    std::vector<double> v(N);
-    TRY(pdgpu_download(ctx, PDGPU_FIELD_THETA, v.data()));
-    pdata.push_back(vtu_array("Theta", "Float64", 1, v));
-  }
-  pdgpu_scalars sc{};
-  TRY(pdgpu_get_scalars(ctx, &sc));
-  const VtuArray time = vtu_array("TIME", "Float64", 1, std::vector<double>{sc.time});
-  const VtuArray pts = vtu_array("Points", "Float64", 3, x);
+  if (has_tag(T, "Nodal_Volume")) pdata.push_back(vtu_array("Nodal_Volume", "Float64", 1, ctx->vol_host));
+  if (has_tag(T, "Damage_Z"))
+    pdata.push_back(vtu_array("Damage_Z", "Float64", 1, std::vector<double>(fr.Z.begin(), fr.Z.end())));
+  if (has_tag(T, "Theta") && !fr.theta.empty()) pdata.push_back(vtu_array("Theta", "Float64", 1, fr.theta));
+  const VtuArray time = vtu_array("TIME", "Float64", 1, std::vector<double>{fr.time});
+  const VtuArray pts = vtu_array("Points", "Float64", 3, fr.x);
   const VtuArray conn = vtu_array("connectivity", "Int64", 1, std::vector<int64_t>{});
   const VtuArray offs = vtu_array("offsets", "Int64", 1, std::vector<int64_t>{});
   const VtuArray types = vtu_array("types", "UInt8", 1, std::vector<uint8_t>{});
@@ -1705,7 +1702,10 @@ int pdgpu_write_vtu(pdgpu_ctx *ctx, const char *path, const char *tags) {
   for (size_t k = pdata.size() + 2; k < order.size(); k++) head += decl(k, -1);
   head += "</Cells>\n</Piece>\n</UnstructuredGrid>\n<AppendedData encoding=\"raw\">\n_";
   FILE *f = std::fopen(path, "wb");
-  if (!f) return fail(ctx, PDGPU_ERR_ARG, "write_vtu: cannot open %s", path);
+  if (!f) {
+    *err = std::string("cannot open ") + path;
+    return false;
+  }
   bool ok = std::fwrite(head.data(), 1, head.size(), f) == head.size();
   for (auto *a : order) {
     const uint64_t nb = a->bytes.size();
@@ -1715,7 +1715,160 @@ int pdgpu_write_vtu(pdgpu_ctx *ctx, const char *path, const char *tags) {
   const char *tail = "\n</AppendedData>\n</VTKFile>\n";
   ok = ok && std::fwrite(tail, 1, std::strlen(tail), f) == std::strlen(tail);
   ok = (std::fclose(f) == 0) && ok;
-  return ok ? PDGPU_OK : fail(ctx, PDGPU_ERR_ARG, "write_vtu: write to %s failed", path);
+  if (!ok) *err = std::string("write to ") + path + " failed";
+  return ok;
+}
+
+// the nodal volumes on the host (constant; copied once)
+int host_volumes(pdgpu_ctx *ctx) {
+  if ((int64_t)ctx->vol_host.size() == ctx->d.n_nodes) return PDGPU_OK;
+  ctx->vol_host.resize((size_t)ctx->d.n_nodes);
+  CK(cudaMemcpy(ctx->vol_host.data(), ctx->d.vol, (size_t)ctx->d.n_nodes * 8, cudaMemcpyDeviceToHost));
+  return PDGPU_OK;
+}
+
+std::string xml_attr(const std::string &tag, const char *key) {
+  const std::string k = std::string(key) + "=\"";
+  const size_t p = tag.find(k);
+  if (p == std::string::npos) return "";
+  const size_t q = tag.find('"', p + k.size());
+  return q == std::string::npos ? "" : tag.substr(p + k.size(), q - p - k.size());
+}
+
+}  // namespace
+
+extern "C" {
+
+int pdgpu_write_vtu(pdgpu_ctx *ctx, const char *path, const char *tags) {
+  if (!ctx || !path) return PDGPU_ERR_ARG;
+  if (!ctx->nodes || !ctx->particles) return fail(ctx, PDGPU_ERR_STATE, "write_vtu: no nodes");
+  const std::string T = tags ? tags : "";
+  const int64_t N = ctx->d.n_nodes;
+  VtuFrame fr;
+  fr.n = N;
+  fr.x.resize(3 * N);
+  TRY(pdgpu_download(ctx, PDGPU_FIELD_X, fr.x.data()));
+  if (has_tag(T, "Displacement")) {
+    fr.u.resize(3 * N);
+    TRY(pdgpu_download(ctx, PDGPU_FIELD_U, fr.u.data()));
+  }
+  if (has_tag(T, "Velocity")) {
+    fr.v.resize(3 * N);
+    TRY(pdgpu_download(ctx, PDGPU_FIELD_V, fr.v.data()));
+  }
+  if (has_tag(T, "Force_Density") || has_tag(T, "Force")) {
+    fr.f.resize(3 * N);
+    TRY(pdgpu_download(ctx, PDGPU_FIELD_F, fr.f.data()));
+  }
+  if (has_tag(T, "Damage_Z")) {
+    fr.Z.resize(N);
+    TRY(pdgpu_download(ctx, PDGPU_FIELD_Z, fr.Z.data()));
+  }
+  if (has_tag(T, "Theta") && ctx->d.theta) {
+    fr.theta.resize(N);
+    TRY(pdgpu_download(ctx, PDGPU_FIELD_THETA, fr.theta.data()));
+  }
+  TRY(host_volumes(ctx));
+  pdgpu_scalars sc{};
+  TRY(pdgpu_get_scalars(ctx, &sc));
+  fr.time = sc.time;
+  std::string err;
+  if (!write_frame(ctx, fr, T, path, &err)) return fail(ctx, PDGPU_ERR_ARG, "write_vtu: %s", err.c_str());
+  return PDGPU_OK;
+}
+
+int pdgpu_write_vtu_async(pdgpu_ctx *ctx, const char *path, const char *tags) {
+  if (!ctx || !path) return PDGPU_ERR_ARG;
+  if (!ctx->nodes || !ctx->particles) return fail(ctx, PDGPU_ERR_STATE, "write_vtu_async: no nodes");
+  // one file in flight: the previous one is finished first
+  TRY(pdgpu_output_wait(ctx));
+  TRY(host_volumes(ctx));
+  DevData &d = ctx->d;
+  const int64_t N = d.n_nodes;
+  const int64_t st = d.dim == 2 ? 2 : 4;
+  // staging layout in doubles: x, u, v, f (device node-vector layout),
+  // theta, Z (floats, packed), time
+  const size_t o_th = (size_t)(4 * st * N), o_z = o_th + (size_t)N, o_t = o_z + (size_t)(N + 1) / 2;
+  const size_t need = o_t + 1;
+  if (ctx->out_doubles < need) {
+    if (ctx->out_dev) dfree(ctx, ctx->out_dev);
+    if (ctx->out_host) cudaFreeHost(ctx->out_host);
+    ctx->out_host = nullptr;
+    ctx->out_doubles = 0;
+    TRY(dalloc(ctx, &ctx->out_dev, need));
+    CK(cudaMallocHost((void **)&ctx->out_host, need * 8));
+    ctx->out_doubles = need;
+  }
+  if (!ctx->out_stream) CK(cudaStreamCreateWithFlags(&ctx->out_stream, cudaStreamNonBlocking));
+  if (!ctx->ev_out0) CK(cudaEventCreateWithFlags(&ctx->ev_out0, cudaEventDisableTiming));
+  if (!ctx->ev_out1) CK(cudaEventCreateWithFlags(&ctx->ev_out1, cudaEventDisableTiming));
+  // the state as of now, in stream order on the context stream (a device
+  // copy: the steps issued next do not wait for the download or the file)
+  cudaStream_t s = ctx->stream;
+  const size_t vb = (size_t)(st * N) * 8;
+  double *o = ctx->out_dev;
+  CK(cudaMemcpyAsync(o, d.x, vb, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(o + st * N, d.u, vb, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(o + 2 * st * N, d.v, vb, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(o + 3 * st * N, d.f, vb, cudaMemcpyDeviceToDevice, s));
+  if (d.theta) CK(cudaMemcpyAsync(o + o_th, d.theta, (size_t)N * 8, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(o + o_z, d.Z, (size_t)N * 4, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(o + o_t, reinterpret_cast<const char *>(d.ctrl) + offsetof(CtrlState, time), 8,
+                     cudaMemcpyDeviceToDevice, s));
+  CK(cudaEventRecord(ctx->ev_out0, s));
+  CK(cudaStreamWaitEvent(ctx->out_stream, ctx->ev_out0, 0));
+  CK(cudaMemcpyAsync(ctx->out_host, o, need * 8, cudaMemcpyDeviceToHost, ctx->out_stream));
+  CK(cudaEventRecord(ctx->ev_out1, ctx->out_stream));
+  ctx->out_rc = PDGPU_OK;
+  ctx->out_err.clear();
+  const std::string P = path, T = tags ? tags : "";
+  const int dim = d.dim, dev = ctx->desc.device;
+  const bool has_theta = d.theta != nullptr;
+  ctx->out_thread = std::thread([ctx, P, T, N, st, dim, dev, has_theta, o_th, o_z, o_t]() {
+    cudaSetDevice(dev);
+    const cudaError_t e = cudaEventSynchronize(ctx->ev_out1);
+    if (e != cudaSuccess) {
+      ctx->out_rc = PDGPU_ERR_CUDA;
+      ctx->out_err = std::string("write_vtu_async: download failed: ") + cudaGetErrorString(e);
+      return;
+    }
+    const double *h = ctx->out_host;
+    VtuFrame fr;
+    fr.n = N;
+    fr.time = h[o_t];
+    auto aos = [&](int k, std::vector<double> *out) {
+      out->assign((size_t)(3 * N), 0.0);
+      const double *src = h + k * st * N;
+      for (int64_t i = 0; i < N; i++)
+        for (int q = 0; q < dim; q++) (*out)[3 * i + q] = src[st * i + q];
+    };
+    aos(0, &fr.x);
+    if (has_tag(T, "Displacement")) aos(1, &fr.u);
+    if (has_tag(T, "Velocity")) aos(2, &fr.v);
+    if (has_tag(T, "Force_Density") || has_tag(T, "Force")) aos(3, &fr.f);
+    if (has_tag(T, "Theta") && has_theta) fr.theta.assign(h + o_th, h + o_th + N);
+    if (has_tag(T, "Damage_Z")) {
+      const float *z = reinterpret_cast<const float *>(h + o_z);
+      fr.Z.assign(z, z + N);
+    }
+    std::string err;
+    if (!write_frame(ctx, fr, T, P.c_str(), &err)) {
+      ctx->out_rc = PDGPU_ERR_ARG;
+      ctx->out_err = "write_vtu_async: " + err;
+    }
+  });
+  return PDGPU_OK;
+}
+
+int pdgpu_output_wait(pdgpu_ctx *ctx) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  if (ctx->out_thread.joinable()) ctx->out_thread.join();
+  if (ctx->out_rc != PDGPU_OK) {
+    const int rc = ctx->out_rc;
+    ctx->out_rc = PDGPU_OK;
+    return fail(ctx, rc, "%s", ctx->out_err.c_str());
+  }
+  return PDGPU_OK;
 }
 
 int pdgpu_restart(pdgpu_ctx *ctx, const char *path, int64_t step) {
@@ -2415,6 +2568,7 @@ int pdgpu_load_state(pdgpu_ctx *ctx, const char *path) {
   c.error_info = 0;
   c.begin_done = c.end_done = 0;
   c.tile_next = c.tile_done = 0;
+  c.bar_count = 0;
   d.restart_step = -1;
   TRY(ul(ctx, d.x, x));
   TRY(ul(ctx, d.u, u));

@@ -393,6 +393,15 @@ class GpuDEMModel:
         integrate_begin (pdgpu_load_state)."""
         self._check(self.lib.pdgpu_load_state(self.ctx, path.encode()))
 
+    def write_vtu_async(self, path: str, tags=("Displacement", "Velocity", "Force", "Force_Density", "Damage_Z",
+                                              "Particle_ID", "Zone_ID", "Fixity", "Nodal_Volume")) -> None:
+        """write_vtu of the state as of now, written while later steps run
+        (pdgpu_write_vtu_async); output_wait() finishes it."""
+        self._check(self.lib.pdgpu_write_vtu_async(self.ctx, path.encode(), ",".join(tags).encode()))
+
+    def output_wait(self) -> None:
+        self._check(self.lib.pdgpu_output_wait(self.ctx))
+
     def restart(self, path: str, step: int) -> None:
         """DEMModel::restart from a file of write_vtu; before integrate_begin."""
         self._check(self.lib.pdgpu_restart(self.ctx, path.encode(), int(step)))

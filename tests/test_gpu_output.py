@@ -109,3 +109,31 @@ def test_restart_continues_the_run(tmp_path):
     assert sb["n"] == n + m_steps and abs(ta - tb) <= 1e-12 * ta
     assert float(np.max(np.abs(ha[:, 3]))) > 0, "the wall never touched the packing"
     assert eu <= 1e-10 and ev <= 1e-10
+
+
+def test_async_output_writes_the_state_of_its_call(tmp_path):
+    """pdgpu_write_vtu_async: the file holds the state as of the call, byte
+    for byte what pdgpu_write_vtu writes then, although steps run while it
+    is written."""
+    sc = _scene()
+    m = _model(sc)
+    try:
+        m.integrate_begin()
+        m.integrate_step(30)
+        a, b = str(tmp_path / "sync.vtu"), str(tmp_path / "async.vtu")
+        m.write_vtu(a)
+        m.write_vtu_async(b)
+        m.integrate_step(50)   # issued while the file is written
+        m.output_wait()
+        assert open(a, "rb").read() == open(b, "rb").read()
+        # a second call waits for nothing left over and writes the newer state
+        c = str(tmp_path / "async2.vtu")
+        m.write_vtu_async(c)
+        m.output_wait()
+        m.sync()
+        d = str(tmp_path / "sync2.vtu")
+        m.write_vtu(d)
+        assert open(c, "rb").read() == open(d, "rb").read()
+        assert open(a, "rb").read() != open(c, "rb").read()
+    finally:
+        m.close()

@@ -95,7 +95,7 @@ def test_autotune_descends_then_tries_skins(monkeypatch):
             (4, 128, 2.0): 0.8, (4, 128, 3.0): 0.95}
     seen = []
 
-    def fake(scene, precision, pd_lanes, tile_nodes, steps, warmup, device=0):
+    def fake(scene, precision, pd_lanes, tile_nodes, steps, warmup, device=0, contact_lanes=0, state=None):
         key = (pd_lanes, tile_nodes, float(scene.search_factor))
         seen.append(key)
         return cost.get(key, 2.0)
