@@ -215,16 +215,18 @@ def measured_peak():
 
 
 def traffic_from_profiles(kernel):
-    """dram bytes per launch recorded by an ncu capture summary in profiles/."""
-    for p in glob.glob(os.path.join(ROOT, "profiles", "*.md")):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    that an ncu capture summary in profiles/ recorded for `kernel`, and the
+    summary's file name; a recorded figure, not measured by this run."""
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
         with open(p) as fh:
             for line in fh:
                 if line.startswith(f"traffic_bytes_per_launch[{kernel}]:"):
                     try:
-                        return float(line.split(":", 1)[1].split()[0])
+                        return float(line.split(":", 1)[1].split()[0]), os.path.basename(p)
                     except ValueError:
                         pass
-    return None
+    return None, None
 
 
 def algorithmic_bytes(kernel, sc, precision):
@@ -508,10 +510,13 @@ def run_ours(args, rank, world):
         avg_s = ms / launches * 1e-3
         if bytes_:
             ach = bytes_ / avg_s / 1e9
+            # the committed ncu capture covers the default workload only
+            traffic, tsrc = traffic_from_profiles(name) if args.workload == "compressive" else (None, None)
             roof = {"kernel": name, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
                     "unit": "GB/s", "frac": round(ach / peak, 4), "peak_source": kind,
-                    # the committed ncu capture covers the default workload only
-                    "traffic": traffic_from_profiles(name) if args.workload == "compressive" else None,
+                    "traffic": traffic,
+                    "traffic_source": (f"recorded by the ncu capture summarised in profiles/{tsrc} "
+                                       "(not measured in this run)") if tsrc else None,
                     "avg_launch_us": round(avg_s * 1e6, 2),
                     "algorithmic_bytes_per_launch": int(bytes_), "units": units}
         else:

@@ -59,3 +59,21 @@ def test_softened_contact_stays_bounded_in_the_reference(tmp_path, dt):
     vmax = _run(tmp_path, dt, kn, int(round(3.0e-5 / dt / 20)) * 20)  # 30 us: through the impact
     print(f"dt {dt:.3e}:", ["%.2e" % v for v in vmax])
     assert max(vmax) < 1.0
+
+
+def test_config0_step_blows_up_in_the_reference_even_with_softened_contact(tmp_path):
+    """Config 0 (two discs, h = R/10) at its configured dt = 1e-7 s: even with
+    the softened contact spring the reference blows up within a few hundred
+    steps of contact, so config 0 runs at scene.stable_dt."""
+    h = R / 10
+    dt = 1e-7
+    spec = scn.two_particle(h_div=10, radius=R, material="RNPBond", v0=-0.1, gap=0.02 * h, nt=600, dt=dt)
+    for c in spec.contact.values():
+        c.kn = scn.stable_kn(1200.0, h * h, dt)
+        c.kn_factor = 1.0
+    scn.write_deck(spec, str(tmp_path))
+    dumps = list(range(100, 601, 100))
+    _, d = refrun.run_reference(str(tmp_path), 600, dumps)
+    vmax = [float(np.max(np.abs(d[k]["v"]))) for k in dumps]
+    print("config 0 step:", ["%.2e" % v for v in vmax])
+    assert max(vmax) > 1e3
