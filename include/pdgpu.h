@@ -402,6 +402,11 @@ PDGPU_API int pdgpu_download_pd_neighbors(pdgpu_ctx *ctx, uint64_t *rowptr, uint
  * Set before the first step. */
 PDGPU_API int pdgpu_set_tuning(pdgpu_ctx *ctx, int32_t pd_lanes, int32_t contact_lanes);
 
+/* CTAs per SM of the contact node pass (1..16, default 4); the pass runs
+ * beside the bond loop and is bound by the latency of its gathers.  Set
+ * before the first step. */
+PDGPU_API int pdgpu_set_contact_grid(pdgpu_ctx *ctx, int32_t ctas_per_sm);
+
 /* Nodes per bond-loop tile (one CTA each); 0 = automatic.  Set before the
  * first step; tiles shrink by themselves when a window outgrows shared
  * memory. */

@@ -78,6 +78,7 @@ SIGNATURES = {
     "pdgpu_influence_params": [c_i32, c_i32, P(c_d), c_i32, P(c_d)],
     "pdgpu_material_constants": [P(MaterialDeck), c_i32, c_d, c_i32, P(c_d), P(c_d), P(c_d)],
     "pdgpu_set_bond_scheme": [c_vp, c_i32],
+    "pdgpu_set_contact_grid": [c_vp, c_i32],
     "pdgpu_bond_scheme": [c_vp, P(c_i32)],
     "pdgpu_load_state": [c_vp, ctypes.c_char_p],
     "pdgpu_build_pd_neighbors": [c_vp],

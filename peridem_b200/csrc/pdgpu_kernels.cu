@@ -592,10 +592,17 @@ constexpr int kCoopBlock = 256;
 // a counter in the step-control state; the last to arrive resets it and
 // advances the generation the others poll.  All blocks of the cooperative
 // launch are resident, so the wait ends unless a block faulted; after
-// kBarTries polls the block records DEV_ERR_BARRIER_TIMEOUT and every block
-// leaves the rebuild at its next barrier (the step's later kernels see the
-// error word and do nothing).  Returns false when the rebuild must stop.
-constexpr unsigned kBarTries = 1u << 22;
+// kBarWaitNs of the GPU's global timer (far beyond any phase of a rebuild)
+// the block records DEV_ERR_BARRIER_TIMEOUT and every block leaves the
+// rebuild at its next barrier (the step's later kernels see the error word
+// and do nothing).  Returns false when the rebuild must stop.
+constexpr unsigned long long kBarWaitNs = 30ull * 1000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ bool grid_bar(CtrlState *c) {
   __shared__ int s_ok;
@@ -610,14 +617,17 @@ __device__ bool grid_bar(CtrlState *c) {
       __threadfence();
       atomicAdd(&c->bar_gen, 1u);
     } else {
-      unsigned t = 0;
+      const unsigned long long t0 = global_ns();
+      unsigned polls = 0;
       while (*gen == g0) {
-        if (++t > kBarTries) {
+        // the clock is read every 256 polls; the poll count is a second,
+        // clock-independent bound (2^31 polls of at least a few ns each)
+        if ((++polls & 255u) == 0 && (global_ns() - t0 > kBarWaitNs || polls > (1u << 31))) {
           ok = 0;
           atomicCAS(&c->error, 0, DEV_ERR_BARRIER_TIMEOUT);
           break;
         }
-        __nanosleep(64);
+        __nanosleep(128);
       }
     }
     __threadfence();

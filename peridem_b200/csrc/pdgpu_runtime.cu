@@ -66,6 +66,7 @@ struct pdgpu_ctx {
   void *scan_tmp = nullptr;
   size_t scan_bytes = 0;
   int pd_lanes = 0, contact_lanes = 4;
+  int contact_ctas = 4;  // CTAs per SM of the contact node pass
   int64_t *rebuild_bsum = nullptr;
   int rebuild_grid = 0;
   // tiled bond loop
@@ -790,7 +791,7 @@ int prepare(pdgpu_ctx *ctx) {
     // four CTAs per SM: the pass is bound by the latency of its gathers (a
     // cold L2 after every step), so it wants many candidates in flight; the
     // CTAs that find no free slot beside the bond loop start as it drains
-    d.contact_grid = 4 * (sms > 0 ? sms : 148);
+    d.contact_grid = ctx->contact_ctas * (sms > 0 ? sms : 148);
   }
   d.cr_blocks = d.contact_grid;
   TRY(dalloc(ctx, &d.cr_partial, (size_t)d.cr_blocks + 1));
@@ -2280,6 +2281,13 @@ int pdgpu_set_tile_nodes(pdgpu_ctx *ctx, int32_t nodes) {
   if (!ctx || nodes < 0 || nodes > 4096) return PDGPU_ERR_ARG;
   if (ctx->prepared) return fail(ctx, PDGPU_ERR_STATE, "set_tile_nodes: tiles are fixed once stepping starts");
   ctx->tile_nodes = nodes;
+  return PDGPU_OK;
+}
+
+int pdgpu_set_contact_grid(pdgpu_ctx *ctx, int32_t ctas_per_sm) {
+  if (!ctx || ctas_per_sm < 1 || ctas_per_sm > 16) return PDGPU_ERR_ARG;
+  if (ctx->prepared) return fail(ctx, PDGPU_ERR_STATE, "set_contact_grid: set it before the first step");
+  ctx->contact_ctas = ctas_per_sm;
   return PDGPU_OK;
 }
 

@@ -145,7 +145,8 @@ class GpuDEMModel:
     def __init__(self, scene: Scene, precision: int = PREC_FP64, device: int = 0,
                  build_neighbors: bool = False, compute_mx: bool = False,
                  contact_capacity: int = 0, wall_pair_capacity: int = 0,
-                 pd_lanes: int = 0, tile_nodes: int = 0, bond_scheme: int = 0):
+                 pd_lanes: int = 0, tile_nodes: int = 0, bond_scheme: int = 0,
+                 contact_lanes: int = 0, contact_ctas: int = 0):
         self.lib = api.lib()
         self.scene = scene
         desc = api.Desc()
@@ -181,6 +182,10 @@ class GpuDEMModel:
             self._check(self.lib.pdgpu_set_tile_nodes(self.ctx, tile_nodes))
         if bond_scheme:
             self._check(self.lib.pdgpu_set_bond_scheme(self.ctx, bond_scheme))
+        if contact_lanes:
+            api.set_lanes(self, 0, contact_lanes)
+        if contact_ctas:
+            self._check(self.lib.pdgpu_set_contact_grid(self.ctx, contact_ctas))
         self._upload(build_neighbors, compute_mx)
 
     # ---- DEMModel::init: upload ModelData -----------------------------------
