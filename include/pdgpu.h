@@ -412,10 +412,13 @@ PDGPU_API int pdgpu_set_contact_grid(pdgpu_ctx *ctx, int32_t ctas_per_sm);
  * memory. */
 PDGPU_API int pdgpu_set_tile_nodes(pdgpu_ctx *ctx, int32_t nodes);
 
-/* How the mixed-precision 2-D bond loop visits bonds (no counterpart in the
- * reference): 0 (default) evaluates a bond whose two nodes share a tile once
- * and hands the far node its share through shared memory (where rows and
- * tiles fit its 16-bit layout); 1 evaluates every bond from both ends.  Set
+/* How the mixed-precision bond loop visits bonds (no counterpart in the
+ * reference): 0 (default) evaluates every bond from both ends, a tile's
+ * nodes in node order; 2 the same with each tile's nodes taken longest row
+ * first (results identical to 0); 1 (2-D) evaluates a bond whose two nodes
+ * share a tile once and hands the far node its share through shared memory
+ * (where rows and tiles fit its 16-bit layout: fewer bond evaluations, but
+ * more shared memory per tile and a barrier between the two halves).  Set
  * before the first step.  pdgpu_bond_scheme reports the one in use (it
  * prepares the context). */
 PDGPU_API int pdgpu_set_bond_scheme(pdgpu_ctx *ctx, int32_t scheme);

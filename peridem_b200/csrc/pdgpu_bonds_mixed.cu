@@ -245,7 +245,9 @@ __device__ __forceinline__ void tile_nodes(const DevData &d, const BondTile &T, 
   const int shift = sizeof(CT) == 2 ? (int)(M.start - T.win_begin) : (int)(-T.win_begin);
   const bool gauss = d.inf.type == PDGPU_INF_GAUSSIAN;
   // every node of a tile computes forces (tiles cover force-computing particles only)
-  for (int64_t i = T.node_begin + threadIdx.x / LPN; i < T.node_end; i += kThreadsFor<DIM, LPN> / LPN) {
+  for (int64_t pos = T.node_begin + threadIdx.x / LPN; pos < T.node_end; pos += kThreadsFor<DIM, LPN> / LPN) {
+    // bond scheme 2: the tile's nodes longest row first
+    const int64_t i = d.node_order ? (int64_t)d.node_order[pos] : pos;
     const int k0 = (int)(s_row[i - p.row0] - kb), k1 = (int)(s_row[i + 1 - p.row0] - kb);
     const int li = (int)(i - T.win_begin);
     float xi[3], ui[3], vi;
@@ -257,7 +259,8 @@ __device__ __forceinline__ void tile_nodes(const DevData &d, const BondTile &T, 
     if (!any_broken<LPN>(s_bits, k0 + bit_off, k1 + bit_off, gm)) {
       // no bond of this node starts broken: no per-bond state test; four
       // bonds in flight per thread (measured: 17 % faster than two on a
-      // bond loop beyond L2, 9 % on config 1)
+      // bond loop beyond L2, 9 % on config 1; packed FP32x2 pairs of bonds
+      // measured 12 % slower on the 2-D compressive test)
 #pragma unroll 4
       for (int k = k0 + lane; k < k1; k += LPN)
         bond<DIM, LAW, true>(d, M, V, xi, ui, mi, (int)s_col[k + col_off] + shift, false, gauss,
@@ -329,7 +332,9 @@ __device__ __forceinline__ void tile_theta(const DevData &d, const BondTile &T, 
   const int bit_off = (int)(kb - 32 * p.word0);
   const int shift = sizeof(CT) == 2 ? (int)(M.start - T.win_begin) : (int)(-T.win_begin);
   const bool gauss = d.inf.type == PDGPU_INF_GAUSSIAN;
-  for (int64_t i = T.node_begin + threadIdx.x / LPN; i < T.node_end; i += kThreadsFor<DIM, LPN> / LPN) {
+  for (int64_t pos = T.node_begin + threadIdx.x / LPN; pos < T.node_end; pos += kThreadsFor<DIM, LPN> / LPN) {
+    // bond scheme 2: the tile's nodes longest row first
+    const int64_t i = d.node_order ? (int64_t)d.node_order[pos] : pos;
     const int k0 = (int)(s_row[i - p.row0] - kb), k1 = (int)(s_row[i + 1 - p.row0] - kb);
     const int li = (int)(i - T.win_begin);
     float xi[3], ui[3], vi;

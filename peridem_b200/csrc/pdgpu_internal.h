@@ -257,6 +257,10 @@ struct DevData {
   uint16_t *sym_col, *sym_pos;
   uint2 *sym_meta;
   int32_t use_sym;
+  // mixed bond loop, per-node form: position p of a tile processes node
+  // node_order[p], the tile's nodes ordered by row length, longest first
+  // (null: node order)
+  int32_t *node_order;
   MixParticle *mixp;
   float4 *xv_mixed;  // per node {x, y, z, vol}: reference coordinates minus the centre's, FP32
   int32_t use16;

@@ -75,7 +75,7 @@ struct pdgpu_ctx {
   size_t tile_smem = 0, tile_smem_state = 0;  // pre-pass stage; FP64 bond loop with m_x, theta
   size_t tile_smem_pd = 0;                     // the bond-loop launch
   size_t tile_smem_sym = 0;                    // the symmetric bond-loop launch (mixed, 2-D)
-  int bond_scheme = 0;                         // 0: symmetric where it applies, 1: per node
+  int bond_scheme = 0;  // 0: per node, 1: symmetric where it applies, 2: per node longest row first
   int32_t *node_tile = nullptr;                // per node its bond tile (-1: none), symmetric form
   int tile_law[5] = {0, 0, 0, 0, 0};           // tiles of law m: [tile_law[m], tile_law[m + 1])
   int64_t tile_nodes = 0;  // nodes per tile (0 = chosen at set-up)
@@ -657,6 +657,32 @@ int prepare_tiles(pdgpu_ctx *ctx) {
               "order each particle's nodes spatially");
 }
 
+// Bond scheme 2: the per-node mixed bond loop walks each tile's nodes longest
+// row first (stable), so the lanes of a warp have rows of similar length
+// where in node order the short rows of a particle's rim idle the lanes
+// beside them.  Each node's own sum is untouched, so results do not change.
+// (On the 2-D compressive test node order measured ~5 % faster: the order
+// scatters a warp's node records across the staged window.)
+int prepare_order(pdgpu_ctx *ctx) {
+  DevData &d = ctx->d;
+  if (d.precision != PDGPU_PREC_MIXED || d.use_sym || ctx->bond_scheme != 2 || ctx->n_tiles == 0)
+    return PDGPU_OK;
+  const int64_t N = d.n_nodes;
+  std::vector<int64_t> row((size_t)N + 1);
+  CK(cudaMemcpy(row.data(), d.pd_row, ((size_t)N + 1) * 8, cudaMemcpyDeviceToHost));
+  std::vector<BondTile> t((size_t)ctx->n_tiles);
+  CK(cudaMemcpy(t.data(), ctx->tiles, t.size() * sizeof(BondTile), cudaMemcpyDeviceToHost));
+  std::vector<int32_t> order((size_t)N);
+  for (int64_t i = 0; i < N; i++) order[i] = (int32_t)i;
+  for (const auto &b : t)
+    std::stable_sort(order.begin() + b.node_begin, order.begin() + b.node_end, [&](int32_t a, int32_t c) {
+      return row[a + 1] - row[a] > row[c + 1] - row[c];
+    });
+  if (!d.node_order) TRY(dalloc(ctx, &d.node_order, (size_t)N));
+  CK(cudaMemcpy(d.node_order, order.data(), (size_t)N * 4, cudaMemcpyHostToDevice));
+  return PDGPU_OK;
+}
+
 // both directions of a bond between two nodes of one tile share their broken
 // state in the symmetric form (see k_sym_bits)
 int sym_bits(pdgpu_ctx *ctx) {
@@ -674,7 +700,7 @@ int sym_bits(pdgpu_ctx *ctx) {
 int prepare_sym(pdgpu_ctx *ctx) {
   DevData &d = ctx->d;
   d.use_sym = 0;
-  if (d.precision != PDGPU_PREC_MIXED || d.dim != 2 || !d.use16 || ctx->bond_scheme != 0 || ctx->n_tiles == 0)
+  if (d.precision != PDGPU_PREC_MIXED || d.dim != 2 || !d.use16 || ctx->bond_scheme != 1 || ctx->n_tiles == 0)
     return PDGPU_OK;
   const int64_t N = d.n_nodes;
   std::vector<int64_t> row((size_t)N + 1);
@@ -902,6 +928,7 @@ int prepare(pdgpu_ctx *ctx) {
   if (d.precision == PDGPU_PREC_MIXED) TRY(prepare_mixed(ctx));
   TRY(prepare_tiles(ctx));
   TRY(prepare_sym(ctx));
+  TRY(prepare_order(ctx));
   ctx->prepared = true;
   return PDGPU_OK;
 }
@@ -2292,7 +2319,7 @@ int pdgpu_set_contact_grid(pdgpu_ctx *ctx, int32_t ctas_per_sm) {
 }
 
 int pdgpu_set_bond_scheme(pdgpu_ctx *ctx, int32_t scheme) {
-  if (!ctx || (scheme != 0 && scheme != 1)) return PDGPU_ERR_ARG;
+  if (!ctx || scheme < 0 || scheme > 2) return PDGPU_ERR_ARG;
   if (ctx->prepared) return fail(ctx, PDGPU_ERR_STATE, "set_bond_scheme: set it before the first step");
   ctx->bond_scheme = scheme;
   return PDGPU_OK;
@@ -2301,7 +2328,7 @@ int pdgpu_set_bond_scheme(pdgpu_ctx *ctx, int32_t scheme) {
 int pdgpu_bond_scheme(pdgpu_ctx *ctx, int32_t *scheme) {
   if (!ctx || !scheme) return PDGPU_ERR_ARG;
   TRY(prepare(ctx));
-  *scheme = ctx->d.use_sym ? 0 : 1;
+  *scheme = ctx->d.use_sym ? 1 : (ctx->d.node_order ? 2 : 0);
   return PDGPU_OK;
 }
 

@@ -384,7 +384,8 @@ class GpuDEMModel:
         self._check(self.lib.pdgpu_write_vtu(self.ctx, path.encode(), ",".join(tags).encode()))
 
     def bond_scheme(self) -> int:
-        """0: symmetric bond visits in the mixed 2-D loop, 1: every bond from both ends."""
+        """Mixed bond loop: 0 every bond from both ends, node order; 1 symmetric
+        bond visits (2-D); 2 every bond from both ends, nodes longest row first."""
         v = ctypes.c_int32()
         self._check(self.lib.pdgpu_bond_scheme(self.ctx, ctypes.byref(v)))
         return v.value

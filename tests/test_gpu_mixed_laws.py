@@ -160,10 +160,32 @@ def test_symmetric_bond_visits_match_per_node_visits(law):
         finally:
             m.close()
     (s0, f0, z0, b0), (s1, f1, z1, b1) = out
-    assert (s0, s1) == (0, 1), "the symmetric scheme should apply to this 2-D scene"
+    assert (s0, s1) == (0, 1), "the symmetric scheme should apply to this 2-D scene when asked"
     assert np.array_equal(b0, b1), int(np.sum(b0 != b1))
     assert np.array_equal(z0, z1), float(np.max(np.abs(z0 - z1)))
     fmax = float(np.max(np.abs(f1)))
     df = float(np.max(np.abs(f0 - f1))) / fmax
     print(f"{law}: broken {int(b0.sum())} (pre-broken {int(bonds.sum())}), f {df:.2e}")
     assert df <= 1e-5, df
+
+
+def test_row_length_order_leaves_results_unchanged():
+    """The per-node loop in node order (scheme 0, the default) against the
+    row-length order (scheme 2): each node sums its own row in the same order
+    either way, so 300 steps of a compression agree to the bit."""
+    from peridem_b200.model import GpuDEMModel, PREC_MIXED
+    sc = scn.build_scene(scn.compressive_2d(n_particles=12, r_range=(R, 1.3 * R), h_div=10, width=10e-3,
+                                            seed=4, nt=10, wall_speed=-2.0))
+    out = []
+    for scheme in (0, 2):
+        m = GpuDEMModel(sc, precision=PREC_MIXED, build_neighbors=True, compute_mx=True, bond_scheme=scheme)
+        try:
+            m.integrate_begin()
+            m.integrate_step(300, graph_steps=50)
+            m.sync()
+            out.append((m.bond_scheme(), m.field("f"), m.field("u"), m.field("Z"), m.field("bonds")))
+        finally:
+            m.close()
+    assert (out[0][0], out[1][0]) == (0, 2)
+    for a, b in zip(out[0][1:], out[1][1:]):
+        assert np.array_equal(a, b)
