@@ -94,9 +94,10 @@ def workload_config(args, sc):
                 "spheres": args.spheres, "sphere_nodes": force}
     else:
         head = {"workload": "2-D compressive test, %d discs/hexagons R~U[1,1.5] mm, h=R/15, "
-                            "horizon 3h, RNPBond, top wall 0.1 m/s, seeded ballistic-deposition packing; "
-                            "timed from the state after an untimed %d-step pre-run of the compression"
-                            % (args.particles, args.prerun),
+                            "horizon 3h, RNPBond, top wall 0.1 m/s, seeded ballistic deposition of the "
+                            "particles' nodes; timed from the state after an untimed pre-run of the "
+                            "compression: %d steps, then 10-step strides until the top wall touches the "
+                            "packing" % (args.particles, args.prerun),
                 "particles": args.particles, "prerun_steps": args.prerun}
     return head | {"nodes": int(sc.n_nodes) if sc is not None else None,
                    "dt": sc.dt if sc is not None else None,
@@ -326,7 +327,7 @@ def run_ours(args, rank, world):
     # the state it reaches (a state snapshot)
     snap, pre_s = None, 0.0
     if args.prerun > 0:
-        snap, pre_s = prerun_state(sc, args, dev)
+        snap, pre_s, pre_steps, pre_touch = prerun_state(sc, args, dev)
     tuned = None
     if args.autotune:
         from peridem_b200.autotune import autotune, CONTACT_LANES
@@ -396,6 +397,9 @@ def run_ours(args, rank, world):
             torch.cuda.synchronize()
             ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                   for _ in range(args.steps)]
+            # hold the stream (untimed) while the host queues every timed
+            # step, so that no event pair brackets host launch latency
+            torch.cuda._sleep(int(min(2e6 * args.steps, 1e9)))
             for k in range(args.steps):
                 flush_l2(flush, k)
                 ev[k][0].record(s)
@@ -418,6 +422,16 @@ def run_ours(args, rank, world):
               "contact_entries": int(after["contact_entries"]),
               "contact_reaction": after["contact_reaction"], "reaction": after["reaction"],
               "max_velocity": after["max_velocity"], "prerun_seconds": round(pre_s, 2)}
+    if snap:
+        window.update({"prerun_steps": pre_steps, "wall_in_contact_at_start": bool(pre_touch)})
+    if sc.test_interval > 0 and args.workload == "compressive":
+        # the compressive-test records of the timed steps: how many carry a
+        # contact reaction on the wall, and its largest magnitude
+        hist = model.history()
+        nwin = max(1, args.steps // sc.test_interval)
+        cr = hist[-nwin:, 3] if len(hist) else np.zeros(0)
+        window.update({"test_records": int(len(cr)), "records_with_wall_contact": int(np.sum(cr != 0.0)),
+                       "wall_contact_reaction_max_abs": float(np.max(np.abs(cr))) if len(cr) else 0.0})
     mixed_end = None
     if prec == PREC_MIXED and args.fp64_arm:
         mixed_end = {"hist": model.history(), "bonds": model.field("bonds"), "Z": model.field("Z"),
@@ -560,8 +574,12 @@ def cpu_reference(args, steps, warmup, load=None):
 
 
 def prerun_state(sc, args, device=0):
-    """The untimed pre-run of the compression (mixed form, graph replay),
-    saved as a state snapshot; returns (path, seconds)."""
+    """The untimed pre-run of the compression (mixed form, graph replay):
+    args.prerun steps, then, for the compressive test, 10-step strides until
+    the top wall is in contact with the packing (a non-zero contact reaction
+    in the latest test record; at most args.prerun_contact_cap more steps),
+    so that the timed window starts under the wall's load.  Saved as a state
+    snapshot; returns (path, seconds, steps run, wall in contact)."""
     from peridem_b200.model import GpuDEMModel, PREC_MIXED
     t0 = time.perf_counter()
     m = GpuDEMModel(sc, precision=PREC_MIXED, device=device, build_neighbors=True, compute_mx=True)
@@ -569,11 +587,20 @@ def prerun_state(sc, args, device=0):
         m.integrate_begin()
         m.integrate_step(args.prerun, graph_steps=min(args.prerun, 500))
         m.sync()
+        steps, touching = args.prerun, False
+        if args.workload == "compressive":
+            while True:
+                touching = m.scalars()["contact_reaction"] != 0.0
+                if touching or steps - args.prerun >= args.prerun_contact_cap:
+                    break
+                m.integrate_step(10, graph_steps=10)
+                m.sync()
+                steps += 10
         path = os.path.join(tempfile.mkdtemp(prefix="pdgpu_bench_"), "prerun.pdsnap")
         m.save_state(path)
     finally:
         m.close()
-    return path, time.perf_counter() - t0
+    return path, time.perf_counter() - t0, steps, touching
 
 
 def prerun_snapshot(args):
@@ -588,9 +615,10 @@ def prerun_snapshot(args):
         import torch
         if not torch.cuda.is_available():
             return None, "from the deck's initial state (no GPU to run the pre-run)"
-        path, _ = prerun_state(build_workload(args), args)
+        path, _, steps, touching = prerun_state(build_workload(args), args)
         return path, ("from the state after the %d-step pre-run of the compression (made on the GPU, "
-                      "loaded by peridem_ref -load)" % args.prerun)
+                      "loaded by peridem_ref -load; top wall %s)"
+                      % (steps, "in contact" if touching else "not in contact"))
     except Exception as e:  # report, do not hide
         return None, f"from the deck's initial state (pre-run failed: {e})"
 
@@ -620,7 +648,10 @@ def main():
     ap.add_argument("--tune-steps", type=int, default=100)
     ap.add_argument("--prerun", type=int, default=20000,
                     help="untimed steps of the compression before the timed window (compressive "
-                         "workload); the state they reach is what every arm times")
+                         "workload), continued until the top wall touches the packing; the state "
+                         "they reach is what every arm times")
+    ap.add_argument("--prerun-contact-cap", type=int, default=60000,
+                    help="at most this many more pre-run steps waiting for the top wall's contact")
     ap.add_argument("--contact-lanes", type=int, default=0, help="lanes per node in the contact pass (0 = auto)")
     ap.add_argument("--profile-window", action="store_true",
                     help="bracket the timed window with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
@@ -678,7 +709,8 @@ def main():
                             "them box walls)" % int(r["nodes"]))
                 elif res.get("snapshot"):
                     what = ("the same scene from the GPU's state after the %d-step pre-run (x, u, v, broken "
-                            "bonds, step and contact control loaded by peridem_ref -load)" % args.prerun)
+                            "bonds, step and contact control loaded by peridem_ref -load)"
+                            % res["window"].get("prerun_steps", args.prerun))
                 else:
                     what = "the same scene"
                 cpu = {"value": r["node_steps_per_s"], "unit": UNIT, "cores": r["threads"],

@@ -420,36 +420,62 @@ def two_particle(h_div: int = 10, radius: float = 1e-3, material: str = "RNPBond
                      ic_velocity=(0.0, v0, 0.0), ic_particles=[1])
 
 
-def deposit_2d(radii: np.ndarray, width: float, gap: float, rng: np.random.Generator,
-               trials: int = 8) -> np.ndarray:
-    """Seeded ballistic deposition of circles (radii) into a box of the given
-    width with a floor at y = 0: circle k falls straight down at a random x
-    (of `trials` draws, the one where it comes to rest lowest) until it
-    rests, at clearance `gap`, on the floor or on the first circle placed
-    before it that it meets.  Side walls at x = 0 and x = width keep the same
-    clearance.  Every circle thus rests on a support below it (a connected
-    chain down to the floor), and no two circles come closer than `gap`.
-    Returns the centres [n, 2]."""
-    n = len(radii)
-    r = np.asarray(radii, dtype=np.float64)
-    cen = np.zeros((n, 2))
-    for k in range(n):
-        best_y, best_x = math.inf, 0.0
-        for x in rng.uniform(gap + r[k], width - gap - r[k], size=trials):
-            y = gap + r[k]
-            if k:
-                dx = x - cen[:k, 0]
-                reach = r[k] + r[:k] + gap
-                near = np.abs(dx) < reach
-                if np.any(near):
-                    # falling from above it stops at the first circle it
-                    # meets: the highest of its resting heights on the
-                    # circles within reach (at or above it, it clears all)
-                    lift = cen[:k, 1][near] + np.sqrt(reach[near] ** 2 - dx[near] ** 2)
-                    y = max(y, float(lift.max()))
-            if y < best_y:
-                best_y, best_x = y, x
+def deposit_2d(offsets: Sequence[np.ndarray], x_lim: Tuple[float, float], floor: np.ndarray, gap: float,
+               rng: np.random.Generator, trials: int = 8) -> np.ndarray:
+    """Seeded ballistic deposition of rigid node sets: body k (node offsets
+    [n_k, 2] from its centre, already rotated and scaled) falls straight down
+    at a random x (of `trials` draws, the one where it comes to rest lowest)
+    until one of its nodes comes within `gap` of a node below it: of the
+    floor nodes `floor` [m, 2] or of a body placed before it.  Every node
+    keeps `gap` from the side walls' inner node columns x_lim = (x_left,
+    x_right).  No two nodes of different bodies start closer than `gap`,
+    and every body rests on the floor or on a body below it, at a clearance
+    of at most gap (1 + 1/64).
+
+    The heights come from an upper envelope of the placed nodes over bins
+    gap/64 wide (per bin its highest node), tested at the widened clearance
+    gap (1 + 1/64): a node lower in the same bin, at most one bin width
+    aside, cannot stop the body higher than the bin's top node does, so
+    the clearance is never below `gap`.  Returns the centres [n, 2]."""
+    w = gap / 64.0
+    ge = gap + w
+    x0 = x_lim[0]
+    nb = int(math.ceil((x_lim[1] - x0) / w)) + 1
+    top_y = np.full(nb, -np.inf)
+    top_x = np.zeros(nb)
+
+    def add(pts):
+        b = np.clip(((pts[:, 0] - x0) / w).astype(np.int64), 0, nb - 1)
+        order = np.lexsort((pts[:, 1], b))
+        b, y, x = b[order], pts[order, 1], pts[order, 0]
+        last = np.r_[b[1:] != b[:-1], True]          # the highest node of each bin
+        b, y, x = b[last], y[last], x[last]
+        up = y > top_y[b]
+        top_y[b[up]] = y[up]
+        top_x[b[up]] = x[up]
+
+    add(np.asarray(floor, dtype=np.float64))
+    m = int(math.ceil(ge / w)) + 1
+    span = np.arange(-m, m + 1)
+    cen = np.zeros((len(offsets), 2))
+    for k, off in enumerate(offsets):
+        off = np.asarray(off, dtype=np.float64)
+        lo = x_lim[0] + gap - float(off[:, 0].min())
+        hi = x_lim[1] - gap - float(off[:, 0].max())
+        if hi < lo:
+            raise ValueError("box too narrow for one particle")
+        xs = rng.uniform(lo, hi, size=trials)
+        xa = xs[:, None] + off[None, :, 0]                      # [trials, nodes]
+        bins = np.clip(((xa - x0) / w).astype(np.int64)[..., None] + span, 0, nb - 1)
+        dx = top_x[bins] - xa[..., None]
+        ty = top_y[bins]
+        ok = (np.abs(dx) < ge) & np.isfinite(ty)
+        lift = np.where(ok, ty - off[None, :, 1, None] + np.sqrt(np.maximum(ge * ge - dx * dx, 0.0)), -np.inf)
+        ys = lift.reshape(trials, -1).max(axis=1)
+        t = int(np.argmin(ys))                                  # the lowest rest (first on ties)
+        best_x, best_y = float(xs[t]), float(ys[t])
         cen[k] = (best_x, best_y)
+        add(cen[k] + off)
     return cen
 
 
@@ -459,7 +485,8 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
                    dt: Optional[float] = None, nt: int = 50000, gravity: float = -10.0,
                    search_factor: float = 5.0, search_interval: int = 40,
                    friction: bool = True, gap: Optional[float] = None,
-                   jitter: float = 0.5, packing: str = "lattice") -> SceneSpec:
+                   jitter: float = 0.5, packing: str = "lattice",
+                   contact_omega_dt: float = 0.3) -> SceneSpec:
     """2-D compression: discs and hexagons (50/50) inside a fixed frame,
     pressed by a top wall moving at ``wall_speed``.  One reference mesh per
     shape at h = R_ref/h_div, scaled per particle, so every particle has the
@@ -471,15 +498,21 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
     radius 0.95 h_min, so nothing starts in contact).
 
     packing "deposit": ballistic deposition (``deposit_2d``) of the
-    particles' bounding circles at clearance ``gap`` (default 0.96 h_min,
-    just beyond the contact radius 0.95 h_min): every particle rests on the
-    floor or on a particle below it, so the wall's load reaches the floor
-    through chains of supports, and no node pair of two bodies starts inside
-    the contact radius (contacts open as the wall presses instead of as
-    preloaded penalty springs).  The top wall starts ``gap`` above the
-    highest node.
+    particles' own nodes at clearance ``gap`` (default 0.96 h_min, just
+    beyond the contact radius 0.95 h_min): each particle falls until one of
+    its nodes comes within ``gap`` of a node of the floor or of a particle
+    below it, so every particle rests on a support, the wall's load reaches
+    the floor through chains of supports, and the packing closes its
+    remaining clearances (each support's at most gap (1 + 1/64), under
+    3 % of h beyond the contact radius) early in the run under gravity.  No node pair of
+    two bodies starts inside the contact radius (contacts open as the
+    packing settles and the wall presses instead of as preloaded penalty
+    springs).  The top wall starts ``gap`` above the highest node.
 
-    With the lattice the top wall starts ``gap`` above the highest particle."""
+    With the lattice the top wall starts ``gap`` above the highest particle.
+
+    The contact stiffness Kn is ``scene.stable_kn`` at omega dt =
+    ``contact_omega_dt`` for a node pair of the smallest mesh size."""
     rng = np.random.default_rng(seed)
     r_ref = r_range[0]
     h_ref = r_ref / h_div
@@ -514,7 +547,21 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
     sites_by_shape = {0: [], 1: []}
     top = 0.0
     if packing == "deposit":
-        cen = deposit_2d(radii, width, gap, rng)
+        # the frame's floor nodes and inner wall columns, as built below
+        # (they do not depend on the frame's height)
+        probe, _ = box_mesh([-t_wall, -t_wall], [width + t_wall, 4.0 * t_wall + 2.0 * h_min], h_min, 2,
+                            hole_lo=[0.5 * h_min, 0.5 * h_min], hole_hi=[width - 0.5 * h_min, 1.0])
+        side = probe[:, 1] > 0.5 * h_min
+        x_lim = (float(probe[side & (probe[:, 0] < 0.5 * width), 0].max()),
+                 float(probe[side & (probe[:, 0] > 0.5 * width), 0].min()))
+        floor = probe[~side][:, :2]
+        meshes = {0: _csv_array(disc_n), 1: _csv_array(hex_n)}
+        offsets = []
+        for p in range(n_particles):
+            scale = csv_float(_f(radii[p])) / r_ref
+            rot = _rotate_z(meshes[int(shapes[p])], csv_float(_f(orients[p])))
+            offsets.append(scale * rot[:, :2])
+        cen = deposit_2d(offsets, x_lim, floor, gap, rng)
     for p in range(n_particles):
         if packing == "deposit":
             cx, cy = float(cen[p, 0]), float(cen[p, 1])
@@ -526,11 +573,7 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
             cx, cy = cx + jx, cy + jy
         sites_by_shape[int(shapes[p])].append(((cx, cy, 0.0), float(radii[p]), float(orients[p])))
         if packing == "deposit":
-            # the highest node of the placed particle (scaled, rotated mesh)
-            mesh = disc_n if shapes[p] == 0 else hex_n
-            o = float(orients[p])
-            ys = cy + (radii[p] / r_ref) * (math.sin(o) * mesh[:, 0] + math.cos(o) * mesh[:, 1])
-            top = max(top, float(ys.max()))
+            top = max(top, cy + float(offsets[p][:, 1].max()))
         else:
             top = max(top, cy + radii[p])
     height = top + gap
@@ -556,7 +599,7 @@ def compressive_2d(n_particles: int = 502, r_range: Tuple[float, float] = (1e-3,
     zones.append(ZoneSpec("top_wall", True, "rectangle",
                           [bar_lo[0], bar_lo[1], 0.0, bar_hi[0], bar_hi[1], 0.0],
                           bar_n, bar_v, wall_mat, all_dofs_constrained=True))
-    kn = stable_kn(1200.0, h_min * h_min, dt)
+    kn = stable_kn(1200.0, h_min * h_min, dt, contact_omega_dt)
     c = ContactSpec(radius_factor=0.95, kn=kn, kn_factor=1.0, epsilon=0.7,
                     friction_on=friction, friction_coeff=0.5, damping_on=True, betan_factor=1.0)
     wall_fixed, wall_moving = n_particles, n_particles + 1

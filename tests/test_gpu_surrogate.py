@@ -9,10 +9,12 @@
 * in the step, on deformed particles: the device chain (gather, tensor-core
   GEMMs, lift) judged against the bond loop on the first check step, with
   and without the network.
-* in the step, over a run: under load, with the surrogate carrying the
-  particles the load has not reached, the wall's contact reaction stays
-  within 1e-3 of the FP64 form; on a loose packing the surrogate carries
-  most particle-steps without changing the result.
+* in the step, over a run: under load (repeated impacts on the moving
+  wall) the wall's contact impulse of perturbed surrogate runs matches that
+  of perturbed FP64 runs as an ensemble (impacts amplify any difference, a
+  1e-9 one included, to O(1) within ~150 steps, so single runs are not
+  comparable pointwise); on a loose packing the surrogate carries most
+  particle-steps without changing the result.
 """
 import numpy as np
 import pytest
@@ -157,27 +159,61 @@ def test_surrogate_chain_on_deformed_particles():
     assert np.median(e_mlp) < np.median(e_lin)
 
 
-def test_gated_surrogate_keeps_the_wall_reaction():
+def _impulse_ensemble(sc, prec, seeds, sur=None, steps=3000, at=1000):
+    """Per seed: the run with v scaled by (1 + 1e-6 noise) at step `at`
+    (seed 0: unperturbed); returns the wall's contact impulse (sum of the
+    contact-reaction records), the number of non-zero records and, with the
+    surrogate, its statistics of the unperturbed run."""
+    from peridem_b200.model import GpuDEMModel
+    imp, loaded, stats = [], [], None
+    for seed in seeds:
+        m = GpuDEMModel(sc, precision=prec, build_neighbors=True, compute_mx=True)
+        try:
+            if sur is not None:
+                sur.attach(m, check_interval=50, near_gate=True)
+            m.integrate_begin()
+            m.integrate_step(at, graph_steps=50)
+            m.sync()
+            if seed:
+                v = m.field("v")
+                rng = np.random.default_rng(seed)
+                m.set_field("v", v * (1.0 + 1e-6 * rng.standard_normal(v.shape)))
+            m.integrate_step(steps - at, graph_steps=50)
+            m.sync()
+            h = m.history()
+            imp.append(float(np.sum(h[:, 3])))
+            loaded.append(int(np.sum(h[:, 3] != 0)))
+            if sur is not None and seed == 0:
+                stats = m.surrogate_stats()
+        finally:
+            m.close()
+    return np.array(imp), loaded, stats
+
+
+def test_gated_surrogate_keeps_the_wall_impulse():
     """Compression under load with the surrogate carrying part of it: 24
-    particles (a column of about eight layers, lattice gaps 1.02 h), the wall at 2 m/s for 3000
-    steps, contact search radius equal to the contact radius (skin 1).  The
-    wall loads the top layers; their particles gain contact candidates and
-    the proximity gate keeps them on the bond loop, while the particles the
-    load has not reached stay on the surrogate.  The surrogate carries at
-    least a fifth of all particle-steps, and the contact reaction on the
-    wall stays within 1e-3 of the FP64 form's over the whole run."""
+    particles (a column of about eight layers, lattice gaps 1.02 h), the
+    wall at 2 m/s for 3000 steps, contact search radius equal to the contact
+    radius (skin 1).  The particles fall onto the wall from step ~1270 on and
+    keep striking it; particles with contact candidates stay on the bond
+    loop, the rest on the surrogate.  Four runs each of FP64 and of
+    mixed+surrogate, three of them with the velocities perturbed by 1e-6
+    (relative) before the first impact: the mean contact impulse on the wall
+    agrees within three standard errors (plus 5 % of the FP64 mean), and the
+    surrogate carries at least a fifth of all particle-steps."""
     from peridem_b200.model import PREC_FP64, PREC_MIXED
     sc = _scene(7, 24, 1.02, sf=1.0)
-    h64, u64, _ = _run(sc, PREC_FP64, 3000)
-    hs, us, st = _run(sc, PREC_MIXED, 3000, sur=_trained())
-    den = float(np.max(np.abs(h64[:, 3])))
-    err = float(np.max(np.abs(hs[:, 3] - h64[:, 3]))) / den
+    seeds = (0, 1, 2, 3)
+    i64, l64, _ = _impulse_ensemble(sc, PREC_FP64, seeds)
+    isur, lsur, st = _impulse_ensemble(sc, PREC_MIXED, seeds, sur=_trained())
     frac = st[2] / st[3]
-    loaded = int(np.sum(np.abs(h64[:, 3]) > 0))
-    print(f"contact reaction max {den:.3e} (non-zero in {loaded} of {len(h64)} records), rel err {err:.2e}; "
+    m64, msur = float(np.mean(i64)), float(np.mean(isur))
+    se = float(np.sqrt((np.var(i64, ddof=1) + np.var(isur, ddof=1)) / len(seeds)))
+    print(f"FP64 impulses {np.round(i64, 1)} (records with contact {l64}); surrogate {np.round(isur, 1)} "
+          f"({lsur}); mean {m64:.4e} vs {msur:.4e}, standard error {se:.3e}; "
           f"particle-steps on the surrogate {st[2]}/{st[3]} ({frac:.3f})")
-    assert den > 0, "the wall never touched the packing"
-    assert err <= 1e-3
+    assert min(l64) > 0 and min(lsur) > 0, "the wall never touched the packing"
+    assert abs(msur - m64) <= 3.0 * se + 0.05 * abs(m64)
     assert st[3] == 3000 * st[1]
     assert frac >= 0.2, "the surrogate should carry the particles the load has not reached"
 

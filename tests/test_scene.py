@@ -62,26 +62,18 @@ def test_compressive_packing_has_no_overlap():
 
 
 def test_deposit_packing_is_settled_and_clear():
-    """Ballistic deposition: no two bounding circles closer than the
-    clearance, each circle resting on the floor or on a circle placed before
-    it (clearance within 1e-9 relative), the top wall just above the highest
-    node, and no node pair of two bodies inside the contact radius."""
+    """Ballistic deposition of the particles' nodes: no node pair of two
+    bodies (walls included) closer than the clearance gap = 0.96 h, so none
+    inside the contact radius; every particle resting on the floor or on a
+    particle below it (its closest node pair to the floor or to another body
+    within gap (1 + 1/64)); the side walls kept at the clearance; the top
+    wall the clearance above the highest node."""
     import math
     import numpy as np
     from scipy.spatial import cKDTree
     from peridem_b200 import scene as scn
-    rng = np.random.default_rng(3)
-    r = rng.uniform(1e-3, 1.5e-3, 60)
-    gap = 1e-5
-    c = scn.deposit_2d(r, 12e-3, gap, rng)
-    d = np.sqrt(((c[:, None, :] - c[None, :, :]) ** 2).sum(-1)) - r[:, None] - r[None, :]
-    np.fill_diagonal(d, np.inf)
-    assert d.min() >= gap * (1 - 1e-9)
-    for k in range(len(r)):
-        on_floor = abs(c[k, 1] - (r[k] + gap)) <= 1e-9 * r[k]
-        on_lower = np.any(np.abs(d[k, :k] - gap) <= 1e-9 * r[k])
-        assert on_floor or on_lower, k
-    assert np.all(c[:, 0] - r >= gap * (1 - 1e-9)) and np.all(c[:, 0] + r <= 12e-3 - gap * (1 - 1e-9))
+    h = 1e-3 / 15
+    gap = 0.96 * h
     spec = scn.compressive_2d(n_particles=40, width=12e-3, seed=1, packing="deposit", nt=10)
     sc = scn.build_scene(spec)
     walls = [p for p in range(sc.n_particles) if sc.p_type[p] == 1]
@@ -89,8 +81,22 @@ def test_deposit_packing_is_settled_and_clear():
     parts = [p for p in range(sc.n_particles) if sc.p_type[p] == 0]
     ymax = max(float(sc.xref[sc.p_start[p]:sc.p_end[p], 1].max()) for p in parts)
     wall_low = float(sc.xref[sc.p_start[top]:sc.p_end[top], 1].min())
-    h = 1e-3 / 15
-    assert math.isclose(wall_low - ymax, 0.96 * h, rel_tol=1e-6)
+    assert math.isclose(wall_low - ymax, gap, rel_tol=1e-6)
     pt = np.asarray(sc.ptid, dtype=np.int64)
-    pairs = cKDTree(sc.xref[:, :2]).query_pairs(float(np.max(sc.c_rc)), output_type="ndarray")
+    tree = cKDTree(sc.xref[:, :2])
+    pairs = tree.query_pairs(gap * (1 - 1e-9), output_type="ndarray")
     assert not np.any(pt[pairs[:, 0]] != pt[pairs[:, 1]])
+    frame = walls[0]
+    for p in parts:
+        a, b = int(sc.p_start[p]), int(sc.p_end[p])
+        # closest node of another body (the top wall excluded: it starts above all)
+        others = np.nonzero((pt != p) & (pt != top))[0]
+        d, _ = cKDTree(sc.xref[others, :2]).query(sc.xref[a:b, :2])
+        assert gap * (1 - 1e-9) <= d.min() <= gap * (1 + 1 / 64) * (1 + 1e-9), (p, d.min() / h)
+    fx = sc.xref[sc.p_start[frame]:sc.p_end[frame]]
+    inner = fx[fx[:, 1] > 0.5 * h]
+    x_left = inner[inner[:, 0] < 6e-3, 0].max()
+    x_right = inner[inner[:, 0] > 6e-3, 0].min()
+    xs = np.concatenate([sc.xref[sc.p_start[p]:sc.p_end[p], 0] for p in parts])
+    assert xs.min() - x_left >= gap * (1 - 1e-9) and x_right - xs.max() >= gap * (1 - 1e-9)
+
