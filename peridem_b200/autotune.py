@@ -38,7 +38,7 @@ LANES = {"mixed": (1, 2, 4), "fp64": (4, 8, 32)}
 TILES = (128, 256, 512, 1024)
 CONTACT_LANES = (1, 2, 4, 8)
 SKINS = (2.0, 3.0, 5.0)
-DEFAULT_CONTACT_LANES = 4
+DEFAULT_CONTACT_LANES = 1
 
 
 @dataclasses.dataclass

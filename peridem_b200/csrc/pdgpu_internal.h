@@ -189,10 +189,13 @@ struct DevData {
 
   // contact candidates (CSR)
   double max_contact_r, search_factor;
+  double rc_max;  // largest contact radius of the zone-pair table (the contact pass's distance pre-filter)
   int64_t search_interval;
   int64_t contact_cap;
   int64_t *c_row;
   int32_t *c_col;
+  int32_t *c_own;  // per candidate entry: its node (written with c_col)
+  uint8_t *c_hit;  // per candidate entry, this step: inside the largest contact radius
   int64_t *c_cnt;  // per-node candidate counts of the last rebuild
   int64_t *c_tmp;  // N+1 scratch for the compaction scan
   int32_t *c_nodes;  // nodes with candidates, ascending
@@ -349,6 +352,7 @@ int set_tile_smem_limit_fp64(int dim, size_t bytes);
 int set_tile_smem_limit_mixed(int dim, size_t bytes);
 
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s);
+void launch_contact_owner(const DevData &d, cudaStream_t s);
 int rebuild_grid_blocks(const DevData &d, int lanes);
 cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, int lanes, int init,
                                    cudaStream_t s);

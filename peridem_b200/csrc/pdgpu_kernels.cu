@@ -872,6 +872,7 @@ __device__ void cand_fill_nodes(const DevData &d, int64_t nn) {
     const int32_t pi = d.ptid[i];
     int64_t out = d.c_row[i];
     const int64_t out_end = d.c_row[i + 1];
+    for (int64_t e = out + l32; e < out_end && e < d.contact_cap; e += 32) d.c_own[e] = i;
     const int cx0 = cell_coord<DIM>(q[0], G, 0), cy0 = cell_coord<DIM>(q[1], G, 1);
     const int cz0 = DIM == 3 ? cell_coord<DIM>(q[2], G, 2) : 0;
     for (int nb = 0; nb < kNb; nb++) {
@@ -978,6 +979,41 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
 }
 
 // ---------------------------------------------------------------------------
+// Distance pass ahead of the contact node pass: one thread per candidate
+// entry marks the entries inside the largest contact radius of the zone-pair
+// table (R < rc_max; every pair the node pass can accept, is_less(R, rc),
+// has R < rc <= rc_max, and R is computed by the same operations there).
+// Flat over the entries, so each thread carries one gather chain instead of
+// a node's whole candidate row.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_contact_near(DevData d) {
+  if (d.ctrl->error) return;
+  const int64_t E = d.ctrl->entries < d.contact_cap ? d.ctrl->entries : d.contact_cap;
+  const double rmax = d.rc_max;
+  for (int64_t e = (int64_t)blockIdx.x * kBlock + threadIdx.x; e < E; e += (int64_t)gridDim.x * kBlock) {
+    const int32_t i = d.c_own[e], j = d.c_col[e];
+    double yi[3], yj[3], yji[3];
+    ldv<DIM>(d.x, i, yi);
+    ldv<DIM>(d.x, j, yj);
+#pragma unroll
+    for (int q = 0; q < 3; q++) yji[q] = yj[q] - yi[q];
+    d.c_hit[e] = len3<DIM>(yji) < rmax ? 1 : 0;
+  }
+}
+
+// the node of every candidate entry, from the compacted lists (after a
+// state snapshot restores them)
+__global__ void k_contact_owner(DevData d) {
+  const int64_t nn = d.ctrl->c_nnodes;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nn; t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t i = d.c_nodes[t];
+    const int2 sp = d.c_span[t];
+    for (int64_t e = sp.x; e < sp.y && e < d.contact_cap; e++) d.c_own[e] = i;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Node pass of DEMModel::computeContactForces (demModel.cpp:832-934):
 // penalty normal force + Coulomb-type friction for candidates inside the
 // zone-pair contact radius; f_i += sum.  Particle-wall pairs inside the
@@ -1040,18 +1076,22 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
     ldv<DIM>(d.v, i, vi);
     double fx = 0.0, fy = 0.0, fz = 0.0, crd = 0.0;
     for (int k = sp.x + lane; k < sp.y; k += LPN) {
+      // most candidates lie in the search skin, beyond every zone pair's
+      // contact radius: k_contact_near marked the others
+      if (!d.c_hit[k]) continue;
       const int32_t j = d.c_col[k];
-      double yj[3], vj[3];
+      double yj[3];
       ldv<DIM>(d.x, j, yj);
+      double yji[3];
+#pragma unroll
+      for (int q = 0; q < 3; q++) yji[q] = yj[q] - yi[q];
+      const double R = len3<DIM>(yji);
+      double vj[3];
       ldv<DIM>(d.v, j, vj);
       const double volj = d.vol[j];
       const int32_t pj = d.ptid[j];
       const int zj = d.nzone[j];
       const bool wall = (d.flags[j] & NODE_WALL) != 0;
-      double yji[3];
-#pragma unroll
-      for (int q = 0; q < 3; q++) yji[q] = yj[q] - yi[q];
-      const double R = len3<DIM>(yji);
       const ContactPair cp = tab ? cps[zi * nz + zj] : d.contact[zi * nz + zj];
       if (is_less(R, cp.rc)) {
         double vji[3], en[3], et[3];
@@ -1732,7 +1772,25 @@ cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, in
   return lanes <= 8 ? rebuild_dim<3, 8>(d, bit, bsum, grid, s) : rebuild_dim<3, 32>(d, bit, bsum, grid, s);
 }
 
+int sm_count() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+void launch_contact_owner(const DevData &d, cudaStream_t s) {
+  k_contact_owner<<<sm_count() * 4, kBlock, 0, s>>>(d);
+}
+
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s) {
+  // the distance pass: eight CTAs per SM, grid-stride over the entries
+  if (d.dim == 2) k_contact_near<2><<<sm_count() * 8, kBlock, 0, s>>>(d);
+  else k_contact_near<3><<<sm_count() * 8, kBlock, 0, s>>>(d);
   const unsigned g = (unsigned)d.contact_grid;
   if (d.dim == 2) {
     if (lanes == 1) k_contact<2, 1><<<g, kBlock, 0, s>>>(d);

@@ -65,7 +65,7 @@ struct pdgpu_ctx {
   double *stage = nullptr;  // N*3 AoS staging
   void *scan_tmp = nullptr;
   size_t scan_bytes = 0;
-  int pd_lanes = 0, contact_lanes = 4;
+  int pd_lanes = 0, contact_lanes = 1;
   int contact_ctas = 4;  // CTAs per SM of the contact node pass
   int64_t *rebuild_bsum = nullptr;
   int rebuild_grid = 0;
@@ -900,6 +900,8 @@ int prepare(pdgpu_ctx *ctx) {
     d.contact_cap = ctx->desc.contact_capacity > 0 ? ctx->desc.contact_capacity
                                                    : std::max<int64_t>(64 * nsearch, 1 << 20);
     TRY(dalloc(ctx, &d.c_col, (size_t)d.contact_cap));
+    TRY(dalloc(ctx, &d.c_own, (size_t)d.contact_cap));
+    TRY(dalloc(ctx, &d.c_hit, (size_t)d.contact_cap));
     d.wp_cap = ctx->desc.wall_pair_capacity > 0 ? (int32_t)ctx->desc.wall_pair_capacity : 2048;
     if (d.wp_cap > 4096) return fail(ctx, PDGPU_ERR_ARG, "wall_pair_capacity is limited to 4096");
     TRY(dalloc(ctx, &d.wp, ctx->hp.size() * (size_t)d.wp_cap));
@@ -1349,8 +1351,13 @@ int pdgpu_upload_contact(pdgpu_ctx *ctx, int32_t nz, const double *rc, const dou
   if (!ctx || nz <= 0 || !rc || !kn || !mu || !betan || !kappa)
     return fail(ctx, PDGPU_ERR_ARG, "upload_contact: bad arguments");
   std::vector<ContactPair> cp((size_t)nz * nz);
-  for (size_t k = 0; k < cp.size(); k++) cp[k] = {rc[k], kn[k], mu[k], betan[k], kappa[k]};
+  double rc_max = 0.0;
+  for (size_t k = 0; k < cp.size(); k++) {
+    cp[k] = {rc[k], kn[k], mu[k], betan[k], kappa[k]};
+    if (rc[k] > rc_max) rc_max = rc[k];  // a NaN radius is skipped: is_less(R, NaN) never holds
+  }
   DevData &d = ctx->d;
+  d.rc_max = rc_max;
   if (!d.contact) TRY(dalloc(ctx, &d.contact, cp.size()));
   CK(cudaMemcpy(d.contact, cp.data(), cp.size() * sizeof(ContactPair), cudaMemcpyHostToDevice));
   d.n_zones = nz;
@@ -2620,6 +2627,8 @@ int pdgpu_load_state(pdgpu_ctx *ctx, const char *path) {
     TRY(ul(ctx, d.c_nodes, cnodes));
     TRY(ul(ctx, reinterpret_cast<int32_t *>(d.c_span), cspan));
     TRY(ul(ctx, d.c_col, ccol));
+    launch_contact_owner(d, ctx->stream);
+    CK(cudaGetLastError());
     TRY(ul(ctx, d.wp, wp));
     TRY(ul(ctx, d.wp_cnt, wpc));
     CK(cudaMemsetAsync(d.fc, 0, (size_t)(st * N) * 8, ctx->stream));
