@@ -435,6 +435,17 @@ PDGPU_API int pdgpu_enable_timing(pdgpu_ctx *ctx, int32_t on);
 PDGPU_API int pdgpu_kernel_times(pdgpu_ctx *ctx, int32_t max_kernels, const char **names, double *ms,
                        int64_t *launches, int32_t *count);
 
+/* Phase clock of the contact-list rebuild (a profiling aid): with on != 0
+ * every later rebuild records the GPU global timer (ns) as its first CTA
+ * passes each grid-wide barrier, in order: start, cells cleared, nodes
+ * counted per cell, cell offsets scanned, nodes scattered, cells sorted,
+ * candidates counted, row offsets scanned, compaction offsets scanned,
+ * lists compacted, and the first CTA's share of the fill done (11 marks).
+ * pdgpu_rebuild_phases copies the marks of the latest rebuild (up to cap)
+ * and sets *count. */
+PDGPU_API int pdgpu_enable_rebuild_phases(pdgpu_ctx *ctx, int32_t on);
+PDGPU_API int pdgpu_rebuild_phases(pdgpu_ctx *ctx, int64_t *ns, int32_t cap, int32_t *count);
+
 /* A batched ensemble (no counterpart in the reference, which runs one scene
  * per process): the uploaded nodes and particles hold n_scenes independent
  * scenes, each a contiguous run of particles (particle_offsets, n_scenes + 1

@@ -195,6 +195,7 @@ struct DevData {
   int64_t *c_row;
   int32_t *c_col;
   int32_t *c_own;  // per candidate entry: its node (written with c_col)
+  unsigned long long *phase_ns;  // rebuild phase clock (null: off), kRebuildPhases marks
   uint8_t *c_hit;  // per candidate entry, this step: inside the largest contact radius
   int64_t *c_cnt;  // per-node candidate counts of the last rebuild
   int64_t *c_tmp;  // N+1 scratch for the compaction scan
@@ -202,6 +203,7 @@ struct DevData {
   int32_t contact_grid;  // blocks of the contact node pass
   Grid grid;
   int32_t *cell_of, *cell_cnt, *cell_start, *cell_fill, *cell_tmp, *cell_nodes;
+  int32_t *cell_pid;  // contact rebuild: the particle of a cell's nodes when they share one, else -1
   int64_t cell_cap;  // max nodes in one cell handled by the in-cell sort
 
   // particle-wall damping pairs
@@ -353,6 +355,7 @@ int set_tile_smem_limit_mixed(int dim, size_t bytes);
 
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s);
 void launch_contact_owner(const DevData &d, cudaStream_t s);
+constexpr int kRebuildPhases = 16;
 int rebuild_grid_blocks(const DevData &d, int lanes);
 cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, int lanes, int init,
                                    cudaStream_t s);

@@ -660,12 +660,22 @@ __device__ bool grid_scan(CtrlState *gc, F in, Tout *out, int64_t n, int64_t *bs
     bsum[blockIdx.x] = s;
   }
   if (!grid_bar(gc)) return false;
-  if (threadIdx.x == 0) {
+  {
+    // carry = sum of the earlier blocks' totals, summed by the whole block
+    // (integers: any order gives the same sum); read past L1, which may
+    // hold this array from an earlier scan of the same launch
     int64_t s = 0;
-    for (int64_t b = 0; b < blockIdx.x; b++) s += bsum[b];
-    carry = s;
+    for (int64_t b = threadIdx.x; b < blockIdx.x; b += blockDim.x) s += __ldcg(bsum + b);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) wsum[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int64_t c = 0;
+      for (int w = 0; w < kCoopBlock / 32; w++) c += wsum[w];
+      carry = c;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   for (int64_t base = b0; base < b1; base += blockDim.x) {
     const int64_t k = base + threadIdx.x;
     const int64_t v = k < b1 ? (int64_t)in(k) : 0;
@@ -746,13 +756,18 @@ __device__ void cand_cells(const DevData &d, uint8_t search_bit, CandWarp<DIM> *
       const int cy0 = (int)((c / G.dims[0]) % G.dims[1]);
       const int cz0 = DIM == 3 ? (int)(c / ((int64_t)G.dims[0] * G.dims[1])) : 0;
       int a = 0, cnt = 0;
+      const int32_t pc_cell = d.cell_pid[c];
       if (t < kNb) {
         const int cx = cx0 + t % 3 - 1, cy = cy0 + (t / 3) % 3 - 1, cz = DIM == 3 ? cz0 + t / 9 - 1 : 0;
         if (cx >= 0 && cx < G.dims[0] && cy >= 0 && cy < G.dims[1] && cz >= 0 &&
             cz < (DIM == 3 ? G.dims[2] : 1)) {
           const int cell = cx + G.dims[0] * (cy + G.dims[1] * cz);
-          a = d.cell_start[cell];
-          cnt = d.cell_start[cell + 1] - a;
+          // a centre cell of one particle finds nothing in a neighbour cell
+          // of that same particle
+          if (pc_cell < 0 || d.cell_pid[cell] != pc_cell) {
+            a = d.cell_start[cell];
+            cnt = d.cell_start[cell + 1] - a;
+          }
         }
       }
       int incl = cnt;
@@ -768,6 +783,12 @@ __device__ void cand_cells(const DevData &d, uint8_t search_bit, CandWarp<DIM> *
     }
     __syncwarp();
     const int total = W.nb_off[kNb];
+    if (total == 0) {
+      // every neighbour cell culled: no candidate for any node of this cell
+      for (int a = s_c + l32; a < e_c; a += 32) d.c_cnt[d.cell_nodes[a]] = 0;
+      __syncwarp();  // the warp's stage is reused by the next cell
+      continue;
+    }
     // centre nodes in sets of up to kCandCentres (one set unless the cell is crowded)
     for (int sb = s_c; sb < e_c; sb += kCandCentres) {
       const int nc = min(kCandCentres, e_c - sb);
@@ -856,7 +877,11 @@ __device__ void cand_cells(const DevData &d, uint8_t search_bit, CandWarp<DIM> *
 
 // Fill pass over the nodes that have candidates (c_nodes[0, nn)): a warp per
 // node walks the same neighbourhood in the same order as the count pass and
-// writes the columns.
+// writes the columns.  Lane t first takes neighbour cell t (empty when it
+// lies outside the grid or holds only nodes of this node's particle); the
+// cells' node ranges, concatenated in traversal order, are then walked 32
+// entries at a time, so each entry costs one chain of loads (its node, then
+// that node's particle and position) whatever cell it sits in.
 template <int DIM>
 __device__ void cand_fill_nodes(const DevData &d, int64_t nn) {
   constexpr int kNb = DIM == 3 ? 27 : 9;
@@ -875,37 +900,55 @@ __device__ void cand_fill_nodes(const DevData &d, int64_t nn) {
     for (int64_t e = out + l32; e < out_end && e < d.contact_cap; e += 32) d.c_own[e] = i;
     const int cx0 = cell_coord<DIM>(q[0], G, 0), cy0 = cell_coord<DIM>(q[1], G, 1);
     const int cz0 = DIM == 3 ? cell_coord<DIM>(q[2], G, 2) : 0;
-    for (int nb = 0; nb < kNb; nb++) {
-      const int cx = cx0 + nb % 3 - 1, cy = cy0 + (nb / 3) % 3 - 1, cz = DIM == 3 ? cz0 + nb / 9 - 1 : 0;
-      if (cx < 0 || cx >= G.dims[0] || cy < 0 || cy >= G.dims[1] || cz < 0 || cz >= (DIM == 3 ? G.dims[2] : 1))
-        continue;
-      const int cell = cx + G.dims[0] * (cy + G.dims[1] * cz);
-      const int a0 = d.cell_start[cell], a1 = d.cell_start[cell + 1];
-      for (int base = a0; base < a1; base += 32) {
-        const int a = base + l32;
-        bool hit = false;
-        int32_t j = -1;
-        if (a < a1) {
-          j = d.cell_nodes[a];
-          if (d.ptid[j] != pi) {
-            double p[3];
-            ldv<DIM>(d.x, j, p);
-            double dd = 0.0;
-#pragma unroll
-            for (int u = 0; u < DIM; u++) {
-              const double df = q[u] - p[u];
-              dd += df * df;
-            }
-            hit = dd < r2;
-          }
+    int a = 0, cnt = 0;
+    if (l32 < kNb) {
+      const int cx = cx0 + l32 % 3 - 1, cy = cy0 + (l32 / 3) % 3 - 1, cz = DIM == 3 ? cz0 + l32 / 9 - 1 : 0;
+      if (cx >= 0 && cx < G.dims[0] && cy >= 0 && cy < G.dims[1] && cz >= 0 && cz < (DIM == 3 ? G.dims[2] : 1)) {
+        const int cell = cx + G.dims[0] * (cy + G.dims[1] * cz);
+        if (d.cell_pid[cell] != pi) {  // a cell of this node's particle only holds no candidate
+          a = d.cell_start[cell];
+          cnt = d.cell_start[cell + 1] - a;
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, hit);
-        if (hit) {
-          const int64_t at = out + __popc(bal & ((1u << l32) - 1u));
-          if (at < out_end && at < d.contact_cap) d.c_col[at] = j;
-        }
-        out += __popc(bal);
       }
+    }
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (l32 >= o) incl += y;
+    }
+    int inc[kNb];
+#pragma unroll
+    for (int c = 0; c < kNb; c++) inc[c] = __shfl_sync(0xffffffffu, incl, c);
+    const int total = inc[kNb - 1];
+    for (int base = 0; base < total; base += 32) {
+      const int g = base + l32;
+      int k = 0;
+#pragma unroll
+      for (int c = 0; c < kNb; c++) k += inc[c] <= g;
+      const int ak = __shfl_sync(0xffffffffu, a, k & 31);
+      const int ek = __shfl_sync(0xffffffffu, incl - cnt, k & 31);
+      bool hit = false;
+      int32_t j = -1;
+      if (g < total) {
+        j = d.cell_nodes[ak + (g - ek)];
+        if (d.ptid[j] != pi) {
+          double p[3];
+          ldv<DIM>(d.x, j, p);
+          double dd = 0.0;
+#pragma unroll
+          for (int u = 0; u < DIM; u++) {
+            const double df = q[u] - p[u];
+            dd += df * df;
+          }
+          hit = dd < r2;
+        }
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, hit);
+      if (hit) {
+        const int64_t at = out + __popc(bal & ((1u << l32) - 1u));
+        if (at < out_end && at < d.contact_cap) d.c_col[at] = j;
+      }
+      out += __popc(bal);
     }
   }
 }
@@ -918,6 +961,13 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
   if (d.ctrl->error || !d.ctrl->update) return;
   CtrlState *gc = d.ctrl;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // phase clock (profiling): the first CTA's time past each barrier
+  int mark = 0;
+  auto stamp = [&]() {
+    if (d.phase_ns && tid == 0 && mark < kRebuildPhases) d.phase_ns[mark] = global_ns();
+    mark++;
+  };
+  stamp();
   const int64_t nth = (int64_t)gridDim.x * blockDim.x;
   const int64_t N = d.n_nodes;
   const Grid G = d.grid;
@@ -928,6 +978,7 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
   if (d.sur_near_gate)
     for (int64_t p = tid; p < d.n_particles; p += nth) d.sur_near[p] = 0;
   if (!grid_bar(gc)) return;
+  stamp();
   for (int64_t i = tid; i < N; i += nth) {
     double p[3];
     ldv<DIM>(d.x, i, p);
@@ -936,31 +987,51 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
     atomicAdd(d.cell_cnt + c, 1);
   }
   if (!grid_bar(gc)) return;
+  stamp();
   const int32_t *cc = d.cell_cnt;
   if (!grid_scan<int32_t>(gc, [cc](int64_t k) { return cc[k]; }, d.cell_start, G.ncells, bsum)) return;
+  stamp();
   for (int64_t i = tid; i < N; i += nth) {
     const int c = d.cell_of[i];
     d.cell_tmp[d.cell_start[c] + atomicAdd(d.cell_fill + c, 1)] = (int32_t)i;
   }
   if (!grid_bar(gc)) return;
+  stamp();
   {
+    // per cell: its nodes in index order (rank counting) and, when they all
+    // belong to one particle, that particle (no candidate joins two nodes
+    // of one particle, so the searches skip a cell of the searching node's
+    // own particle)
     const int lane = threadIdx.x & 31;
     for (int64_t c = tid >> 5; c < G.ncells; c += nth >> 5) {
       const int s = d.cell_start[c], e = d.cell_start[c + 1];
+      int32_t pmin = INT32_MAX, pmax = -1;
       for (int a = s + lane; a < e; a += 32) {
         const int32_t va = d.cell_tmp[a];
         int rank = 0;
         for (int b = s; b < e; b++) rank += d.cell_tmp[b] < va;
         d.cell_nodes[s + rank] = va;
+        const int32_t p = d.ptid[va];
+        pmin = min(pmin, p);
+        pmax = max(pmax, p);
       }
+      for (int o = 16; o > 0; o >>= 1) {
+        pmin = min(pmin, __shfl_xor_sync(0xffffffffu, pmin, o));
+        pmax = max(pmax, __shfl_xor_sync(0xffffffffu, pmax, o));
+      }
+      if (lane == 0) d.cell_pid[c] = (e > s && pmin == pmax) ? pmin : -1;
     }
   }
   if (!grid_bar(gc)) return;
+  stamp();
   cand_cells<DIM, LPN, false>(d, search_bit, stage);
   if (!grid_bar(gc)) return;
+  stamp();
   const int64_t *cn = d.c_cnt;
   if (!grid_scan<int64_t>(gc, [cn](int64_t k) { return cn[k]; }, d.c_row, N, bsum)) return;
+  stamp();
   if (!grid_scan<int64_t>(gc, [cn](int64_t k) { return (int64_t)(cn[k] > 0); }, d.c_tmp, N, bsum)) return;
+  stamp();
   for (int64_t i = tid; i < N; i += nth)
     if (cn[i] > 0) {
       d.c_nodes[d.c_tmp[i]] = (int32_t)i;
@@ -969,7 +1040,9 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
     }
   if (tid == 0) d.ctrl->c_nnodes = d.c_tmp[N];
   if (!grid_bar(gc)) return;  // the compacted list is complete
+  stamp();
   cand_fill_nodes<DIM>(d, d.c_tmp[N]);
+  stamp();  // the first CTA's share of the fill done
   if (tid == 0) {
     const int64_t total = d.c_row[N];
     d.ctrl->entries = total;

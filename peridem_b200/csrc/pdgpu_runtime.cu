@@ -434,9 +434,11 @@ int ensure_cells(pdgpu_ctx *ctx, const Grid &g) {
   dfree(ctx, d.cell_cnt);
   dfree(ctx, d.cell_start);
   dfree(ctx, d.cell_fill);
+  dfree(ctx, d.cell_pid);
   TRY(dalloc(ctx, &d.cell_cnt, (size_t)g.ncells + 1));
   TRY(dalloc(ctx, &d.cell_start, (size_t)g.ncells + 1));
   TRY(dalloc(ctx, &d.cell_fill, (size_t)g.ncells + 1));
+  TRY(dalloc(ctx, &d.cell_pid, (size_t)g.ncells + 1));
   CK(cudaMemset(d.cell_cnt, 0, ((size_t)g.ncells + 1) * 4));
   CK(cudaMemset(d.cell_fill, 0, ((size_t)g.ncells + 1) * 4));
   d.grid = g;
@@ -2353,6 +2355,37 @@ int pdgpu_enable_timing(pdgpu_ctx *ctx, int32_t on) {
     ctx->ms[i] = 0.0;
     ctx->launches[i] = 0;
   }
+  return PDGPU_OK;
+}
+
+int pdgpu_enable_rebuild_phases(pdgpu_ctx *ctx, int32_t on) {
+  if (!ctx) return PDGPU_ERR_ARG;
+  DevData &d = ctx->d;
+  if (on && !d.phase_ns) {
+    TRY(dalloc(ctx, &d.phase_ns, (size_t)kRebuildPhases));
+    CK(cudaMemset(d.phase_ns, 0, kRebuildPhases * sizeof(unsigned long long)));
+  } else if (!on && d.phase_ns) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    d.phase_ns = nullptr;  // the buffer stays with the context's allocations
+  }
+  if (ctx->gexec) {  // kernels in a graph hold the DevData they were captured with
+    cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_rebuild_phases(pdgpu_ctx *ctx, int64_t *ns, int32_t cap, int32_t *count) {
+  if (!ctx || !count || cap < 0 || (cap > 0 && !ns)) return PDGPU_ERR_ARG;
+  *count = 0;
+  if (!ctx->d.phase_ns) return PDGPU_OK;
+  unsigned long long h[kRebuildPhases];
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(h, ctx->d.phase_ns, sizeof h, cudaMemcpyDeviceToHost));
+  int n = 0;
+  while (n < kRebuildPhases && h[n] != 0) n++;
+  for (int k = 0; k < n && k < cap; k++) ns[k] = (int64_t)h[k];
+  *count = n < cap ? n : cap;
   return PDGPU_OK;
 }
 

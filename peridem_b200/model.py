@@ -383,6 +383,17 @@ class GpuDEMModel:
         """DEMModel::output: the current state as a .vtu file (pdgpu_write_vtu)."""
         self._check(self.lib.pdgpu_write_vtu(self.ctx, path.encode(), ",".join(tags).encode()))
 
+    def rebuild_phases(self, on: Optional[bool] = None) -> List[int]:
+        """Phase clock of the contact-list rebuild (pdgpu_enable_rebuild_phases /
+        pdgpu_rebuild_phases): with `on` given, switch recording; returns the
+        latest rebuild's marks (GPU global timer, ns)."""
+        if on is not None:
+            self._check(self.lib.pdgpu_enable_rebuild_phases(self.ctx, 1 if on else 0))
+        buf = (ctypes.c_int64 * 16)()
+        n = ctypes.c_int32()
+        self._check(self.lib.pdgpu_rebuild_phases(self.ctx, buf, 16, ctypes.byref(n)))
+        return list(buf[:n.value])
+
     def bond_scheme(self) -> int:
         """Mixed bond loop: 0 every bond from both ends, node order; 1 symmetric
         bond visits (2-D); 2 every bond from both ends, nodes longest row first."""
