@@ -398,15 +398,17 @@ PDGPU_API int pdgpu_download_pd_neighbors(pdgpu_ctx *ctx, uint64_t *rowptr, uint
 
 /* Launch shape of the bond loop and the contact kernel: lanes per node
  * (4, 8, 16 or 32 for the bond loop, also 1 or 2 in the mixed form; 1, 2,
- * 4, 8 or 32 for the contact node pass, default 1: a distance pass over
- * the flat candidate entries leaves it few entries per node, which one
- * thread then sums in list order); 0 keeps the current choice.  Set before
- * the first step. */
+ * 4, 8 or 32 for the contact pass, default 1).  With 1 the contact pass is
+ * one warp-cooperative kernel: a warp walks the candidate entries of 32
+ * nodes, coalesced, and each node's lane adds its contributions in list
+ * order; with more, a flat distance pass marks the entries inside the
+ * largest contact radius and a node pass sums them with that many lanes
+ * per node.  0 keeps the current choice.  Set before the first step. */
 PDGPU_API int pdgpu_set_tuning(pdgpu_ctx *ctx, int32_t pd_lanes, int32_t contact_lanes);
 
-/* CTAs per SM of the contact node pass (1..16, default 4); the pass and
- * the distance pass ahead of it run beside the bond loop and are bound by
- * the latency of their gathers.  Set before the first step. */
+/* CTAs per SM of the contact node pass (1..16, default 2); it runs beside
+ * the bond loop and is bound by the latency of its gathers.  Set before the
+ * first step. */
 PDGPU_API int pdgpu_set_contact_grid(pdgpu_ctx *ctx, int32_t ctas_per_sm);
 
 /* Nodes per bond-loop tile (one CTA each); 0 = automatic.  Set before the

@@ -1226,6 +1226,189 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
 }
 
 // ---------------------------------------------------------------------------
+// The contact node pass in one kernel, warp-cooperative (the default, one
+// lane per node): a warp takes 32 consecutive compacted nodes, whose
+// candidate rows are consecutive in the entry array, and walks their
+// entries 32 at a time, coalesced.  Each lane finds its entry's node among
+// the warp's (binary search over the row starts, held one per lane), takes
+// that node's position and velocity by shuffle, and reads only the
+// candidate's position unless the pair is inside the largest contact
+// radius.  The rare contributions are then handed, in entry order, to the
+// lane that owns the node, which adds them in the reference's order (normal
+// part, then friction part, candidate by candidate).  Results equal the
+// node pass with one lane per node.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_contact_warp(DevData d) {
+  __shared__ ContactPair cps[kZonePairsSmem];
+  __shared__ double scr[kBlock];
+  const int l32 = threadIdx.x & 31;
+  const int nz = d.n_zones;
+  const bool tab = nz * nz <= kZonePairsSmem;
+  const int64_t nn_raw = d.ctrl->c_nnodes;
+  const int err = d.ctrl->error;
+  if (tab)
+    for (int a = threadIdx.x; a < nz * nz; a += kBlock) cps[a] = d.contact[a];
+  for (int64_t p = (int64_t)blockIdx.x * kBlock + threadIdx.x; p < d.n_particles; p += (int64_t)gridDim.x * kBlock) {
+    // particle centres (position, velocity) of this step for the damping pass
+    const int64_t c = d.particles[p].center;
+    double xc[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
+    ldv<DIM>(d.x, c, xc);
+    ldv<DIM>(d.v, c, vc);
+    double *o = d.pcen + 8 * p;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      o[q] = xc[q];
+      o[3 + q] = vc[q];
+    }
+  }
+  __syncthreads();
+  const int64_t nn = err ? 0 : nn_raw;
+  const double rmax = d.rc_max;
+  const int64_t nwarps = (int64_t)gridDim.x * (kBlock / 32);
+  double crd_acc = 0.0;
+  for (int64_t w = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5; w * 32 < nn; w += nwarps) {
+    const int64_t t = w * 32 + l32;
+    const bool own = t < nn;
+    const int nval = (int)min((int64_t)32, nn - w * 32);  // lanes with a node
+    int32_t i = 0;
+    int2 sp = make_int2(0, 0);
+    double yi[3] = {0, 0, 0}, vi[3] = {0, 0, 0};
+    int32_t pi = -1;
+    int zi = 0;
+    if (own) {
+      i = d.c_nodes[t];
+      sp = d.c_span[t];
+      pi = d.ptid[i];
+      zi = d.nzone[i];
+      ldv<DIM>(d.x, i, yi);
+      ldv<DIM>(d.v, i, vi);
+    }
+    const int e0 = __shfl_sync(0xffffffffu, sp.x, 0);
+    const int e1 = __shfl_sync(0xffffffffu, sp.y, nval - 1);
+    double fx = 0.0, fy = 0.0, fz = 0.0, crd = 0.0;
+    for (int base = e0; base < e1; base += 32) {
+      const int e = base + l32;
+      // the entry's node: the last lane whose row starts at or before e
+      int o = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int cnd = o + step;
+        const int st = __shfl_sync(0xffffffffu, sp.x, cnd & 31);
+        if (cnd < nval && st <= e) o = cnd;
+      }
+      double yo[3], vo[3];
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        yo[q] = __shfl_sync(0xffffffffu, yi[q], o);
+        vo[q] = __shfl_sync(0xffffffffu, vi[q], o);
+      }
+      const int32_t po = __shfl_sync(0xffffffffu, pi, o);
+      const int zo = __shfl_sync(0xffffffffu, zi, o);
+      double cxn = 0.0, cyn = 0.0, czn = 0.0, cxt = 0.0, cyt = 0.0, czt = 0.0, cr = 0.0;
+      bool contrib = false;
+      if (e < e1) {
+        const int32_t j = d.c_col[e];
+        double yj[3];
+        ldv<DIM>(d.x, j, yj);
+        double yji[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) yji[q] = yj[q] - yo[q];
+        const double R = len3<DIM>(yji);
+        if (R < rmax) {
+          double vj[3];
+          ldv<DIM>(d.v, j, vj);
+          const double volj = d.vol[j];
+          const int32_t pj = d.ptid[j];
+          const int zj = d.nzone[j];
+          const bool wall = (d.flags[j] & NODE_WALL) != 0;
+          const ContactPair cp = tab ? cps[zo * nz + zj] : d.contact[zo * nz + zj];
+          if (is_less(R, cp.rc)) {
+            double vji[3], en[3], et[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+              vji[q] = vj[q] - vo[q];
+              en[q] = yji[q] / R;
+            }
+            const double vn = dot3<DIM>(vji, en);
+#pragma unroll
+            for (int q = 0; q < 3; q++) et[q] = vji[q] - vn * en[q];
+            const double etl = len3<DIM>(et);
+            if (is_greater(etl, 0.)) {
+#pragma unroll
+              for (int q = 0; q < 3; q++) et[q] = et[q] / etl;
+            } else {
+              et[0] = et[1] = et[2] = 0.0;
+            }
+            double sf = cp.kn * (R - cp.rc) * volj;
+            if (sf > 0.) sf = 0.;
+            const double mf = cp.mu * sf;
+            cxn = sf * en[0];
+            cyn = sf * en[1];
+            czn = sf * en[2];
+            cxt = mf * et[0];
+            cyt = mf * et[1];
+            czt = mf * et[2];
+            contrib = true;
+            if (wall) {
+              const int slot = atomicAdd(d.wp_cnt + po, 1);
+              if (slot < d.wp_cap) d.wp[(int64_t)po * d.wp_cap + slot] = j;
+              else set_error(d.ctrl, DEV_ERR_WALLPAIR_OVERFLOW, po);
+            }
+            if (d.pwall_test ? d.pwall_test[pj] != 0 : pj == d.test_wall) {
+              const int td = d.test_dir;
+              cr = td == 0 ? cxn + cxt : (td == 1 ? cyn + cyt : czn + czt);
+            } else {
+              cr = -0.0;  // marks "no test-wall term" (never added)
+            }
+          }
+        }
+      }
+      // hand the contributions to their nodes' lanes in entry order
+      unsigned m = __ballot_sync(0xffffffffu, contrib);
+      while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        const int dst = __shfl_sync(0xffffffffu, o, src);
+        const double ax = __shfl_sync(0xffffffffu, cxn, src), ay = __shfl_sync(0xffffffffu, cyn, src);
+        const double bx = __shfl_sync(0xffffffffu, cxt, src), by = __shfl_sync(0xffffffffu, cyt, src);
+        const double c = __shfl_sync(0xffffffffu, cr, src);
+        double az = 0.0, bz = 0.0;
+        if constexpr (DIM == 3) {
+          az = __shfl_sync(0xffffffffu, czn, src);
+          bz = __shfl_sync(0xffffffffu, czt, src);
+        }
+        if (l32 == dst) {
+          fx += ax;
+          fy += ay;
+          if constexpr (DIM == 3) fz += az;
+          fx += bx;
+          fy += by;
+          if constexpr (DIM == 3) fz += bz;
+          if (!(c == 0.0 && signbit(c))) crd += c;
+        }
+      }
+    }
+    if (own) {
+      if (fx != 0.0 || fy != 0.0 || (DIM == 3 && fz != 0.0)) {
+        const double f[3] = {fx, fy, fz};
+        stv<DIM>(d.fc, i, f);
+      }
+      crd_acc += crd * d.vol[i];
+      if (d.cr_t) d.cr_t[t] = crd * d.vol[i];
+    }
+  }
+  // deterministic per-block partial of the test wall's contact reaction
+  scr[threadIdx.x] = crd_acc;
+  __syncthreads();
+  for (int h = kBlock / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) scr[threadIdx.x] += scr[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) d.cr_partial[blockIdx.x] = scr[0];
+}
+
+// ---------------------------------------------------------------------------
 // Particle damping of DEMModel::computeContactForces (demModel.cpp:937-1050):
 // particle-particle through particle centres and particle-wall through the
 // condensed wall nodes.  One block per particle; the force density is applied
@@ -1861,10 +2044,15 @@ void launch_contact_owner(const DevData &d, cudaStream_t s) {
 }
 
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s) {
+  const unsigned g = (unsigned)d.contact_grid;
+  if (lanes == 1) {  // one kernel, a warp per 32 nodes
+    if (d.dim == 2) k_contact_warp<2><<<g, kBlock, 0, s>>>(d);
+    else k_contact_warp<3><<<g, kBlock, 0, s>>>(d);
+    return;
+  }
   // the distance pass: eight CTAs per SM, grid-stride over the entries
   if (d.dim == 2) k_contact_near<2><<<sm_count() * 8, kBlock, 0, s>>>(d);
   else k_contact_near<3><<<sm_count() * 8, kBlock, 0, s>>>(d);
-  const unsigned g = (unsigned)d.contact_grid;
   if (d.dim == 2) {
     if (lanes == 1) k_contact<2, 1><<<g, kBlock, 0, s>>>(d);
     else if (lanes == 2) k_contact<2, 2><<<g, kBlock, 0, s>>>(d);

@@ -66,7 +66,7 @@ struct pdgpu_ctx {
   void *scan_tmp = nullptr;
   size_t scan_bytes = 0;
   int pd_lanes = 0, contact_lanes = 1;
-  int contact_ctas = 4;  // CTAs per SM of the contact node pass
+  int contact_ctas = 2;  // CTAs per SM of the contact node pass (two fit beside the bond loop)
   int64_t *rebuild_bsum = nullptr;
   int rebuild_grid = 0;
   // tiled bond loop
