@@ -491,6 +491,32 @@ def run_ours(args, rank, world):
                     "particle_steps": steps_all, "fraction_on": round(steps_on / max(steps_all, 1), 4)})
     sc_vals = model.scalars()
 
+    # phase clock of the contact-list rebuild (--rebuild-phases R): the next
+    # R rebuilds after the window, one-step graphs, per-phase median (us)
+    rebuild_phases = None
+    if args.rebuild_phases > 0 and sc.multi_particle:
+        names = ["clear", "count nodes per cell", "scan cell offsets", "scatter", "in-cell sort",
+                 "count candidates", "scan row offsets", "scan compaction offsets", "compact",
+                 "fill (first CTA's share)"]
+        model.rebuild_phases(True)
+        runs = []
+        for _ in range(args.rebuild_phases):
+            u0 = model.scalars()["contact_updates"]
+            for _ in range(1000):
+                model.integrate_step(1, graph_steps=1)
+                model.sync()
+                if model.scalars()["contact_updates"] != u0:
+                    break
+            t = model.rebuild_phases()
+            if len(t) >= 2:
+                runs.append(np.diff(np.asarray(t, dtype=np.float64)) / 1e3)
+        model.rebuild_phases(False)
+        if runs:
+            n = min(len(r) for r in runs)
+            med = np.median(np.stack([r[:n] for r in runs]), axis=0)
+            rebuild_phases = {"rebuilds": len(runs), "first_cta_done_us": round(float(med.sum()), 1),
+                              "phases_us": {nm: round(float(x), 1) for nm, x in zip(names, med)}}
+
     # end to end through the host-buffer call: H2D of u, v, x and D2H of
     # u, v, x, f every step (pinned buffers)
     N = sc.n_nodes
@@ -542,6 +568,7 @@ def run_ours(args, rank, world):
     return {"value": value, "ms_per_step": total_ms / args.steps, "e2e": e2e, "roofline": roof,
             "kernels": kt, "clocks": clk.summary(), "gpu_launches": gpu_launches, "autotune": tuned,
             "surrogate": sur, "fp64": fp64, "window": window, "snapshot": snap,
+            "rebuild_phases": rebuild_phases,
             "scalars": {k: sc_vals[k] for k in ("n", "contact_updates", "contact_entries",
                                                  "contact_update_interval", "broken_bonds",
                                                  "reaction", "contact_reaction")},
@@ -653,6 +680,9 @@ def main():
     ap.add_argument("--prerun-contact-cap", type=int, default=60000,
                     help="at most this many more pre-run steps waiting for the top wall's contact")
     ap.add_argument("--contact-lanes", type=int, default=0, help="lanes per node in the contact pass (0 = auto)")
+    ap.add_argument("--rebuild-phases", type=int, default=0,
+                    help="after the window, time this many contact-list rebuilds phase by phase "
+                         "(GPU global timer at each grid-wide barrier) and report the medians")
     ap.add_argument("--profile-window", action="store_true",
                     help="bracket the timed window with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--no-fp64", dest="fp64_arm", action="store_false",
@@ -741,6 +771,8 @@ def main():
             line["error_vs_fp64"] = f64["error_of_mixed"]
         if res.get("autotune"):
             line["autotune"] = res["autotune"]
+        if res.get("rebuild_phases"):
+            line["rebuild_phases"] = res["rebuild_phases"]
         if res.get("surrogate"):
             line["surrogate"] = res["surrogate"]
         print(json.dumps(line))
