@@ -437,6 +437,26 @@ PDGPU_API int pdgpu_enable_timing(pdgpu_ctx *ctx, int32_t on);
 PDGPU_API int pdgpu_kernel_times(pdgpu_ctx *ctx, int32_t max_kernels, const char **names, double *ms,
                        int64_t *launches, int32_t *count);
 
+/* Strain and stress at the quadrature points of linear triangles (2-D) from
+ * the context's current displacement: the Strain_Stress output of
+ * DEMModel::output (demModel.cpp:2026-2072), i.e. fe::getCurrentQuadPoints
+ * and fe::getStrainStress (fe/meshUtil.cpp:170-420) with
+ * fe::TriElem::getQuadDatas (fe/triElem.cpp:60-95), evaluated on the GPU in
+ * the reference's order (strain and stress as 32-bit floats, as
+ * util::SymMatrix3 keeps them, returned widened to double).  conn[3e..3e+2]
+ * are element e's global node ids; ref_points (xi, eta per point) the
+ * reference-triangle quadrature points, nq = 1 or 3 (the reference's rules of
+ * order 1 and 2); nu, lambda, mu and plane_strain per element (the
+ * particle material's Material::computeMaterialProperties and deck flag).
+ * Writes three entries per element, as the reference stores them (entries
+ * past the rule's points zero): xq[3 (3e + q) + c] the current position,
+ * strain and stress[6 (3e + q) + k] with k = xx, yy, zz, yz, xz, xy.
+ * Synchronous; host buffers. */
+PDGPU_API int pdgpu_strain_stress_tri(pdgpu_ctx *ctx, int64_t n_elements, const int64_t *conn, int32_t nq,
+                                      const double *ref_points, const double *nu, const double *lambda,
+                                      const double *mu, const uint8_t *plane_strain, double *xq, double *strain,
+                                      double *stress);
+
 /* Phase clock of the contact-list rebuild (a profiling aid): with on != 0
  * every later rebuild records the GPU global timer (ns) as its first CTA
  * passes each grid-wide barrier, in order: start, cells cleared, nodes

@@ -29,6 +29,7 @@ UNITS = [
     ("pdgpu_runtime.cu", []),
     ("pdgpu_decks.cu", ["--fmad=false"]),
     ("pdgpu_meshsize.cu", ["--fmad=false"]),
+    ("pdgpu_strain.cu", ["--fmad=false"]),
 ]
 
 

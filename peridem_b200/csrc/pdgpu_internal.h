@@ -355,6 +355,11 @@ int set_tile_smem_limit_mixed(int dim, size_t bytes);
 
 void launch_contact_force(const DevData &d, int lanes, cudaStream_t s);
 void launch_contact_owner(const DevData &d, cudaStream_t s);
+// strain and stress at the quadrature points of linear triangles (2-D):
+// three entries per element, nq <= 3 points (pts: xi, eta per point)
+cudaError_t launch_strain_tri(const DevData &d, int64_t n_elem, const int64_t *conn, int nq, const double *pts,
+                              const double *nu, const double *lam, const double *mu, const uint8_t *plane_strain,
+                              double *xq, double *strain, double *stress, cudaStream_t s);
 constexpr int kRebuildPhases = 16;
 int rebuild_grid_blocks(const DevData &d, int lanes);
 cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, int lanes, int init,

@@ -383,6 +383,28 @@ class GpuDEMModel:
         """DEMModel::output: the current state as a .vtu file (pdgpu_write_vtu)."""
         self._check(self.lib.pdgpu_write_vtu(self.ctx, path.encode(), ",".join(tags).encode()))
 
+    def strain_stress_tri(self, conn: np.ndarray, order: int, nu, lam, mu, plane_strain):
+        """Quadrature-point strain and stress of linear triangles (2-D) from the
+        current displacement (pdgpu_strain_stress_tri): conn [m, 3] global
+        node ids, quadrature order 1 or 2, per-element (or scalar) nu,
+        lambda, mu and plane-strain flag.  Returns xq [3 m, 3], strain and
+        stress [3 m, 6] (xx, yy, zz, yz, xz, xy), three entries per element
+        as the reference stores them."""
+        from . import fe
+        conn = np.ascontiguousarray(conn, dtype=np.int64).reshape(-1, 3)
+        m = len(conn)
+        pts = np.ascontiguousarray(fe.tri_points(order))
+        arr = [np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=np.float64), (m,))) for a in (nu, lam, mu)]
+        ps = np.ascontiguousarray(np.broadcast_to(np.asarray(plane_strain, dtype=np.uint8), (m,)))
+        xq = np.zeros((3 * m, 3))
+        strain = np.zeros((3 * m, 6))
+        stress = np.zeros((3 * m, 6))
+        self._check(self.lib.pdgpu_strain_stress_tri(
+            self.ctx, m, _ptr(conn, ctypes.c_int64), len(pts), _ptr(pts, ctypes.c_double),
+            *(_ptr(a, ctypes.c_double) for a in arr), _ptr(ps, ctypes.c_uint8),
+            _ptr(xq, ctypes.c_double), _ptr(strain, ctypes.c_double), _ptr(stress, ctypes.c_double)))
+        return xq, strain, stress
+
     def rebuild_phases(self, on: Optional[bool] = None) -> List[int]:
         """Phase clock of the contact-list rebuild (pdgpu_enable_rebuild_phases /
         pdgpu_rebuild_phases): with `on` given, switch recording; returns the

@@ -1,0 +1,56 @@
+"""pdgpu_strain_stress_tri (the Strain_Stress output on the GPU) against the
+reference's own fe::getCurrentQuadPoints / fe::getStrainStress: bit for bit
+with tests/golden/strain_tri.npz (made by the reference from the same
+two-particle scene's nodes and displacement), orders 1 and 2, plane strain
+and plane stress; argument checks on the host."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(HERE, "golden")]
+
+pytestmark = pytest.mark.gpu
+
+G = np.load(os.path.join(HERE, "golden", "strain_tri.npz"))
+
+
+def _model():
+    import make_strain_golden as mk
+    from peridem_b200 import scene as scn
+    from peridem_b200.model import GpuDEMModel, PREC_FP64
+    sc = scn.build_scene(mk.scene_spec())
+    m = GpuDEMModel(sc, precision=PREC_FP64, build_neighbors=True, compute_mx=True)
+    m.set_field("u", G["u"])
+    return m
+
+
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("ps", [0, 1])
+def test_strain_stress_matches_reference(order, ps):
+    nu, lam, mu = G["material"]
+    m = _model()
+    try:
+        xq, e, s = m.strain_stress_tri(G["conn"], order, nu, lam, mu, ps)
+    finally:
+        m.close()
+    k = f"o{order}_ps{ps}"
+    assert np.array_equal(xq, G[k + "_xq"]), float(np.max(np.abs(xq - G[k + "_xq"])))
+    assert np.array_equal(e, G[k + "_strain"]), float(np.max(np.abs(e - G[k + "_strain"])))
+    assert np.array_equal(s, G[k + "_stress"]), float(np.max(np.abs(s - G[k + "_stress"])))
+
+
+def test_strain_stress_refuses_bad_arguments():
+    from peridem_b200 import api
+    m = _model()
+    try:
+        bad = np.array(G["conn"])
+        bad[3, 1] = 10 ** 6
+        with pytest.raises(api.PdgpuError):
+            m.strain_stress_tri(bad, 1, 0.25, 1.0, 1.0, 0)
+        with pytest.raises(ValueError):
+            m.strain_stress_tri(G["conn"], 3, 0.25, 1.0, 1.0, 0)
+    finally:
+        m.close()
