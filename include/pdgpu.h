@@ -457,6 +457,14 @@ PDGPU_API int pdgpu_strain_stress_tri(pdgpu_ctx *ctx, int64_t n_elements, const 
                                       const double *mu, const uint8_t *plane_strain, double *xq, double *strain,
                                       double *stress);
 
+/* The same for linear tetrahedra (3-D, conn[4e..4e+3]) with the one-point
+ * rule (the centroid), the reference's only tetrahedron rule that fits the
+ * three entries it stores per element (fe::TetElem, fe/tetElem.cpp: J^-1 by
+ * util::inv, derivatives by util::dot); entries 1 and 2 of each element zero. */
+PDGPU_API int pdgpu_strain_stress_tet(pdgpu_ctx *ctx, int64_t n_elements, const int64_t *conn, const double *nu,
+                                      const double *lambda, const double *mu, double *xq, double *strain,
+                                      double *stress);
+
 /* Phase clock of the contact-list rebuild (a profiling aid): with on != 0
  * every later rebuild records the GPU global timer (ns) as its first CTA
  * passes each grid-wide barrier, in order: start, cells cleared, nodes

@@ -81,3 +81,74 @@ def strain_stress_tri(xref, u, conn, points, nu, lam, mu, plane_strain):
         strain[:, q] = e
         stress[:, q] = t
     return xq.reshape(m * 3, 3), strain.reshape(m * 3, 6), stress.reshape(m * 3, 6)
+
+
+def strain_stress_tet(xref, u, conn, lam, mu):
+    """Linear tetrahedra, one-point rule (fe::TetElem, src/fe/tetElem.cpp:
+    J rows x_k - x_0, util::det by cofactors along the first row, util::inv
+    as the adjugate times 1/det, util::dot for the derivatives; the position
+    (((0 + N0 x0) + N1 x1) + N2 x2) + N3 x3 plus u_i N_i); strain terms per
+    node xx, yy, xy, zz, yz, xz; three entries per element.  Returns xq
+    [3 m, 3], strain, stress [3 m, 6]."""
+    xref = np.asarray(xref, dtype=np.float64)
+    u = np.asarray(u, dtype=np.float64)
+    conn = np.asarray(conn, dtype=np.int64)
+    m = len(conn)
+    X = [xref[conn[:, k]] for k in range(4)]
+    U = [u[conn[:, k]] for k in range(4)]
+    M = [[X[r + 1][:, c] - X[0][:, c] for c in range(3)] for r in range(3)]
+    det = (M[0][0] * (M[1][1] * M[2][2] - M[2][1] * M[1][2])
+           - M[0][1] * (M[1][0] * M[2][2] - M[2][0] * M[1][2])
+           + M[0][2] * (M[1][0] * M[2][1] - M[2][0] * M[1][1]))
+    di = 1. / det
+    n = [[None] * 3 for _ in range(3)]
+    n[0][0] = di * (M[1][1] * M[2][2] - M[2][1] * M[1][2])
+    n[0][1] = -di * (M[0][1] * M[2][2] - M[2][1] * M[0][2])
+    n[0][2] = di * (M[0][1] * M[1][2] - M[1][1] * M[0][2])
+    n[1][0] = -di * (M[1][0] * M[2][2] - M[2][0] * M[1][2])
+    n[1][1] = di * (M[0][0] * M[2][2] - M[2][0] * M[0][2])
+    n[1][2] = -di * (M[0][0] * M[1][2] - M[1][0] * M[0][2])
+    n[2][0] = di * (M[1][0] * M[2][1] - M[2][0] * M[1][1])
+    n[2][1] = -di * (M[0][0] * M[2][1] - M[2][0] * M[0][1])
+    n[2][2] = di * (M[0][0] * M[1][1] - M[1][0] * M[0][1])
+    r = [(-1.0, -1.0, -1.0), (1.0, 0.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0)]
+    d = []
+    for k in range(4):
+        row = []
+        for a in range(3):
+            v = np.zeros(m)
+            for b in range(3):
+                v = v + n[a][b] * r[k][b]
+            row.append(v)
+        d.append(row)
+    e = np.zeros((m, 6), dtype=F32)
+    for k in range(4):
+        ux, uy, uz = U[k][:, 0], U[k][:, 1], U[k][:, 2]
+        e[:, 0] = _f(e[:, 0].astype(np.float64) + (ux + d[k][0]))
+        e[:, 1] = _f(e[:, 1].astype(np.float64) + (uy + d[k][1]))
+        e[:, 5] = _f(e[:, 5].astype(np.float64) + (0.5 * ux * d[k][1] + 0.5 * uy * d[k][0]))
+        e[:, 2] = _f(e[:, 2].astype(np.float64) + (uz + d[k][2]))
+        e[:, 3] = _f(e[:, 3].astype(np.float64) + (0.5 * uy * d[k][2] + 0.5 * uz * d[k][1]))
+        e[:, 4] = _f(e[:, 4].astype(np.float64) + (0.5 * ux * d[k][2] + 0.5 * uz * d[k][0]))
+    tr = ((e[:, 0] + e[:, 1]) + e[:, 2]).astype(np.float64)
+    lam_ = np.asarray(lam, dtype=np.float64)
+    mu2 = 2.0 * np.asarray(mu, dtype=np.float64)
+    t = np.zeros((m, 6), dtype=F32)
+    for a in (0, 1, 2):
+        t[:, a] = _f(lam_ * tr + mu2 * e[:, a].astype(np.float64))
+    for a in (3, 4, 5):
+        t[:, a] = _f(mu2 * e[:, a].astype(np.float64))
+    N = (1. - 0.25 - 0.25 - 0.25, 0.25, 0.25, 0.25)
+    xq = np.zeros((m, 3, 3))
+    strain = np.zeros((m, 3, 6))
+    stress = np.zeros((m, 3, 6))
+    for c in range(3):
+        p = np.zeros(m)
+        for k in range(4):
+            p = p + N[k] * X[k][:, c]
+        for k in range(4):
+            p = p + U[k][:, c] * N[k]
+        xq[:, 0, c] = p
+    strain[:, 0] = e
+    stress[:, 0] = t
+    return xq.reshape(m * 3, 3), strain.reshape(m * 3, 6), stress.reshape(m * 3, 6)

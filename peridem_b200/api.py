@@ -107,6 +107,7 @@ SIGNATURES = {
     "pdgpu_kernel_times": [c_vp, c_i32, P(ctypes.c_char_p), P(c_d), P(c_i64), P(c_i32)],
     "pdgpu_strain_stress_tri": [c_vp, c_i64, P(c_i64), c_i32, P(c_d), P(c_d), P(c_d), P(c_d), P(ctypes.c_uint8),
                                 P(c_d), P(c_d), P(c_d)],
+    "pdgpu_strain_stress_tet": [c_vp, c_i64, P(c_i64), P(c_d), P(c_d), P(c_d), P(c_d), P(c_d), P(c_d)],
     "pdgpu_enable_rebuild_phases": [c_vp, c_i32],
     "pdgpu_rebuild_phases": [c_vp, P(c_i64), c_i32, P(c_i32)],
     "pdgpu_compute_pd_forces": [c_vp],

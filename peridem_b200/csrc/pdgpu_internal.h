@@ -360,6 +360,10 @@ void launch_contact_owner(const DevData &d, cudaStream_t s);
 cudaError_t launch_strain_tri(const DevData &d, int64_t n_elem, const int64_t *conn, int nq, const double *pts,
                               const double *nu, const double *lam, const double *mu, const uint8_t *plane_strain,
                               double *xq, double *strain, double *stress, cudaStream_t s);
+// the same for linear tetrahedra (3-D), the one-point rule
+cudaError_t launch_strain_tet(const DevData &d, int64_t n_elem, const int64_t *conn, const double *nu,
+                              const double *lam, const double *mu, double *xq, double *strain, double *stress,
+                              cudaStream_t s);
 constexpr int kRebuildPhases = 16;
 int rebuild_grid_blocks(const DevData &d, int lanes);
 cudaError_t launch_contact_rebuild(const DevData &d, int64_t *bsum, int grid, int lanes, int init,

@@ -2358,40 +2358,50 @@ int pdgpu_enable_timing(pdgpu_ctx *ctx, int32_t on) {
   return PDGPU_OK;
 }
 
-int pdgpu_strain_stress_tri(pdgpu_ctx *ctx, int64_t n_elements, const int64_t *conn, int32_t nq,
-                            const double *ref_points, const double *nu, const double *lambda, const double *mu,
-                            const uint8_t *plane_strain, double *xq, double *strain, double *stress) {
-  if (!ctx || n_elements < 0 || (n_elements > 0 && (!conn || !ref_points || !nu || !lambda || !mu ||
-                                                    !plane_strain || !xq || !strain || !stress)))
+}  // extern "C"
+
+namespace {
+
+// host side of the strain/stress output: checks, device copies of the
+// element data, the kernel, the three entries per element back to the host
+int strain_stress(pdgpu_ctx *ctx, const char *who, int nv, int64_t n_elements, const int64_t *conn, int32_t nq,
+                  const double *ref_points, const double *nu, const double *lambda, const double *mu,
+                  const uint8_t *plane_strain, double *xq, double *strain, double *stress) {
+  if (!ctx || n_elements < 0 || (n_elements > 0 && (!conn || (nv == 3 && (!ref_points || !plane_strain)) || !nu ||
+                                                    !lambda || !mu || !xq || !strain || !stress)))
     return PDGPU_ERR_ARG;
-  if (!ctx->nodes) return fail(ctx, PDGPU_ERR_STATE, "strain_stress_tri: upload nodes first");
+  if (!ctx->nodes) return fail(ctx, PDGPU_ERR_STATE, "%s: upload nodes first", who);
   DevData &d = ctx->d;
-  if (d.dim != 2) return fail(ctx, PDGPU_ERR_ARG, "strain_stress_tri: triangles need a 2-D context");
-  if (nq < 1 || nq > 3)
-    return fail(ctx, PDGPU_ERR_ARG, "strain_stress_tri: %d quadrature points (the reference keeps three entries "
-                "per triangle; rules of 1 or 3 points)", nq);
-  for (int64_t k = 0; k < 3 * n_elements; k++)
+  if (d.dim != (nv == 3 ? 2 : 3))
+    return fail(ctx, PDGPU_ERR_ARG, "%s: %s need a %d-D context", who, nv == 3 ? "triangles" : "tetrahedra",
+                nv == 3 ? 2 : 3);
+  if (nv == 3 && (nq < 1 || nq > 3))
+    return fail(ctx, PDGPU_ERR_ARG, "%s: %d quadrature points (the reference keeps three entries per triangle; "
+                "rules of 1 or 3 points)", who, nq);
+  for (int64_t k = 0; k < (int64_t)nv * n_elements; k++)
     if (conn[k] < 0 || conn[k] >= d.n_nodes)
-      return fail(ctx, PDGPU_ERR_ARG, "strain_stress_tri: element %lld names node %lld of %lld",
-                  (long long)(k / 3), (long long)conn[k], (long long)d.n_nodes);
+      return fail(ctx, PDGPU_ERR_ARG, "%s: element %lld names node %lld of %lld", who, (long long)(k / nv),
+                  (long long)conn[k], (long long)d.n_nodes);
   if (n_elements == 0) return PDGPU_OK;
   const size_t m = (size_t)n_elements;
   int64_t *dconn = nullptr;
   double *dmat = nullptr, *dout = nullptr;
   uint8_t *dps = nullptr;
-  cudaError_t e = cudaMalloc(&dconn, 3 * m * sizeof(int64_t));
+  cudaError_t e = cudaMalloc(&dconn, (size_t)nv * m * sizeof(int64_t));
   if (e == cudaSuccess) e = cudaMalloc(&dmat, 3 * m * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&dps, m);
   if (e == cudaSuccess) e = cudaMalloc(&dout, 3 * m * 15 * sizeof(double));
   cudaStream_t s = ctx->stream;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dconn, conn, 3 * m * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dconn, conn, (size_t)nv * m * sizeof(int64_t), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dmat, nu, m * sizeof(double), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dmat + m, lambda, m * sizeof(double), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dmat + 2 * m, mu, m * sizeof(double), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dps, plane_strain, m, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && nv == 3) e = cudaMemcpyAsync(dps, plane_strain, m, cudaMemcpyHostToDevice, s);
   double *oxq = dout, *ost = dout + 9 * m, *oss = dout + 27 * m;
   if (e == cudaSuccess)
-    e = launch_strain_tri(d, n_elements, dconn, nq, ref_points, dmat, dmat + m, dmat + 2 * m, dps, oxq, ost, oss, s);
+    e = nv == 3 ? launch_strain_tri(d, n_elements, dconn, nq, ref_points, dmat, dmat + m, dmat + 2 * m, dps, oxq,
+                                    ost, oss, s)
+                : launch_strain_tet(d, n_elements, dconn, dmat, dmat + m, dmat + 2 * m, oxq, ost, oss, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(xq, oxq, 9 * m * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(strain, ost, 18 * m * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(stress, oss, 18 * m * sizeof(double), cudaMemcpyDeviceToHost, s);
@@ -2401,8 +2411,25 @@ int pdgpu_strain_stress_tri(pdgpu_ctx *ctx, int64_t n_elements, const int64_t *c
   cudaFree(dps);
   cudaFree(dout);
   if (e != cudaSuccess || es != cudaSuccess)
-    return fail(ctx, PDGPU_ERR_CUDA, "strain_stress_tri: %s", cudaGetErrorString(e != cudaSuccess ? e : es));
+    return fail(ctx, PDGPU_ERR_CUDA, "%s: %s", who, cudaGetErrorString(e != cudaSuccess ? e : es));
   return device_error(ctx);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pdgpu_strain_stress_tri(pdgpu_ctx *ctx, int64_t n_elements, const int64_t *conn, int32_t nq,
+                            const double *ref_points, const double *nu, const double *lambda, const double *mu,
+                            const uint8_t *plane_strain, double *xq, double *strain, double *stress) {
+  return strain_stress(ctx, "strain_stress_tri", 3, n_elements, conn, nq, ref_points, nu, lambda, mu, plane_strain,
+                       xq, strain, stress);
+}
+
+int pdgpu_strain_stress_tet(pdgpu_ctx *ctx, int64_t n_elements, const int64_t *conn, const double *nu,
+                            const double *lambda, const double *mu, double *xq, double *strain, double *stress) {
+  return strain_stress(ctx, "strain_stress_tet", 4, n_elements, conn, 1, nullptr, nu, lambda, mu, nullptr, xq,
+                       strain, stress);
 }
 
 int pdgpu_enable_rebuild_phases(pdgpu_ctx *ctx, int32_t on) {

@@ -111,7 +111,115 @@ __global__ void __launch_bounds__(kStrainBlock)
   }
 }
 
+// Linear tetrahedra (3-D), the one-point rule (the centroid; the
+// reference's only tetrahedron rule that fits the three entries it stores
+// per element): J rows x_k - x_0 (k = 1..3), detJ by cofactors along the
+// first row, J^-1 as the adjugate times 1/detJ (util::inv), dN/dx = J^-1 r
+// (util::dot) for r = (-1, -1, -1), (1, 0, 0), (0, 1, 0), (0, 0, 1)
+// (fe::TetElem::getQuadDatas); the position (((0 + N0 x0) + N1 x1) + N2 x2) +
+// N3 x3 per component plus u_i N_i; strain per node i: xx, yy, xy, then zz,
+// yz, xz; no plane-strain or plane-stress rule in 3-D.
+__global__ void __launch_bounds__(kStrainBlock)
+    k_strain_tet(const double *__restrict__ xref, const double *__restrict__ u, int64_t n_elem,
+                 const int64_t *__restrict__ conn, const double *__restrict__ nu, const double *__restrict__ lam,
+                 const double *__restrict__ mu, double *__restrict__ xq, double *__restrict__ strain,
+                 double *__restrict__ stress) {
+  const int64_t e = (int64_t)blockIdx.x * kStrainBlock + threadIdx.x;
+  if (e >= n_elem) return;
+  double x[4][3], uu[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int64_t i = conn[4 * e + k];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      x[k][c] = xref[4 * i + c];
+      uu[k][c] = u[4 * i + c];
+    }
+  }
+  double m[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) m[r][c] = x[r + 1][c] - x[0][c];
+  const double det = m[0][0] * (m[1][1] * m[2][2] - m[2][1] * m[1][2]) -
+                     m[0][1] * (m[1][0] * m[2][2] - m[2][0] * m[1][2]) +
+                     m[0][2] * (m[1][0] * m[2][1] - m[2][0] * m[1][1]);
+  const double di = 1. / det;
+  double n[3][3];
+  n[0][0] = di * (m[1][1] * m[2][2] - m[2][1] * m[1][2]);
+  n[0][1] = -di * (m[0][1] * m[2][2] - m[2][1] * m[0][2]);
+  n[0][2] = di * (m[0][1] * m[1][2] - m[1][1] * m[0][2]);
+  n[1][0] = -di * (m[1][0] * m[2][2] - m[2][0] * m[1][2]);
+  n[1][1] = di * (m[0][0] * m[2][2] - m[2][0] * m[0][2]);
+  n[1][2] = -di * (m[0][0] * m[1][2] - m[1][0] * m[0][2]);
+  n[2][0] = di * (m[1][0] * m[2][1] - m[2][0] * m[1][1]);
+  n[2][1] = -di * (m[0][0] * m[2][1] - m[2][0] * m[0][1]);
+  n[2][2] = di * (m[0][0] * m[1][1] - m[1][0] * m[0][1]);
+  const double r[4][3] = {{-1.0, -1.0, -1.0}, {1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+  double dn[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      double v = 0.0;
+#pragma unroll
+      for (int b = 0; b < 3; b++) v += n[a][b] * r[k][b];
+      dn[k][a] = v;
+    }
+  float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // xx, yy, zz, yz, xz, xy
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    s[0] = acc(s[0], uu[k][0] + dn[k][0]);
+    s[1] = acc(s[1], uu[k][1] + dn[k][1]);
+    s[5] = acc(s[5], 0.5 * uu[k][0] * dn[k][1] + 0.5 * uu[k][1] * dn[k][0]);
+    s[2] = acc(s[2], uu[k][2] + dn[k][2]);
+    s[3] = acc(s[3], 0.5 * uu[k][1] * dn[k][2] + 0.5 * uu[k][2] * dn[k][1]);
+    s[4] = acc(s[4], 0.5 * uu[k][0] * dn[k][2] + 0.5 * uu[k][2] * dn[k][0]);
+  }
+  const double lam_e = lam[e], mu2 = 2.0 * mu[e];
+  (void)nu;
+  const double tr = (double)((s[0] + s[1]) + s[2]);
+  float t[6];
+  t[0] = (float)(lam_e * tr + mu2 * (double)s[0]);
+  t[5] = (float)(mu2 * (double)s[5]);
+  t[4] = (float)(mu2 * (double)s[4]);
+  t[1] = (float)(lam_e * tr + mu2 * (double)s[1]);
+  t[3] = (float)(mu2 * (double)s[3]);
+  t[2] = (float)(lam_e * tr + mu2 * (double)s[2]);
+  const double N[4] = {1. - 0.25 - 0.25 - 0.25, 0.25, 0.25, 0.25};
+  double c[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    double p = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) p += N[k] * x[k][a];
+#pragma unroll
+    for (int k = 0; k < 4; k++) p += uu[k][a] * N[k];
+    c[a] = p;
+  }
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const int64_t o = 3 * e + q;
+#pragma unroll
+    for (int a = 0; a < 3; a++) xq[3 * o + a] = q == 0 ? c[a] : 0.0;
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+      strain[6 * o + a] = q == 0 ? (double)s[a] : 0.0;
+      stress[6 * o + a] = q == 0 ? (double)t[a] : 0.0;
+    }
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_strain_tet(const DevData &d, int64_t n_elem, const int64_t *conn, const double *nu,
+                              const double *lam, const double *mu, double *xq, double *strain, double *stress,
+                              cudaStream_t s) {
+  if (n_elem <= 0) return cudaSuccess;
+  const unsigned g = (unsigned)((n_elem + kStrainBlock - 1) / kStrainBlock);
+  k_strain_tet<<<g, kStrainBlock, 0, s>>>(d.xref, d.u, n_elem, conn, nu, lam, mu, xq, strain, stress);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_strain_tri(const DevData &d, int64_t n_elem, const int64_t *conn, int nq, const double *pts,
                               const double *nu, const double *lam, const double *mu, const uint8_t *plane_strain,

@@ -21,8 +21,9 @@ from typing import Dict, List, Tuple
 
 import numpy as np
 
-# vtk cell type of a linear triangle (util::vtk_type_triangle)
+# vtk cell types of a linear triangle and tetrahedron (util::vtk_type_*)
 VTK_TRIANGLE = 5
+VTK_TETRA = 10
 
 # reference-triangle quadrature points per order, in the reference's order
 TRI_POINTS: Dict[int, List[Tuple[float, float]]] = {
@@ -57,3 +58,25 @@ def grid_triangles(x: np.ndarray, h: float) -> np.ndarray:
         else:
             tris += [(k0, k1, k3), (k1, k2, k3)]
     return np.array(tris, dtype=np.int64).reshape(-1, 3)
+
+
+def grid_tetrahedra(x: np.ndarray, h: float) -> np.ndarray:
+    """Linear tetrahedra over a cubic grid of spacing h (nodes x [n, 3]):
+    every grid cube whose eight corners are nodes becomes six tetrahedra
+    around its main diagonal (one per order of the three axis steps).
+    Returns connectivity [m, 4] (node ids)."""
+    ijk = np.round(np.asarray(x)[:, :3] / h).astype(np.int64)
+    index = {tuple(int(v) for v in p): k for k, p in enumerate(ijk)}
+    steps = ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0))
+    tets = []
+    for p0, k0 in sorted(index.items()):
+        corners = [(p0[0] + a, p0[1] + b, p0[2] + c) for a in (0, 1) for b in (0, 1) for c in (0, 1)]
+        if any(q not in index for q in corners):
+            continue
+        for order in steps:
+            path, cur = [k0], list(p0)
+            for ax in order:
+                cur[ax] += 1
+                path.append(index[tuple(cur)])
+            tets.append(path)
+    return np.array(tets, dtype=np.int64).reshape(-1, 4)

@@ -405,6 +405,21 @@ class GpuDEMModel:
             _ptr(xq, ctypes.c_double), _ptr(strain, ctypes.c_double), _ptr(stress, ctypes.c_double)))
         return xq, strain, stress
 
+    def strain_stress_tet(self, conn: np.ndarray, nu, lam, mu):
+        """Quadrature-point strain and stress of linear tetrahedra (3-D) from
+        the current displacement, one-point rule (pdgpu_strain_stress_tet):
+        conn [m, 4]; returns xq [3 m, 3], strain and stress [3 m, 6]."""
+        conn = np.ascontiguousarray(conn, dtype=np.int64).reshape(-1, 4)
+        m = len(conn)
+        arr = [np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=np.float64), (m,))) for a in (nu, lam, mu)]
+        xq = np.zeros((3 * m, 3))
+        strain = np.zeros((3 * m, 6))
+        stress = np.zeros((3 * m, 6))
+        self._check(self.lib.pdgpu_strain_stress_tet(
+            self.ctx, m, _ptr(conn, ctypes.c_int64), *(_ptr(a, ctypes.c_double) for a in arr),
+            _ptr(xq, ctypes.c_double), _ptr(strain, ctypes.c_double), _ptr(stress, ctypes.c_double)))
+        return xq, strain, stress
+
     def rebuild_phases(self, on: Optional[bool] = None) -> List[int]:
         """Phase clock of the contact-list rebuild (pdgpu_enable_rebuild_phases /
         pdgpu_rebuild_phases): with `on` given, switch recording; returns the

@@ -1,8 +1,9 @@
-"""pdgpu_strain_stress_tri (the Strain_Stress output on the GPU) against the
-reference's own fe::getCurrentQuadPoints / fe::getStrainStress: bit for bit
-with tests/golden/strain_tri.npz (made by the reference from the same
-two-particle scene's nodes and displacement), orders 1 and 2, plane strain
-and plane stress; argument checks on the host."""
+"""pdgpu_strain_stress_tri / _tet (the Strain_Stress output on the GPU)
+against the reference's own fe::getCurrentQuadPoints / fe::getStrainStress:
+bit for bit with tests/golden/strain_tri.npz (made by the reference from the
+same two-particle scene's nodes and displacement; orders 1 and 2, plane
+strain and plane stress) and strain_tet.npz (a two-sphere column's
+tetrahedra, the one-point rule); argument checks on the host."""
 import os
 import sys
 
@@ -54,3 +55,23 @@ def test_strain_stress_refuses_bad_arguments():
             m.strain_stress_tri(G["conn"], 3, 0.25, 1.0, 1.0, 0)
     finally:
         m.close()
+
+
+GT = np.load(os.path.join(HERE, "golden", "strain_tet.npz"))
+
+
+def test_tet_strain_stress_matches_reference():
+    import make_strain_golden as mk
+    from peridem_b200 import scene as scn
+    from peridem_b200.model import GpuDEMModel, PREC_FP64
+    nu, lam, mu = GT["material"]
+    sc = scn.build_scene(mk.scene_spec_3d())
+    m = GpuDEMModel(sc, precision=PREC_FP64, build_neighbors=True, compute_mx=True)
+    try:
+        m.set_field("u", GT["u"])
+        xq, e, s = m.strain_stress_tet(GT["conn"], nu, lam, mu)
+    finally:
+        m.close()
+    assert np.array_equal(xq, GT["o1_xq"]), float(np.max(np.abs(xq - GT["o1_xq"])))
+    assert np.array_equal(e, GT["o1_strain"]), float(np.max(np.abs(e - GT["o1_strain"])))
+    assert np.array_equal(s, GT["o1_stress"]), float(np.max(np.abs(s - GT["o1_stress"])))

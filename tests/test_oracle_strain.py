@@ -53,3 +53,24 @@ def test_fixtures_reproduce_with_the_reference():
     xq, e, s = mk.run_reference(G["xref"], G["u"], G["conn"], 2, 1, nu, lam, mu)
     assert np.array_equal(xq, G["o2_ps1_xq"]) and np.array_equal(e, G["o2_ps1_strain"])
     assert np.array_equal(s, G["o2_ps1_stress"])
+
+
+GT = np.load(os.path.join(HERE, "golden", "strain_tet.npz"))
+
+
+def test_tet_restatement_matches_reference_fixtures():
+    nu, lam, mu = GT["material"]
+    m = len(GT["conn"])
+    xq, e, s = fe_strain.strain_stress_tet(GT["xref"], GT["u"], GT["conn"], np.full(m, lam), np.full(m, mu))
+    assert np.array_equal(xq, GT["o1_xq"])
+    assert np.array_equal(e, GT["o1_strain"])
+    assert np.array_equal(s, GT["o1_stress"])
+
+
+def test_tet_fixture_mesh_is_the_column_scene():
+    import make_strain_golden as mk
+    from peridem_b200 import scene as scn
+    spec = mk.scene_spec_3d()
+    sc = scn.build_scene(spec)
+    assert np.array_equal(np.asarray(sc.xref), GT["xref"])
+    assert np.array_equal(mk.mesh_3d(sc, spec), GT["conn"])
