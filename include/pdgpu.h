@@ -465,6 +465,14 @@ PDGPU_API int pdgpu_strain_stress_tet(pdgpu_ctx *ctx, int64_t n_elements, const 
                                       const double *lambda, const double *mu, double *xq, double *strain,
                                       double *stress);
 
+/* The file VtkParticleWriter::appendStrainStress writes
+ * (vtkParticleWriter.cpp:444-495, output_strain_<n>.vtu): the quadrature
+ * points as points (no cells), point arrays Strain and Stress of six
+ * components named xx, yy, zz, yz, xz, xy, and the context's time as TIME,
+ * as raw appended VTK XML (pdgpu_write_vtu's format). */
+PDGPU_API int pdgpu_write_strain_vtu(pdgpu_ctx *ctx, const char *path, int64_t n_points, const double *xq,
+                                     const double *strain, const double *stress);
+
 /* Phase clock of the contact-list rebuild (a profiling aid): with on != 0
  * every later rebuild records the GPU global timer (ns) as its first CTA
  * passes each grid-wide barrier, in order: start, cells cleared, nodes

@@ -108,6 +108,7 @@ SIGNATURES = {
     "pdgpu_strain_stress_tri": [c_vp, c_i64, P(c_i64), c_i32, P(c_d), P(c_d), P(c_d), P(c_d), P(ctypes.c_uint8),
                                 P(c_d), P(c_d), P(c_d)],
     "pdgpu_strain_stress_tet": [c_vp, c_i64, P(c_i64), P(c_d), P(c_d), P(c_d), P(c_d), P(c_d), P(c_d)],
+    "pdgpu_write_strain_vtu": [c_vp, ctypes.c_char_p, c_i64, P(c_d), P(c_d), P(c_d)],
     "pdgpu_enable_rebuild_phases": [c_vp, c_i32],
     "pdgpu_rebuild_phases": [c_vp, P(c_i64), c_i32, P(c_i32)],
     "pdgpu_compute_pd_forces": [c_vp],

@@ -1632,6 +1632,7 @@ struct VtuArray {
   std::string name, type;
   int comps;
   std::vector<unsigned char> bytes;
+  std::vector<std::string> comp_names;  // optional; x, y, z for three components
 };
 
 template <typename T>
@@ -1663,6 +1664,9 @@ struct VtuFrame {
   std::vector<double> x, u, v, f, theta;
   std::vector<float> Z;
 };
+
+bool write_points_vtu(const char *path, int64_t N, double t, const std::vector<double> &points,
+                      const std::vector<VtuArray> &pdata, std::string *err);
 
 // The arrays of VtkParticleWriter::appendNodes (vtkParticleWriter.cpp:39-270),
 // in its order, as raw appended VTK XML.  Host work only (safe on another
@@ -1701,8 +1705,15 @@ bool write_frame(const pdgpu_ctx *ctx, const VtuFrame &fr, const std::string &T,
   if (has_tag(T, "Damage_Z"))
     pdata.push_back(vtu_array("Damage_Z", "Float64", 1, std::vector<double>(fr.Z.begin(), fr.Z.end())));
   if (has_tag(T, "Theta") && !fr.theta.empty()) pdata.push_back(vtu_array("Theta", "Float64", 1, fr.theta));
-  const VtuArray time = vtu_array("TIME", "Float64", 1, std::vector<double>{fr.time});
-  const VtuArray pts = vtu_array("Points", "Float64", 3, fr.x);
+  return write_points_vtu(path, N, fr.time, fr.x, pdata, err);
+}
+
+// A points-only unstructured grid (no cells) with a TIME field and the given
+// point arrays, as raw appended VTK XML.
+bool write_points_vtu(const char *path, int64_t N, double t, const std::vector<double> &points,
+                      const std::vector<VtuArray> &pdata, std::string *err) {
+  const VtuArray time = vtu_array("TIME", "Float64", 1, std::vector<double>{t});
+  const VtuArray pts = vtu_array("Points", "Float64", 3, points);
   const VtuArray conn = vtu_array("connectivity", "Int64", 1, std::vector<int64_t>{});
   const VtuArray offs = vtu_array("offsets", "Int64", 1, std::vector<int64_t>{});
   const VtuArray types = vtu_array("types", "UInt8", 1, std::vector<uint8_t>{});
@@ -1723,7 +1734,12 @@ bool write_frame(const pdgpu_ctx *ctx, const VtuFrame &fr, const std::string &T,
     std::string s = "<DataArray type=\"" + a.type + "\" Name=\"" + a.name + "\"";
     if (a.comps > 1) {
       s += " NumberOfComponents=\"" + std::to_string(a.comps) + "\"";
-      if (a.comps == 3) s += " ComponentName0=\"x\" ComponentName1=\"y\" ComponentName2=\"z\"";
+      if (!a.comp_names.empty()) {
+        for (size_t c = 0; c < a.comp_names.size(); c++)
+          s += " ComponentName" + std::to_string(c) + "=\"" + a.comp_names[c] + "\"";
+      } else if (a.comps == 3) {
+        s += " ComponentName0=\"x\" ComponentName1=\"y\" ComponentName2=\"z\"";
+      }
     }
     if (tuples >= 0) s += " NumberOfTuples=\"" + std::to_string(tuples) + "\"";
     s += " format=\"appended\" offset=\"" + std::to_string(off[k]) + "\"/>\n";
@@ -2430,6 +2446,24 @@ int pdgpu_strain_stress_tet(pdgpu_ctx *ctx, int64_t n_elements, const int64_t *c
                             const double *lambda, const double *mu, double *xq, double *strain, double *stress) {
   return strain_stress(ctx, "strain_stress_tet", 4, n_elements, conn, 1, nullptr, nu, lambda, mu, nullptr, xq,
                        strain, stress);
+}
+
+int pdgpu_write_strain_vtu(pdgpu_ctx *ctx, const char *path, int64_t n_points, const double *xq,
+                           const double *strain, const double *stress) {
+  if (!ctx || !path || n_points < 0 || (n_points > 0 && (!xq || !strain || !stress))) return PDGPU_ERR_ARG;
+  CtrlState c;
+  TRY(read_ctrl(ctx, &c));
+  const size_t n = (size_t)n_points;
+  std::vector<VtuArray> pdata;
+  const std::vector<std::string> names{"xx", "yy", "zz", "yz", "xz", "xy"};
+  pdata.push_back(vtu_array("Strain", "Float64", 6, std::vector<double>(strain, strain + 6 * n)));
+  pdata.back().comp_names = names;
+  pdata.push_back(vtu_array("Stress", "Float64", 6, std::vector<double>(stress, stress + 6 * n)));
+  pdata.back().comp_names = names;
+  std::string err;
+  if (!write_points_vtu(path, n_points, c.time, std::vector<double>(xq, xq + 3 * n), pdata, &err))
+    return fail(ctx, PDGPU_ERR_ARG, "write_strain_vtu: %s", err.c_str());
+  return PDGPU_OK;
 }
 
 int pdgpu_enable_rebuild_phases(pdgpu_ctx *ctx, int32_t on) {

@@ -420,6 +420,13 @@ class GpuDEMModel:
             _ptr(xq, ctypes.c_double), _ptr(strain, ctypes.c_double), _ptr(stress, ctypes.c_double)))
         return xq, strain, stress
 
+    def write_strain_vtu(self, path: str, xq: np.ndarray, strain: np.ndarray, stress: np.ndarray) -> None:
+        """output_strain_<n>.vtu as VtkParticleWriter::appendStrainStress writes
+        it (pdgpu_write_strain_vtu), from strain_stress_tri/_tet results."""
+        xq, strain, stress = (np.ascontiguousarray(a, dtype=np.float64) for a in (xq, strain, stress))
+        self._check(self.lib.pdgpu_write_strain_vtu(self.ctx, path.encode(), len(xq), _ptr(xq, ctypes.c_double),
+                                                    _ptr(strain, ctypes.c_double), _ptr(stress, ctypes.c_double)))
+
     def rebuild_phases(self, on: Optional[bool] = None) -> List[int]:
         """Phase clock of the contact-list rebuild (pdgpu_enable_rebuild_phases /
         pdgpu_rebuild_phases): with `on` given, switch recording; returns the

@@ -75,3 +75,23 @@ def test_tet_strain_stress_matches_reference():
     assert np.array_equal(xq, GT["o1_xq"]), float(np.max(np.abs(xq - GT["o1_xq"])))
     assert np.array_equal(e, GT["o1_strain"]), float(np.max(np.abs(e - GT["o1_strain"])))
     assert np.array_equal(s, GT["o1_stress"]), float(np.max(np.abs(s - GT["o1_stress"])))
+
+
+def test_strain_vtu_holds_the_arrays(tmp_path):
+    """pdgpu_write_strain_vtu: the quadrature points as points, Strain and
+    Stress with components xx..xy, TIME (VtkParticleWriter::appendStrainStress)."""
+    from test_gpu_output import _read
+    nu, lam, mu = G["material"]
+    m = _model()
+    try:
+        xq, e, s = m.strain_stress_tri(G["conn"], 2, nu, lam, mu, 1)
+        path = str(tmp_path / "output_strain_0.vtu")
+        m.write_strain_vtu(path, xq, e, s)
+    finally:
+        m.close()
+    root, arrays = _read(path)
+    assert np.array_equal(arrays["Points"], xq)
+    assert np.array_equal(arrays["Strain"], e) and np.array_equal(arrays["Stress"], s)
+    da = [d for d in root.iter("DataArray") if d.get("Name") == "Strain"][0]
+    assert [da.get(f"ComponentName{k}") for k in range(6)] == ["xx", "yy", "zz", "yz", "xz", "xy"]
+    assert arrays["TIME"].shape == (1, 1)
