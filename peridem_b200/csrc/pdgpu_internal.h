@@ -310,6 +310,11 @@ void launch_sur_gather(const double *u, const SurPart *parts, int P, int n_nodes
 void launch_sur_scatter(double *f, const SurPart *parts, int P, int n_nodes, const float *F, int ldf,
                         const uint8_t *on, const uint8_t *near, const CtrlState *ctrl, double *err2,
                         unsigned long long *count, cudaStream_t s);
+// the projection fused with the gather (CUDA cores, phi^T staged in shared
+// memory): sur_fused_setup(kpad) != 0 when it fits and is set up
+int sur_fused_setup(int kpad);
+void launch_sur_gather_project(const double *u, const SurPart *parts, int P, int n_nodes, int kpad,
+                               const void *phiT, void *xy, cudaStream_t s);
 void launch_sur_gate(const DevData &d, const SurPart *parts, int P, const double *err2, float z_gate,
                      double err_gate, cudaStream_t s);
 void launch_pack_vec(const DevData &d, const double *aos3, double *dst, cudaStream_t s);

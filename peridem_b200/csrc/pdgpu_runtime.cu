@@ -105,6 +105,7 @@ struct pdgpu_ctx {
   std::vector<SurShape> sur;
   GemmProblem *sur_probs = nullptr;  // device: 5 stages x shapes
   int sur_max_p = 0, sur_max_k = 0;
+  bool sur_fused = false;  // projection and lift fused with gather and scatter (all shapes fit)
   double *sur_err2 = nullptr;        // per particle: squared error, squared norm (last check)
   int32_t *sur_errflag = nullptr;    // a tensor-core wait timed out
   unsigned long long *sur_count = nullptr;  // particle-steps on the surrogate, covered
@@ -971,13 +972,22 @@ void pd_forces(pdgpu_ctx *ctx) {
 void sur_forward(pdgpu_ctx *ctx, cudaStream_t s) {
   const DevData &d = ctx->d;
   const int ns = (int)ctx->sur.size();
-  for (auto &S : ctx->sur) launch_sur_gather(d.u, S.parts, S.P, S.n_nodes, S.A, S.kpad, nullptr, s);
   const int pm = ctx->sur_max_p, km = ctx->sur_max_k;
-  launch_tc_gemm_grouped(ctx->sur_probs + 0 * ns, ns, pm, 32, 32, ctx->sur_errflag, s);    // projection
-  launch_tc_gemm_grouped(ctx->sur_probs + 1 * ns, ns, pm, 256, 256, ctx->sur_errflag, s);  // layer 1
-  launch_tc_gemm_grouped(ctx->sur_probs + 2 * ns, ns, pm, 256, 256, ctx->sur_errflag, s);  // layer 2
-  launch_tc_gemm_grouped(ctx->sur_probs + 3 * ns, ns, pm, 32, 32, ctx->sur_errflag, s);    // layer 3
-  launch_tc_gemm_grouped(ctx->sur_probs + 4 * ns, ns, pm, km, 256, ctx->sur_errflag, s);   // lift
+  if (ctx->sur_fused) {
+    // gather + projection on CUDA cores (phi^T in shared memory: a long
+    // reduction of little work per row, which the tensor-core tiles would
+    // walk serially on a few CTAs)
+    for (auto &S : ctx->sur) launch_sur_gather_project(d.u, S.parts, S.P, S.n_nodes, S.kpad, S.phiT, S.xy, s);
+  } else {
+    for (auto &S : ctx->sur) launch_sur_gather(d.u, S.parts, S.P, S.n_nodes, S.A, S.kpad, nullptr, s);
+    launch_tc_gemm_grouped(ctx->sur_probs + 0 * ns, ns, pm, 32, 32, ctx->sur_errflag, s);  // projection
+  }
+  // 64-column tiles: four (layers) and kpad / 64 (lift) CTAs per 128-row
+  // tile instead of one and kpad / 256
+  launch_tc_gemm_grouped(ctx->sur_probs + 1 * ns, ns, pm, 256, 64, ctx->sur_errflag, s);  // layer 1
+  launch_tc_gemm_grouped(ctx->sur_probs + 2 * ns, ns, pm, 256, 64, ctx->sur_errflag, s);  // layer 2
+  launch_tc_gemm_grouped(ctx->sur_probs + 3 * ns, ns, pm, 32, 32, ctx->sur_errflag, s);   // layer 3
+  launch_tc_gemm_grouped(ctx->sur_probs + 4 * ns, ns, pm, km, 64, ctx->sur_errflag, s);   // lift
 }
 
 // After the bond loop: surrogate forces into f (ordinary steps) or, on check
@@ -2071,6 +2081,7 @@ int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape 
   }
   TRY(dalloc(ctx, &ctx->sur_probs, probs.size()));
   CK(cudaMemcpy(ctx->sur_probs, probs.data(), probs.size() * sizeof(GemmProblem), cudaMemcpyHostToDevice));
+  ctx->sur_fused = sur_fused_setup(ctx->sur_max_k) != 0;
   TRY(dalloc(ctx, &ctx->sur_err2, 2 * ctx->hp.size()));
   CK(cudaMemset(ctx->sur_err2, 0, 2 * ctx->hp.size() * 8));
   TRY(dalloc(ctx, &ctx->sur_errflag, 1));

@@ -16,6 +16,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "pdgpu_internal.h"
@@ -226,6 +227,53 @@ __global__ void k_adam(float *p, float *m, float *v, const float *g, int64_t n, 
   }
 }
 
+// Gather and projection in one pass.  The projection x = A phi^T has one
+// row per particle, 32 columns and K = 2 n_nodes: a long reduction with
+// little work per row, which the tensor-core tiles walk serially on a few
+// CTAs.  Here one CTA per row (rows 0..P-1, and row P, the zero input): the
+// body-frame displacement, rounded to BF16 (the GEMM's A operand), goes to
+// shared memory, and each warp forms four of the 32 dot products with FP32
+// accumulation, reading phi^T through the read-only cache (every CTA of an
+// SM reads the same 32 rows), written as BF16 into xy[:, 32:64].
+__global__ void __launch_bounds__(256) k_gather_project(const double *__restrict__ u,
+                                                        const SurPart *__restrict__ parts, int P, int n_nodes,
+                                                        int kpad, const __nv_bfloat16 *__restrict__ phiT,
+                                                        __nv_bfloat16 *__restrict__ xy) {
+  extern __shared__ __align__(16) float s_row[];  // kpad
+  const int k = blockIdx.x;
+  if (k > P) return;
+  if (k < P) {
+    const SurPart sp = parts[k];
+    const double uc0 = u[2 * sp.center], uc1 = u[2 * sp.center + 1];
+    for (int a = threadIdx.x; a < kpad / 2; a += blockDim.x) {
+      float b0 = 0.f, b1 = 0.f;
+      if (a < n_nodes) {
+        const int64_t i = sp.start + a;
+        const double d0 = u[2 * i] - uc0, d1 = u[2 * i + 1] - uc1;
+        b0 = (float)((sp.c * d0 + sp.s * d1) * sp.inv_scale);
+        b1 = (float)((-sp.s * d0 + sp.c * d1) * sp.inv_scale);
+      }
+      s_row[2 * a] = __bfloat162float(__float2bfloat16(b0));
+      s_row[2 * a + 1] = __bfloat162float(__float2bfloat16(b1));
+    }
+  } else {
+    for (int a = threadIdx.x; a < kpad; a += blockDim.x) s_row[a] = 0.f;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int j = warp; j < 32; j += (int)(blockDim.x >> 5)) {
+    const __nv_bfloat162 *ph = reinterpret_cast<const __nv_bfloat162 *>(phiT + (size_t)j * kpad);
+    float acc = 0.f;
+    for (int a = lane; a < kpad / 2; a += 32) {
+      const float2 w = __bfloat1622float2(__ldg(ph + a));
+      acc += s_row[2 * a] * w.x;
+      acc += s_row[2 * a + 1] * w.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) xy[(size_t)k * 64 + 32 + j] = __float2bfloat16(acc);
+  }
+}
+
 unsigned blocks(int64_t n, int t) {
   const int64_t b = (n + t - 1) / t;
   return (unsigned)(b < 4096 ? (b > 0 ? b : 1) : 4096);
@@ -242,6 +290,21 @@ void launch_sur_scatter(double *f, const SurPart *parts, int P, int n_nodes, con
                         const uint8_t *on, const uint8_t *near, const CtrlState *ctrl, double *err2,
                         unsigned long long *count, cudaStream_t s) {
   if (P > 0) sur::k_scatter<<<P, 256, 0, s>>>(f, parts, P, n_nodes, F, ldf, on, near, ctrl, err2, count);
+}
+
+size_t sur_project_smem(int kpad) { return (size_t)4 * kpad; }
+
+void launch_sur_gather_project(const double *u, const SurPart *parts, int P, int n_nodes, int kpad,
+                               const void *phiT, void *xy, cudaStream_t s) {
+  sur::k_gather_project<<<P + 1, 256, sur_project_smem(kpad), s>>>(u, parts, P, n_nodes, kpad,
+                                                                  (const __nv_bfloat16 *)phiT, (__nv_bfloat16 *)xy);
+}
+
+int sur_fused_setup(int kpad) {
+  // the fused kernel keeps one row (kpad floats) in shared memory
+  if (sur_project_smem(kpad) > 227 * 1024 - 1024) return 0;
+  return cudaFuncSetAttribute(sur::k_gather_project, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sur_project_smem(kpad)) == cudaSuccess;
 }
 
 void launch_sur_gate(const DevData &d, const SurPart *parts, int P, const double *err2, float z_gate,
