@@ -218,7 +218,7 @@ struct DevData {
   int2 *c_span;          // [c_row[i], c_row[i + 1]) of compacted node t = c_nodes[t]
   uint16_t *nzone;        // zone of each node's particle
   DampParticle *dpart;   // per particle: bounding radius, density, zone, type
-  double *pcen;          // per particle: centre position and velocity (8 doubles), this step
+  double *pcen;          // per particle, this step: {x, y, z, bounding radius, vx, vy, vz, -}
 
   // boundary conditions: per BC node, a run of entries applied in set order
   int32_t n_ubc_sets, n_fbc_sets;
@@ -307,16 +307,29 @@ int launch_tc_gemm_grouped(const GemmProblem *probs, int n_probs, int max_m, int
 // learned surrogate around the GEMMs (pdgpu_surrogate.cu)
 void launch_sur_gather(const double *u, const SurPart *parts, int P, int n_nodes, void *A, int lda, float *Af,
                        cudaStream_t s);
-void launch_sur_scatter(double *f, const SurPart *parts, int P, int n_nodes, const float *F, int ldf,
-                        const uint8_t *on, const uint8_t *near, const CtrlState *ctrl, double *err2,
-                        unsigned long long *count, cudaStream_t s);
-// the projection fused with the gather (CUDA cores, phi^T staged in shared
-// memory): sur_fused_setup(kpad) != 0 when it fits and is set up
+
+// one surrogate shape as the per-step kernels see it (one launch covers
+// every shape: blockIdx.y is the shape, blockIdx.x the particle row)
+struct SurShapeDev {
+  const SurPart *parts;
+  int32_t P, n_nodes, kpad, pad;
+  const void *phiT;  // 32 x kpad BF16
+  void *xy;          // (P + 1) x 64 BF16: [network output | projected input]
+  const float *F;    // (P + 1) x kpad FP32: the lift's output
+};
+
+// the projection fused with the gather (CUDA cores; phi^T read through the
+// read-only cache, each element for several rows): sur_fused_setup(kpad) != 0
+// when its rows fit shared memory
 int sur_fused_setup(int kpad);
-void launch_sur_gather_project(const double *u, const SurPart *parts, int P, int n_nodes, int kpad,
-                               const void *phiT, void *xy, cudaStream_t s);
-void launch_sur_gate(const DevData &d, const SurPart *parts, int P, const double *err2, float z_gate,
-                     double err_gate, cudaStream_t s);
+void launch_sur_gather_project(const double *u, const SurShapeDev *shapes, int n_shapes, int max_p, int max_kpad,
+                               cudaStream_t s);
+void launch_sur_scatter_all(double *f, const SurShapeDev *shapes, int n_shapes, int max_p, const uint8_t *on,
+                            const uint8_t *near, const CtrlState *ctrl, double *err2, unsigned long long *count,
+                            cudaStream_t s);
+void launch_sur_gate_all(const DevData &d, const SurShapeDev *shapes, int n_shapes, int max_p, const double *err2,
+                         float z_gate, double err_gate, cudaStream_t s);
+
 void launch_pack_vec(const DevData &d, const double *aos3, double *dst, cudaStream_t s);
 void launch_unpack_vec(const DevData &d, const double *src, double *aos3, cudaStream_t s);
 void launch_apply_ic(const DevData &d, cudaStream_t s);

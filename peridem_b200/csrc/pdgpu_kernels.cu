@@ -1123,12 +1123,13 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
       double xc[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
       ldv<DIM>(d.x, c, xc);
       ldv<DIM>(d.v, c, vc);
-      double *o = d.pcen + 8 * p;
+      double *o = d.pcen + 8 * p;  // {x, y, z, bounding radius, vx, vy, vz, -}
 #pragma unroll
       for (int q = 0; q < 3; q++) {
         o[q] = xc[q];
-        o[3 + q] = vc[q];
+        o[4 + q] = vc[q];
       }
+      o[3] = d.dpart[p].bound_r;
     }
   }
   __syncthreads();
@@ -1255,12 +1256,15 @@ __global__ void __launch_bounds__(kBlock) k_contact_warp(DevData d) {
     double xc[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
     ldv<DIM>(d.x, c, xc);
     ldv<DIM>(d.v, c, vc);
+    // record {x, y, z, bounding radius, vx, vy, vz, -}: the damping pass's
+    // pair search reads only the first 32 bytes
     double *o = d.pcen + 8 * p;
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       o[q] = xc[q];
-      o[3 + q] = vc[q];
+      o[4 + q] = vc[q];
     }
+    o[3] = d.dpart[p].bound_r;
   }
   __syncthreads();
   const int64_t nn = err ? 0 : nn_raw;
@@ -1438,21 +1442,25 @@ __global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
   double xc[3], vc[3];
   for (int q = 0; q < 3; q++) {
     xc[q] = d.pcen[8 * p + q];
-    vc[q] = d.pcen[8 * p + 3 + q];
+    vc[q] = d.pcen[8 * p + 4 + q];
   }
   double acc[3] = {0.0, 0.0, 0.0};
-  // particle-particle, over the particles of this particle's scene
+  // particle-particle, over the particles of this particle's scene: first
+  // the 32-byte {centre, radius} record only, against the largest reach any
+  // zone pair allows
   for (int q = P.q0 + threadIdx.x; q < P.q1; q += blockDim.x) {
     if (q == p) continue;
+    const double2 c01 = *reinterpret_cast<const double2 *>(d.pcen + 8 * q);
+    const double2 c2r = *reinterpret_cast<const double2 *>(d.pcen + 8 * q + 2);
+    double xcj[3] = {c01.x - xc[0], c01.y - xc[1], c2r.x - xc[2]};
+    const double d2 = xcj[0] * xcj[0] + xcj[1] * xcj[1] + xcj[2] * xcj[2];
+    const double reach_max = c2r.y + Ri + 1.01 * d.rc_max;
+    if (d2 > 1.0625 * reach_max * reach_max) continue;
     const DampParticle Q = d.dpart[q];
     if (Q.type != 0) continue;
     const double Rj = Q.bound_r;
-    double xcj[3], vcj[3];
-    for (int t = 0; t < 3; t++) {
-      xcj[t] = d.pcen[8 * q + t] - xc[t];
-      vcj[t] = d.pcen[8 * q + 3 + t] - vc[t];
-    }
-    const double d2 = xcj[0] * xcj[0] + xcj[1] * xcj[1] + xcj[2] * xcj[2];
+    double vcj[3];
+    for (int t = 0; t < 3; t++) vcj[t] = d.pcen[8 * q + 4 + t] - vc[t];
     const ContactPair cp = tab ? cps[P.zone * nz + Q.zone] : d.contact[P.zone * nz + Q.zone];
     const double reach = Rj + Ri + 1.01 * cp.rc;
     // pairs well beyond the reach cannot pass the relative-tolerance test

@@ -105,7 +105,9 @@ struct pdgpu_ctx {
   std::vector<SurShape> sur;
   GemmProblem *sur_probs = nullptr;  // device: 5 stages x shapes
   int sur_max_p = 0, sur_max_k = 0;
-  bool sur_fused = false;  // projection and lift fused with gather and scatter (all shapes fit)
+  bool sur_fused = false;  // projection fused with the gather (the row fits shared memory)
+  SurShapeDev *sur_dev = nullptr;  // device: the shapes as the per-step kernels see them
+  int sur_max_rows = 0;            // largest particle count of a shape
   double *sur_err2 = nullptr;        // per particle: squared error, squared norm (last check)
   int32_t *sur_errflag = nullptr;    // a tensor-core wait timed out
   unsigned long long *sur_count = nullptr;  // particle-steps on the surrogate, covered
@@ -974,10 +976,10 @@ void sur_forward(pdgpu_ctx *ctx, cudaStream_t s) {
   const int ns = (int)ctx->sur.size();
   const int pm = ctx->sur_max_p, km = ctx->sur_max_k;
   if (ctx->sur_fused) {
-    // gather + projection on CUDA cores (phi^T in shared memory: a long
+    // gather + projection on CUDA cores, every shape in one launch (a long
     // reduction of little work per row, which the tensor-core tiles would
     // walk serially on a few CTAs)
-    for (auto &S : ctx->sur) launch_sur_gather_project(d.u, S.parts, S.P, S.n_nodes, S.kpad, S.phiT, S.xy, s);
+    launch_sur_gather_project(d.u, ctx->sur_dev, ns, ctx->sur_max_rows, km, s);
   } else {
     for (auto &S : ctx->sur) launch_sur_gather(d.u, S.parts, S.P, S.n_nodes, S.A, S.kpad, nullptr, s);
     launch_tc_gemm_grouped(ctx->sur_probs + 0 * ns, ns, pm, 32, 32, ctx->sur_errflag, s);  // projection
@@ -994,13 +996,10 @@ void sur_forward(pdgpu_ctx *ctx, cudaStream_t s) {
 // steps, the comparison with the bond loop and the gate.
 void sur_apply(pdgpu_ctx *ctx, cudaStream_t s) {
   const DevData &d = ctx->d;
-  for (auto &S : ctx->sur) {
-    launch_sur_scatter(d.f, S.parts, S.P, S.n_nodes, S.F, S.kpad, d.sur_on, d.sur_near, d.ctrl, nullptr,
-                       ctx->sur_count, s);
-    launch_sur_scatter(d.f, S.parts, S.P, S.n_nodes, S.F, S.kpad, d.sur_on, d.sur_near, d.ctrl, ctx->sur_err2,
-                       ctx->sur_count, s);
-    launch_sur_gate(d, S.parts, S.P, ctx->sur_err2, ctx->sur_z_gate, ctx->sur_err_gate, s);
-  }
+  const int ns = (int)ctx->sur.size();
+  launch_sur_scatter_all(d.f, ctx->sur_dev, ns, ctx->sur_max_rows, d.sur_on, d.sur_near, d.ctrl, ctx->sur_err2,
+                         ctx->sur_count, s);
+  launch_sur_gate_all(d, ctx->sur_dev, ns, ctx->sur_max_rows, ctx->sur_err2, ctx->sur_z_gate, ctx->sur_err_gate, s);
 }
 
 // Contact forces and particle damping depend on positions and velocities
@@ -2082,6 +2081,13 @@ int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape 
   TRY(dalloc(ctx, &ctx->sur_probs, probs.size()));
   CK(cudaMemcpy(ctx->sur_probs, probs.data(), probs.size() * sizeof(GemmProblem), cudaMemcpyHostToDevice));
   ctx->sur_fused = sur_fused_setup(ctx->sur_max_k) != 0;
+  std::vector<SurShapeDev> sd;
+  for (auto &S : ctx->sur) {
+    sd.push_back(SurShapeDev{S.parts, S.P, S.n_nodes, S.kpad, 0, S.phiT, S.xy, S.F});
+    ctx->sur_max_rows = std::max(ctx->sur_max_rows, S.P);
+  }
+  TRY(dalloc(ctx, &ctx->sur_dev, sd.size()));
+  CK(cudaMemcpy(ctx->sur_dev, sd.data(), sd.size() * sizeof(SurShapeDev), cudaMemcpyHostToDevice));
   TRY(dalloc(ctx, &ctx->sur_err2, 2 * ctx->hp.size()));
   CK(cudaMemset(ctx->sur_err2, 0, 2 * ctx->hp.size() * 8));
   TRY(dalloc(ctx, &ctx->sur_errflag, 1));

@@ -49,79 +49,21 @@ __global__ void k_gather(const double *__restrict__ u, const SurPart *__restrict
   }
 }
 
-// Body-frame FP32 force rows -> f of the particles on the surrogate
-// (ordinary steps); with err2 != NULL (check steps) the squared difference
-// to the bond loop's f and the squared norm of f are summed per particle
-// instead.  Row P of F is the chain's output for a zero input (row P of the
-// gathered input is never written): it is subtracted, so zero deformation
-// gives exactly zero force whatever the roundings of the chain.  count[0]
-// counts particle-steps on the surrogate, count[1] particle-steps covered.
-__global__ void k_scatter(double *__restrict__ f, const SurPart *__restrict__ parts, int P, int n_nodes,
-                          const float *__restrict__ F, int ldf, const uint8_t *__restrict__ on,
-                          const uint8_t *__restrict__ near, const CtrlState *ctrl, double *__restrict__ err2,
-                          unsigned long long *__restrict__ count) {
-  __shared__ double red[2][32];
-  const int k = blockIdx.x;
-  if (k >= P || ctrl->error) return;
-  const SurPart sp = parts[k];
-  const bool check = err2 != nullptr;
-  if (check != (ctrl->sur_check != 0)) return;  // scatter on ordinary steps, compare on check steps
-  const bool use = !check && on[sp.particle] && !near[sp.particle];
-  if (threadIdx.x == 0) {
-    if (use) atomicAdd(&count[0], 1ull);
-    atomicAdd(&count[1], 1ull);
-  }
-  if (!check && !use) return;
-  const float *F0 = F + (size_t)P * ldf;
-  double e = 0.0, nrm = 0.0;
-  for (int a = threadIdx.x; a < n_nodes; a += blockDim.x) {
-    const float g0 = F[(size_t)k * ldf + 2 * a] - F0[2 * a];
-    const float g1 = F[(size_t)k * ldf + 2 * a + 1] - F0[2 * a + 1];
-    // fscale R(theta) g
-    const double f0 = sp.fscale * (sp.c * (double)g0 - sp.s * (double)g1);
-    const double f1 = sp.fscale * (sp.s * (double)g0 + sp.c * (double)g1);
-    const int64_t i = sp.start + a;
-    if (check) {
-      const double r0 = f[2 * i], r1 = f[2 * i + 1];
-      e += (f0 - r0) * (f0 - r0) + (f1 - r1) * (f1 - r1);
-      nrm += r0 * r0 + r1 * r1;
-    } else {
-      f[2 * i] = f0;
-      f[2 * i + 1] = f1;
-    }
-  }
-  if (!check) return;
-  for (int o = 16; o > 0; o >>= 1) {
-    e += __shfl_xor_sync(0xffffffffu, e, o);
-    nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    red[0][threadIdx.x >> 5] = e;
-    red[1][threadIdx.x >> 5] = nrm;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double se = 0.0, sn = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
-      se += red[0][w];
-      sn += red[1][w];
-    }
-    err2[2 * sp.particle] = se;
-    err2[2 * sp.particle + 1] = sn;
-  }
-}
+// Body-frame FP32 force rows -> f (k_scatter_all below): row P of F is the
+// chain's output for a zero input (row P of the gathered input is never
+// written): it is subtracted, so zero deformation gives exactly zero force
+// whatever the roundings of the chain.  count[0] counts particle-steps on
+// the surrogate, count[1] particle-steps covered.
 
 // Check steps: a particle keeps (or gets) the surrogate when none of its
 // bonds is broken, its damage Z = max |S| / s_c stays below z_gate and the
 // surrogate's force error against the bond loop, |f_s - f|, is below
 // err_gate max(|f|, floor); one CTA per surrogate particle.
-__global__ void k_gate(const DevData d, const SurPart *__restrict__ parts, int P, const double *__restrict__ err2,
-                       float z_gate, double err_gate2) {
+__device__ void gate_one(const DevData &d, const SurPart &sp, const double *__restrict__ err2, float z_gate,
+                         double err_gate2) {
   __shared__ int broken_s;
   __shared__ float zmax_s;
-  const int k = blockIdx.x;
-  if (k >= P || d.ctrl->error || !d.ctrl->sur_check) return;
-  const SurPart sp = parts[k];
+  if (d.ctrl->error || !d.ctrl->sur_check) return;
   const DevParticle &Pp = d.particles[sp.particle];
   if (threadIdx.x == 0) {
     broken_s = 0;
@@ -230,48 +172,132 @@ __global__ void k_adam(float *p, float *m, float *v, const float *g, int64_t n, 
 // Gather and projection in one pass.  The projection x = A phi^T has one
 // row per particle, 32 columns and K = 2 n_nodes: a long reduction with
 // little work per row, which the tensor-core tiles walk serially on a few
-// CTAs.  Here one CTA per row (rows 0..P-1, and row P, the zero input): the
-// body-frame displacement, rounded to BF16 (the GEMM's A operand), goes to
-// shared memory, and each warp forms four of the 32 dot products with FP32
-// accumulation, reading phi^T through the read-only cache (every CTA of an
-// SM reads the same 32 rows), written as BF16 into xy[:, 32:64].
+// CTAs.  Here a CTA takes kProjRows rows (particles; row P is the zero
+// input): their body-frame displacements, rounded to BF16 (the GEMM's A
+// operand), go to shared memory, and each warp forms four of the 32 columns
+// for all of them with FP32 accumulation, so that every element of phi^T it
+// reads (through the read-only cache) serves kProjRows rows.  Written as
+// BF16 into xy[:, 32:64].
+constexpr int kProjRows = 8;
+
 __global__ void __launch_bounds__(256) k_gather_project(const double *__restrict__ u,
-                                                        const SurPart *__restrict__ parts, int P, int n_nodes,
-                                                        int kpad, const __nv_bfloat16 *__restrict__ phiT,
-                                                        __nv_bfloat16 *__restrict__ xy) {
-  extern __shared__ __align__(16) float s_row[];  // kpad
-  const int k = blockIdx.x;
-  if (k > P) return;
-  if (k < P) {
-    const SurPart sp = parts[k];
-    const double uc0 = u[2 * sp.center], uc1 = u[2 * sp.center + 1];
-    for (int a = threadIdx.x; a < kpad / 2; a += blockDim.x) {
-      float b0 = 0.f, b1 = 0.f;
-      if (a < n_nodes) {
-        const int64_t i = sp.start + a;
-        const double d0 = u[2 * i] - uc0, d1 = u[2 * i + 1] - uc1;
-        b0 = (float)((sp.c * d0 + sp.s * d1) * sp.inv_scale);
-        b1 = (float)((-sp.s * d0 + sp.c * d1) * sp.inv_scale);
+                                                        const SurShapeDev *__restrict__ shapes) {
+  extern __shared__ __align__(16) float s_rows[];  // kProjRows x kpad
+  const SurShapeDev S = shapes[blockIdx.y];
+  const int k0 = blockIdx.x * kProjRows, kpad = S.kpad;
+  if (k0 > S.P) return;
+  for (int r = 0; r < kProjRows; r++) {
+    const int k = k0 + r;
+    float *row = s_rows + (size_t)r * kpad;
+    if (k < S.P) {
+      const SurPart sp = S.parts[k];
+      const double uc0 = u[2 * sp.center], uc1 = u[2 * sp.center + 1];
+      for (int a = threadIdx.x; a < kpad / 2; a += blockDim.x) {
+        float b0 = 0.f, b1 = 0.f;
+        if (a < S.n_nodes) {
+          const int64_t i = sp.start + a;
+          const double d0 = u[2 * i] - uc0, d1 = u[2 * i + 1] - uc1;
+          b0 = (float)((sp.c * d0 + sp.s * d1) * sp.inv_scale);
+          b1 = (float)((-sp.s * d0 + sp.c * d1) * sp.inv_scale);
+        }
+        row[2 * a] = __bfloat162float(__float2bfloat16(b0));
+        row[2 * a + 1] = __bfloat162float(__float2bfloat16(b1));
       }
-      s_row[2 * a] = __bfloat162float(__float2bfloat16(b0));
-      s_row[2 * a + 1] = __bfloat162float(__float2bfloat16(b1));
+    } else {  // the zero input (k == P) and rows past it
+      for (int a = threadIdx.x; a < kpad; a += blockDim.x) row[a] = 0.f;
     }
-  } else {
-    for (int a = threadIdx.x; a < kpad; a += blockDim.x) s_row[a] = 0.f;
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const __nv_bfloat16 *phiT = (const __nv_bfloat16 *)S.phiT;
+  __nv_bfloat16 *xy = (__nv_bfloat16 *)S.xy;
   for (int j = warp; j < 32; j += (int)(blockDim.x >> 5)) {
     const __nv_bfloat162 *ph = reinterpret_cast<const __nv_bfloat162 *>(phiT + (size_t)j * kpad);
-    float acc = 0.f;
+    float acc[kProjRows];
+#pragma unroll
+    for (int r = 0; r < kProjRows; r++) acc[r] = 0.f;
     for (int a = lane; a < kpad / 2; a += 32) {
       const float2 w = __bfloat1622float2(__ldg(ph + a));
-      acc += s_row[2 * a] * w.x;
-      acc += s_row[2 * a + 1] * w.y;
+#pragma unroll
+      for (int r = 0; r < kProjRows; r++) {
+        const float2 v = reinterpret_cast<const float2 *>(s_rows + (size_t)r * kpad)[a];
+        acc[r] += v.x * w.x;
+        acc[r] += v.y * w.y;
+      }
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) xy[(size_t)k * 64 + 32 + j] = __float2bfloat16(acc);
+#pragma unroll
+    for (int r = 0; r < kProjRows; r++) {
+      float v = acc[r];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      const int k = k0 + r;
+      if (lane == 0 && k <= S.P) xy[(size_t)k * 64 + 32 + j] = __float2bfloat16(v);
+    }
   }
+}
+
+// k_scatter for every shape in one launch, the step's kind read on the
+// device: the forces into f on ordinary steps, the comparison on check steps
+__global__ void k_scatter_all(double *__restrict__ f, const SurShapeDev *__restrict__ shapes,
+                              const uint8_t *__restrict__ on, const uint8_t *__restrict__ near,
+                              const CtrlState *ctrl, double *__restrict__ err2,
+                              unsigned long long *__restrict__ count) {
+  __shared__ double red[2][32];
+  const SurShapeDev S = shapes[blockIdx.y];
+  const int k = blockIdx.x;
+  if (k >= S.P || ctrl->error) return;
+  const SurPart sp = S.parts[k];
+  const bool check = ctrl->sur_check != 0;
+  const bool use = !check && on[sp.particle] && !near[sp.particle];
+  if (threadIdx.x == 0) {
+    if (use) atomicAdd(&count[0], 1ull);
+    atomicAdd(&count[1], 1ull);
+  }
+  if (!check && !use) return;
+  const int ldf = S.kpad;
+  const float *F = S.F, *F0 = S.F + (size_t)S.P * ldf;
+  double e = 0.0, nrm = 0.0;
+  for (int a = threadIdx.x; a < S.n_nodes; a += blockDim.x) {
+    const float g0 = F[(size_t)k * ldf + 2 * a] - F0[2 * a];
+    const float g1 = F[(size_t)k * ldf + 2 * a + 1] - F0[2 * a + 1];
+    const double f0 = sp.fscale * (sp.c * (double)g0 - sp.s * (double)g1);
+    const double f1 = sp.fscale * (sp.s * (double)g0 + sp.c * (double)g1);
+    const int64_t i = sp.start + a;
+    if (check) {
+      const double r0 = f[2 * i], r1 = f[2 * i + 1];
+      e += (f0 - r0) * (f0 - r0) + (f1 - r1) * (f1 - r1);
+      nrm += r0 * r0 + r1 * r1;
+    } else {
+      f[2 * i] = f0;
+      f[2 * i + 1] = f1;
+    }
+  }
+  if (!check) return;
+  for (int o = 16; o > 0; o >>= 1) {
+    e += __shfl_xor_sync(0xffffffffu, e, o);
+    nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = e;
+    red[1][threadIdx.x >> 5] = nrm;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double se = 0.0, sn = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      se += red[0][w];
+      sn += red[1][w];
+    }
+    err2[2 * sp.particle] = se;
+    err2[2 * sp.particle + 1] = sn;
+  }
+}
+
+// k_gate for every shape in one launch
+__global__ void k_gate_all(const DevData d, const SurShapeDev *__restrict__ shapes, const double *__restrict__ err2,
+                           float z_gate, double err_gate2) {
+  const SurShapeDev S = shapes[blockIdx.y];
+  if ((int)blockIdx.x >= S.P) return;
+  gate_one(d, S.parts[blockIdx.x], err2, z_gate, err_gate2);
 }
 
 unsigned blocks(int64_t n, int t) {
@@ -286,30 +312,33 @@ void launch_sur_gather(const double *u, const SurPart *parts, int P, int n_nodes
   if (P > 0) sur::k_gather<<<P, 256, 0, s>>>(u, parts, P, n_nodes, (__nv_bfloat16 *)A, lda, Af);
 }
 
-void launch_sur_scatter(double *f, const SurPart *parts, int P, int n_nodes, const float *F, int ldf,
-                        const uint8_t *on, const uint8_t *near, const CtrlState *ctrl, double *err2,
-                        unsigned long long *count, cudaStream_t s) {
-  if (P > 0) sur::k_scatter<<<P, 256, 0, s>>>(f, parts, P, n_nodes, F, ldf, on, near, ctrl, err2, count);
+size_t sur_project_smem(int kpad) { return (size_t)4 * sur::kProjRows * kpad; }
+
+void launch_sur_gather_project(const double *u, const SurShapeDev *shapes, int n_shapes, int max_p, int max_kpad,
+                               cudaStream_t s) {
+  const dim3 g((unsigned)((max_p + 1 + sur::kProjRows - 1) / sur::kProjRows), (unsigned)n_shapes);
+  sur::k_gather_project<<<g, 256, sur_project_smem(max_kpad), s>>>(u, shapes);
 }
 
-size_t sur_project_smem(int kpad) { return (size_t)4 * kpad; }
+void launch_sur_scatter_all(double *f, const SurShapeDev *shapes, int n_shapes, int max_p, const uint8_t *on,
+                            const uint8_t *near, const CtrlState *ctrl, double *err2, unsigned long long *count,
+                            cudaStream_t s) {
+  if (max_p > 0) sur::k_scatter_all<<<dim3((unsigned)max_p, (unsigned)n_shapes), 256, 0, s>>>(f, shapes, on, near,
+                                                                                             ctrl, err2, count);
+}
 
-void launch_sur_gather_project(const double *u, const SurPart *parts, int P, int n_nodes, int kpad,
-                               const void *phiT, void *xy, cudaStream_t s) {
-  sur::k_gather_project<<<P + 1, 256, sur_project_smem(kpad), s>>>(u, parts, P, n_nodes, kpad,
-                                                                  (const __nv_bfloat16 *)phiT, (__nv_bfloat16 *)xy);
+void launch_sur_gate_all(const DevData &d, const SurShapeDev *shapes, int n_shapes, int max_p, const double *err2,
+                         float z_gate, double err_gate, cudaStream_t s) {
+  if (max_p > 0)
+    sur::k_gate_all<<<dim3((unsigned)max_p, (unsigned)n_shapes), 256, 0, s>>>(d, shapes, err2, z_gate,
+                                                                             err_gate * err_gate);
 }
 
 int sur_fused_setup(int kpad) {
-  // the fused kernel keeps one row (kpad floats) in shared memory
+  // the fused kernel keeps kProjRows rows (kpad floats each) in shared memory
   if (sur_project_smem(kpad) > 227 * 1024 - 1024) return 0;
   return cudaFuncSetAttribute(sur::k_gather_project, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)sur_project_smem(kpad)) == cudaSuccess;
-}
-
-void launch_sur_gate(const DevData &d, const SurPart *parts, int P, const double *err2, float z_gate,
-                     double err_gate, cudaStream_t s) {
-  if (P > 0) sur::k_gate<<<P, 256, 0, s>>>(d, parts, P, err2, z_gate, err_gate * err_gate);
 }
 
 }  // namespace pdgpu
