@@ -549,6 +549,16 @@ PDGPU_API int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_
                                   const double *scale, int32_t check_interval, double z_gate,
                                   double err_gate, int32_t near_gate);
 
+/* Which kernels evaluate the surrogate in the step (call before
+ * pdgpu_set_surrogate; no counterpart in the reference): 0 (default) CUDA
+ * cores, four launches per step — gather with projection, the three layers,
+ * and the lift with the scatter into f beside the bond loop; 1 the tcgen05
+ * GEMMs the training uses (projection, layers and lift as grouped GEMMs, the
+ * scatter after the bond loop).  Both take BF16 operands with FP32
+ * accumulation and round activations to BF16; they differ in summation
+ * order only. */
+PDGPU_API int pdgpu_set_surrogate_chain(pdgpu_ctx *ctx, int32_t kind);
+
 /* Particles on the surrogate now and particles it covers; and, summed over
  * the steps so far, particle-steps whose force came from the surrogate and
  * particle-steps of the particles it covers. */

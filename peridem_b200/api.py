@@ -121,6 +121,7 @@ SIGNATURES = {
     "pdgpu_restart": [c_vp, ctypes.c_char_p, c_i64],
     "pdgpu_set_scenes": [c_vp, c_i32, P(c_i64), P(c_i64)],
     "pdgpu_get_scene_history": [c_vp, c_i32, P(c_d), P(c_d), P(c_d), P(c_d), c_i64, P(c_i64)],
+    "pdgpu_set_surrogate_chain": [c_vp, c_i32],
     "pdgpu_set_surrogate": [c_vp, c_i32, c_vp, P(c_d), P(c_d), P(c_d), P(c_d), c_i32, c_d, c_d, c_i32],
     "pdgpu_surrogate_stats": [c_vp, P(c_i64), P(c_i64), P(c_i64), P(c_i64)],
     "pdgpu_surrogate_errors": [c_vp, P(c_d), c_i64],

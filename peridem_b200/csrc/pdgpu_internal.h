@@ -315,15 +315,38 @@ struct SurShapeDev {
   int32_t P, n_nodes, kpad, pad;
   const void *phiT;  // 32 x kpad BF16
   void *xy;          // (P + 1) x 64 BF16: [network output | projected input]
-  const float *F;    // (P + 1) x kpad FP32: the lift's output
+  float *F;          // (P + 1) x kpad FP32: body-frame forces (check steps)
+  float *xpart;      // (P + 1) x n_chunks x 32 FP32: the projection's partial sums
+  int32_t n_chunks, pad2;
+  // the CUDA-core chain: layer weights BF16 as [in / 8][out][8] (eight
+  // consecutive inputs of one output in 16 bytes), FP32 biases, and the lift
+  // BF16 as [kpad][64] (per dof its weights of the 64 coefficients)
+  const void *w1q, *w2q, *w3q;
+  const float *b1, *b2, *b3;
+  const void *lift;
 };
 
-// the projection fused with the gather (CUDA cores; phi^T read through the
-// read-only cache, each element for several rows): sur_fused_setup(kpad) != 0
-// when its rows fit shared memory
-int sur_fused_setup(int kpad);
-void launch_sur_gather_project(const double *u, const SurShapeDev *shapes, int n_shapes, int max_p, int max_kpad,
-                               cudaStream_t s);
+int sm_count();  // SMs of the current device
+
+// The surrogate's chain on CUDA cores, every shape in one launch per stage,
+// the shapes by value in the kernel parameters (at most kMaxSurShapes):
+// gather + projection in node chunks (sur_n_chunks(n_nodes) partial sums
+// per row), the three layers, and the lift fused with the scatter into f
+// (ordinary steps; on check steps into F, compared with the bond loop by
+// launch_sur_check_all after it).
+constexpr int kMaxSurShapes = 16;
+struct SurShapes {
+  SurShapeDev s[kMaxSurShapes];
+  int32_t n;
+};
+int sur_n_chunks(int n_nodes);
+void launch_sur_gather_project(const double *u, const SurShapes &shapes, int max_p, int max_nodes, cudaStream_t s);
+void launch_sur_mlp(const SurShapes &shapes, int max_p, cudaStream_t s);
+void launch_sur_lift_scatter(double *f, const SurShapes &shapes, int max_p, int max_nodes, const uint8_t *on,
+                             const uint8_t *near, const CtrlState *ctrl, unsigned long long *count, cudaStream_t s);
+void launch_sur_check_all(const DevData &d, const SurShapes &shapes, double *err2, float z_gate, double err_gate,
+                          cudaStream_t s);
+// the tensor-core chain's scatter (F from the lift GEMM) and gate
 void launch_sur_scatter_all(double *f, const SurShapeDev *shapes, int n_shapes, int max_p, const uint8_t *on,
                             const uint8_t *near, const CtrlState *ctrl, double *err2, unsigned long long *count,
                             cudaStream_t s);

@@ -1447,36 +1447,51 @@ __global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
   double acc[3] = {0.0, 0.0, 0.0};
   // particle-particle, over the particles of this particle's scene: first
   // the 32-byte {centre, radius} record only, against the largest reach any
-  // zone pair allows
-  for (int q = P.q0 + threadIdx.x; q < P.q1; q += blockDim.x) {
-    if (q == p) continue;
-    const double2 c01 = *reinterpret_cast<const double2 *>(d.pcen + 8 * q);
-    const double2 c2r = *reinterpret_cast<const double2 *>(d.pcen + 8 * q + 2);
-    double xcj[3] = {c01.x - xc[0], c01.y - xc[1], c2r.x - xc[2]};
-    const double d2 = xcj[0] * xcj[0] + xcj[1] * xcj[1] + xcj[2] * xcj[2];
-    const double reach_max = c2r.y + Ri + 1.01 * d.rc_max;
-    if (d2 > 1.0625 * reach_max * reach_max) continue;
-    const DampParticle Q = d.dpart[q];
-    if (Q.type != 0) continue;
-    const double Rj = Q.bound_r;
-    double vcj[3];
-    for (int t = 0; t < 3; t++) vcj[t] = d.pcen[8 * q + 4 + t] - vc[t];
-    const ContactPair cp = tab ? cps[P.zone * nz + Q.zone] : d.contact[P.zone * nz + Q.zone];
-    const double reach = Rj + Ri + 1.01 * cp.rc;
-    // pairs well beyond the reach cannot pass the relative-tolerance test
-    if (d2 > 1.0625 * reach * reach) continue;
-    const double dist = sqrt(d2);
-    if (is_less(dist, reach)) {
-      const double vol_pj = kPi * Rj * Rj;
-      const double m1 = rhoi * vol_pi, m2 = Q.density * vol_pj;
-      const double meq = 2. * m1 * m2 / (m1 + m2);  // util::equivalentMass
-      const double bn = cp.betan * sqrt(cp.kappa * cp.rc * meq);
-      double hat[3] = {0.0, 0.0, 0.0};
-      if (is_greater(dist, 0.))
-        for (int t = 0; t < 3; t++) hat[t] = xcj[t] / dist;
-      double vm = vcj[0] * hat[0] + vcj[1] * hat[1] + vcj[2] * hat[2];
-      if (vm > 0.) vm = 0.;
-      for (int t = 0; t < 3; t++) acc[t] += bn * vm * hat[t] / vol_pi;
+  // zone pair allows; kDampBatch records in flight per thread, each thread
+  // still visiting its particles in increasing order
+  constexpr int kDampBatch = 4;
+  for (int q0 = P.q0 + threadIdx.x; q0 < P.q1; q0 += kDampBatch * blockDim.x) {
+    double2 c01b[kDampBatch], c2rb[kDampBatch];
+#pragma unroll
+    for (int t = 0; t < kDampBatch; t++) {
+      const int q = q0 + t * (int)blockDim.x;
+      c01b[t] = c2rb[t] = make_double2(0.0, 0.0);
+      if (q < P.q1) {
+        c01b[t] = *reinterpret_cast<const double2 *>(d.pcen + 8 * q);
+        c2rb[t] = *reinterpret_cast<const double2 *>(d.pcen + 8 * q + 2);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < kDampBatch; t++) {
+      const int q = q0 + t * (int)blockDim.x;
+      if (q >= P.q1 || q == p) continue;
+      const double2 c01 = c01b[t], c2r = c2rb[t];
+      double xcj[3] = {c01.x - xc[0], c01.y - xc[1], c2r.x - xc[2]};
+      const double d2 = xcj[0] * xcj[0] + xcj[1] * xcj[1] + xcj[2] * xcj[2];
+      const double reach_max = c2r.y + Ri + 1.01 * d.rc_max;
+      if (d2 > 1.0625 * reach_max * reach_max) continue;
+      const DampParticle Q = d.dpart[q];
+      if (Q.type != 0) continue;
+      const double Rj = Q.bound_r;
+      double vcj[3];
+      for (int c = 0; c < 3; c++) vcj[c] = d.pcen[8 * q + 4 + c] - vc[c];
+      const ContactPair cp = tab ? cps[P.zone * nz + Q.zone] : d.contact[P.zone * nz + Q.zone];
+      const double reach = Rj + Ri + 1.01 * cp.rc;
+      // pairs well beyond the reach cannot pass the relative-tolerance test
+      if (d2 > 1.0625 * reach * reach) continue;
+      const double dist = sqrt(d2);
+      if (is_less(dist, reach)) {
+        const double vol_pj = kPi * Rj * Rj;
+        const double m1 = rhoi * vol_pi, m2 = Q.density * vol_pj;
+        const double meq = 2. * m1 * m2 / (m1 + m2);  // util::equivalentMass
+        const double bn = cp.betan * sqrt(cp.kappa * cp.rc * meq);
+        double hat[3] = {0.0, 0.0, 0.0};
+        if (is_greater(dist, 0.))
+          for (int c = 0; c < 3; c++) hat[c] = xcj[c] / dist;
+        double vm = vcj[0] * hat[0] + vcj[1] * hat[1] + vcj[2] * hat[2];
+        if (vm > 0.) vm = 0.;
+        for (int c = 0; c < 3; c++) acc[c] += bn * vm * hat[c] / vol_pi;
+      }
     }
   }
   // particle-wall: unique wall nodes within the contact radius of any node

@@ -100,14 +100,18 @@ struct pdgpu_ctx {
     void *phiT = nullptr, *lift = nullptr, *w1 = nullptr, *w2 = nullptr, *w3 = nullptr;
     float *b1 = nullptr, *b2 = nullptr, *b3 = nullptr;
     void *A = nullptr, *xy = nullptr, *h1 = nullptr, *h2 = nullptr;
-    float *F = nullptr;
+    float *F = nullptr, *xpart = nullptr;
+    void *w1q = nullptr, *w2q = nullptr, *w3q = nullptr;  // CUDA-core chain layouts
   };
   std::vector<SurShape> sur;
   GemmProblem *sur_probs = nullptr;  // device: 5 stages x shapes
   int sur_max_p = 0, sur_max_k = 0;
-  bool sur_fused = false;  // projection fused with the gather (the row fits shared memory)
-  SurShapeDev *sur_dev = nullptr;  // device: the shapes as the per-step kernels see them
+  bool sur_fused = false;  // the CUDA-core chain runs
+  int sur_chain = 0;       // requested chain: 0 CUDA cores, 1 tensor-core GEMMs
+  SurShapeDev *sur_dev = nullptr;  // device: the shapes as the tensor-core chain's kernels see them
+  SurShapes sur_shapes{};          // the same, by value for the CUDA-core chain
   int sur_max_rows = 0;            // largest particle count of a shape
+  int sur_max_nodes = 0;           // largest node count of a shape
   double *sur_err2 = nullptr;        // per particle: squared error, squared norm (last check)
   int32_t *sur_errflag = nullptr;    // a tensor-core wait timed out
   unsigned long long *sur_count = nullptr;  // particle-steps on the surrogate, covered
@@ -976,14 +980,19 @@ void sur_forward(pdgpu_ctx *ctx, cudaStream_t s) {
   const int ns = (int)ctx->sur.size();
   const int pm = ctx->sur_max_p, km = ctx->sur_max_k;
   if (ctx->sur_fused) {
-    // gather + projection on CUDA cores, every shape in one launch (a long
-    // reduction of little work per row, which the tensor-core tiles would
-    // walk serially on a few CTAs)
-    launch_sur_gather_project(d.u, ctx->sur_dev, ns, ctx->sur_max_rows, km, s);
-  } else {
-    for (auto &S : ctx->sur) launch_sur_gather(d.u, S.parts, S.P, S.n_nodes, S.A, S.kpad, nullptr, s);
-    launch_tc_gemm_grouped(ctx->sur_probs + 0 * ns, ns, pm, 32, 32, ctx->sur_errflag, s);  // projection
+    // CUDA cores, every shape in one launch per stage: gather + projection
+    // (a long reduction of little work per row, which tensor-core tiles walk
+    // serially on a few CTAs), the three layers (a few rows per SM), and the
+    // lift with the scatter into f for the particles whose tiles the bond
+    // loop skips
+    launch_sur_gather_project(d.u, ctx->sur_shapes, ctx->sur_max_rows, ctx->sur_max_nodes, s);
+    launch_sur_mlp(ctx->sur_shapes, ctx->sur_max_rows, s);
+    launch_sur_lift_scatter(d.f, ctx->sur_shapes, ctx->sur_max_rows, ctx->sur_max_nodes, d.sur_on, d.sur_near,
+                            d.ctrl, ctx->sur_count, s);
+    return;
   }
+  for (auto &S : ctx->sur) launch_sur_gather(d.u, S.parts, S.P, S.n_nodes, S.A, S.kpad, nullptr, s);
+  launch_tc_gemm_grouped(ctx->sur_probs + 0 * ns, ns, pm, 32, 32, ctx->sur_errflag, s);  // projection
   // 64-column tiles: four (layers) and kpad / 64 (lift) CTAs per 128-row
   // tile instead of one and kpad / 256
   launch_tc_gemm_grouped(ctx->sur_probs + 1 * ns, ns, pm, 256, 64, ctx->sur_errflag, s);  // layer 1
@@ -992,11 +1001,16 @@ void sur_forward(pdgpu_ctx *ctx, cudaStream_t s) {
   launch_tc_gemm_grouped(ctx->sur_probs + 4 * ns, ns, pm, km, 64, ctx->sur_errflag, s);   // lift
 }
 
-// After the bond loop: surrogate forces into f (ordinary steps) or, on check
-// steps, the comparison with the bond loop and the gate.
+// After the bond loop: on check steps the comparison with the bond loop and
+// the gate; with the tensor-core chain also the surrogate forces into f on
+// ordinary steps.
 void sur_apply(pdgpu_ctx *ctx, cudaStream_t s) {
   const DevData &d = ctx->d;
   const int ns = (int)ctx->sur.size();
+  if (ctx->sur_fused) {
+    launch_sur_check_all(d, ctx->sur_shapes, ctx->sur_err2, ctx->sur_z_gate, ctx->sur_err_gate, s);
+    return;
+  }
   launch_sur_scatter_all(d.f, ctx->sur_dev, ns, ctx->sur_max_rows, d.sur_on, d.sur_near, d.ctrl, ctx->sur_err2,
                          ctx->sur_count, s);
   launch_sur_gate_all(d, ctx->sur_dev, ns, ctx->sur_max_rows, ctx->sur_err2, ctx->sur_z_gate, ctx->sur_err_gate, s);
@@ -2058,6 +2072,17 @@ int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape 
     TRY(f32(in.b1, 256, &S.b1));
     TRY(f32(in.b2, 256, &S.b2));
     TRY(f32(in.b3, 32, &S.b3));
+    // CUDA-core chain: W[out][in] -> [in / 8][out][8]
+    auto blocked = [&](const float *w, int n_out, int n_in, void **dst) -> int {
+      std::vector<float> h((size_t)n_out * n_in);
+      for (int cb = 0; cb < n_in / 8; cb++)
+        for (int j = 0; j < n_out; j++)
+          for (int t = 0; t < 8; t++) h[((size_t)cb * n_out + j) * 8 + t] = w[(size_t)j * n_in + 8 * cb + t];
+      return bf(h.data(), 1, h.size(), h.size(), 1, dst);
+    };
+    TRY(blocked(in.w1, 256, 32, &S.w1q));
+    TRY(blocked(in.w2, 256, 256, &S.w2q));
+    TRY(blocked(in.w3, 32, 256, &S.w3q));
     const int M = S.P + 1;  // row P: the zero input
     __nv_bfloat16 *A, *xy, *h1, *h2;
     TRY(dalloc(ctx, &A, (size_t)M * S.kpad));
@@ -2066,6 +2091,7 @@ int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape 
     TRY(dalloc(ctx, &h1, (size_t)M * 256));
     TRY(dalloc(ctx, &h2, (size_t)M * 256));
     TRY(dalloc(ctx, &S.F, (size_t)M * S.kpad));
+    TRY(dalloc(ctx, &S.xpart, (size_t)M * sur_n_chunks(S.n_nodes) * 32));
     S.A = A, S.xy = xy, S.h1 = h1, S.h2 = h2;
     // x = A phi^T -> xy[:, 32:64]; h1 = tanh(x W1^T + b1); h2 = tanh(h1 W2^T + b2);
     // y = h2 W3^T + b3 -> xy[:, 0:32]; F = xy lift^T
@@ -2080,11 +2106,17 @@ int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape 
   }
   TRY(dalloc(ctx, &ctx->sur_probs, probs.size()));
   CK(cudaMemcpy(ctx->sur_probs, probs.data(), probs.size() * sizeof(GemmProblem), cudaMemcpyHostToDevice));
-  ctx->sur_fused = sur_fused_setup(ctx->sur_max_k) != 0;
+  ctx->sur_fused = ctx->sur_chain == 0 && n_shapes <= kMaxSurShapes;
   std::vector<SurShapeDev> sd;
   for (auto &S : ctx->sur) {
-    sd.push_back(SurShapeDev{S.parts, S.P, S.n_nodes, S.kpad, 0, S.phiT, S.xy, S.F});
+    sd.push_back(SurShapeDev{S.parts, S.P, S.n_nodes, S.kpad, 0, S.phiT, S.xy, S.F, S.xpart,
+                             sur_n_chunks(S.n_nodes), 0, S.w1q, S.w2q, S.w3q, S.b1, S.b2, S.b3, S.lift});
     ctx->sur_max_rows = std::max(ctx->sur_max_rows, S.P);
+    ctx->sur_max_nodes = std::max(ctx->sur_max_nodes, S.n_nodes);
+  }
+  if (ctx->sur_fused) {
+    ctx->sur_shapes.n = (int32_t)sd.size();
+    for (size_t k = 0; k < sd.size(); k++) ctx->sur_shapes.s[k] = sd[k];
   }
   TRY(dalloc(ctx, &ctx->sur_dev, sd.size()));
   CK(cudaMemcpy(ctx->sur_dev, sd.data(), sd.size() * sizeof(SurShapeDev), cudaMemcpyHostToDevice));
@@ -2357,6 +2389,13 @@ int pdgpu_set_contact_grid(pdgpu_ctx *ctx, int32_t ctas_per_sm) {
   if (!ctx || ctas_per_sm < 1 || ctas_per_sm > 16) return PDGPU_ERR_ARG;
   if (ctx->prepared) return fail(ctx, PDGPU_ERR_STATE, "set_contact_grid: set it before the first step");
   ctx->contact_ctas = ctas_per_sm;
+  return PDGPU_OK;
+}
+
+int pdgpu_set_surrogate_chain(pdgpu_ctx *ctx, int32_t kind) {
+  if (!ctx || kind < 0 || kind > 1) return PDGPU_ERR_ARG;
+  if (!ctx->sur.empty()) return fail(ctx, PDGPU_ERR_STATE, "set_surrogate_chain: set it before set_surrogate");
+  ctx->sur_chain = kind;
   return PDGPU_OK;
 }
 

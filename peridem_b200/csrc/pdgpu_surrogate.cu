@@ -169,68 +169,439 @@ __global__ void k_adam(float *p, float *m, float *v, const float *g, int64_t n, 
   }
 }
 
+// ---- the CUDA-core chain of the step; the shapes travel by value in the
+// kernel parameters, so that no CTA waits on a load of them ----
+
 // Gather and projection in one pass.  The projection x = A phi^T has one
 // row per particle, 32 columns and K = 2 n_nodes: a long reduction with
-// little work per row, which the tensor-core tiles walk serially on a few
-// CTAs.  Here a CTA takes kProjRows rows (particles; row P is the zero
-// input): their body-frame displacements, rounded to BF16 (the GEMM's A
-// operand), go to shared memory, and each warp forms four of the 32 columns
-// for all of them with FP32 accumulation, so that every element of phi^T it
-// reads (through the read-only cache) serves kProjRows rows.  Written as
-// BF16 into xy[:, 32:64].
+// little work per row, which tensor-core tiles walk serially on a few CTAs.
+// Here the reduction is split over CTAs: a CTA takes kProjRows rows
+// (particles; row P is the zero input) and kProjNodes nodes of them.  Its
+// phi^T elements are requested first (they do not depend on the gather);
+// the body-frame displacements, rounded to BF16 (the GEMM's A operand), go
+// to shared memory; warp w forms columns 4w..4w+3 for all rows, each lane
+// over kProjNodes / 32 nodes, FP32 accumulation, and a butterfly leaves lane
+// l the sum of (column 4w + l / 8, row l % 8).  The CTA's partial sums go to
+// xpart[row][chunk][32]; the layers' kernel adds the chunks in a fixed
+// order, so the result does not depend on scheduling.
 constexpr int kProjRows = 8;
+constexpr int kProjNodes = 128;
+constexpr int kProjThreads = 256;
 
-__global__ void __launch_bounds__(256) k_gather_project(const double *__restrict__ u,
-                                                        const SurShapeDev *__restrict__ shapes) {
-  extern __shared__ __align__(16) float s_rows[];  // kProjRows x kpad
-  const SurShapeDev S = shapes[blockIdx.y];
-  const int k0 = blockIdx.x * kProjRows, kpad = S.kpad;
-  if (k0 > S.P) return;
-  for (int r = 0; r < kProjRows; r++) {
-    const int k = k0 + r;
-    float *row = s_rows + (size_t)r * kpad;
-    if (k < S.P) {
-      const SurPart sp = S.parts[k];
-      const double uc0 = u[2 * sp.center], uc1 = u[2 * sp.center + 1];
-      for (int a = threadIdx.x; a < kpad / 2; a += blockDim.x) {
-        float b0 = 0.f, b1 = 0.f;
-        if (a < S.n_nodes) {
-          const int64_t i = sp.start + a;
-          const double d0 = u[2 * i] - uc0, d1 = u[2 * i + 1] - uc1;
-          b0 = (float)((sp.c * d0 + sp.s * d1) * sp.inv_scale);
-          b1 = (float)((-sp.s * d0 + sp.c * d1) * sp.inv_scale);
-        }
-        row[2 * a] = __bfloat162float(__float2bfloat16(b0));
-        row[2 * a + 1] = __bfloat162float(__float2bfloat16(b1));
+__global__ void __launch_bounds__(kProjThreads, 4) k_gather_project(const double *__restrict__ u,
+                                                                 const __grid_constant__ SurShapes shapes) {
+  // per row pair p and node a: (row 2p x, row 2p+1 x, row 2p y, row 2p+1 y)
+  __shared__ __align__(16) float4 s_rows[kProjRows / 2][kProjNodes];
+  __shared__ int64_t s_node[kProjRows][2];  // first node, centre node
+  __shared__ double s_rot[kProjRows][3];    // c, s, 1 / scale
+  const SurShapeDev &S = shapes.s[blockIdx.z];
+  const int k0 = blockIdx.x * kProjRows, a0 = blockIdx.y * kProjNodes;
+  if (k0 > S.P || a0 >= S.n_nodes) return;
+  const int nrow = min(kProjRows, S.P - k0);  // rows with a particle; the rest are zero
+  const int na = min(kProjNodes, S.n_nodes - a0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int kPairs = kProjNodes / 32;  // nodes per lane (a node: one BF16 pair of a phi^T row)
+  const __nv_bfloat162 *ph = reinterpret_cast<const __nv_bfloat162 *>(S.phiT);
+  const int half = S.kpad / 2;  // phi^T row j: half BF16 pairs, pair a = node a
+  __nv_bfloat162 wb[4][kPairs];
+#pragma unroll
+  for (int t = 0; t < 4; t++)
+#pragma unroll
+    for (int m = 0; m < kPairs; m++) {
+      const int a = lane + 32 * m;
+      wb[t][m] = a < na ? __ldg(ph + (size_t)(4 * warp + t) * half + a0 + a) : __floats2bfloat162_rn(0.f, 0.f);
+    }
+  if ((int)threadIdx.x < nrow) {
+    const SurPart sp = S.parts[k0 + threadIdx.x];
+    s_node[threadIdx.x][0] = sp.start;
+    s_node[threadIdx.x][1] = sp.center;
+    s_rot[threadIdx.x][0] = sp.c;
+    s_rot[threadIdx.x][1] = sp.s;
+    s_rot[threadIdx.x][2] = sp.inv_scale;
+  }
+  __syncthreads();
+  constexpr int kItems = kProjRows * kProjNodes / kProjThreads;  // (row, node) pairs per thread
+  {
+    double2 v[kItems], c[kItems];
+#pragma unroll
+    for (int q = 0; q < kItems; q++) {
+      const int e = threadIdx.x + q * kProjThreads, r = e / kProjNodes, a = e % kProjNodes;
+      v[q] = c[q] = make_double2(0.0, 0.0);
+      if (r < nrow && a < na) {
+        v[q] = *reinterpret_cast<const double2 *>(u + 2 * (s_node[r][0] + a0 + a));
+        c[q] = *reinterpret_cast<const double2 *>(u + 2 * s_node[r][1]);
       }
-    } else {  // the zero input (k == P) and rows past it
-      for (int a = threadIdx.x; a < kpad; a += blockDim.x) row[a] = 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < kItems; q++) {
+      const int e = threadIdx.x + q * kProjThreads, r = e / kProjNodes, a = e % kProjNodes;
+      float b0 = 0.f, b1 = 0.f;
+      if (r < nrow && a < na) {
+        const double *R = s_rot[r];
+        const double d0 = v[q].x - c[q].x, d1 = v[q].y - c[q].y;
+        // R(-theta) d / scale
+        b0 = (float)((R[0] * d0 + R[1] * d1) * R[2]);
+        b1 = (float)((-R[1] * d0 + R[0] * d1) * R[2]);
+      }
+      float *o = reinterpret_cast<float *>(&s_rows[r >> 1][a]) + (r & 1);
+      o[0] = __bfloat162float(__float2bfloat16(b0));
+      o[2] = __bfloat162float(__float2bfloat16(b1));
     }
   }
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const __nv_bfloat16 *phiT = (const __nv_bfloat16 *)S.phiT;
-  __nv_bfloat16 *xy = (__nv_bfloat16 *)S.xy;
-  for (int j = warp; j < 32; j += (int)(blockDim.x >> 5)) {
-    const __nv_bfloat162 *ph = reinterpret_cast<const __nv_bfloat162 *>(phiT + (size_t)j * kpad);
-    float acc[kProjRows];
+  // two rows per packed FMA: acc[4 t + p] holds (column 4 warp + t) for rows
+  // 2p and 2p + 1, each element summed in the same order as a scalar loop
+  float2 acc[16];
 #pragma unroll
-    for (int r = 0; r < kProjRows; r++) acc[r] = 0.f;
-    for (int a = lane; a < kpad / 2; a += 32) {
-      const float2 w = __bfloat1622float2(__ldg(ph + a));
+  for (int q = 0; q < 16; q++) acc[q] = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int r = 0; r < kProjRows; r++) {
-        const float2 v = reinterpret_cast<const float2 *>(s_rows + (size_t)r * kpad)[a];
-        acc[r] += v.x * w.x;
-        acc[r] += v.y * w.y;
+  for (int m = 0; m < kPairs; m++) {
+    const int a = lane + 32 * m;
+    float2 w[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) w[t] = __bfloat1622float2(wb[t][m]);
+#pragma unroll
+    for (int p = 0; p < kProjRows / 2; p++) {
+      const float4 x = s_rows[p][a];
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        acc[4 * t + p] = __ffma2_rn(make_float2(x.x, x.y), make_float2(w[t].x, w[t].x), acc[4 * t + p]);
+        acc[4 * t + p] = __ffma2_rn(make_float2(x.z, x.w), make_float2(w[t].y, w[t].y), acc[4 * t + p]);
       }
     }
+  }
+  float v[32];  // v[8 t + r]: column 4 warp + t, row r
 #pragma unroll
-    for (int r = 0; r < kProjRows; r++) {
-      float v = acc[r];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      const int k = k0 + r;
-      if (lane == 0 && k <= S.P) xy[(size_t)k * 64 + 32 + j] = __float2bfloat16(v);
+  for (int q = 0; q < 16; q++) {
+    v[2 * q] = acc[q].x;
+    v[2 * q + 1] = acc[q].y;
+  }
+  // butterfly: after the stage of offset o a lane keeps the half of its
+  // values selected by (lane & o); lane l ends with the total of v[l]
+#pragma unroll
+  for (int o = 16, n = 32; o >= 1; o >>= 1, n >>= 1) {
+    const bool upper = (lane & o) != 0;
+#pragma unroll
+    for (int q = 0; q < n / 2; q++) {
+      const float send = upper ? v[q] : v[q + n / 2];
+      const float keep = upper ? v[q + n / 2] : v[q];
+      v[q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  const int t = lane >> 3, r = lane & 7;
+  if (k0 + r <= S.P)
+    S.xpart[((size_t)(k0 + r) * S.n_chunks + blockIdx.y) * 32 + 4 * warp + t] = v[0];
+}
+
+// eight BF16 (16 bytes) -> FP32
+__device__ __forceinline__ void unpack8(const uint4 w, float *o) {
+  const uint32_t v[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+  for (int t = 0; t < 4; t++) {
+    o[2 * t] = __uint_as_float(v[t] << 16);
+    o[2 * t + 1] = __uint_as_float(v[t] & 0xffff0000u);
+  }
+}
+
+// The three layers of the network for kMlpRows rows (rows 0..P, P the zero
+// input) per CTA on CUDA cores.  The projected input x is the sum of the
+// projection's chunks in chunk order, rounded to BF16 (and stored in
+// xy[:, 32:64] for the lift).  A layer's weights (16-byte loads,
+// [in / 8][out][8]) are read once per CTA and serve all its rows: those of
+// layers 1 and 3 and the first block of layer 2 are requested before the
+// input arrives, and each further block of layer 2 while the previous one
+// is in use.  Activations stay in shared memory, rounded to BF16 as the
+// tensor-core chain stores them.
+//   h1 = tanh(x W1^T + b1), h2 = tanh(h1 W2^T + b2)   thread = output column
+//   y  = h2 W3^T + b3 -> xy[:, 0:32]                   warp = 32 inputs, lane = column
+constexpr int kMlpRows = 8;
+constexpr int kMlpCols = 256;                 // outputs of layers 1 and 2
+constexpr int kMlpThreads = 2 * kMlpCols;     // two threads per output: rows 0-3 and 4-7
+constexpr int kMlpPairs = kMlpRows / 4;       // row pairs per thread
+constexpr int kMlpBlock = 4;  // 16-byte weight loads in flight per thread in layer 2
+
+// Activations are kept per row pair: in[p][c] = (row 2p, row 2p + 1) of
+// input c, so that one packed FMA serves two rows.
+// acc[p] += in[p0 + p][8 cb .. 8 cb + 7] . w (eight inputs, kMlpPairs row pairs)
+__device__ __forceinline__ void rows_dot8(const float2 *__restrict__ in, int ldin, int cb, const uint4 wv,
+                                          float2 *acc) {
+  float w[8];
+  unpack8(wv, w);
+#pragma unroll
+  for (int p = 0; p < kMlpPairs; p++) {
+    const float4 *src = reinterpret_cast<const float4 *>(in + p * ldin + 8 * cb);
+    float2 x = acc[p];
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      const float4 a = src[h];
+      x = __ffma2_rn(make_float2(a.x, a.y), make_float2(w[2 * h], w[2 * h]), x);
+      x = __ffma2_rn(make_float2(a.z, a.w), make_float2(w[2 * h + 1], w[2 * h + 1]), x);
+    }
+    acc[p] = x;
+  }
+}
+
+// out[p0 + p][j] = BF16(tanh(acc[p] + b))
+__device__ __forceinline__ void store_tanh(const float2 *acc, float b, float2 *out, int j) {
+#pragma unroll
+  for (int p = 0; p < kMlpPairs; p++)
+    out[p * kMlpCols + j] = make_float2(__bfloat162float(__float2bfloat16(tanhf(acc[p].x + b))),
+                                        __bfloat162float(__float2bfloat16(tanhf(acc[p].y + b))));
+}
+
+__global__ void __launch_bounds__(kMlpThreads) k_mlp(const __grid_constant__ SurShapes shapes) {
+  __shared__ __align__(16) float2 s_x[kMlpRows / 2 * 32];
+  __shared__ __align__(16) float2 s_h[2][kMlpRows / 2 * kMlpCols];
+  const SurShapeDev &S = shapes.s[blockIdx.y];
+  const int k0 = blockIdx.x * kMlpRows;
+  if (k0 > S.P) return;
+  const int nrow = min(kMlpRows, S.P + 1 - k0);
+  const int j = threadIdx.x % kMlpCols, p0 = (threadIdx.x / kMlpCols) * kMlpPairs;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint4 *w1 = (const uint4 *)S.w1q, *w2 = (const uint4 *)S.w2q, *w3 = (const uint4 *)S.w3q;
+  uint4 v1[4], v2[kMlpBlock];
+#pragma unroll
+  for (int t = 0; t < 4; t++) v1[t] = __ldg(w1 + t * kMlpCols + j);
+#pragma unroll
+  for (int t = 0; t < kMlpBlock; t++) v2[t] = __ldg(w2 + t * kMlpCols + j);
+  const float b1 = S.b1[j], b2 = S.b2[j];
+  __nv_bfloat16 *xy = (__nv_bfloat16 *)S.xy;
+  for (int e = threadIdx.x; e < kMlpRows * 32; e += blockDim.x) {
+    const int r = e >> 5, c = e & 31;
+    float x = 0.f;
+    if (r < nrow) {
+      const float *xp = S.xpart + (size_t)(k0 + r) * S.n_chunks * 32 + c;
+      for (int ch = 0; ch < S.n_chunks; ch++) x += xp[32 * ch];
+      const __nv_bfloat16 xb = __float2bfloat16(x);
+      xy[(size_t)(k0 + r) * 64 + 32 + c] = xb;
+      x = __bfloat162float(xb);
+    }
+    reinterpret_cast<float *>(&s_x[(r >> 1) * 32 + c])[r & 1] = x;
+  }
+  __syncthreads();
+  float2 acc[kMlpPairs];
+#pragma unroll
+  for (int p = 0; p < kMlpPairs; p++) acc[p] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int t = 0; t < 4; t++) rows_dot8(s_x + p0 * 32, 32, t, v1[t], acc);
+  store_tanh(acc, b1, s_h[0] + p0 * kMlpCols, j);
+  __syncthreads();
+#pragma unroll
+  for (int p = 0; p < kMlpPairs; p++) acc[p] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int cb0 = 0; cb0 < 256 / 8; cb0 += kMlpBlock) {
+    uint4 cur[kMlpBlock];
+#pragma unroll
+    for (int t = 0; t < kMlpBlock; t++) cur[t] = v2[t];
+    if (cb0 + kMlpBlock < 256 / 8)
+#pragma unroll
+      for (int t = 0; t < kMlpBlock; t++) v2[t] = __ldg(w2 + (cb0 + kMlpBlock + t) * kMlpCols + j);
+#pragma unroll
+    for (int t = 0; t < kMlpBlock; t++) rows_dot8(s_h[0] + p0 * kMlpCols, kMlpCols, cb0 + t, cur[t], acc);
+  }
+  store_tanh(acc, b2, s_h[1] + p0 * kMlpCols, j);
+  __syncthreads();
+  // layer 3: warp w sums inputs 16 w .. 16 w + 15 for all rows (lane =
+  // output column); partial sums in s_h[0] as [warp][row][column]
+  float2 acc3[kMlpRows / 2];
+#pragma unroll
+  for (int p = 0; p < kMlpRows / 2; p++) acc3[p] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const int cb = 2 * warp + t;
+    float w[8];
+    unpack8(__ldg(w3 + cb * 32 + lane), w);
+#pragma unroll
+    for (int p = 0; p < kMlpRows / 2; p++) {
+      const float4 *src = reinterpret_cast<const float4 *>(s_h[1] + p * kMlpCols + 8 * cb);
+      float2 x = acc3[p];
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        const float4 a = src[h];
+        x = __ffma2_rn(make_float2(a.x, a.y), make_float2(w[2 * h], w[2 * h]), x);
+        x = __ffma2_rn(make_float2(a.z, a.w), make_float2(w[2 * h + 1], w[2 * h + 1]), x);
+      }
+      acc3[p] = x;
+    }
+  }
+  float *red = reinterpret_cast<float *>(s_h[0]);  // 16 warps x 8 rows x 32 = 2 x 2048 floats: s_h[0] and s_h[1]
+  __syncthreads();  // every warp has read h2 before red overwrites it
+#pragma unroll
+  for (int p = 0; p < kMlpRows / 2; p++) {
+    red[(warp * kMlpRows + 2 * p) * 32 + lane] = acc3[p].x;
+    red[(warp * kMlpRows + 2 * p + 1) * 32 + lane] = acc3[p].y;
+  }
+  __syncthreads();
+  if (threadIdx.x < kMlpRows * 32) {
+    const int r = threadIdx.x >> 5, c = threadIdx.x & 31;
+    float y = 0.f;
+    for (int w = 0; w < kMlpThreads / 32; w++) y += red[(w * kMlpRows + r) * 32 + c];
+    if (r < nrow) xy[(size_t)(k0 + r) * 64 + c] = __float2bfloat16(y + S.b3[c]);
+  }
+}
+
+// The lift fused with the scatter, on the tensor cores by warp-level MMA
+// (m16n8k16, BF16 operands, FP32 accumulation): a CTA takes kLiftRows - 1
+// particles plus the zero input (row P) as the 16 rows of one tile, and
+// kLiftNodes nodes (2 kLiftNodes dofs, four 8-dof column tiles per warp);
+// K = 64 (the coefficients [y | x]).  A lane's accumulators hold, per column
+// tile, one node's two components for two rows, so g = F_k - F_P (the zero
+// input's row of the same tile, fetched from the lane that holds it: zero
+// deformation gives exactly zero force) is rotated and stored as it stands.
+// Ordinary steps: f_i = fscale R(theta) g for the particles on the
+// surrogate, whose tiles the bond loop skips, so that this runs beside it;
+// check steps: g into F for the comparison after the bond loop.  count[0]
+// counts particle-steps on the surrogate, count[1] particle-steps covered.
+constexpr int kLiftRows = 16;           // 15 particles + the zero input
+constexpr int kLiftNodes = 128;
+constexpr int kLiftThreads = 256;       // 8 warps x 4 column tiles x 4 nodes
+constexpr int kLiftTiles = 2 * kLiftNodes / 8 / (kLiftThreads / 32);
+
+__device__ __forceinline__ void mma_bf16_16816(float *d, const uint32_t *a, const uint32_t *b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(kLiftThreads) k_lift_scatter(double *__restrict__ f,
+                                                               const __grid_constant__ SurShapes shapes,
+                                                               const uint8_t *__restrict__ on,
+                                                               const uint8_t *__restrict__ near,
+                                                               const CtrlState *ctrl,
+                                                               unsigned long long *__restrict__ count) {
+  __shared__ SurPart s_part[kLiftRows - 1];
+  __shared__ int s_use[kLiftRows - 1];
+  const SurShapeDev &S = shapes.s[blockIdx.z];
+  const int k0 = blockIdx.x * (kLiftRows - 1), a0 = blockIdx.y * kLiftNodes;
+  if (k0 >= S.P || a0 >= S.n_nodes) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+  const int nrow = min(kLiftRows - 1, S.P - k0);
+  // B fragments: lift[dof][c] (row-major [kpad][64]); the warp's column tiles
+  // cover dofs d0 + 8 t .. d0 + 8 t + 7; dofs past 2 n_nodes are zero rows
+  const uint32_t *L = (const uint32_t *)S.lift;  // BF16 pairs: L[dof * 32 + c / 2]
+  const int d0 = 2 * a0 + warp * 8 * kLiftTiles;
+  uint32_t b[kLiftTiles][4][2];
+#pragma unroll
+  for (int t = 0; t < kLiftTiles; t++) {
+    const int dof = d0 + 8 * t + g;
+    const bool in = dof < S.kpad;
+#pragma unroll
+    for (int ks = 0; ks < 4; ks++) {
+      b[t][ks][0] = in ? __ldg(L + (size_t)dof * 32 + 8 * ks + tig) : 0u;
+      b[t][ks][1] = in ? __ldg(L + (size_t)dof * 32 + 8 * ks + 4 + tig) : 0u;
+    }
+  }
+  // A fragments: rows g and g + 8 of the tile; tile row 15 (and rows past
+  // the shape's particles) read the zero input's row P
+  const uint32_t *X = (const uint32_t *)S.xy;  // BF16 pairs: xy[row * 32 + c / 2]
+  const int ra = (g < nrow) ? k0 + g : S.P;
+  const int rb = (g + 8 < nrow) ? k0 + g + 8 : S.P;
+  uint32_t av[4][4];
+#pragma unroll
+  for (int ks = 0; ks < 4; ks++) {
+    av[ks][0] = X[(size_t)ra * 32 + 8 * ks + tig];
+    av[ks][1] = X[(size_t)rb * 32 + 8 * ks + tig];
+    av[ks][2] = X[(size_t)ra * 32 + 8 * ks + 4 + tig];
+    av[ks][3] = X[(size_t)rb * 32 + 8 * ks + 4 + tig];
+  }
+  const bool check = ctrl->sur_check != 0;
+  const bool error = ctrl->error != 0;
+  if (threadIdx.x < kLiftRows - 1) {
+    int use = 0;
+    if ((int)threadIdx.x < nrow) {
+      const SurPart sp = S.parts[k0 + threadIdx.x];
+      s_part[threadIdx.x] = sp;
+      use = check || (on[sp.particle] && !near[sp.particle]);
+    }
+    s_use[threadIdx.x] = use;
+  }
+  __syncthreads();
+  if (error) return;
+  int n_use = 0;
+#pragma unroll
+  for (int r = 0; r < kLiftRows - 1; r++) n_use += s_use[r];
+  if (threadIdx.x == 0 && blockIdx.y == 0) {
+    if (!check && n_use) atomicAdd(&count[0], (unsigned long long)n_use);
+    atomicAdd(&count[1], (unsigned long long)nrow);
+  }
+  if (n_use == 0) return;  // uniform over the CTA
+  float acc[kLiftTiles][4];
+#pragma unroll
+  for (int t = 0; t < kLiftTiles; t++) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[t][q] = 0.f;
+#pragma unroll
+    for (int ks = 0; ks < 4; ks++) mma_bf16_16816(acc[t], av[ks], b[t][ks]);
+  }
+  // lanes 28..31 hold tile row 15 (g = 7, second half): the zero input
+  const int ua = g < nrow && s_use[g], ub = g + 8 < nrow && s_use[g + 8];
+#pragma unroll
+  for (int t = 0; t < kLiftTiles; t++) {
+    const float p0 = __shfl_sync(0xffffffffu, acc[t][2], 28 + tig);
+    const float p1 = __shfl_sync(0xffffffffu, acc[t][3], 28 + tig);
+    const int a = (d0 + 8 * t) / 2 + tig;  // node of this lane's dofs 2a, 2a + 1
+    if (a >= S.n_nodes) continue;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = g + 8 * h;
+      if (!(h ? ub : ua)) continue;
+      const float g0 = acc[t][2 * h] - p0, g1 = acc[t][2 * h + 1] - p1;
+      if (check) {
+        *reinterpret_cast<float2 *>(S.F + (size_t)(k0 + r) * S.kpad + 2 * a) = make_float2(g0, g1);
+      } else {
+        const SurPart &sp = s_part[r];
+        const double f0 = sp.fscale * (sp.c * (double)g0 - sp.s * (double)g1);
+        const double f1 = sp.fscale * (sp.s * (double)g0 + sp.c * (double)g1);
+        *reinterpret_cast<double2 *>(f + 2 * (sp.start + a)) = make_double2(f0, f1);
+      }
+    }
+  }
+}
+
+// Check steps, after the bond loop: per particle |f_s - f|^2 and |f|^2 from
+// the body-frame rows F, then the gate; a grid of one CTA per SM that leaves
+// at once on other steps.
+__global__ void __launch_bounds__(256) k_check_all(const DevData d, const __grid_constant__ SurShapes shapes,
+                                                   double *__restrict__ err2, float z_gate, double err_gate2) {
+  __shared__ double red[2][8];
+  if (d.ctrl->error || !d.ctrl->sur_check) return;
+  for (int sh = 0; sh < shapes.n; sh++) {
+    const SurShapeDev &S = shapes.s[sh];
+    for (int k = blockIdx.x; k < S.P; k += gridDim.x) {
+      const SurPart sp = S.parts[k];
+      const float *F = S.F + (size_t)k * S.kpad;
+      double e = 0.0, nrm = 0.0;
+      for (int a = threadIdx.x; a < S.n_nodes; a += blockDim.x) {
+        const double g0 = F[2 * a], g1 = F[2 * a + 1];
+        const double f0 = sp.fscale * (sp.c * g0 - sp.s * g1);
+        const double f1 = sp.fscale * (sp.s * g0 + sp.c * g1);
+        const int64_t i = sp.start + a;
+        const double r0 = d.f[2 * i], r1 = d.f[2 * i + 1];
+        e += (f0 - r0) * (f0 - r0) + (f1 - r1) * (f1 - r1);
+        nrm += r0 * r0 + r1 * r1;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+        nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+      }
+      if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = e;
+        red[1][threadIdx.x >> 5] = nrm;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double se = 0.0, sn = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+          se += red[0][w];
+          sn += red[1][w];
+        }
+        err2[2 * sp.particle] = se;
+        err2[2 * sp.particle + 1] = sn;
+      }
+      gate_one(d, sp, err2, z_gate, err_gate2);
+      __syncthreads();  // before red and the gate's shared words are reused
     }
   }
 }
@@ -312,12 +683,10 @@ void launch_sur_gather(const double *u, const SurPart *parts, int P, int n_nodes
   if (P > 0) sur::k_gather<<<P, 256, 0, s>>>(u, parts, P, n_nodes, (__nv_bfloat16 *)A, lda, Af);
 }
 
-size_t sur_project_smem(int kpad) { return (size_t)4 * sur::kProjRows * kpad; }
-
-void launch_sur_gather_project(const double *u, const SurShapeDev *shapes, int n_shapes, int max_p, int max_kpad,
-                               cudaStream_t s) {
-  const dim3 g((unsigned)((max_p + 1 + sur::kProjRows - 1) / sur::kProjRows), (unsigned)n_shapes);
-  sur::k_gather_project<<<g, 256, sur_project_smem(max_kpad), s>>>(u, shapes);
+void launch_sur_gather_project(const double *u, const SurShapes &shapes, int max_p, int max_nodes, cudaStream_t s) {
+  const dim3 g((unsigned)((max_p + 1 + sur::kProjRows - 1) / sur::kProjRows),
+               (unsigned)((max_nodes + sur::kProjNodes - 1) / sur::kProjNodes), (unsigned)shapes.n);
+  sur::k_gather_project<<<g, sur::kProjThreads, 0, s>>>(u, shapes);
 }
 
 void launch_sur_scatter_all(double *f, const SurShapeDev *shapes, int n_shapes, int max_p, const uint8_t *on,
@@ -334,12 +703,25 @@ void launch_sur_gate_all(const DevData &d, const SurShapeDev *shapes, int n_shap
                                                                              err_gate * err_gate);
 }
 
-int sur_fused_setup(int kpad) {
-  // the fused kernel keeps kProjRows rows (kpad floats each) in shared memory
-  if (sur_project_smem(kpad) > 227 * 1024 - 1024) return 0;
-  return cudaFuncSetAttribute(sur::k_gather_project, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sur_project_smem(kpad)) == cudaSuccess;
+void launch_sur_mlp(const SurShapes &shapes, int max_p, cudaStream_t s) {
+  const dim3 g((unsigned)((max_p + 1 + sur::kMlpRows - 1) / sur::kMlpRows), (unsigned)shapes.n);
+  sur::k_mlp<<<g, sur::kMlpThreads, 0, s>>>(shapes);
 }
+
+void launch_sur_lift_scatter(double *f, const SurShapes &shapes, int max_p, int max_nodes, const uint8_t *on,
+                             const uint8_t *near, const CtrlState *ctrl, unsigned long long *count, cudaStream_t s) {
+  if (max_p <= 0) return;
+  const dim3 g((unsigned)((max_p + sur::kLiftRows - 2) / (sur::kLiftRows - 1)),
+               (unsigned)((max_nodes + sur::kLiftNodes - 1) / sur::kLiftNodes), (unsigned)shapes.n);
+  sur::k_lift_scatter<<<g, sur::kLiftThreads, 0, s>>>(f, shapes, on, near, ctrl, count);
+}
+
+void launch_sur_check_all(const DevData &d, const SurShapes &shapes, double *err2, float z_gate, double err_gate,
+                          cudaStream_t s) {
+  sur::k_check_all<<<(unsigned)sm_count(), 256, 0, s>>>(d, shapes, err2, z_gate, err_gate * err_gate);
+}
+
+int sur_n_chunks(int n_nodes) { return (n_nodes + sur::kProjNodes - 1) / sur::kProjNodes; }
 
 }  // namespace pdgpu
 

@@ -524,11 +524,16 @@ class Surrogate:
         return fscale, force_floor(sc, zones)
 
     def attach(self, model, check_interval: int = 50, z_gate: float = 0.5, err_gate: float = 0.05,
-               near_gate: bool = True) -> None:
+               near_gate: bool = True, chain: str = "cuda") -> None:
         """Install on a GpuDEMModel (mixed precision, before integrate_begin):
         per shape the projection phi^T / sx, the three layers and the lift
         [psi, kphi sx] of [network output, scaled coefficients].  With
-        ``near_gate`` particles with contact candidates stay on the bond loop."""
+        ``near_gate`` particles with contact candidates stay on the bond loop.
+        ``chain``: "cuda" runs the chain on CUDA cores (four launches per
+        step), "tensor" on the tcgen05 GEMMs (the training kernels)."""
+        if chain not in ("cuda", "tensor"):
+            raise ValueError(f"chain {chain!r}: 'cuda' or 'tensor'")
+        model._check(model.lib.pdgpu_set_surrogate_chain(model.ctx, 0 if chain == "cuda" else 1))
         sc = model.scene
         fscale, floor = self.scales(sc)
         keep = []

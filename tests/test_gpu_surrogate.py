@@ -6,9 +6,9 @@
 * training: on held-out bond-loop samples, the network's force error is
   below that of the same reduced model without it (the bond loop's tangent
   on the modes alone): what the network gains.
-* in the step, on deformed particles: the device chain (gather, tensor-core
-  GEMMs, lift) judged against the bond loop on the first check step, with
-  and without the network.
+* in the step, on deformed particles: the device chain judged against the
+  bond loop on the first check step, with and without the network; the
+  CUDA-core chain the step runs against the tensor-core GEMM chain.
 * in the step, over a run: under load (repeated impacts on the moving
   wall) the wall's contact impulse of perturbed surrogate runs matches that
   of perturbed FP64 runs as an ensemble (impacts amplify any difference, a
@@ -109,17 +109,11 @@ def _run(sc, prec, steps, sur=None, near=True, chk=50):
         m.close()
 
 
-def test_surrogate_chain_on_deformed_particles():
-    """Every particle of a held-out packing gets a deformation in its
+def _deformed_packing(s):
+    """A held-out packing whose every particle gets a deformation in its
     shape's modes with an RMS nodal displacement of 2e-7 of the reference
-    mesh (peak bond stretch a few tenths of the critical stretch, inside the
-    gate, where the material law is already nonlinear); on the first step
-    the bond loop runs for all particles and the scatter compares the
-    surrogate's force with it, per particle."""
-    import copy
+    mesh (peak bond stretch a few tenths of the critical stretch)."""
     from peridem_b200 import surrogate as sg
-    from peridem_b200.model import GpuDEMModel, PREC_MIXED
-    s = _trained()
     sc = _scene(9, 12, 1.02)
     rng = np.random.default_rng(11)
     u = np.zeros((sc.n_nodes, 3))
@@ -128,28 +122,45 @@ def test_surrogate_chain_on_deformed_particles():
             c = rng.standard_normal(sg.RANK)
             c *= 2e-7 / np.linalg.norm(c)
             sg._place(sc, u, p, (S.phi @ c) * np.sqrt(S.n_nodes))
+    return sc, u
+
+
+def _check_step_errors(sc, u, model, chain="cuda"):
+    """The first check step's comparison per particle (err2 rows of the
+    particles the surrogate covers) and the largest damage Z."""
+    from peridem_b200.model import GpuDEMModel, PREC_MIXED
+    m = GpuDEMModel(sc, precision=PREC_MIXED, build_neighbors=True, compute_mx=True)
+    try:
+        model.attach(m, check_interval=50, near_gate=False, chain=chain)
+        # after integrate_begin (forces of the undeformed state): the first
+        # step moves u by gravity alone, a rigid translation
+        m.integrate_begin()
+        m.set_field("u", u)
+        m.integrate_step(1)
+        m.sync()
+        e = m.surrogate_errors()
+        zmax = float(np.max(m.field("Z")))
+    finally:
+        m.close()
+    return e[e[:, 1] > 0], zmax
+
+
+def test_surrogate_chain_on_deformed_particles():
+    """On the first step the bond loop runs for all particles and the
+    surrogate's force is compared with it, per particle: the network beats
+    the tangent part alone, inside the stretch gate."""
+    import copy
+    s = _trained()
+    sc, u = _deformed_packing(s)
     linear = copy.deepcopy(s)
     for S in linear.shapes:   # the network's output is zero: the tangent part alone
         S.W[2] = np.zeros_like(S.W[2])
         S.b[2] = np.zeros_like(S.b[2])
 
     def errors(model):
-        m = GpuDEMModel(sc, precision=PREC_MIXED, build_neighbors=True, compute_mx=True)
-        try:
-            model.attach(m, check_interval=50, near_gate=False)
-            # after integrate_begin (forces of the undeformed state): the
-            # first step moves u by gravity alone, a rigid translation
-            m.integrate_begin()
-            m.set_field("u", u)
-            m.integrate_step(1)
-            m.sync()
-            e = m.surrogate_errors()
-            zmax = float(np.max(m.field("Z")))
-        finally:
-            m.close()
+        e, zmax = _check_step_errors(sc, u, model)
         assert zmax < 0.5, zmax   # inside the stretch gate
-        sel = e[:, 1] > 0
-        return np.sqrt(e[sel, 0] / e[sel, 1])
+        return np.sqrt(e[:, 0] / e[:, 1])
 
     e_mlp, e_lin = errors(s), errors(linear)
     print(f"in-step relative force error per particle: network median {np.median(e_mlp):.4f} max "
@@ -157,6 +168,26 @@ def test_surrogate_chain_on_deformed_particles():
     assert len(e_mlp) == len(e_lin) > 0
     assert e_mlp.max() < 0.05
     assert np.median(e_mlp) < np.median(e_lin)
+
+
+def test_cuda_core_chain_matches_tensor_core_chain():
+    """The step's CUDA-core chain (gather with projection, fused layers, lift
+    with the scatter) against the tcgen05 GEMM chain the training uses, on
+    the same deformed packing: both take BF16 operands with FP32
+    accumulation and differ in summation order only.  Per particle, the
+    difference of the two surrogate forces is bounded by the triangle
+    inequality through their errors against the same bond-loop force:
+    | |f_a - f| - |f_b - f| | <= 2e-3 |f|."""
+    s = _trained()
+    sc, u = _deformed_packing(s)
+    ea, _ = _check_step_errors(sc, u, s, chain="cuda")
+    eb, _ = _check_step_errors(sc, u, s, chain="tensor")
+    assert len(ea) == len(eb) > 0
+    np.testing.assert_array_equal(ea[:, 1], eb[:, 1])   # the same bond loop
+    da, db, nf = np.sqrt(ea[:, 0]), np.sqrt(eb[:, 0]), np.sqrt(ea[:, 1])
+    print(f"chain difference per particle, max |e_a - e_b| / |f| = {np.max(np.abs(da - db) / nf):.2e}; "
+          f"errors against the bond loop {np.median(da / nf):.4f} / {np.median(db / nf):.4f}")
+    assert np.all(np.abs(da - db) <= 2e-3 * nf)
 
 
 def _impulse_ensemble(sc, prec, seeds, sur=None, steps=3000, at=1000):
