@@ -44,6 +44,8 @@ struct ContactPair {
   double rc, kn, mu, betan, kappa;
 };
 
+constexpr int kDampGroup = 4;  // particles per damping CTA, at most (static shared memory)
+
 struct DampParticle {
   double bound_r, density;
   int32_t zone, type;
@@ -218,6 +220,10 @@ struct DevData {
   int2 *c_span;          // [c_row[i], c_row[i + 1]) of compacted node t = c_nodes[t]
   uint16_t *nzone;        // zone of each node's particle
   DampParticle *dpart;   // per particle: bounding radius, density, zone, type
+  // damping CTAs: group g holds particles damp_group[g] .. damp_group[g + 1] - 1
+  // (consecutive, one scene, at most kDampGroup); null: one particle per CTA
+  int32_t *damp_group;
+  int32_t n_damp_groups;
   double *pcen;          // per particle, this step: {x, y, z, bounding radius, vx, vy, vz, -}
 
   // boundary conditions: per BC node, a run of entries applied in set order

@@ -1421,136 +1421,167 @@ __global__ void __launch_bounds__(kBlock) k_contact_warp(DevData d) {
 constexpr int kDampBlock = 128;
 constexpr int kWallSort = 4096;
 
+// One CTA per group of up to kDampGroup consecutive particles of one scene
+// (d.damp_group; one particle per CTA without it): each particle record
+// loaded in the particle-particle loop serves the whole group.  A thread
+// visits the same particles q in the same order for every member as the
+// one-particle form, and keeps a partial sum per member and component in
+// shared memory, so the sums are those of the one-particle form bit for bit.
 __global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
   __shared__ int32_t wn[kWallSort];
   __shared__ double red[3][kDampBlock / 32];
   __shared__ ContactPair cps[kZonePairsSmem];
-  const int p = blockIdx.x;
-  const DampParticle P = d.dpart[p];
+  __shared__ double s_acc[kDampGroup][3][kDampBlock];  // member, component, thread
+  __shared__ double s_c[kDampGroup][8];                // centre (3), centre velocity (3), radius, density
+  __shared__ int s_zone[kDampGroup], s_type[kDampGroup];
+  const int p0 = d.damp_group ? d.damp_group[blockIdx.x] : (int)blockIdx.x;
+  const int np = d.damp_group ? d.damp_group[blockIdx.x + 1] - p0 : 1;
   const int nz = d.n_zones;
   const bool tab = nz * nz <= kZonePairsSmem;
-  int nw = d.wp_cnt[p];
   if (tab)
     for (int a = threadIdx.x; a < nz * nz; a += blockDim.x) cps[a] = d.contact[a];
-  __syncthreads();
-  if (P.type != 0) return;
-  if (d.ctrl->error) return;
-  const double Ri = P.bound_r;
-  const double vol_pi = kPi * Ri * Ri;
-  const double rhoi = P.density;
-  const int st = dim == 2 ? 2 : 4;
-  double xc[3], vc[3];
-  for (int q = 0; q < 3; q++) {
-    xc[q] = d.pcen[8 * p + q];
-    vc[q] = d.pcen[8 * p + 4 + q];
+  if ((int)threadIdx.x < np) {
+    const int p = p0 + threadIdx.x;
+    const DampParticle P = d.dpart[p];
+    for (int q = 0; q < 3; q++) {
+      s_c[threadIdx.x][q] = d.pcen[8 * p + q];
+      s_c[threadIdx.x][3 + q] = d.pcen[8 * p + 4 + q];
+    }
+    s_c[threadIdx.x][6] = P.bound_r;
+    s_c[threadIdx.x][7] = P.density;
+    s_zone[threadIdx.x] = P.zone;
+    s_type[threadIdx.x] = P.type;
   }
-  double acc[3] = {0.0, 0.0, 0.0};
-  // particle-particle, over the particles of this particle's scene: first
-  // the 32-byte {centre, radius} record only, against the largest reach any
-  // zone pair allows; kDampBatch records in flight per thread, each thread
-  // still visiting its particles in increasing order
+  for (int e = threadIdx.x; e < kDampGroup * 3 * kDampBlock; e += blockDim.x) (&s_acc[0][0][0])[e] = 0.0;
+  __syncthreads();
+  bool any = false;
+  for (int k = 0; k < np; k++) any |= s_type[k] == 0;
+  if (!any) return;
+  if (d.ctrl->error) return;
+  const DampParticle G = d.dpart[p0];  // the group's scene: its particles q0 .. q1 - 1
+  // particle-particle, over the particles of the scene: first the 32-byte
+  // {centre, radius} record only, against the largest reach any zone pair
+  // allows; kDampBatch records in flight per thread, each thread visiting
+  // its particles in increasing order
   constexpr int kDampBatch = 4;
-  for (int q0 = P.q0 + threadIdx.x; q0 < P.q1; q0 += kDampBatch * blockDim.x) {
+  for (int qb = G.q0 + threadIdx.x; qb < G.q1; qb += kDampBatch * blockDim.x) {
     double2 c01b[kDampBatch], c2rb[kDampBatch];
 #pragma unroll
     for (int t = 0; t < kDampBatch; t++) {
-      const int q = q0 + t * (int)blockDim.x;
+      const int q = qb + t * (int)blockDim.x;
       c01b[t] = c2rb[t] = make_double2(0.0, 0.0);
-      if (q < P.q1) {
+      if (q < G.q1) {
         c01b[t] = *reinterpret_cast<const double2 *>(d.pcen + 8 * q);
         c2rb[t] = *reinterpret_cast<const double2 *>(d.pcen + 8 * q + 2);
       }
     }
 #pragma unroll
     for (int t = 0; t < kDampBatch; t++) {
-      const int q = q0 + t * (int)blockDim.x;
-      if (q >= P.q1 || q == p) continue;
+      const int q = qb + t * (int)blockDim.x;
+      if (q >= G.q1) continue;
       const double2 c01 = c01b[t], c2r = c2rb[t];
-      double xcj[3] = {c01.x - xc[0], c01.y - xc[1], c2r.x - xc[2]};
-      const double d2 = xcj[0] * xcj[0] + xcj[1] * xcj[1] + xcj[2] * xcj[2];
-      const double reach_max = c2r.y + Ri + 1.01 * d.rc_max;
-      if (d2 > 1.0625 * reach_max * reach_max) continue;
-      const DampParticle Q = d.dpart[q];
-      if (Q.type != 0) continue;
-      const double Rj = Q.bound_r;
-      double vcj[3];
-      for (int c = 0; c < 3; c++) vcj[c] = d.pcen[8 * q + 4 + c] - vc[c];
-      const ContactPair cp = tab ? cps[P.zone * nz + Q.zone] : d.contact[P.zone * nz + Q.zone];
-      const double reach = Rj + Ri + 1.01 * cp.rc;
-      // pairs well beyond the reach cannot pass the relative-tolerance test
-      if (d2 > 1.0625 * reach * reach) continue;
-      const double dist = sqrt(d2);
-      if (is_less(dist, reach)) {
-        const double vol_pj = kPi * Rj * Rj;
-        const double m1 = rhoi * vol_pi, m2 = Q.density * vol_pj;
-        const double meq = 2. * m1 * m2 / (m1 + m2);  // util::equivalentMass
-        const double bn = cp.betan * sqrt(cp.kappa * cp.rc * meq);
-        double hat[3] = {0.0, 0.0, 0.0};
-        if (is_greater(dist, 0.))
-          for (int c = 0; c < 3; c++) hat[c] = xcj[c] / dist;
-        double vm = vcj[0] * hat[0] + vcj[1] * hat[1] + vcj[2] * hat[2];
-        if (vm > 0.) vm = 0.;
-        for (int c = 0; c < 3; c++) acc[c] += bn * vm * hat[c] / vol_pi;
-      }
-    }
-  }
-  // particle-wall: unique wall nodes within the contact radius of any node
-  if (nw > d.wp_cap) nw = d.wp_cap;
-  if (nw > kWallSort) nw = kWallSort;  // capacity is validated on the host
-  int sz = 1;
-  while (sz < nw) sz <<= 1;
-  for (int a = threadIdx.x; a < sz; a += blockDim.x)
-    wn[a] = a < nw ? d.wp[(int64_t)p * d.wp_cap + a] : INT32_MAX;
-  __syncthreads();
-  for (int k = 2; k <= sz; k <<= 1)
-    for (int jj = k >> 1; jj > 0; jj >>= 1) {
-      for (int a = threadIdx.x; a < sz; a += blockDim.x) {
-        const int b = a ^ jj;
-        if (b > a) {
-          const bool up = (a & k) == 0;
-          const int32_t va = wn[a], vb = wn[b];
-          if ((va > vb) == up) {
-            wn[a] = vb;
-            wn[b] = va;
-          }
+      for (int k = 0; k < np; k++) {
+        if (s_type[k] != 0 || q == p0 + k) continue;
+        const double *C = s_c[k];
+        const double Ri = C[6];
+        double xcj[3] = {c01.x - C[0], c01.y - C[1], c2r.x - C[2]};
+        const double d2 = xcj[0] * xcj[0] + xcj[1] * xcj[1] + xcj[2] * xcj[2];
+        const double reach_max = c2r.y + Ri + 1.01 * d.rc_max;
+        if (d2 > 1.0625 * reach_max * reach_max) continue;
+        const DampParticle Q = d.dpart[q];
+        if (Q.type != 0) continue;
+        const double Rj = Q.bound_r;
+        double vcj[3];
+        for (int c = 0; c < 3; c++) vcj[c] = d.pcen[8 * q + 4 + c] - C[3 + c];
+        const ContactPair cp = tab ? cps[s_zone[k] * nz + Q.zone] : d.contact[s_zone[k] * nz + Q.zone];
+        const double reach = Rj + Ri + 1.01 * cp.rc;
+        // pairs well beyond the reach cannot pass the relative-tolerance test
+        if (d2 > 1.0625 * reach * reach) continue;
+        const double dist = sqrt(d2);
+        if (is_less(dist, reach)) {
+          const double vol_pi = kPi * Ri * Ri;
+          const double vol_pj = kPi * Rj * Rj;
+          const double m1 = C[7] * vol_pi, m2 = Q.density * vol_pj;
+          const double meq = 2. * m1 * m2 / (m1 + m2);  // util::equivalentMass
+          const double bn = cp.betan * sqrt(cp.kappa * cp.rc * meq);
+          double hat[3] = {0.0, 0.0, 0.0};
+          if (is_greater(dist, 0.))
+            for (int c = 0; c < 3; c++) hat[c] = xcj[c] / dist;
+          double vm = vcj[0] * hat[0] + vcj[1] * hat[1] + vcj[2] * hat[2];
+          if (vm > 0.) vm = 0.;
+          for (int c = 0; c < 3; c++) s_acc[k][c][threadIdx.x] += bn * vm * hat[c] / vol_pi;
         }
       }
-      __syncthreads();
     }
-  for (int a = threadIdx.x; a < nw; a += blockDim.x) {
-    const int32_t k = wn[a];
-    if (a > 0 && wn[a - 1] == k) continue;
-    const int zk = d.nzone[k];
-    const ContactPair cp = tab ? cps[P.zone * nz + zk] : d.contact[P.zone * nz + zk];
-    const double meq = rhoi * vol_pi;
-    const double bn = cp.betan * sqrt(cp.kappa * cp.rc * meq);
-    double xk[3] = {0, 0, 0}, vk[3] = {0, 0, 0};
-    for (int t = 0; t < dim; t++) {
-      xk[t] = d.x[st * (int64_t)k + t] - xc[t];
-      vk[t] = d.v[st * (int64_t)k + t] - vc[t];
+  }
+  // per member: particle-wall (unique wall nodes within the contact radius
+  // of any node), then the block reduction
+  const int st = dim == 2 ? 2 : 4;
+  for (int k = 0; k < np; k++) {
+    if (s_type[k] != 0) continue;  // uniform over the CTA
+    const int p = p0 + k;
+    const double *C = s_c[k];
+    const double Ri = C[6], vol_pi = kPi * Ri * Ri, rhoi = C[7];
+    int nw = d.wp_cnt[p];
+    if (nw > d.wp_cap) nw = d.wp_cap;
+    if (nw > kWallSort) nw = kWallSort;  // capacity is validated on the host
+    int sz = 1;
+    while (sz < nw) sz <<= 1;
+    for (int a = threadIdx.x; a < sz; a += blockDim.x)
+      wn[a] = a < nw ? d.wp[(int64_t)p * d.wp_cap + a] : INT32_MAX;
+    __syncthreads();
+    for (int kk = 2; kk <= sz; kk <<= 1)
+      for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+        for (int a = threadIdx.x; a < sz; a += blockDim.x) {
+          const int b = a ^ jj;
+          if (b > a) {
+            const bool up = (a & kk) == 0;
+            const int32_t va = wn[a], vb = wn[b];
+            if ((va > vb) == up) {
+              wn[a] = vb;
+              wn[b] = va;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    double acc[3] = {s_acc[k][0][threadIdx.x], s_acc[k][1][threadIdx.x], s_acc[k][2][threadIdx.x]};
+    for (int a = threadIdx.x; a < nw; a += blockDim.x) {
+      const int32_t w = wn[a];
+      if (a > 0 && wn[a - 1] == w) continue;
+      const int zk = d.nzone[w];
+      const ContactPair cp = tab ? cps[s_zone[k] * nz + zk] : d.contact[s_zone[k] * nz + zk];
+      const double meq = rhoi * vol_pi;
+      const double bn = cp.betan * sqrt(cp.kappa * cp.rc * meq);
+      double xk[3] = {0, 0, 0}, vk[3] = {0, 0, 0};
+      for (int t = 0; t < dim; t++) {
+        xk[t] = d.x[st * (int64_t)w + t] - C[t];
+        vk[t] = d.v[st * (int64_t)w + t] - C[3 + t];
+      }
+      const double l = sqrt(xk[0] * xk[0] + xk[1] * xk[1] + xk[2] * xk[2]);
+      double hat[3] = {0.0, 0.0, 0.0};
+      if (is_greater(l, 0.))
+        for (int t = 0; t < 3; t++) hat[t] = xk[t] / l;
+      double vm = vk[0] * hat[0] + vk[1] * hat[1] + vk[2] * hat[2];
+      if (vm > 0.) vm = 0.;
+      for (int t = 0; t < 3; t++) acc[t] += bn * vm * hat[t] / vol_pi;
     }
-    const double l = sqrt(xk[0] * xk[0] + xk[1] * xk[1] + xk[2] * xk[2]);
-    double hat[3] = {0.0, 0.0, 0.0};
-    if (is_greater(l, 0.))
-      for (int t = 0; t < 3; t++) hat[t] = xk[t] / l;
-    double vm = vk[0] * hat[0] + vk[1] * hat[1] + vk[2] * hat[2];
-    if (vm > 0.) vm = 0.;
-    for (int t = 0; t < 3; t++) acc[t] += bn * vm * hat[t] / vol_pi;
-  }
-  // block reduction (fixed order)
-  for (int t = 0; t < 3; t++) {
-    double v = acc[t];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) red[t][threadIdx.x >> 5] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
+    // block reduction (fixed order)
     for (int t = 0; t < 3; t++) {
-      double s = 0.0;
-      for (int w = 0; w < kDampBlock / 32; w++) s += red[t][w];
-      d.fdamp[4 * p + t] = s;
+      double v = acc[t];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0) red[t][threadIdx.x >> 5] = v;
     }
-    d.wp_cnt[p] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int t = 0; t < 3; t++) {
+        double s = 0.0;
+        for (int w = 0; w < kDampBlock / 32; w++) s += red[t][w];
+        d.fdamp[4 * p + t] = s;
+      }
+      d.wp_cnt[p] = 0;
+    }
+    __syncthreads();  // before wn and red are reused
   }
 }
 
@@ -2099,7 +2130,7 @@ void launch_scene_post(const DevData &d, cudaStream_t s) {
 
 void launch_damping(const DevData &d, cudaStream_t s) {
   if (d.n_particles <= 0) return;
-  k_damping<<<d.n_particles, kDampBlock, 0, s>>>(d, d.dim);
+  k_damping<<<d.damp_group ? d.n_damp_groups : d.n_particles, kDampBlock, 0, s>>>(d, d.dim);
 }
 
 void launch_external(const DevData &d, cudaStream_t s) {

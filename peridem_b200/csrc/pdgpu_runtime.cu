@@ -902,6 +902,21 @@ int prepare(pdgpu_ctx *ctx) {
     }
     TRY(dalloc(ctx, &d.dpart, dp.size()));
     CK(cudaMemcpy(d.dpart, dp.data(), dp.size() * sizeof(DampParticle), cudaMemcpyHostToDevice));
+    // damping CTAs: with many particles, groups of consecutive particles of
+    // one scene share each particle record they load (about 400 groups)
+    const int group = std::min(kDampGroup, std::max(1, (int)(dp.size() / 400)));
+    if (group > 1) {
+      std::vector<int32_t> g{0};
+      for (size_t p = 0; p < dp.size();) {
+        size_t e = p + 1;
+        while (e < dp.size() && (int)(e - p) < group && dp[e].q0 == dp[p].q0 && dp[e].q1 == dp[p].q1) e++;
+        g.push_back((int32_t)e);
+        p = e;
+      }
+      d.n_damp_groups = (int32_t)g.size() - 1;
+      TRY(dalloc(ctx, &d.damp_group, g.size()));
+      CK(cudaMemcpy(d.damp_group, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    }
     TRY(dalloc(ctx, &d.pcen, 8 * dp.size()));
     CK(cudaMemset(d.pcen, 0, 8 * dp.size() * 8));
   }
