@@ -324,15 +324,22 @@ struct SurShapeDev {
   float *F;          // (P + 1) x kpad FP32: body-frame forces (check steps)
   float *xpart;      // (P + 1) x n_chunks x 32 FP32: the projection's partial sums
   int32_t n_chunks, pad2;
-  // the CUDA-core chain: layer weights BF16 as [in / 8][out][8] (eight
-  // consecutive inputs of one output in 16 bytes), FP32 biases, and the lift
-  // BF16 as [kpad][64] (per dof its weights of the 64 coefficients)
-  const void *w1q, *w2q, *w3q;
+  // the CUDA-core chain's warp-MMA operands, BF16 row-major [out][in] with
+  // each row's 16-bit pairs permuted within chunks of 64 inputs (32 for a
+  // 32-input row) so that one lane's fragments of a chunk are contiguous
+  // (sur_kperm): layer weights, the lift [kpad][64]; FP32 biases
+  const void *w1m, *w2m, *w3m;
   const float *b1, *b2, *b3;
-  const void *lift;
+  const void *liftm;
 };
 
 int sm_count();  // SMs of the current device
+
+// Position of 16-bit pair w (0 <= w < 32 or 16) in a K-permuted chunk of a
+// row: a chunk holds ks m16n8k16 k-steps (4 for 64 inputs, 2 for 32); pair w
+// = 8 kl + 4 h + t (k-step kl, fragment register h, lane t of a quad) goes
+// to t * 2 ks + 2 kl + h, so that lane t's 2 ks pairs are adjacent.
+__host__ __device__ inline int sur_kperm(int w, int ks) { return (w % 4) * 2 * ks + 2 * (w / 8) + (w / 4) % 2; }
 
 // The surrogate's chain on CUDA cores, every shape in one launch per stage,
 // the shapes by value in the kernel parameters (at most kMaxSurShapes):

@@ -101,7 +101,7 @@ struct pdgpu_ctx {
     float *b1 = nullptr, *b2 = nullptr, *b3 = nullptr;
     void *A = nullptr, *xy = nullptr, *h1 = nullptr, *h2 = nullptr;
     float *F = nullptr, *xpart = nullptr;
-    void *w1q = nullptr, *w2q = nullptr, *w3q = nullptr;  // CUDA-core chain layouts
+    void *w1m = nullptr, *w2m = nullptr, *w3m = nullptr, *liftm = nullptr;  // CUDA-core chain layouts
   };
   std::vector<SurShape> sur;
   GemmProblem *sur_probs = nullptr;  // device: 5 stages x shapes
@@ -2087,17 +2087,22 @@ int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape 
     TRY(f32(in.b1, 256, &S.b1));
     TRY(f32(in.b2, 256, &S.b2));
     TRY(f32(in.b3, 32, &S.b3));
-    // CUDA-core chain: W[out][in] -> [in / 8][out][8]
-    auto blocked = [&](const float *w, int n_out, int n_in, void **dst) -> int {
-      std::vector<float> h((size_t)n_out * n_in);
-      for (int cb = 0; cb < n_in / 8; cb++)
-        for (int j = 0; j < n_out; j++)
-          for (int t = 0; t < 8; t++) h[((size_t)cb * n_out + j) * 8 + t] = w[(size_t)j * n_in + 8 * cb + t];
+    // CUDA-core chain: warp-MMA operands with K permuted in chunks of 64
+    // inputs (sur_kperm)
+    auto kperm = [&](const float *src, int rows, int rows_pad, int K, void **dst) -> int {
+      std::vector<float> h((size_t)rows_pad * K, 0.f);
+      const int cw = std::min(K, 64) / 2, ks = cw / 8;  // pairs and k-steps per chunk
+      for (int r = 0; r < rows; r++)
+        for (int c = 0; c < K; c++) {
+          const int chunk = c / (2 * cw), pw = (c % (2 * cw)) / 2;
+          h[(size_t)r * K + chunk * 2 * cw + 2 * sur_kperm(pw, ks) + c % 2] = src[(size_t)r * K + c];
+        }
       return bf(h.data(), 1, h.size(), h.size(), 1, dst);
     };
-    TRY(blocked(in.w1, 256, 32, &S.w1q));
-    TRY(blocked(in.w2, 256, 256, &S.w2q));
-    TRY(blocked(in.w3, 32, 256, &S.w3q));
+    TRY(kperm(in.w1, 256, 256, 32, &S.w1m));
+    TRY(kperm(in.w2, 256, 256, 256, &S.w2m));
+    TRY(kperm(in.w3, 32, 32, 256, &S.w3m));
+    TRY(kperm(in.psi, K, S.kpad, 64, &S.liftm));
     const int M = S.P + 1;  // row P: the zero input
     __nv_bfloat16 *A, *xy, *h1, *h2;
     TRY(dalloc(ctx, &A, (size_t)M * S.kpad));
@@ -2125,7 +2130,7 @@ int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape 
   std::vector<SurShapeDev> sd;
   for (auto &S : ctx->sur) {
     sd.push_back(SurShapeDev{S.parts, S.P, S.n_nodes, S.kpad, 0, S.phiT, S.xy, S.F, S.xpart,
-                             sur_n_chunks(S.n_nodes), 0, S.w1q, S.w2q, S.w3q, S.b1, S.b2, S.b3, S.lift});
+                             sur_n_chunks(S.n_nodes), 0, S.w1m, S.w2m, S.w3m, S.b1, S.b2, S.b3, S.liftm});
     ctx->sur_max_rows = std::max(ctx->sur_max_rows, S.P);
     ctx->sur_max_nodes = std::max(ctx->sur_max_nodes, S.n_nodes);
   }

@@ -293,170 +293,7 @@ __global__ void __launch_bounds__(kProjThreads, 4) k_gather_project(const double
     S.xpart[((size_t)(k0 + r) * S.n_chunks + blockIdx.y) * 32 + 4 * warp + t] = v[0];
 }
 
-// eight BF16 (16 bytes) -> FP32
-__device__ __forceinline__ void unpack8(const uint4 w, float *o) {
-  const uint32_t v[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-  for (int t = 0; t < 4; t++) {
-    o[2 * t] = __uint_as_float(v[t] << 16);
-    o[2 * t + 1] = __uint_as_float(v[t] & 0xffff0000u);
-  }
-}
-
-// The three layers of the network for kMlpRows rows (rows 0..P, P the zero
-// input) per CTA on CUDA cores.  The projected input x is the sum of the
-// projection's chunks in chunk order, rounded to BF16 (and stored in
-// xy[:, 32:64] for the lift).  A layer's weights (16-byte loads,
-// [in / 8][out][8]) are read once per CTA and serve all its rows: those of
-// layers 1 and 3 and the first block of layer 2 are requested before the
-// input arrives, and each further block of layer 2 while the previous one
-// is in use.  Activations stay in shared memory, rounded to BF16 as the
-// tensor-core chain stores them.
-//   h1 = tanh(x W1^T + b1), h2 = tanh(h1 W2^T + b2)   thread = output column
-//   y  = h2 W3^T + b3 -> xy[:, 0:32]                   warp = 32 inputs, lane = column
-constexpr int kMlpRows = 8;
-constexpr int kMlpCols = 256;                 // outputs of layers 1 and 2
-constexpr int kMlpThreads = 2 * kMlpCols;     // two threads per output: rows 0-3 and 4-7
-constexpr int kMlpPairs = kMlpRows / 4;       // row pairs per thread
-constexpr int kMlpBlock = 4;  // 16-byte weight loads in flight per thread in layer 2
-
-// Activations are kept per row pair: in[p][c] = (row 2p, row 2p + 1) of
-// input c, so that one packed FMA serves two rows.
-// acc[p] += in[p0 + p][8 cb .. 8 cb + 7] . w (eight inputs, kMlpPairs row pairs)
-__device__ __forceinline__ void rows_dot8(const float2 *__restrict__ in, int ldin, int cb, const uint4 wv,
-                                          float2 *acc) {
-  float w[8];
-  unpack8(wv, w);
-#pragma unroll
-  for (int p = 0; p < kMlpPairs; p++) {
-    const float4 *src = reinterpret_cast<const float4 *>(in + p * ldin + 8 * cb);
-    float2 x = acc[p];
-#pragma unroll
-    for (int h = 0; h < 4; h++) {
-      const float4 a = src[h];
-      x = __ffma2_rn(make_float2(a.x, a.y), make_float2(w[2 * h], w[2 * h]), x);
-      x = __ffma2_rn(make_float2(a.z, a.w), make_float2(w[2 * h + 1], w[2 * h + 1]), x);
-    }
-    acc[p] = x;
-  }
-}
-
-// out[p0 + p][j] = BF16(tanh(acc[p] + b))
-__device__ __forceinline__ void store_tanh(const float2 *acc, float b, float2 *out, int j) {
-#pragma unroll
-  for (int p = 0; p < kMlpPairs; p++)
-    out[p * kMlpCols + j] = make_float2(__bfloat162float(__float2bfloat16(tanhf(acc[p].x + b))),
-                                        __bfloat162float(__float2bfloat16(tanhf(acc[p].y + b))));
-}
-
-__global__ void __launch_bounds__(kMlpThreads) k_mlp(const __grid_constant__ SurShapes shapes) {
-  __shared__ __align__(16) float2 s_x[kMlpRows / 2 * 32];
-  __shared__ __align__(16) float2 s_h[2][kMlpRows / 2 * kMlpCols];
-  const SurShapeDev &S = shapes.s[blockIdx.y];
-  const int k0 = blockIdx.x * kMlpRows;
-  if (k0 > S.P) return;
-  const int nrow = min(kMlpRows, S.P + 1 - k0);
-  const int j = threadIdx.x % kMlpCols, p0 = (threadIdx.x / kMlpCols) * kMlpPairs;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint4 *w1 = (const uint4 *)S.w1q, *w2 = (const uint4 *)S.w2q, *w3 = (const uint4 *)S.w3q;
-  uint4 v1[4], v2[kMlpBlock];
-#pragma unroll
-  for (int t = 0; t < 4; t++) v1[t] = __ldg(w1 + t * kMlpCols + j);
-#pragma unroll
-  for (int t = 0; t < kMlpBlock; t++) v2[t] = __ldg(w2 + t * kMlpCols + j);
-  const float b1 = S.b1[j], b2 = S.b2[j];
-  __nv_bfloat16 *xy = (__nv_bfloat16 *)S.xy;
-  for (int e = threadIdx.x; e < kMlpRows * 32; e += blockDim.x) {
-    const int r = e >> 5, c = e & 31;
-    float x = 0.f;
-    if (r < nrow) {
-      const float *xp = S.xpart + (size_t)(k0 + r) * S.n_chunks * 32 + c;
-      for (int ch = 0; ch < S.n_chunks; ch++) x += xp[32 * ch];
-      const __nv_bfloat16 xb = __float2bfloat16(x);
-      xy[(size_t)(k0 + r) * 64 + 32 + c] = xb;
-      x = __bfloat162float(xb);
-    }
-    reinterpret_cast<float *>(&s_x[(r >> 1) * 32 + c])[r & 1] = x;
-  }
-  __syncthreads();
-  float2 acc[kMlpPairs];
-#pragma unroll
-  for (int p = 0; p < kMlpPairs; p++) acc[p] = make_float2(0.f, 0.f);
-#pragma unroll
-  for (int t = 0; t < 4; t++) rows_dot8(s_x + p0 * 32, 32, t, v1[t], acc);
-  store_tanh(acc, b1, s_h[0] + p0 * kMlpCols, j);
-  __syncthreads();
-#pragma unroll
-  for (int p = 0; p < kMlpPairs; p++) acc[p] = make_float2(0.f, 0.f);
-#pragma unroll
-  for (int cb0 = 0; cb0 < 256 / 8; cb0 += kMlpBlock) {
-    uint4 cur[kMlpBlock];
-#pragma unroll
-    for (int t = 0; t < kMlpBlock; t++) cur[t] = v2[t];
-    if (cb0 + kMlpBlock < 256 / 8)
-#pragma unroll
-      for (int t = 0; t < kMlpBlock; t++) v2[t] = __ldg(w2 + (cb0 + kMlpBlock + t) * kMlpCols + j);
-#pragma unroll
-    for (int t = 0; t < kMlpBlock; t++) rows_dot8(s_h[0] + p0 * kMlpCols, kMlpCols, cb0 + t, cur[t], acc);
-  }
-  store_tanh(acc, b2, s_h[1] + p0 * kMlpCols, j);
-  __syncthreads();
-  // layer 3: warp w sums inputs 16 w .. 16 w + 15 for all rows (lane =
-  // output column); partial sums in s_h[0] as [warp][row][column]
-  float2 acc3[kMlpRows / 2];
-#pragma unroll
-  for (int p = 0; p < kMlpRows / 2; p++) acc3[p] = make_float2(0.f, 0.f);
-#pragma unroll
-  for (int t = 0; t < 2; t++) {
-    const int cb = 2 * warp + t;
-    float w[8];
-    unpack8(__ldg(w3 + cb * 32 + lane), w);
-#pragma unroll
-    for (int p = 0; p < kMlpRows / 2; p++) {
-      const float4 *src = reinterpret_cast<const float4 *>(s_h[1] + p * kMlpCols + 8 * cb);
-      float2 x = acc3[p];
-#pragma unroll
-      for (int h = 0; h < 4; h++) {
-        const float4 a = src[h];
-        x = __ffma2_rn(make_float2(a.x, a.y), make_float2(w[2 * h], w[2 * h]), x);
-        x = __ffma2_rn(make_float2(a.z, a.w), make_float2(w[2 * h + 1], w[2 * h + 1]), x);
-      }
-      acc3[p] = x;
-    }
-  }
-  float *red = reinterpret_cast<float *>(s_h[0]);  // 16 warps x 8 rows x 32 = 2 x 2048 floats: s_h[0] and s_h[1]
-  __syncthreads();  // every warp has read h2 before red overwrites it
-#pragma unroll
-  for (int p = 0; p < kMlpRows / 2; p++) {
-    red[(warp * kMlpRows + 2 * p) * 32 + lane] = acc3[p].x;
-    red[(warp * kMlpRows + 2 * p + 1) * 32 + lane] = acc3[p].y;
-  }
-  __syncthreads();
-  if (threadIdx.x < kMlpRows * 32) {
-    const int r = threadIdx.x >> 5, c = threadIdx.x & 31;
-    float y = 0.f;
-    for (int w = 0; w < kMlpThreads / 32; w++) y += red[(w * kMlpRows + r) * 32 + c];
-    if (r < nrow) xy[(size_t)(k0 + r) * 64 + c] = __float2bfloat16(y + S.b3[c]);
-  }
-}
-
-// The lift fused with the scatter, on the tensor cores by warp-level MMA
-// (m16n8k16, BF16 operands, FP32 accumulation): a CTA takes kLiftRows - 1
-// particles plus the zero input (row P) as the 16 rows of one tile, and
-// kLiftNodes nodes (2 kLiftNodes dofs, four 8-dof column tiles per warp);
-// K = 64 (the coefficients [y | x]).  A lane's accumulators hold, per column
-// tile, one node's two components for two rows, so g = F_k - F_P (the zero
-// input's row of the same tile, fetched from the lane that holds it: zero
-// deformation gives exactly zero force) is rotated and stored as it stands.
-// Ordinary steps: f_i = fscale R(theta) g for the particles on the
-// surrogate, whose tiles the bond loop skips, so that this runs beside it;
-// check steps: g into F for the comparison after the bond loop.  count[0]
-// counts particle-steps on the surrogate, count[1] particle-steps covered.
-constexpr int kLiftRows = 16;           // 15 particles + the zero input
-constexpr int kLiftNodes = 128;
-constexpr int kLiftThreads = 256;       // 8 warps x 4 column tiles x 4 nodes
-constexpr int kLiftTiles = 2 * kLiftNodes / 8 / (kLiftThreads / 32);
-
+// ---- warp-level MMA (m16n8k16, BF16 operands, FP32 accumulation) ----
 __device__ __forceinline__ void mma_bf16_16816(float *d, const uint32_t *a, const uint32_t *b) {
   asm volatile(
       "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -464,6 +301,181 @@ __device__ __forceinline__ void mma_bf16_16816(float *d, const uint32_t *a, cons
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
+
+// physical column of logical column c (0..63) of a K-permuted 64-column row
+__device__ __forceinline__ int perm_col64(int c) { return 2 * sur_kperm(c >> 1, 4) + (c & 1); }
+
+// A fragments of k-step ks from a row-major BF16 tile in shared memory (ld
+// elements per row, logical column order): rows g and g + 8
+__device__ __forceinline__ void frag_a(const __nv_bfloat16 *A, int ld, int ks, int g, int tig, uint32_t *a) {
+  const uint32_t *r0 = reinterpret_cast<const uint32_t *>(A + g * ld) + 8 * ks + tig;
+  const uint32_t *r1 = reinterpret_cast<const uint32_t *>(A + (g + 8) * ld) + 8 * ks + tig;
+  a[0] = r0[0];
+  a[1] = r1[0];
+  a[2] = r0[4];
+  a[3] = r1[4];
+}
+
+// B fragments of the four k-steps of a 64-input K-permuted chunk (row_chunk:
+// the chunk's first 32-bit pair): lane t's eight pairs are adjacent
+__device__ __forceinline__ void frag_b_load(const uint32_t *row_chunk, int tig, uint4 *q) {
+  const uint4 *src = reinterpret_cast<const uint4 *>(row_chunk + 8 * tig);
+  q[0] = __ldg(src);
+  q[1] = __ldg(src + 1);
+}
+__device__ __forceinline__ void frag_b_of(const uint4 *q, int kl, uint32_t *b) {
+  const uint4 v = q[kl >> 1];
+  b[0] = (kl & 1) ? v.z : v.x;
+  b[1] = (kl & 1) ? v.w : v.y;
+}
+
+// The three layers of the network for 16 rows (rows 0..P, P the zero input)
+// per CTA by warp MMA.  The projected input x is the sum of the
+// projection's chunks in chunk order, rounded to BF16 (and stored in xy for
+// the lift); activations stay in shared memory as BF16 rows (padded so that
+// fragment loads do not conflict), with the bias and tanh applied to the
+// FP32 accumulators as the tensor-core chain does.  Weight fragments come
+// from the K-permuted rows, 32 bytes per lane and 64-input chunk, the next
+// chunk requested while the current one is multiplied.
+//   h1 = tanh(x W1^T + b1), h2 = tanh(h1 W2^T + b2): warp w, columns 32w..32w+31
+//   y  = h2 W3^T + b3 -> xy (columns 0..31): warps 0-3, eight columns each
+constexpr int kMlpRows = 16;
+constexpr int kMlpThreads = 256;
+constexpr int kMlpLdX = 32 + 8, kMlpLdH = 256 + 8;
+
+__global__ void __launch_bounds__(kMlpThreads) k_mlp(const __grid_constant__ SurShapes shapes) {
+  __shared__ __align__(16) __nv_bfloat16 s_x[kMlpRows * kMlpLdX];
+  __shared__ __align__(16) __nv_bfloat16 s_h1[kMlpRows * kMlpLdH];
+  __shared__ __align__(16) __nv_bfloat16 s_h2[kMlpRows * kMlpLdH];
+  const SurShapeDev &S = shapes.s[blockIdx.y];
+  const int k0 = blockIdx.x * kMlpRows;
+  if (k0 > S.P) return;
+  const int nrow = min(kMlpRows, S.P + 1 - k0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+  const uint32_t *W1 = (const uint32_t *)S.w1m, *W2 = (const uint32_t *)S.w2m, *W3 = (const uint32_t *)S.w3m;
+  // layer 1's weights (32 inputs: one chunk of two k-steps, 16 bytes per lane)
+  uint4 w1q[4];
+#pragma unroll
+  for (int t = 0; t < 4; t++) w1q[t] = __ldg(reinterpret_cast<const uint4 *>(W1 + (32 * warp + 8 * t + g) * 16) + tig);
+  // layer 2's first chunk
+  uint4 bq[2][4][2];
+#pragma unroll
+  for (int t = 0; t < 4; t++) frag_b_load(W2 + (32 * warp + 8 * t + g) * 128, tig, bq[0][t]);
+  __nv_bfloat16 *xy = (__nv_bfloat16 *)S.xy;
+  for (int e = threadIdx.x; e < kMlpRows * 32; e += blockDim.x) {
+    const int r = e >> 5, c = e & 31;
+    float x = 0.f;
+    if (r < nrow) {
+      const float *xp = S.xpart + (size_t)(k0 + r) * S.n_chunks * 32 + c;
+      for (int ch = 0; ch < S.n_chunks; ch++) x += xp[32 * ch];
+    }
+    const __nv_bfloat16 xb = __float2bfloat16(x);
+    if (r < nrow) xy[(size_t)(k0 + r) * 64 + perm_col64(32 + c)] = xb;
+    s_x[r * kMlpLdX + c] = xb;
+  }
+  __syncthreads();
+  float acc[4][4];
+  // layer 1
+#pragma unroll
+  for (int t = 0; t < 4; t++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[t][q] = 0.f;
+#pragma unroll
+  for (int kl = 0; kl < 2; kl++) {
+    uint32_t a[4];
+    frag_a(s_x, kMlpLdX, kl, g, tig, a);
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const uint32_t b[2] = {kl ? w1q[t].z : w1q[t].x, kl ? w1q[t].w : w1q[t].y};
+      mma_bf16_16816(acc[t], a, b);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 4; t++) {
+    const int col = 32 * warp + 8 * t + 2 * tig;
+    const float b0 = S.b1[col], b1 = S.b1[col + 1];
+    *reinterpret_cast<__nv_bfloat162 *>(s_h1 + g * kMlpLdH + col) =
+        __floats2bfloat162_rn(tanhf(acc[t][0] + b0), tanhf(acc[t][1] + b1));
+    *reinterpret_cast<__nv_bfloat162 *>(s_h1 + (g + 8) * kMlpLdH + col) =
+        __floats2bfloat162_rn(tanhf(acc[t][2] + b0), tanhf(acc[t][3] + b1));
+  }
+  __syncthreads();
+  // layer 2: four 64-input chunks
+#pragma unroll
+  for (int t = 0; t < 4; t++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[t][q] = 0.f;
+#pragma unroll
+  for (int ch = 0; ch < 4; ch++) {
+    if (ch + 1 < 4)
+#pragma unroll
+      for (int t = 0; t < 4; t++) frag_b_load(W2 + (32 * warp + 8 * t + g) * 128 + 32 * (ch + 1), tig, bq[(ch + 1) & 1][t]);
+#pragma unroll
+    for (int kl = 0; kl < 4; kl++) {
+      uint32_t a[4];
+      frag_a(s_h1, kMlpLdH, 4 * ch + kl, g, tig, a);
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        uint32_t b[2];
+        frag_b_of(bq[ch & 1][t], kl, b);
+        mma_bf16_16816(acc[t], a, b);
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 4; t++) {
+    const int col = 32 * warp + 8 * t + 2 * tig;
+    const float b0 = S.b2[col], b1 = S.b2[col + 1];
+    *reinterpret_cast<__nv_bfloat162 *>(s_h2 + g * kMlpLdH + col) =
+        __floats2bfloat162_rn(tanhf(acc[t][0] + b0), tanhf(acc[t][1] + b1));
+    *reinterpret_cast<__nv_bfloat162 *>(s_h2 + (g + 8) * kMlpLdH + col) =
+        __floats2bfloat162_rn(tanhf(acc[t][2] + b0), tanhf(acc[t][3] + b1));
+  }
+  __syncthreads();
+  // layer 3: warp w < 4 forms columns 8w..8w+7
+  if (warp >= 4) return;
+  float y[4] = {0.f, 0.f, 0.f, 0.f};
+  uint4 b3q[4][2];
+#pragma unroll
+  for (int ch = 0; ch < 4; ch++) frag_b_load(W3 + (8 * warp + g) * 128 + 32 * ch, tig, b3q[ch]);
+#pragma unroll
+  for (int ch = 0; ch < 4; ch++)
+#pragma unroll
+    for (int kl = 0; kl < 4; kl++) {
+      uint32_t a[4], b[2];
+      frag_a(s_h2, kMlpLdH, 4 * ch + kl, g, tig, a);
+      frag_b_of(b3q[ch], kl, b);
+      mma_bf16_16816(y, a, b);
+    }
+  const int col = 8 * warp + 2 * tig;
+  const float b0 = S.b3[col], b1 = S.b3[col + 1];
+  if (g < nrow) {
+    xy[(size_t)(k0 + g) * 64 + perm_col64(col)] = __float2bfloat16(y[0] + b0);
+    xy[(size_t)(k0 + g) * 64 + perm_col64(col + 1)] = __float2bfloat16(y[1] + b1);
+  }
+  if (g + 8 < nrow) {
+    xy[(size_t)(k0 + g + 8) * 64 + perm_col64(col)] = __float2bfloat16(y[2] + b0);
+    xy[(size_t)(k0 + g + 8) * 64 + perm_col64(col + 1)] = __float2bfloat16(y[3] + b1);
+  }
+}
+
+// The lift fused with the scatter, by warp MMA: a CTA takes kLiftRows - 1
+// particles plus the zero input (row P) as the 16 rows of one tile, and
+// kLiftNodes nodes (2 kLiftNodes dofs, four 8-dof column tiles per warp);
+// K = 64 (the coefficients [y | x], stored K-permuted like the lift's rows,
+// so that each lane's fragments of a row are 32 contiguous bytes).  A lane's
+// accumulators hold, per column tile, one node's two components for two
+// rows, so g = F_k - F_P (the zero input's row of the same tile, fetched
+// from the lane that holds it: zero deformation gives exactly zero force) is
+// rotated and stored as it stands.  Ordinary steps: f_i = fscale R(theta) g
+// for the particles on the surrogate, whose tiles the bond loop skips, so
+// that this runs beside it; check steps: g into F for the comparison after
+// the bond loop.  count[0] counts particle-steps on the surrogate, count[1]
+// particle-steps covered.
+constexpr int kLiftRows = 16;           // 15 particles + the zero input
+constexpr int kLiftNodes = 128;
+constexpr int kLiftThreads = 256;       // 8 warps x 4 column tiles x 4 nodes
+constexpr int kLiftTiles = 2 * kLiftNodes / 8 / (kLiftThreads / 32);
 
 __global__ void __launch_bounds__(kLiftThreads) k_lift_scatter(double *__restrict__ f,
                                                                const __grid_constant__ SurShapes shapes,
@@ -478,34 +490,25 @@ __global__ void __launch_bounds__(kLiftThreads) k_lift_scatter(double *__restric
   if (k0 >= S.P || a0 >= S.n_nodes) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
   const int nrow = min(kLiftRows - 1, S.P - k0);
-  // B fragments: lift[dof][c] (row-major [kpad][64]); the warp's column tiles
-  // cover dofs d0 + 8 t .. d0 + 8 t + 7; dofs past 2 n_nodes are zero rows
-  const uint32_t *L = (const uint32_t *)S.lift;  // BF16 pairs: L[dof * 32 + c / 2]
+  // B fragments: the lift's K-permuted rows [kpad][64]; the warp's column
+  // tiles cover dofs d0 + 8 t .. d0 + 8 t + 7 (rows past 2 n_nodes are zero)
+  const uint32_t *L = (const uint32_t *)S.liftm;
   const int d0 = 2 * a0 + warp * 8 * kLiftTiles;
-  uint32_t b[kLiftTiles][4][2];
+  uint4 bq[kLiftTiles][2];
 #pragma unroll
   for (int t = 0; t < kLiftTiles; t++) {
     const int dof = d0 + 8 * t + g;
-    const bool in = dof < S.kpad;
-#pragma unroll
-    for (int ks = 0; ks < 4; ks++) {
-      b[t][ks][0] = in ? __ldg(L + (size_t)dof * 32 + 8 * ks + tig) : 0u;
-      b[t][ks][1] = in ? __ldg(L + (size_t)dof * 32 + 8 * ks + 4 + tig) : 0u;
-    }
+    if (dof < S.kpad) frag_b_load(L + (size_t)dof * 32, tig, bq[t]);
+    else bq[t][0] = bq[t][1] = make_uint4(0, 0, 0, 0);
   }
   // A fragments: rows g and g + 8 of the tile; tile row 15 (and rows past
   // the shape's particles) read the zero input's row P
-  const uint32_t *X = (const uint32_t *)S.xy;  // BF16 pairs: xy[row * 32 + c / 2]
+  const uint32_t *X = (const uint32_t *)S.xy;
   const int ra = (g < nrow) ? k0 + g : S.P;
   const int rb = (g + 8 < nrow) ? k0 + g + 8 : S.P;
-  uint32_t av[4][4];
-#pragma unroll
-  for (int ks = 0; ks < 4; ks++) {
-    av[ks][0] = X[(size_t)ra * 32 + 8 * ks + tig];
-    av[ks][1] = X[(size_t)rb * 32 + 8 * ks + tig];
-    av[ks][2] = X[(size_t)ra * 32 + 8 * ks + 4 + tig];
-    av[ks][3] = X[(size_t)rb * 32 + 8 * ks + 4 + tig];
-  }
+  uint4 aq[2][2];
+  frag_b_load(X + (size_t)ra * 32, tig, aq[0]);
+  frag_b_load(X + (size_t)rb * 32, tig, aq[1]);
   const bool check = ctrl->sur_check != 0;
   const bool error = ctrl->error != 0;
   if (threadIdx.x < kLiftRows - 1) {
@@ -529,11 +532,24 @@ __global__ void __launch_bounds__(kLiftThreads) k_lift_scatter(double *__restric
   if (n_use == 0) return;  // uniform over the CTA
   float acc[kLiftTiles][4];
 #pragma unroll
-  for (int t = 0; t < kLiftTiles; t++) {
+  for (int t = 0; t < kLiftTiles; t++)
 #pragma unroll
     for (int q = 0; q < 4; q++) acc[t][q] = 0.f;
 #pragma unroll
-    for (int ks = 0; ks < 4; ks++) mma_bf16_16816(acc[t], av[ks], b[t][ks]);
+  for (int kl = 0; kl < 4; kl++) {
+    uint32_t ar[2], br[2], a[4];
+    frag_b_of(aq[0], kl, ar);  // row g: pairs (h = 0, h = 1)
+    frag_b_of(aq[1], kl, br);  // row g + 8
+    a[0] = ar[0];
+    a[1] = br[0];
+    a[2] = ar[1];
+    a[3] = br[1];
+#pragma unroll
+    for (int t = 0; t < kLiftTiles; t++) {
+      uint32_t b[2];
+      frag_b_of(bq[t], kl, b);
+      mma_bf16_16816(acc[t], a, b);
+    }
   }
   // lanes 28..31 hold tile row 15 (g = 7, second half): the zero input
   const int ua = g < nrow && s_use[g], ub = g + 8 < nrow && s_use[g + 8];
