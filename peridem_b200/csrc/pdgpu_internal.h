@@ -319,7 +319,8 @@ void launch_sur_gather(const double *u, const SurPart *parts, int P, int n_nodes
 struct SurShapeDev {
   const SurPart *parts;
   int32_t P, n_nodes, kpad, pad;
-  const void *phiT;  // 32 x kpad BF16
+  const void *phiT;  // 32 x kpad BF16; the CUDA-core chain's copy: 32 rows of
+                     // sur_n_chunks(n_nodes) x 256 BF16, K-permuted (sur_kperm)
   void *xy;          // (P + 1) x 64 BF16: [network output | projected input]
   float *F;          // (P + 1) x kpad FP32: body-frame forces (check steps)
   float *xpart;      // (P + 1) x n_chunks x 32 FP32: the projection's partial sums

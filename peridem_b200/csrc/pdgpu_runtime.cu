@@ -102,6 +102,7 @@ struct pdgpu_ctx {
     void *A = nullptr, *xy = nullptr, *h1 = nullptr, *h2 = nullptr;
     float *F = nullptr, *xpart = nullptr;
     void *w1m = nullptr, *w2m = nullptr, *w3m = nullptr, *liftm = nullptr;  // CUDA-core chain layouts
+    void *phim = nullptr;
   };
   std::vector<SurShape> sur;
   GemmProblem *sur_probs = nullptr;  // device: 5 stages x shapes
@@ -2103,6 +2104,14 @@ int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape 
     TRY(kperm(in.w2, 256, 256, 256, &S.w2m));
     TRY(kperm(in.w3, 32, 32, 256, &S.w3m));
     TRY(kperm(in.psi, K, S.kpad, 64, &S.liftm));
+    {
+      // phi^T rows padded with zeros to whole 128-node chunks of the projection
+      const int kc = sur_n_chunks(in.n_nodes) * 256;
+      std::vector<float> h((size_t)32 * kc, 0.f);
+      for (int j = 0; j < 32; j++)
+        for (int c = 0; c < K; c++) h[(size_t)j * kc + c] = in.phi_t[(size_t)j * K + c];
+      TRY(kperm(h.data(), 32, 32, kc, &S.phim));
+    }
     const int M = S.P + 1;  // row P: the zero input
     __nv_bfloat16 *A, *xy, *h1, *h2;
     TRY(dalloc(ctx, &A, (size_t)M * S.kpad));
@@ -2129,7 +2138,7 @@ int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape 
   ctx->sur_fused = ctx->sur_chain == 0 && n_shapes <= kMaxSurShapes;
   std::vector<SurShapeDev> sd;
   for (auto &S : ctx->sur) {
-    sd.push_back(SurShapeDev{S.parts, S.P, S.n_nodes, S.kpad, 0, S.phiT, S.xy, S.F, S.xpart,
+    sd.push_back(SurShapeDev{S.parts, S.P, S.n_nodes, S.kpad, 0, ctx->sur_chain == 0 ? S.phim : S.phiT, S.xy, S.F, S.xpart,
                              sur_n_chunks(S.n_nodes), 0, S.w1m, S.w2m, S.w3m, S.b1, S.b2, S.b3, S.liftm});
     ctx->sur_max_rows = std::max(ctx->sur_max_rows, S.P);
     ctx->sur_max_nodes = std::max(ctx->sur_max_nodes, S.n_nodes);

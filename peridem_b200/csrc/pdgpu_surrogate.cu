@@ -172,127 +172,6 @@ __global__ void k_adam(float *p, float *m, float *v, const float *g, int64_t n, 
 // ---- the CUDA-core chain of the step; the shapes travel by value in the
 // kernel parameters, so that no CTA waits on a load of them ----
 
-// Gather and projection in one pass.  The projection x = A phi^T has one
-// row per particle, 32 columns and K = 2 n_nodes: a long reduction with
-// little work per row, which tensor-core tiles walk serially on a few CTAs.
-// Here the reduction is split over CTAs: a CTA takes kProjRows rows
-// (particles; row P is the zero input) and kProjNodes nodes of them.  Its
-// phi^T elements are requested first (they do not depend on the gather);
-// the body-frame displacements, rounded to BF16 (the GEMM's A operand), go
-// to shared memory; warp w forms columns 4w..4w+3 for all rows, each lane
-// over kProjNodes / 32 nodes, FP32 accumulation, and a butterfly leaves lane
-// l the sum of (column 4w + l / 8, row l % 8).  The CTA's partial sums go to
-// xpart[row][chunk][32]; the layers' kernel adds the chunks in a fixed
-// order, so the result does not depend on scheduling.
-constexpr int kProjRows = 8;
-constexpr int kProjNodes = 128;
-constexpr int kProjThreads = 256;
-
-__global__ void __launch_bounds__(kProjThreads, 4) k_gather_project(const double *__restrict__ u,
-                                                                 const __grid_constant__ SurShapes shapes) {
-  // per row pair p and node a: (row 2p x, row 2p+1 x, row 2p y, row 2p+1 y)
-  __shared__ __align__(16) float4 s_rows[kProjRows / 2][kProjNodes];
-  __shared__ int64_t s_node[kProjRows][2];  // first node, centre node
-  __shared__ double s_rot[kProjRows][3];    // c, s, 1 / scale
-  const SurShapeDev &S = shapes.s[blockIdx.z];
-  const int k0 = blockIdx.x * kProjRows, a0 = blockIdx.y * kProjNodes;
-  if (k0 > S.P || a0 >= S.n_nodes) return;
-  const int nrow = min(kProjRows, S.P - k0);  // rows with a particle; the rest are zero
-  const int na = min(kProjNodes, S.n_nodes - a0);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  constexpr int kPairs = kProjNodes / 32;  // nodes per lane (a node: one BF16 pair of a phi^T row)
-  const __nv_bfloat162 *ph = reinterpret_cast<const __nv_bfloat162 *>(S.phiT);
-  const int half = S.kpad / 2;  // phi^T row j: half BF16 pairs, pair a = node a
-  __nv_bfloat162 wb[4][kPairs];
-#pragma unroll
-  for (int t = 0; t < 4; t++)
-#pragma unroll
-    for (int m = 0; m < kPairs; m++) {
-      const int a = lane + 32 * m;
-      wb[t][m] = a < na ? __ldg(ph + (size_t)(4 * warp + t) * half + a0 + a) : __floats2bfloat162_rn(0.f, 0.f);
-    }
-  if ((int)threadIdx.x < nrow) {
-    const SurPart sp = S.parts[k0 + threadIdx.x];
-    s_node[threadIdx.x][0] = sp.start;
-    s_node[threadIdx.x][1] = sp.center;
-    s_rot[threadIdx.x][0] = sp.c;
-    s_rot[threadIdx.x][1] = sp.s;
-    s_rot[threadIdx.x][2] = sp.inv_scale;
-  }
-  __syncthreads();
-  constexpr int kItems = kProjRows * kProjNodes / kProjThreads;  // (row, node) pairs per thread
-  {
-    double2 v[kItems], c[kItems];
-#pragma unroll
-    for (int q = 0; q < kItems; q++) {
-      const int e = threadIdx.x + q * kProjThreads, r = e / kProjNodes, a = e % kProjNodes;
-      v[q] = c[q] = make_double2(0.0, 0.0);
-      if (r < nrow && a < na) {
-        v[q] = *reinterpret_cast<const double2 *>(u + 2 * (s_node[r][0] + a0 + a));
-        c[q] = *reinterpret_cast<const double2 *>(u + 2 * s_node[r][1]);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < kItems; q++) {
-      const int e = threadIdx.x + q * kProjThreads, r = e / kProjNodes, a = e % kProjNodes;
-      float b0 = 0.f, b1 = 0.f;
-      if (r < nrow && a < na) {
-        const double *R = s_rot[r];
-        const double d0 = v[q].x - c[q].x, d1 = v[q].y - c[q].y;
-        // R(-theta) d / scale
-        b0 = (float)((R[0] * d0 + R[1] * d1) * R[2]);
-        b1 = (float)((-R[1] * d0 + R[0] * d1) * R[2]);
-      }
-      float *o = reinterpret_cast<float *>(&s_rows[r >> 1][a]) + (r & 1);
-      o[0] = __bfloat162float(__float2bfloat16(b0));
-      o[2] = __bfloat162float(__float2bfloat16(b1));
-    }
-  }
-  __syncthreads();
-  // two rows per packed FMA: acc[4 t + p] holds (column 4 warp + t) for rows
-  // 2p and 2p + 1, each element summed in the same order as a scalar loop
-  float2 acc[16];
-#pragma unroll
-  for (int q = 0; q < 16; q++) acc[q] = make_float2(0.f, 0.f);
-#pragma unroll
-  for (int m = 0; m < kPairs; m++) {
-    const int a = lane + 32 * m;
-    float2 w[4];
-#pragma unroll
-    for (int t = 0; t < 4; t++) w[t] = __bfloat1622float2(wb[t][m]);
-#pragma unroll
-    for (int p = 0; p < kProjRows / 2; p++) {
-      const float4 x = s_rows[p][a];
-#pragma unroll
-      for (int t = 0; t < 4; t++) {
-        acc[4 * t + p] = __ffma2_rn(make_float2(x.x, x.y), make_float2(w[t].x, w[t].x), acc[4 * t + p]);
-        acc[4 * t + p] = __ffma2_rn(make_float2(x.z, x.w), make_float2(w[t].y, w[t].y), acc[4 * t + p]);
-      }
-    }
-  }
-  float v[32];  // v[8 t + r]: column 4 warp + t, row r
-#pragma unroll
-  for (int q = 0; q < 16; q++) {
-    v[2 * q] = acc[q].x;
-    v[2 * q + 1] = acc[q].y;
-  }
-  // butterfly: after the stage of offset o a lane keeps the half of its
-  // values selected by (lane & o); lane l ends with the total of v[l]
-#pragma unroll
-  for (int o = 16, n = 32; o >= 1; o >>= 1, n >>= 1) {
-    const bool upper = (lane & o) != 0;
-#pragma unroll
-    for (int q = 0; q < n / 2; q++) {
-      const float send = upper ? v[q] : v[q + n / 2];
-      const float keep = upper ? v[q + n / 2] : v[q];
-      v[q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
-    }
-  }
-  const int t = lane >> 3, r = lane & 7;
-  if (k0 + r <= S.P)
-    S.xpart[((size_t)(k0 + r) * S.n_chunks + blockIdx.y) * 32 + 4 * warp + t] = v[0];
-}
-
 // ---- warp-level MMA (m16n8k16, BF16 operands, FP32 accumulation) ----
 __device__ __forceinline__ void mma_bf16_16816(float *d, const uint32_t *a, const uint32_t *b) {
   asm volatile(
@@ -327,6 +206,110 @@ __device__ __forceinline__ void frag_b_of(const uint4 *q, int kl, uint32_t *b) {
   const uint4 v = q[kl >> 1];
   b[0] = (kl & 1) ? v.z : v.x;
   b[1] = (kl & 1) ? v.w : v.y;
+}
+
+// Gather and projection in one pass, by warp MMA.  The projection
+// x = A phi^T has one row per particle, 32 columns and K = 2 n_nodes: a long
+// reduction with little work per row.  It is split over CTAs: a CTA takes
+// kProjRows rows (particles; row P is the zero input) and kProjNodes nodes
+// (256 of K).  Its phi^T fragments (K-permuted rows, 32 bytes per lane and
+// 64-input chunk) are requested first; the body-frame displacements,
+// rounded to BF16, go to shared memory; warp w forms column tile w % 4 over
+// half of the CTA's K, and the two halves are added in a fixed order.  The
+// CTA's partial sums go to xpart[row][chunk][32]; the layers' kernel adds
+// the chunks in a fixed order, so the result does not depend on scheduling.
+constexpr int kProjRows = 16;
+constexpr int kProjNodes = 128;
+constexpr int kProjThreads = 256;
+constexpr int kProjLd = 2 * kProjNodes + 8;  // BF16 per row of the displacement tile
+
+__global__ void __launch_bounds__(kProjThreads) k_gather_project(const double *__restrict__ u,
+                                                                 const __grid_constant__ SurShapes shapes) {
+  __shared__ __align__(16) __nv_bfloat16 s_a[kProjRows * kProjLd];
+  __shared__ __align__(16) float s_red[kProjRows][32];
+  __shared__ int64_t s_node[kProjRows][2];  // first node, centre node
+  __shared__ double s_rot[kProjRows][3];    // c, s, 1 / scale
+  const SurShapeDev &S = shapes.s[blockIdx.z];
+  const int k0 = blockIdx.x * kProjRows, a0 = blockIdx.y * kProjNodes;
+  if (k0 > S.P || a0 >= S.n_nodes) return;
+  const int nrow = min(kProjRows, S.P - k0);  // rows with a particle; the rest are zero
+  const int na = min(kProjNodes, S.n_nodes - a0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+  const int nt = warp & 3, half = warp >> 2;  // column tile, half of the CTA's K
+  // phi^T: row 8 nt + g, the two 64-input chunks of this half
+  const uint32_t *ph = (const uint32_t *)S.phiT + (size_t)(8 * nt + g) * (S.n_chunks * 128) + blockIdx.y * 128;
+  uint4 bq[2][2];
+#pragma unroll
+  for (int c = 0; c < 2; c++) frag_b_load(ph + 32 * (2 * half + c), tig, bq[c]);
+  if ((int)threadIdx.x < nrow) {
+    const SurPart sp = S.parts[k0 + threadIdx.x];
+    s_node[threadIdx.x][0] = sp.start;
+    s_node[threadIdx.x][1] = sp.center;
+    s_rot[threadIdx.x][0] = sp.c;
+    s_rot[threadIdx.x][1] = sp.s;
+    s_rot[threadIdx.x][2] = sp.inv_scale;
+  }
+  __syncthreads();
+  constexpr int kItems = kProjRows * kProjNodes / kProjThreads;  // (row, node) pairs per thread
+  constexpr int kBatch = 4;
+#pragma unroll
+  for (int q0 = 0; q0 < kItems; q0 += kBatch) {
+    double2 v[kBatch], c[kBatch];
+#pragma unroll
+    for (int q = 0; q < kBatch; q++) {
+      const int e = threadIdx.x + (q0 + q) * kProjThreads, r = e / kProjNodes, a = e % kProjNodes;
+      v[q] = c[q] = make_double2(0.0, 0.0);
+      if (r < nrow && a < na) {
+        v[q] = *reinterpret_cast<const double2 *>(u + 2 * (s_node[r][0] + a0 + a));
+        c[q] = *reinterpret_cast<const double2 *>(u + 2 * s_node[r][1]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kBatch; q++) {
+      const int e = threadIdx.x + (q0 + q) * kProjThreads, r = e / kProjNodes, a = e % kProjNodes;
+      float b0 = 0.f, b1 = 0.f;
+      if (r < nrow && a < na) {
+        const double *R = s_rot[r];
+        const double d0 = v[q].x - c[q].x, d1 = v[q].y - c[q].y;
+        // R(-theta) d / scale
+        b0 = (float)((R[0] * d0 + R[1] * d1) * R[2]);
+        b1 = (float)((-R[1] * d0 + R[0] * d1) * R[2]);
+      }
+      *reinterpret_cast<__nv_bfloat162 *>(s_a + r * kProjLd + 2 * a) = __floats2bfloat162_rn(b0, b1);
+    }
+  }
+  __syncthreads();
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int c = 0; c < 2; c++)
+#pragma unroll
+    for (int kl = 0; kl < 4; kl++) {
+      uint32_t a[4], b[2];
+      frag_a(s_a, kProjLd, 4 * (2 * half + c) + kl, g, tig, a);
+      frag_b_of(bq[c], kl, b);
+      mma_bf16_16816(acc, a, b);
+    }
+  // rows g and g + 8, columns 8 nt + 2 tig (+1): the second half adds its
+  // partial sums to the first half's
+  const int col = 8 * nt + 2 * tig;
+  if (half == 1) {
+    s_red[g][col] = acc[0];
+    s_red[g][col + 1] = acc[1];
+    s_red[g + 8][col] = acc[2];
+    s_red[g + 8][col + 1] = acc[3];
+  }
+  __syncthreads();
+  if (half == 1) return;
+  float *xp = S.xpart + blockIdx.y * 32 + col;
+  const size_t ld = (size_t)S.n_chunks * 32;
+  if (k0 + g <= S.P) {
+    xp[(k0 + g) * ld] = acc[0] + s_red[g][col];
+    xp[(k0 + g) * ld + 1] = acc[1] + s_red[g][col + 1];
+  }
+  if (k0 + g + 8 <= S.P) {
+    xp[(k0 + g + 8) * ld] = acc[2] + s_red[g + 8][col];
+    xp[(k0 + g + 8) * ld + 1] = acc[3] + s_red[g + 8][col + 1];
+  }
 }
 
 // The three layers of the network for 16 rows (rows 0..P, P the zero input)
