@@ -225,6 +225,7 @@ struct DevData {
   int32_t *damp_group;
   int32_t n_damp_groups;
   double *pcen;          // per particle, this step: {x, y, z, bounding radius, vx, vy, vz, -}
+  float4 *pcen32;        // the same centre and bounding radius in FP32 (damping pre-filter)
 
   // boundary conditions: per BC node, a run of entries applied in set order
   int32_t n_ubc_sets, n_fbc_sets;

@@ -1130,6 +1130,7 @@ __global__ void __launch_bounds__(kBlock) k_contact(DevData d) {
         o[4 + q] = vc[q];
       }
       o[3] = d.dpart[p].bound_r;
+      d.pcen32[p] = make_float4((float)xc[0], (float)xc[1], (float)xc[2], (float)o[3]);
     }
   }
   __syncthreads();
@@ -1265,6 +1266,7 @@ __global__ void __launch_bounds__(kBlock) k_contact_warp(DevData d) {
       o[4 + q] = vc[q];
     }
     o[3] = d.dpart[p].bound_r;
+    d.pcen32[p] = make_float4((float)xc[0], (float)xc[1], (float)xc[2], (float)o[3]);
   }
   __syncthreads();
   const int64_t nn = err ? 0 : nn_raw;
@@ -1434,6 +1436,7 @@ __global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
   __shared__ double s_acc[kDampGroup][3][kDampBlock];  // member, component, thread
   __shared__ double s_c[kDampGroup][8];                // centre (3), centre velocity (3), radius, density
   __shared__ int s_zone[kDampGroup], s_type[kDampGroup];
+  __shared__ float4 s_cf[kDampGroup];                  // FP32 centre and radius
   const int p0 = d.damp_group ? d.damp_group[blockIdx.x] : (int)blockIdx.x;
   const int np = d.damp_group ? d.damp_group[blockIdx.x + 1] - p0 : 1;
   const int nz = d.n_zones;
@@ -1449,6 +1452,7 @@ __global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
     }
     s_c[threadIdx.x][6] = P.bound_r;
     s_c[threadIdx.x][7] = P.density;
+    s_cf[threadIdx.x] = d.pcen32[p];
     s_zone[threadIdx.x] = P.zone;
     s_type[threadIdx.x] = P.type;
   }
@@ -1459,29 +1463,33 @@ __global__ void __launch_bounds__(kDampBlock) k_damping(DevData d, int dim) {
   if (!any) return;
   if (d.ctrl->error) return;
   const DampParticle G = d.dpart[p0];  // the group's scene: its particles q0 .. q1 - 1
-  // particle-particle, over the particles of the scene: first the 32-byte
-  // {centre, radius} record only, against the largest reach any zone pair
-  // allows; kDampBatch records in flight per thread, each thread visiting
-  // its particles in increasing order
+  // particle-particle, over the particles of the scene: first the 16-byte
+  // FP32 {centre, radius} record, against the largest reach any zone pair
+  // allows with a 10 % margin over the FP64 test below (coordinates rounded
+  // to FP32 move a distance by far less), so that only pairs that test can
+  // pass read the FP64 record; kDampBatch records in flight per thread, each
+  // thread visiting its particles in increasing order
   constexpr int kDampBatch = 4;
+  const float rc_f = (float)(1.01 * d.rc_max);
   for (int qb = G.q0 + threadIdx.x; qb < G.q1; qb += kDampBatch * blockDim.x) {
-    double2 c01b[kDampBatch], c2rb[kDampBatch];
+    float4 cf[kDampBatch];
 #pragma unroll
     for (int t = 0; t < kDampBatch; t++) {
       const int q = qb + t * (int)blockDim.x;
-      c01b[t] = c2rb[t] = make_double2(0.0, 0.0);
-      if (q < G.q1) {
-        c01b[t] = *reinterpret_cast<const double2 *>(d.pcen + 8 * q);
-        c2rb[t] = *reinterpret_cast<const double2 *>(d.pcen + 8 * q + 2);
-      }
+      cf[t] = q < G.q1 ? d.pcen32[q] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 #pragma unroll
     for (int t = 0; t < kDampBatch; t++) {
       const int q = qb + t * (int)blockDim.x;
       if (q >= G.q1) continue;
-      const double2 c01 = c01b[t], c2r = c2rb[t];
       for (int k = 0; k < np; k++) {
         if (s_type[k] != 0 || q == p0 + k) continue;
+        const float4 pf = s_cf[k];
+        const float ex = cf[t].x - pf.x, ey = cf[t].y - pf.y, ez = cf[t].z - pf.z;
+        const float rm = cf[t].w + pf.w + rc_f;
+        if (ex * ex + ey * ey + ez * ez > 1.17f * rm * rm) continue;
+        const double2 c01 = *reinterpret_cast<const double2 *>(d.pcen + 8 * q);
+        const double2 c2r = *reinterpret_cast<const double2 *>(d.pcen + 8 * q + 2);
         const double *C = s_c[k];
         const double Ri = C[6];
         double xcj[3] = {c01.x - C[0], c01.y - C[1], c2r.x - C[2]};

@@ -920,6 +920,8 @@ int prepare(pdgpu_ctx *ctx) {
     }
     TRY(dalloc(ctx, &d.pcen, 8 * dp.size()));
     CK(cudaMemset(d.pcen, 0, 8 * dp.size() * 8));
+    TRY(dalloc(ctx, &d.pcen32, dp.size()));
+    CK(cudaMemset(d.pcen32, 0, dp.size() * sizeof(float4)));
   }
   if (ctx->desc.multi_particle) {
     d.contact_cap = ctx->desc.contact_capacity > 0 ? ctx->desc.contact_capacity
