@@ -563,20 +563,28 @@ __global__ void __launch_bounds__(kThreadsFor<DIM, LPN>) k_bonds_mixed(DevData d
   __shared__ int s_tile[2];
   if (d.ctrl->error) return;
   constexpr bool state = LAW == LAW_STATE && !PRE;  // the pre-pass needs no m, theta stage
+  // learned surrogate: off check steps, its particles' tiles are left out —
+  // by claiming from the list of the other tiles the contact rebuild wrote
+  // this step where there is one, else by a test of each claimed tile
+  const bool sur_step = d.sur_on != nullptr && !d.ctrl->sur_check;
+  const bool listed = !PRE && sur_step && d.tile_live != nullptr;
+  auto claim = [&]() -> int {
+    const int c = (int)atomicAdd(&d.ctrl->tile_next, 1u);
+    if (!listed) return c;
+    return c < min((int)*d.tile_live_n, d.n_tile_live_src) ? d.tile_live[c] : n_tiles;
+  };
   if (threadIdx.x == 0) {
     bar_init(&bar);
-    s_tile[0] = (int)atomicAdd(&d.ctrl->tile_next, 1u);
+    s_tile[0] = claim();
   }
   __syncthreads();
   uint32_t parity = 0;
   int k = 0;
   int t = s_tile[0];
-  // learned surrogate: off check steps, its particles' tiles are skipped
-  const bool sur_step = d.sur_on != nullptr && !d.ctrl->sur_check;
   while (t < n_tiles) {
     const BondTile T = tiles[t];
     if (sur_step && d.sur_on[T.particle] && !d.sur_near[T.particle]) {
-      if (threadIdx.x == 0) s_tile[(k + 1) & 1] = (int)atomicAdd(&d.ctrl->tile_next, 1u);
+      if (threadIdx.x == 0) s_tile[(k + 1) & 1] = claim();
       __syncthreads();
       t = s_tile[(k + 1) & 1];
       k++;
@@ -604,7 +612,7 @@ __global__ void __launch_bounds__(kThreadsFor<DIM, LPN>) k_bonds_mixed(DevData d
       if (p.bit_bytes) bulk_load(s_bits, d.bond_bits + p.word0, p.bit_bytes, &bar);
       bulk_load(s_row, d.pd_row + p.row0, p.row_bytes, &bar);
       bulk_load(s_xv, d.xv_mixed + T.win_begin, 16u * (uint32_t)w, &bar);
-      s_tile[(k + 1) & 1] = (int)atomicAdd(&d.ctrl->tile_next, 1u);
+      s_tile[(k + 1) & 1] = claim();
     }
     const MixParticle M = d.mixp[T.particle];
 
@@ -656,6 +664,8 @@ __global__ void __launch_bounds__(kThreadsFor<DIM, LPN>) k_bonds_mixed(DevData d
     if (atomicAdd(&d.ctrl->tile_done, 1u) == gridDim.x - 1) {
       atomicExch(&d.ctrl->tile_next, 0u);
       atomicExch(&d.ctrl->tile_done, 0u);
+      // the surrogate's tile list is rebuilt by the next step's rebuild kernel
+      if (!PRE && d.tile_live) atomicExch(d.tile_live_n, 0u);
     }
   }
 }

@@ -301,6 +301,15 @@ struct DevData {
   // the surrogate when sur_on && !sur_near.
   uint8_t *sur_on;
   uint8_t *sur_near;
+  // with the surrogate, one bond-loop launch over all tiles and a contact
+  // rebuild every step: the rebuild kernel lists the tiles of the particles
+  // off the surrogate (tile_live[0 .. *tile_live_n)), and the bond loop
+  // claims from that list off check steps; tile_particle[t] is tile t's
+  // particle.  Null otherwise.
+  int32_t *tile_live;
+  uint32_t *tile_live_n;
+  const int32_t *tile_particle;
+  int32_t n_tile_live_src;
   int32_t sur_interval;
   int32_t sur_near_gate;
 };

@@ -953,12 +953,30 @@ __device__ void cand_fill_nodes(const DevData &d, int64_t nn) {
   }
 }
 
+// The learned surrogate's list of the tiles the bond loop runs this step:
+// those of the particles not on the surrogate (sur_on && !sur_near is the
+// test the surrogate's scatter applies).  The order follows the atomic
+// claims; each tile's forces do not depend on it.
+__device__ void list_live_tiles(const DevData &d) {
+  if (!d.tile_live) return;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < d.n_tile_live_src; t += gridDim.x * blockDim.x) {
+    const int p = d.tile_particle[t];
+    if (d.sur_on[p] && !d.sur_near[p]) continue;
+    const unsigned k = atomicAdd(d.tile_live_n, 1u);
+    if (k < (unsigned)d.n_tile_live_src) d.tile_live[k] = t;
+  }
+}
+
 template <int DIM, int LPN>
 __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8_t search_bit,
                                                                int64_t *bsum) {
   extern __shared__ __align__(16) unsigned char cand_smem[];
   CandWarp<DIM> *stage = reinterpret_cast<CandWarp<DIM> *>(cand_smem);
-  if (d.ctrl->error || !d.ctrl->update) return;
+  if (d.ctrl->error) return;
+  if (!d.ctrl->update) {
+    list_live_tiles(d);
+    return;
+  }
   CtrlState *gc = d.ctrl;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   // phase clock (profiling): the first CTA's time past each barrier
@@ -1040,6 +1058,7 @@ __global__ void __launch_bounds__(kCoopBlock) k_contact_rebuild(DevData d, uint8
     }
   if (tid == 0) d.ctrl->c_nnodes = d.c_tmp[N];
   if (!grid_bar(gc)) return;  // the compacted list is complete
+  list_live_tiles(d);          // the proximity flags are final
   stamp();
   cand_fill_nodes<DIM>(d, d.c_tmp[N]);
   stamp();  // the first CTA's share of the fill done

@@ -586,6 +586,41 @@ int prepare_mixed(pdgpu_ctx *ctx) {
 // Tiles of the bond loop: every force-computing particle is cut into runs of
 // tile_nodes consecutive nodes; the device finds each tile's neighbour window
 // and the largest window fixes the shared-memory stage.
+// The learned surrogate's list of bond-loop tiles (written each step by the
+// contact rebuild kernel, read by the bond loop): kept when the surrogate is
+// set, the steps rebuild contact lists (multi-particle scenes) and one
+// bond-loop launch covers every tile (a single material law).
+int setup_tile_list(pdgpu_ctx *ctx) {
+  DevData &d = ctx->d;
+  if (d.tile_live) {
+    dfree(ctx, d.tile_live);
+    dfree(ctx, d.tile_live_n);
+    int32_t *tp0 = const_cast<int32_t *>(d.tile_particle);
+    dfree(ctx, tp0);
+    d.tile_live = nullptr;
+    d.tile_live_n = nullptr;
+    d.tile_particle = nullptr;
+    d.n_tile_live_src = 0;
+  }
+  int laws = 0;
+  for (int m = 0; m < 4; m++) laws += ctx->tile_law[m + 1] > ctx->tile_law[m];
+  if (ctx->sur.empty() || !ctx->desc.multi_particle || !ctx->tiles || ctx->n_tiles <= 0 || laws != 1)
+    return PDGPU_OK;
+  std::vector<BondTile> t((size_t)ctx->n_tiles);
+  CK(cudaMemcpy(t.data(), ctx->tiles, t.size() * sizeof(BondTile), cudaMemcpyDeviceToHost));
+  std::vector<int32_t> part(t.size());
+  for (size_t k = 0; k < t.size(); k++) part[k] = t[k].particle;
+  int32_t *tp;
+  TRY(dalloc(ctx, &tp, part.size()));
+  CK(cudaMemcpy(tp, part.data(), part.size() * 4, cudaMemcpyHostToDevice));
+  TRY(dalloc(ctx, &d.tile_live, part.size()));
+  TRY(dalloc(ctx, &d.tile_live_n, 1));
+  CK(cudaMemset(d.tile_live_n, 0, 4));
+  d.tile_particle = tp;
+  d.n_tile_live_src = ctx->n_tiles;
+  return PDGPU_OK;
+}
+
 int prepare_tiles(pdgpu_ctx *ctx) {
   DevData &d = ctx->d;
   const bool mixed = d.precision == PDGPU_PREC_MIXED;
@@ -660,7 +695,7 @@ int prepare_tiles(pdgpu_ctx *ctx) {
     ctx->tile_smem_state = ss;
     ctx->tile_smem_pd = pd;
     ctx->tile_nodes = tn;
-    return PDGPU_OK;
+    return setup_tile_list(ctx);
   }
   return fail(ctx, PDGPU_ERR_ARG,
               "a particle's bonds reach too far in node order for the shared-memory stage; "
@@ -1537,6 +1572,8 @@ int pdgpu_init_contact(pdgpu_ctx *ctx) {
   launch_ctrl(ctx->d, 2, ctx->stream);
   CK(launch_contact_rebuild(ctx->d, ctx->rebuild_bsum, ctx->rebuild_grid, ctx->contact_lanes, 1,
                             ctx->stream));
+  // no bond loop follows this rebuild: clear the surrogate's tile list
+  if (ctx->d.tile_live) CK(cudaMemsetAsync(ctx->d.tile_live_n, 0, 4, ctx->stream));
   TRY(device_error(ctx));
   ctx->contact_init = true;
   return PDGPU_OK;
@@ -2173,7 +2210,7 @@ int pdgpu_set_surrogate(pdgpu_ctx *ctx, int32_t n_shapes, const pdgpu_sur_shape 
     cudaGraphExecDestroy(ctx->gexec);
     ctx->gexec = nullptr;
   }
-  return PDGPU_OK;
+  return setup_tile_list(ctx);  // when the bond tiles exist already
 }
 
 int pdgpu_surrogate_stats(pdgpu_ctx *ctx, int64_t *n_on, int64_t *n_total, int64_t *steps_on,
