@@ -1848,60 +1848,80 @@ __global__ void __launch_bounds__(1024) k_postprocess(const __grid_constant__ De
 // k_verlet_second); then the last CTA to finish runs the post-processing (as
 // k_postprocess) when `post` is set.
 // ---------------------------------------------------------------------------
+constexpr int kEndNodes = 2;  // nodes per thread of the step-end kernel
+
 template <int DIM, bool VERLET>
 __global__ void __launch_bounds__(kBlock) k_step_end(const __grid_constant__ DevData d, int post) {
   __shared__ int last;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n_step = d.ctrl->n;
-  if (i < d.n_nodes && !d.ctrl->error) {
-    // the node's own loads first (independent of its flags), then the sums;
-    // the contact force only where the node searches (elsewhere it is never
-    // written and its lines are cold)
-    const uint8_t fl = d.flags[i];
-    const int32_t p = d.ptid[i];
-    double f[3] = {0.0, 0.0, 0.0}, fa[3];
-    ldv<DIM>(d.f, i, fa);
-    if (fl & NODE_ACTIVE) {
+  // each thread takes kEndNodes nodes, kBlock apart, and issues the node
+  // loads of all of them (independent of their flags) before the sums
+  const int64_t base = (int64_t)blockIdx.x * (kBlock * kEndNodes) + threadIdx.x;
+  if (!d.ctrl->error) {
+    uint8_t fl[kEndNodes];
+    int32_t pid[kEndNodes];
+    double fa[kEndNodes][3];
 #pragma unroll
-      for (int q = 0; q < DIM; q++) f[q] = fa[q];
-      if (d.fc && (fl & (NODE_SEARCH | NODE_SEARCH0))) {
-        double c[3];
-        ldv<DIM>(d.fc, i, c);
-        if (c[0] != 0.0 || c[1] != 0.0 || (DIM == 3 && c[2] != 0.0)) {
-#pragma unroll
-          for (int q = 0; q < DIM; q++) f[q] += c[q];
-          const double z[3] = {0.0, 0.0, 0.0};
-          stv<DIM>(d.fc, i, z);
-        }
+    for (int k = 0; k < kEndNodes; k++) {
+      const int64_t i = base + (int64_t)k * kBlock;
+      fl[k] = 0;
+      pid[k] = 0;
+      if (i < d.n_nodes) {
+        fl[k] = d.flags[i];
+        pid[k] = d.ptid[i];
+        ldv<DIM>(d.f, i, fa[k]);
       }
     }
-    if (fl & NODE_PARTICLE) {
 #pragma unroll
-      for (int q = 0; q < DIM; q++) f[q] += d.fdamp[4 * p + q];
-    }
-    double rho = 0.0;
-    if (d.gravity_on || (VERLET && (fl & NODE_ACTIVE))) rho = d.particles[p].density;
-    if (d.gravity_on) {
+    for (int k = 0; k < kEndNodes; k++) {
+      const int64_t i = base + (int64_t)k * kBlock;
+      if (i >= d.n_nodes) continue;
+      const int32_t p = pid[k];
+      double f[3] = {0.0, 0.0, 0.0};
+      // the contact force only where the node searches (elsewhere it is never
+      // written and its lines are cold)
+      if (fl[k] & NODE_ACTIVE) {
 #pragma unroll
-      for (int q = 0; q < DIM; q++) f[q] += rho * d.gravity[q];
-    }
-    if (fl & NODE_FBC) {  // through a copy, so that f stays in registers
-      double fb[3] = {f[0], f[1], f[2]};
-      apply_fbc<DIM>(d, d.fbc_of[i], d.ctrl->time, fb);
+        for (int q = 0; q < DIM; q++) f[q] = fa[k][q];
+        if (d.fc && (fl[k] & (NODE_SEARCH | NODE_SEARCH0))) {
+          double c[3];
+          ldv<DIM>(d.fc, i, c);
+          if (c[0] != 0.0 || c[1] != 0.0 || (DIM == 3 && c[2] != 0.0)) {
 #pragma unroll
-      for (int q = 0; q < 3; q++) f[q] = fb[q];
-    }
-    stv<DIM>(d.f, i, f);
-    if (VERLET && (fl & NODE_ACTIVE)) {
-      const uint8_t fix = d.fix[i];
-      double v[3];
-      ldv<DIM>(d.v, i, v);
-      const double k = 0.5 * (d.dt / rho);
+            for (int q = 0; q < DIM; q++) f[q] += c[q];
+            const double z[3] = {0.0, 0.0, 0.0};
+            stv<DIM>(d.fc, i, z);
+          }
+        }
+      }
+      if (fl[k] & NODE_PARTICLE) {
 #pragma unroll
-      for (int dof = 0; dof < DIM; dof++)
-        if (!((fix >> dof) & 1u)) v[dof] += k * f[dof];
-      stv<DIM>(d.v, i, v);
-      d.vmag[i] = len3<DIM>(v);
+        for (int q = 0; q < DIM; q++) f[q] += d.fdamp[4 * p + q];
+      }
+      double rho = 0.0;
+      if (d.gravity_on || (VERLET && (fl[k] & NODE_ACTIVE))) rho = d.particles[p].density;
+      if (d.gravity_on) {
+#pragma unroll
+        for (int q = 0; q < DIM; q++) f[q] += rho * d.gravity[q];
+      }
+      if (fl[k] & NODE_FBC) {  // through a copy, so that f stays in registers
+        double fb[3] = {f[0], f[1], f[2]};
+        apply_fbc<DIM>(d, d.fbc_of[i], d.ctrl->time, fb);
+#pragma unroll
+        for (int q = 0; q < 3; q++) f[q] = fb[q];
+      }
+      stv<DIM>(d.f, i, f);
+      if (VERLET && (fl[k] & NODE_ACTIVE)) {
+        const uint8_t fix = d.fix[i];
+        double v[3];
+        ldv<DIM>(d.v, i, v);
+        const double kk = 0.5 * (d.dt / rho);
+#pragma unroll
+        for (int dof = 0; dof < DIM; dof++)
+          if (!((fix >> dof) & 1u)) v[dof] += kk * f[dof];
+        stv<DIM>(d.v, i, v);
+        d.vmag[i] = len3<DIM>(v);
+      }
     }
   }
   // the post-processing tail only on the steps that record test output
@@ -2178,7 +2198,7 @@ void launch_step_begin(const DevData &d, int verlet, cudaStream_t s) {
 }
 
 void launch_step_end(const DevData &d, int verlet, int post, cudaStream_t s) {
-  const unsigned g = blocks_for(d.n_nodes, kBlock);
+  const unsigned g = blocks_for(d.n_nodes, kBlock * kEndNodes);
   if (d.dim == 2) {
     if (verlet) k_step_end<2, true><<<g, kBlock, 0, s>>>(d, post);
     else k_step_end<2, false><<<g, kBlock, 0, s>>>(d, post);
