@@ -313,40 +313,46 @@ __global__ void __launch_bounds__(kProjThreads) k_gather_project(const double *_
 }
 
 // The three layers of the network for 16 rows (rows 0..P, P the zero input)
-// per CTA by warp MMA.  The projected input x is the sum of the
+// per CTA by warp MMA, 16 warps.  The projected input x is the sum of the
 // projection's chunks in chunk order, rounded to BF16 (and stored in xy for
 // the lift); activations stay in shared memory as BF16 rows (padded so that
 // fragment loads do not conflict), with the bias and tanh applied to the
-// FP32 accumulators as the tensor-core chain does.  Weight fragments come
-// from the K-permuted rows, 32 bytes per lane and 64-input chunk, the next
-// chunk requested while the current one is multiplied.
-//   h1 = tanh(x W1^T + b1), h2 = tanh(h1 W2^T + b2): warp w, columns 32w..32w+31
-//   y  = h2 W3^T + b3 -> xy (columns 0..31): warps 0-3, eight columns each
+// FP32 accumulators as the tensor-core chain does.  Every weight fragment a
+// warp needs (K-permuted rows, 32 bytes per lane and 64-input chunk) is
+// requested at the start, so that the layers wait for one round of loads.
+//   h1 = tanh(x W1^T + b1), h2 = tanh(h1 W2^T + b2): warp w, columns 16w..16w+15
+//   y  = h2 W3^T + b3 -> xy (columns 0..31): warp w, columns 8 (w % 4).., inputs
+//        64 (w / 4)..; the four input quarters added in a fixed order
 constexpr int kMlpRows = 16;
-constexpr int kMlpThreads = 256;
+constexpr int kMlpThreads = 512;
 constexpr int kMlpLdX = 32 + 8, kMlpLdH = 256 + 8;
 
 __global__ void __launch_bounds__(kMlpThreads) k_mlp(const __grid_constant__ SurShapes shapes) {
   __shared__ __align__(16) __nv_bfloat16 s_x[kMlpRows * kMlpLdX];
   __shared__ __align__(16) __nv_bfloat16 s_h1[kMlpRows * kMlpLdH];
   __shared__ __align__(16) __nv_bfloat16 s_h2[kMlpRows * kMlpLdH];
+  __shared__ float s_y[4][kMlpRows][32];  // layer 3's partial sums per input quarter
   const SurShapeDev &S = shapes.s[blockIdx.y];
   const int k0 = blockIdx.x * kMlpRows;
   if (k0 > S.P) return;
   const int nrow = min(kMlpRows, S.P + 1 - k0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
   const uint32_t *W1 = (const uint32_t *)S.w1m, *W2 = (const uint32_t *)S.w2m, *W3 = (const uint32_t *)S.w3m;
-  // layer 1's weights (32 inputs: one chunk of two k-steps, 16 bytes per lane)
-  uint4 w1q[4];
+  // every weight fragment of this warp: layer 1 (32 inputs: one chunk of two
+  // k-steps, 16 bytes per lane), layer 2 (four chunks), layer 3 (one chunk)
+  uint4 w1q[2], w2q[4][2][2], w3q[2];
 #pragma unroll
-  for (int t = 0; t < 4; t++) w1q[t] = __ldg(reinterpret_cast<const uint4 *>(W1 + (32 * warp + 8 * t + g) * 16) + tig);
-  // layer 2's first chunk
-  uint4 bq[2][4][2];
+  for (int t = 0; t < 2; t++)
+    w1q[t] = __ldg(reinterpret_cast<const uint4 *>(W1 + (16 * warp + 8 * t + g) * 16) + tig);
 #pragma unroll
-  for (int t = 0; t < 4; t++) frag_b_load(W2 + (32 * warp + 8 * t + g) * 128, tig, bq[0][t]);
+  for (int ch = 0; ch < 4; ch++)
+#pragma unroll
+    for (int t = 0; t < 2; t++) frag_b_load(W2 + (16 * warp + 8 * t + g) * 128 + 32 * ch, tig, w2q[ch][t]);
+  const int nt3 = warp & 3, q3 = warp >> 2;  // layer 3: column tile, input quarter
+  frag_b_load(W3 + (8 * nt3 + g) * 128 + 32 * q3, tig, w3q);
   __nv_bfloat16 *xy = (__nv_bfloat16 *)S.xy;
-  for (int e = threadIdx.x; e < kMlpRows * 32; e += blockDim.x) {
-    const int r = e >> 5, c = e & 31;
+  {
+    const int r = threadIdx.x >> 5, c = threadIdx.x & 31;  // kMlpThreads = kMlpRows x 32
     float x = 0.f;
     if (r < nrow) {
       const float *xp = S.xpart + (size_t)(k0 + r) * S.n_chunks * 32 + c;
@@ -357,10 +363,10 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp(const __grid_constant__ Sur
     s_x[r * kMlpLdX + c] = xb;
   }
   __syncthreads();
-  float acc[4][4];
+  float acc[2][4];
   // layer 1
 #pragma unroll
-  for (int t = 0; t < 4; t++)
+  for (int t = 0; t < 2; t++)
 #pragma unroll
     for (int q = 0; q < 4; q++) acc[t][q] = 0.f;
 #pragma unroll
@@ -368,14 +374,14 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp(const __grid_constant__ Sur
     uint32_t a[4];
     frag_a(s_x, kMlpLdX, kl, g, tig, a);
 #pragma unroll
-    for (int t = 0; t < 4; t++) {
+    for (int t = 0; t < 2; t++) {
       const uint32_t b[2] = {kl ? w1q[t].z : w1q[t].x, kl ? w1q[t].w : w1q[t].y};
       mma_bf16_16816(acc[t], a, b);
     }
   }
 #pragma unroll
-  for (int t = 0; t < 4; t++) {
-    const int col = 32 * warp + 8 * t + 2 * tig;
+  for (int t = 0; t < 2; t++) {
+    const int col = 16 * warp + 8 * t + 2 * tig;
     const float b0 = S.b1[col], b1 = S.b1[col + 1];
     *reinterpret_cast<__nv_bfloat162 *>(s_h1 + g * kMlpLdH + col) =
         __floats2bfloat162_rn(tanhf(acc[t][0] + b0), tanhf(acc[t][1] + b1));
@@ -385,29 +391,25 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp(const __grid_constant__ Sur
   __syncthreads();
   // layer 2: four 64-input chunks
 #pragma unroll
-  for (int t = 0; t < 4; t++)
+  for (int t = 0; t < 2; t++)
 #pragma unroll
     for (int q = 0; q < 4; q++) acc[t][q] = 0.f;
 #pragma unroll
-  for (int ch = 0; ch < 4; ch++) {
-    if (ch + 1 < 4)
-#pragma unroll
-      for (int t = 0; t < 4; t++) frag_b_load(W2 + (32 * warp + 8 * t + g) * 128 + 32 * (ch + 1), tig, bq[(ch + 1) & 1][t]);
+  for (int ch = 0; ch < 4; ch++)
 #pragma unroll
     for (int kl = 0; kl < 4; kl++) {
       uint32_t a[4];
       frag_a(s_h1, kMlpLdH, 4 * ch + kl, g, tig, a);
 #pragma unroll
-      for (int t = 0; t < 4; t++) {
+      for (int t = 0; t < 2; t++) {
         uint32_t b[2];
-        frag_b_of(bq[ch & 1][t], kl, b);
+        frag_b_of(w2q[ch][t], kl, b);
         mma_bf16_16816(acc[t], a, b);
       }
     }
-  }
 #pragma unroll
-  for (int t = 0; t < 4; t++) {
-    const int col = 32 * warp + 8 * t + 2 * tig;
+  for (int t = 0; t < 2; t++) {
+    const int col = 16 * warp + 8 * t + 2 * tig;
     const float b0 = S.b2[col], b1 = S.b2[col + 1];
     *reinterpret_cast<__nv_bfloat162 *>(s_h2 + g * kMlpLdH + col) =
         __floats2bfloat162_rn(tanhf(acc[t][0] + b0), tanhf(acc[t][1] + b1));
@@ -415,30 +417,29 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp(const __grid_constant__ Sur
         __floats2bfloat162_rn(tanhf(acc[t][2] + b0), tanhf(acc[t][3] + b1));
   }
   __syncthreads();
-  // layer 3: warp w < 4 forms columns 8w..8w+7
-  if (warp >= 4) return;
+  // layer 3: this warp's column tile over its quarter of the inputs
   float y[4] = {0.f, 0.f, 0.f, 0.f};
-  uint4 b3q[4][2];
 #pragma unroll
-  for (int ch = 0; ch < 4; ch++) frag_b_load(W3 + (8 * warp + g) * 128 + 32 * ch, tig, b3q[ch]);
-#pragma unroll
-  for (int ch = 0; ch < 4; ch++)
-#pragma unroll
-    for (int kl = 0; kl < 4; kl++) {
-      uint32_t a[4], b[2];
-      frag_a(s_h2, kMlpLdH, 4 * ch + kl, g, tig, a);
-      frag_b_of(b3q[ch], kl, b);
-      mma_bf16_16816(y, a, b);
-    }
-  const int col = 8 * warp + 2 * tig;
-  const float b0 = S.b3[col], b1 = S.b3[col + 1];
-  if (g < nrow) {
-    xy[(size_t)(k0 + g) * 64 + perm_col64(col)] = __float2bfloat16(y[0] + b0);
-    xy[(size_t)(k0 + g) * 64 + perm_col64(col + 1)] = __float2bfloat16(y[1] + b1);
+  for (int kl = 0; kl < 4; kl++) {
+    uint32_t a[4], b[2];
+    frag_a(s_h2, kMlpLdH, 4 * q3 + kl, g, tig, a);
+    frag_b_of(w3q, kl, b);
+    mma_bf16_16816(y, a, b);
   }
-  if (g + 8 < nrow) {
-    xy[(size_t)(k0 + g + 8) * 64 + perm_col64(col)] = __float2bfloat16(y[2] + b0);
-    xy[(size_t)(k0 + g + 8) * 64 + perm_col64(col + 1)] = __float2bfloat16(y[3] + b1);
+  {
+    const int col = 8 * nt3 + 2 * tig;
+    s_y[q3][g][col] = y[0];
+    s_y[q3][g][col + 1] = y[1];
+    s_y[q3][g + 8][col] = y[2];
+    s_y[q3][g + 8][col + 1] = y[3];
+  }
+  __syncthreads();
+  {
+    const int r = threadIdx.x >> 5, c = threadIdx.x & 31;
+    if (r < nrow) {
+      const float v = ((s_y[0][r][c] + s_y[1][r][c]) + s_y[2][r][c]) + s_y[3][r][c];
+      xy[(size_t)(k0 + r) * 64 + perm_col64(c)] = __float2bfloat16(v + S.b3[c]);
+    }
   }
 }
 
