@@ -3,16 +3,16 @@
 // is projected on 32 displacement modes, mapped by an MLP 32-256-256-32
 // (tanh) to residual force coefficients, and [network output, projected
 // input] is lifted by [residual force modes, tangent force of each mode] to
-// the body-frame force density; f_i = fscale R(theta) f_b.  The GEMMs run on
-// the tensor cores (pdgpu_tc.cu); this file holds the element-wise and
-// data-movement kernels around them, for inference in the step and for
-// training:
-//   gather   u -> BF16 rows (and FP32 rows for snapshots)
-//   scatter  FP32 rows -> f (surrogate particles only) and, on check steps,
-//            per-particle error of the surrogate against the bond loop
-//   gate     per-particle verdict on check steps
-//   training: MSE gradient, tanh backward, column sums (bias gradients),
-//            BF16 transpose, Adam
+// the body-frame force density; f_i = fscale R(theta) f_b.  This file holds
+//   the step's chain, by warp-level BF16 MMA beside the bond loop:
+//            gather + projection (partial sums per node chunk), the three
+//            layers, the lift with the scatter into f; after the bond
+//            loop, the check-step comparison and the gate
+//   the kernels around the tcgen05 GEMMs (pdgpu_tc.cu) of the other chain
+//   and of training:
+//            gather u -> BF16 rows (and FP32 rows for snapshots), scatter of
+//            FP32 rows -> f, gate; MSE gradient, tanh backward, column sums
+//            (bias gradients), BF16 transpose, Adam
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
