@@ -1,8 +1,9 @@
 """Host-side logic without a GPU: the surrogate's body-frame transforms and
 basis completion, the scene builder's sequential record chain, the
 autotuner's search order, the bench's workload descriptions and its
-layout-independent algorithmic byte count, and the early stop of the
-surrogate's snapshot collection (solver faked)."""
+layout-independent algorithmic byte count, the early stop of the
+surrogate's snapshot collection (solver faked) and the safety margin of the
+damping pass's FP32 pair pre-filter."""
 import numpy as np
 import pytest
 
@@ -247,3 +248,36 @@ def test_library_deck_constants_equal_the_reference_dump():
             assert rc == 0
             n = {0: 6, 1: 2, 2: 1, 3: 3}[int(init["p_mat_type"][p])]
             assert list(got)[:n] == [float(v) for v in mp[p, :n]], (name, kind, p)
+
+
+def test_damping_fp32_prefilter_never_rejects_a_pair_the_fp64_test_passes():
+    """The particle-damping pair search first tests FP32 copies of the
+    centres and bounding radii, d2 > 1.17 (R_i + R_j + 1.01 rc_max)^2, and
+    only the pairs it keeps reach the FP64 test of the one-particle form,
+    d2 > 1.0625 reach_max^2 (then the exact contact test).  Restated here in
+    NumPy with the kernel's FP32 operation order, over random pairs in a box
+    far from the origin (where rounding the coordinates to FP32 costs the
+    most) and pairs placed right at the FP64 threshold: no pair the FP64
+    test keeps is rejected by the FP32 one."""
+    rng = np.random.default_rng(5)
+    n = 200000
+    f32 = np.float32
+    ri = rng.uniform(0.8e-3, 1.6e-3, n)
+    rj = rng.uniform(0.8e-3, 1.6e-3, n)
+    rc = 1.01 * 2.0e-4
+    reach = rj + ri + rc
+    ci = rng.uniform(-0.1, 0.1, (n, 3)) + 0.5          # centres around 0.5 m
+    # half the pairs just inside the FP64 threshold, half anywhere nearby
+    d = np.where(rng.random(n) < 0.5, np.sqrt(1.0625) * reach * (1 - 1e-12),
+                 rng.uniform(0.0, 1.5, n) * reach)
+    u = rng.normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    cj = ci + d[:, None] * u
+    dx = cj - ci
+    keep64 = ~((dx * dx).sum(1) > 1.0625 * reach * reach)
+    e = cj.astype(f32) - ci.astype(f32)
+    d2f = (e[:, 0] * e[:, 0] + e[:, 1] * e[:, 1]) + e[:, 2] * e[:, 2]
+    rmf = (rj.astype(f32) + ri.astype(f32)) + f32(rc)
+    keep32 = ~(d2f > f32(1.17) * rmf * rmf)
+    assert keep64.sum() > n // 3
+    assert not np.any(keep64 & ~keep32)
